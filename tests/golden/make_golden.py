@@ -1,0 +1,224 @@
+"""Generate the golden fixtures in this directory by running ipie itself.
+
+Run from the repository root with ipie's source tree available:
+
+    python tests/golden/make_golden.py /path/to/ipie-checkout
+
+ipie needs ``plum`` and ``h5py``, which are absent here; the small stand-ins in
+``_ref_shims/`` are put first on ``sys.path``.  mpi4py is absent, so ipie
+selects its single-process ``FakeComm``.  Everything runs ipie's numpy (CPU)
+path.  Fixtures are small ``.npz`` files: inputs that cannot be regenerated
+from ``ipie_b200.synthetic`` plus ipie's outputs.  Synthetic inputs are
+regenerated in the tests and checked against the stored checksums.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IPIE_SRC", "")
+sys.path.insert(0, os.path.join(HERE, "_ref_shims"))
+sys.path.insert(0, REF)
+sys.path.insert(0, ROOT)
+
+import h5py  # noqa: E402  (the in-memory shim)
+
+from ipie.estimators.greens_function_single_det import greens_function_single_det  # noqa: E402
+from ipie.estimators.local_energy_sd import (  # noqa: E402
+    local_energy_single_det_rhf_batch,
+    local_energy_single_det_uhf_batch,
+)
+from ipie.hamiltonians.generic import Generic as HamGeneric  # noqa: E402
+from ipie.propagation.operations import apply_exponential, propagate_one_body  # noqa: E402
+from ipie.propagation.overlap import calc_overlap_single_det_uhf  # noqa: E402
+from ipie.propagation.phaseless_generic import PhaselessGeneric  # noqa: E402
+from ipie.qmc.afqmc import AFQMC  # noqa: E402
+from ipie.systems.generic import Generic  # noqa: E402
+from ipie.trial_wavefunction.single_det import SingleDet  # noqa: E402
+from ipie.utils.mpi import MPIHandler  # noqa: E402
+from ipie.walkers.walkers_dispatch import UHFWalkersTrial  # noqa: E402
+
+from ipie_b200 import synthetic  # noqa: E402
+
+
+def checksum(a):
+    a = np.ascontiguousarray(a)
+    return np.array([a.real.sum(), (a.real ** 2).sum(), np.abs(a).max()])
+
+
+def build(sysw, nwalkers, dt=0.005):
+    ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
+    trial = SingleDet(sysw.psi.copy(), (sysw.nup, sysw.ndown), sysw.nbasis)
+    trial.half_rotate(ham)
+    walkers = UHFWalkersTrial(trial, sysw.init.copy(), sysw.nup, sysw.ndown, sysw.nbasis, nwalkers, MPIHandler())
+    walkers.build(trial)
+    prop = PhaselessGeneric(dt)
+    prop.build(ham, trial, walkers, MPIHandler())
+    return ham, trial, walkers, prop
+
+
+def kernels_fixture(name, sysw, nwalkers, seed):
+    """Per-kernel inputs and ipie outputs on perturbed walkers."""
+    ham, trial, walkers, prop = build(sysw, nwalkers)
+    rng = np.random.default_rng(seed)
+    M, na, nb, X = sysw.nbasis, sysw.nup, sysw.ndown, sysw.nchol
+    W = nwalkers
+    pa = walkers.phia + 0.2 * (rng.normal(size=(W, M, na)) + 1j * rng.normal(size=(W, M, na)))
+    pb = walkers.phib + 0.2 * (rng.normal(size=(W, M, nb)) + 1j * rng.normal(size=(W, M, nb)))
+    walkers.phia = pa.copy()
+    walkers.phib = pb.copy()
+    out = dict(phia_in=pa, phib_in=pb)
+    out["ovlp"] = greens_function_single_det(walkers, trial)
+    out["Ghalfa"] = walkers.Ghalfa.copy()
+    out["Ghalfb"] = walkers.Ghalfb.copy()
+    out["vbias"] = trial.calc_force_bias(ham, walkers, MPIHandler())
+    xs = rng.normal(size=(X, W)) + 0.3j * rng.normal(size=(X, W))
+    out["xshifted"] = xs
+    vhs = prop.construct_VHS(ham, xs.copy())
+    out["VHS"] = vhs
+    phia_exp = pa.copy()
+    for iw in range(W):
+        phia_exp[iw] = apply_exponential(phia_exp[iw], vhs[iw], 6)
+    out["phia_exp"] = phia_exp
+    out["phia_onebody"] = propagate_one_body(pa.copy(), prop.expH1[0])
+    out["phib_onebody"] = propagate_one_body(pb.copy(), prop.expH1[1])
+    out["ovlp_overlap"] = calc_overlap_single_det_uhf(walkers, trial)
+    system = Generic((sysw.nup, sysw.ndown))
+    out["energy_uhf"] = local_energy_single_det_uhf_batch(system, ham, walkers, trial)
+    if sysw.nup == sysw.ndown:
+        walkers.rhf = True
+        out["energy_rhf"] = local_energy_single_det_rhf_batch(system, ham, walkers, trial)
+        walkers.Ghalfa = out["Ghalfa"].copy()
+        walkers.rhf = False
+    walkers.ovlp = out["ovlp"].copy()
+    detR = walkers.reortho()
+    out["reortho_phia"] = walkers.phia.copy()
+    out["reortho_phib"] = walkers.phib.copy()
+    out["reortho_ovlp"] = walkers.ovlp.copy()
+    out["reortho_detR"] = np.array(detR)
+    out["mf_shift"] = prop.mf_shift
+    out["expH1"] = prop.expH1
+    out["rchola"] = trial._rchola
+    out["rcholb"] = trial._rcholb
+    out["rH1a"] = trial._rH1a
+    out["rH1b"] = trial._rH1b
+    out["h1e_mod"] = ham.h1e_mod
+    out["chol_checksum"] = checksum(sysw.chol)
+    out["psi_checksum"] = checksum(sysw.psi)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name)
+
+
+def run_fixture(name, sysw, nwalkers, num_blocks, seed, snap_steps=()):
+    """ipie's own AFQMC.build(...).run() end to end; block estimates + final walker state."""
+    ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
+    trial = SingleDet(sysw.psi.copy(), (sysw.nup, sysw.ndown), sysw.nbasis)
+    trial.half_rotate(ham)
+    afqmc = AFQMC.build(
+        (sysw.nup, sysw.ndown),
+        ham,
+        trial,
+        num_walkers=nwalkers,
+        seed=seed,
+        num_steps_per_block=25,
+        num_blocks=num_blocks,
+        timestep=0.005,
+        stabilize_freq=5,
+        pop_control_freq=5,
+        verbose=False,
+    )
+    h5py.FILES.clear()
+    afqmc.run(estimator_filename="golden_run.h5", verbose=False)
+    store = h5py.FILES["golden_run.h5"]
+    data = store["block_size_1/data/000000000"][: num_blocks + 1]
+    w = afqmc.walkers
+    out = dict(
+        blocks=data,
+        weight=np.array(w.weight),
+        unscaled_weight=np.array(w.unscaled_weight),
+        ovlp=np.array(w.ovlp),
+        hybrid_energy=np.array(w.hybrid_energy),
+        phia=np.array(w.phia),
+        phib=np.array(w.phib),
+        total_weight=np.array(afqmc.pcontrol.total_weight),
+        chol_checksum=checksum(sysw.chol),
+        psi_checksum=checksum(sysw.psi),
+    )
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name, "ETotal per block", data[:, 3].real if data.shape[1] > 3 else data)
+
+
+def known_answer_inputs(name):
+    """Inputs of three of ipie's own known-answer unit tests.
+
+    * ``walkers/tests/test_population_control.py:30-81`` (pair branch),
+    * ``estimators/tests/test_generic.py:51-69`` (local energy of a trial),
+    * ``estimators/tests/test_estimators.py:27-41`` (energy estimator).
+    The constants those tests assert are restated in the fixture tests.
+    """
+    from ipie.utils.misc import dotdict
+    from ipie.utils.testing import (
+        build_test_case_handlers_mpi,
+        gen_random_test_instances,
+        generate_hamiltonian,
+        get_random_nomsd,
+    )
+    from ipie.utils.testing import build_random_trial
+
+    out = {}
+    # (a) pair branch: capture the builder's inputs by replaying its RNG use.
+    nelec, nmo, nwalkers, nsteps = (5, 5), 10, 10, 10
+    np.random.seed(7)
+    h1e, chol, _, _ = generate_hamiltonian(nmo, nelec, cplx=False)
+    trial, init = build_random_trial(nelec, nmo, num_dets=1, wfn_type="opt", trial_type="phmsd", complex_trial=True)
+    ham = HamGeneric(h1e=np.array([h1e, h1e]), chol=chol.reshape((-1, nmo ** 2)).T.copy(), ecore=0)
+    trial.half_rotate(ham)
+    trial.calculate_energy(Generic(nelec), ham)
+    out["pb_h1e"] = np.array([h1e, h1e])
+    out["pb_chol"] = chol.reshape((-1, nmo ** 2)).T.copy()
+    out["pb_psi"] = np.hstack([trial.psi0a, trial.psi0b])
+    out["pb_init"] = init
+    out["pb_eshift"] = np.array(trial.energy)
+    qmc = dotdict({"dt": 0.005, "nstblz": 5, "nwalkers": nwalkers, "batched": True, "hybrid": True,
+                   "num_steps": nsteps, "population_control": "pair_branch"})
+    d = build_test_case_handlers_mpi(nelec, nmo, MPIHandler(), num_dets=1, complex_trial=True, options=qmc, seed=7)
+    out["pb_weight"] = np.array(d.walkers.weight)
+    out["pb_unscaled_weight"] = np.array(d.walkers.unscaled_weight)
+    out["pb_phia"] = np.array(d.walkers.phia)
+    out["pb_phib"] = np.array(d.walkers.phib)
+    # (b) local energy of a random real single determinant.
+    np.random.seed(7)
+    nmo, nelec = 24, (4, 2)
+    h1e, chol, enuc, _ = generate_hamiltonian(nmo, nelec, cplx=False)
+    _, wfn = get_random_nomsd(nelec[0], nelec[1], nmo, ndet=1, cplx=False)
+    out["le_h1e"] = np.array([h1e, h1e])
+    out["le_chol"] = chol.reshape((-1, nmo * nmo)).T.copy()
+    out["le_ecore"] = np.array(enuc)
+    out["le_psi"] = wfn[0]
+    # (c) energy estimator on random half-rotated integrals.
+    system, ham, walkers, trial = gen_random_test_instances(10, 8, 30, 10)
+    out["ee_psi"] = trial.psi
+    out["ee_phia"] = np.array(walkers.phia)
+    out["ee_phib"] = np.array(walkers.phib)
+    out["ee_rchola"] = trial._rchola
+    out["ee_rcholb"] = trial._rcholb
+    out["ee_rH1a"] = trial._rH1a
+    out["ee_rH1b"] = trial._rH1b
+    out["ee_h1e"] = ham.H1
+    out["ee_chol"] = ham.chol
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name)
+
+
+if __name__ == "__main__":
+    c0 = synthetic.workload("c0_rhf_m26")
+    kernels_fixture("kernels_rhf_m26.npz", c0, nwalkers=8, seed=11)
+    uhf = synthetic.generate(30, (6, 4), 90, decay=30.0, seed=5, uhf=True)
+    kernels_fixture("kernels_uhf_m30.npz", uhf, nwalkers=6, seed=12)
+    c0s = synthetic.workload("c0_rhf_m26", chol_scale="stable")
+    run_fixture("run_rhf_m26.npz", c0s, nwalkers=16, num_blocks=3, seed=7)
+    gentle = synthetic.generate(30, (6, 4), 90, decay=30.0, seed=5, uhf=True, chol_scale=0.1)
+    run_fixture("run_uhf_m30.npz", gentle, nwalkers=12, num_blocks=3, seed=9)
+    known_answer_inputs("known_answers.npz")

@@ -1,0 +1,178 @@
+"""Pin the CPU oracle against ipie's own outputs and known-answer constants.
+
+The fixtures in ``tests/golden`` were produced by ``tests/golden/make_golden.py``
+running ipie's numpy path.  These tests run on CPU only.
+"""
+import numpy as np
+import pytest
+
+from oracle import afqmc_oracle as O
+from tests._systems import RUN_PARAMS, checksum, fixture_system, load, oracle_system
+
+KERNEL_FIXTURES = ["kernels_rhf_m26.npz", "kernels_uhf_m30.npz"]
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("name", KERNEL_FIXTURES)
+def test_fixture_inputs_regenerate(name):
+    f = load(name)
+    s = fixture_system(name)
+    np.testing.assert_allclose(checksum(s.chol), f["chol_checksum"], rtol=1e-13)
+    np.testing.assert_allclose(checksum(s.psi), f["psi_checksum"], rtol=1e-13)
+
+
+@pytest.mark.parametrize("name", KERNEL_FIXTURES)
+def test_oracle_setup_matches_ipie(name):
+    f = load(name)
+    S = oracle_system(fixture_system(name))
+    assert rel(S.h1e_mod, f["h1e_mod"]) < 1e-13
+    assert rel(S.rchola, f["rchola"]) < 1e-13
+    assert rel(S.rcholb, f["rcholb"]) < 1e-13
+    assert rel(S.rH1a, f["rH1a"]) < 1e-13
+    assert rel(S.mf_shift, f["mf_shift"]) < 1e-12
+    assert rel(S.expH1, f["expH1"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", KERNEL_FIXTURES)
+def test_oracle_kernels_match_ipie(name):
+    f = load(name)
+    S = oracle_system(fixture_system(name))
+    W = f["phia_in"].shape[0]
+    w = O.Walkers.from_initial(S.psi, S.nup, W)
+    w.phia = f["phia_in"].copy()
+    w.phib = f["phib_in"].copy()
+    ovlp = O.greens_function(S, w)
+    assert rel(ovlp, f["ovlp"]) < 1e-11
+    assert rel(w.Ghalfa, f["Ghalfa"]) < 1e-11
+    assert rel(w.Ghalfb, f["Ghalfb"]) < 1e-11
+    assert rel(O.force_bias(S, w), f["vbias"]) < 1e-12
+    vhs = O.construct_vhs(S, f["xshifted"])
+    assert rel(vhs, f["VHS"]) < 1e-13
+    assert rel(O.apply_exponential(f["phia_in"].copy(), f["VHS"], 6), f["phia_exp"]) < 1e-13
+    assert rel(O.propagate_one_body(f["phia_in"], S.expH1[0]), f["phia_onebody"]) < 1e-13
+    assert rel(O.propagate_one_body(f["phib_in"], S.expH1[1]), f["phib_onebody"]) < 1e-13
+    assert rel(O.overlap(S, w), f["ovlp_overlap"]) < 1e-11
+    assert rel(O.local_energy_single_det_uhf_batch(S, w), f["energy_uhf"]) < 1e-11
+    if "energy_rhf" in f:
+        assert rel(O.local_energy_single_det_rhf_batch(S, w), f["energy_rhf"]) < 1e-11
+    w.ovlp = ovlp.copy()
+    detR = O.reortho(S, w)
+    assert rel(w.phia, f["reortho_phia"]) < 1e-12
+    assert rel(w.phib, f["reortho_phib"]) < 1e-12
+    assert rel(detR, f["reortho_detR"]) < 1e-12
+    assert rel(w.ovlp, f["reortho_ovlp"]) < 1e-11
+
+
+@pytest.mark.parametrize("name", sorted(RUN_PARAMS))
+def test_oracle_run_matches_ipie_afqmc_run(name):
+    """Full ``AFQMC.build(...).run()`` including reortho, pair branch and block energies."""
+    f = load(name)
+    p = RUN_PARAMS[name]
+    s = fixture_system(name)
+    np.testing.assert_allclose(checksum(s.chol), f["chol_checksum"], rtol=1e-13)
+    S = oracle_system(s)
+    w = O.Walkers.from_initial(s.init, s.nup, p["nwalkers"])
+    O.greens_function(S, w)
+    w.ovlp = O.greens_function(S, w)
+    blocks = O.run_afqmc(S, w, num_blocks=p["num_blocks"], seed=p["seed"])
+    ref = f["blocks"]
+    # ipie's block row: Weight, WeightFactor, HybridEnergy, ENumer, EDenom, ETotal, E1Body, E2Body
+    for b, row in zip(blocks, ref):
+        assert abs(b["Weight"] - row[0].real) <= 1e-10 * abs(row[0])
+        assert abs(b["HybridEnergy"] - row[2].real) <= 1e-10 * max(abs(row[2]), 1.0)
+        assert abs(b["ETotal"] - row[5].real) <= 1e-10 * abs(row[5])
+        assert abs(b["E1Body"] - row[6].real) <= 1e-10 * abs(row[6])
+        assert abs(b["E2Body"] - row[7].real) <= 1e-10 * abs(row[7])
+    assert rel(w.weight, f["weight"]) < 1e-10
+    assert rel(w.unscaled_weight, f["unscaled_weight"]) < 1e-10
+    assert rel(w.ovlp, f["ovlp"]) < 1e-10
+    assert rel(w.hybrid_energy, f["hybrid_energy"]) < 1e-10
+    assert rel(w.phia, f["phia"]) < 1e-10
+    assert rel(w.phib, f["phib"]) < 1e-10
+
+
+def test_known_answer_pair_branch():
+    """ipie ``walkers/tests/test_population_control.py:30-81``: weights after 10 steps.
+
+    The test's single-determinant particle-hole trial is run here as the
+    equivalent ``SingleDet`` (same orbitals); ipie's loop in
+    ``utils/testing.py:519-528`` is restated: step with ``eshift = E_trial``,
+    reortho, pop control, every step.
+    """
+    f = load("known_answers.npz")
+    M = f["pb_h1e"].shape[-1]
+    S = O.System(M, 5, 5, f["pb_h1e"], f["pb_chol"], 0.0, f["pb_psi"]).build()
+    w = O.Walkers.from_initial(f["pb_init"], 5, 10)
+    w.ovlp = O.greens_function(S, w)
+    np.random.seed(7)
+    pc = O.PopController(10)
+    eshift = complex(f["pb_eshift"])
+    for _ in range(10):
+        O.propagate_walkers(S, w, eshift)
+        O.reortho(S, w)
+        pc.pop_control(w)
+        O.greens_function(S, w)
+    # constants asserted by ipie's own test
+    assert w.weight[0] == pytest.approx(0.2571750688329709, rel=1e-9)
+    assert w.weight[1] == pytest.approx(1.0843219322894988, rel=1e-9)
+    assert w.weight[2] == pytest.approx(0.8338283613093604, rel=1e-9)
+    assert w.phia[9][0, 0] == pytest.approx(-0.0005573508035052743 + 0.12432250308987346j, rel=1e-9)
+    assert rel(w.weight, f["pb_weight"]) < 1e-9
+    assert rel(w.unscaled_weight, f["pb_unscaled_weight"]) < 1e-9
+
+
+def test_known_answer_local_energy():
+    """ipie ``estimators/tests/test_generic.py:51-69``: energy of a random real determinant."""
+    f = load("known_answers.npz")
+    M = f["le_h1e"].shape[-1]
+    S = O.System(M, 4, 2, f["le_h1e"], f["le_chol"], float(f["le_ecore"]), f["le_psi"]).build()
+    _, gh = O.trial_density(S.psi, 4, 2)
+    e = O.local_energy_of_density(S, gh[0], gh[1])
+    assert e[0].real == pytest.approx(20.6826247016273, rel=1e-11)
+    assert e[1].real == pytest.approx(23.0173528796140, rel=1e-11)
+    assert e[2].real == pytest.approx(-2.3347281779866, rel=1e-11)
+
+
+def test_known_answer_energy_estimator():
+    """ipie ``estimators/tests/test_estimators.py:27-41``: ENumer on random half-rotated integrals."""
+    f = load("known_answers.npz")
+    S = O.System(10, 8, 8, f["ee_h1e"], f["ee_chol"], 0.0, f["ee_psi"]).build()
+    S.rchola, S.rcholb = f["ee_rchola"], f["ee_rcholb"]
+    S.rH1a, S.rH1b = f["ee_rH1a"], f["ee_rH1b"]
+    w = O.Walkers.from_initial(f["ee_psi"], 8, 10)
+    w.phia, w.phib = f["ee_phia"].copy(), f["ee_phib"].copy()
+    est = O.energy_estimate(S, w)
+    assert est["ENumer"] == pytest.approx(-754.0373585215561, rel=1e-11)
+    assert est["ENumer"] / est["EDenom"] == pytest.approx(-75.40373585215562, rel=1e-11)
+
+
+def test_pair_branch_single_process_copy_semantics():
+    """Every killed walker becomes a copy of the highest-index clone (ipie FakeComm tags)."""
+    W = 12
+    w = O.Walkers.from_initial(np.eye(4, 2), 1, W)
+    w.phia = np.arange(W, dtype=np.complex128)[:, None, None] * np.ones((W, 4, 1))
+    w.weight = np.array([0.01, 3.0, 0.05, 1.0, 6.0, 1.0, 0.02, 1.0, 5.0, 1.0, 1.0, 1.0])
+    draws = iter([0.9, 0.1, 0.1])
+    neww, status = O.pair_branch(w, 4.0, 0.1, rand=lambda: next(draws))
+    cloned = np.nonzero(status == 2)[0]
+    killed = np.nonzero(status == 0)[0]
+    assert len(cloned) == len(killed) == 3
+    last = cloned.max()
+    for k in killed:
+        assert w.phia[k][0, 0] == last
+        assert w.weight[k] == neww[last]
+    assert 0.0 in neww
+
+
+def test_pop_control_zero_weight_raises():
+    """``PopController.pop_control`` raises ValueError when the total weight vanishes
+    (ipie ``walkers/pop_controller.py:103-107``)."""
+    w = O.Walkers.from_initial(np.eye(4, 2), 1, 4)
+    w.weight[:] = 0.0
+    with pytest.raises(ValueError):
+        O.PopController(4).pop_control(w)
