@@ -1,0 +1,396 @@
+"""Walker-step throughput of the B200 phaseless-AFQMC drop-in.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A "step" is one AFQMC step of ipie's driver loop over the whole walker batch:
+reortho every 5 steps, propagation (Green's function, one-body, force bias,
+field shift, VHS, exp(VHS), one-body, overlap, weights), weight clip, pair
+branch every 5 steps, accumulation, and the local energy every 25 steps.
+Default workload: nbasis 200, 32+32 electrons, 1600 Cholesky vectors,
+2048 walkers, dt 0.005 (synthetic Hamiltonian, seeded).
+
+``value`` is walker-steps/s over the timed steps with all state resident in
+HBM (auxiliary fields drawn on the device).  ``e2e`` runs the same steps
+through the public API with the auxiliary fields supplied from pinned host
+memory each step and the weights read back each step.  ``--impl reference``
+times the CPU oracle (numpy restatement of ipie's path) on the host cores.
+With torchrun (N > 1) every rank runs an independent replica (weak scaling);
+the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "c2_rhf_m200": dict(nbasis=200, nocc=32, nchol=1600, decay=200.0, walkers=2048, uhf=False),
+    "c1_uhf_m108": dict(nbasis=108, nocc=15, nchol=600, decay=100.0, walkers=640, uhf=True),
+    "c4_rhf_m76": dict(nbasis=76, nocc=10, nchol=400, decay=30.0, walkers=512, uhf=False),
+    "c0_rhf_m26": dict(nbasis=26, nocc=5, nchol=120, decay=30.0, walkers=64, uhf=False),
+}
+
+
+def flops_per_walker(M, na, nb, X):
+    """Algorithmic real FLOPs per walker (complex mult-add = 8, real x complex = 4)."""
+    P = M * (M + 1) // 2
+    spins = [n for n in (na, nb) if n > 0]
+    f = {
+        "greens_function": sum(12 * M * n * n + 8 * n ** 3 for n in spins),
+        "force_bias": sum(4 * X * n * M for n in spins),
+        "one_body": sum(2 * 4 * M * M * n for n in spins),
+        "taylor": sum(48 * M * M * n for n in spins),
+        "vhs": 4 * P * X,
+        "overlap": sum(4 * M * n * n + 8 * n ** 3 for n in spins),
+    }
+    energy = sum(4 * X * n * n * M + 8 * X * n * n + 4 * X * n * M for n in spins)
+    return f, energy
+
+
+def load_peaks():
+    peaks = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        peaks.update({k: d[k] for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained") if k in d})
+        peaks["source"] = "measured"
+    # FP64 peak: cuBLAS DGEMM 8192^3 measured on this pool's B200 (profiles/peaks_fp64.md)
+    peaks["fp64_tflops"] = 35.47
+    return peaks
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(ngpus):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier_max(value, world):
+    import torch
+
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_afqmc(wl, walkers, rng, seed):
+    from ipie_b200 import AFQMC, Generic, SingleDet, synthetic
+
+    p = WORKLOADS[wl]
+    s = synthetic.generate(p["nbasis"], p["nocc"], p["nchol"], p["decay"], seed=7, uhf=p["uhf"], chol_scale="stable")
+    ham = Generic(s.h1e, s.chol, s.ecore)
+    trial = SingleDet(s.psi, (s.nup, s.ndown), s.nbasis)
+    trial.half_rotate(ham)
+    af = AFQMC.build((s.nup, s.ndown), ham, trial, num_walkers=walkers, seed=seed, num_steps_per_block=25,
+                     num_blocks=10 ** 6, timestep=0.005, stabilize_freq=5, pop_control_freq=5, verbose=False, rng=rng)
+    return af, s
+
+
+def cpu_oracle_rate(wl, walkers_sample=64, steps=2, energy_walkers=2):
+    """Oracle (numpy port) walker-steps/s on the host cores for a bounded sample."""
+    from ipie_b200 import synthetic
+    from oracle import afqmc_oracle as O
+
+    p = WORKLOADS[wl]
+    s = synthetic.generate(p["nbasis"], p["nocc"], p["nchol"], p["decay"], seed=7, uhf=p["uhf"], chol_scale="stable")
+    S = O.System(s.nbasis, s.nup, s.ndown, s.h1e, s.chol, s.ecore, s.psi).build()
+    w = O.Walkers.from_initial(s.init, s.nup, walkers_sample)
+    np.random.seed(7)
+    O.greens_function(S, w)
+    t0 = time.perf_counter()
+    for step in range(1, steps + 1):
+        O.propagate_walkers(S, w, 0.0)
+    t_prop = (time.perf_counter() - t0) / (steps * walkers_sample)
+    sub = w.copy()
+    sub.phia, sub.phib = w.phia[:energy_walkers].copy(), w.phib[:energy_walkers].copy()
+    sub.log_shift = w.log_shift[:energy_walkers]
+    t0 = time.perf_counter()
+    O.greens_function(S, sub)
+    O.local_energy_single_det_uhf_batch(S, sub)
+    t_en = (time.perf_counter() - t0) / energy_walkers
+    rate = 1.0 / (t_prop + t_en / 25.0)
+    sample = (f"{walkers_sample} walkers x {steps} propagation steps + local energy of {energy_walkers} walkers "
+              f"(amortised 1 per 25 steps), same system")
+    return rate, sample, t_prop, t_en
+
+
+def blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+
+        info = threadpool_info()
+        return max((i.get("num_threads", 1) for i in info), default=os.cpu_count())
+    except Exception:
+        return os.cpu_count()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = args.workload
+    p = WORKLOADS[wl]
+    rates = []
+    sample = ""
+    for _ in range(max(args.warmup, 0)):
+        pass  # the oracle has no warm-up state; each timed step is an independent bounded sample
+    for _ in range(max(args.steps, 1)):
+        r, sample, _, _ = cpu_oracle_rate(wl, walkers_sample=args.ref_walkers, steps=1, energy_walkers=1)
+        rates.append(r)
+    value = float(np.median(rates))
+    cores = blas_threads()
+    line = {
+        "impl": "reference",
+        "metric": "walker-steps/s (plain FP64 phaseless AFQMC step)",
+        "value": value,
+        "unit": "walker-steps/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": p["walkers"] / value * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": wl, **{k: p[k] for k in ("nbasis", "nocc", "nchol", "walkers")}, "dt": 0.005},
+        "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    from ipie_b200 import _lib
+    from ipie_b200.propagation import PhaseTimer
+
+    rank, world, local = dist_setup(args.gpus)
+    wl = args.workload
+    p = WORKLOADS[wl]
+    W = args.walkers or p["walkers"]
+    M, na, nb, X = p["nbasis"], p["nocc"], p["nocc"], p["nchol"]
+    peaks = load_peaks()
+
+    # ---------------- device-resident run (value) ----------------
+    af, s = build_afqmc(wl, W, "device", 7 + rank)
+    af.setup_run()
+    step = 0
+    for _ in range(args.warmup):
+        step += 1
+        af.step(step)
+    torch.cuda.synchronize()
+    timer = PhaseTimer()
+    af.propagator.timer = timer
+    launches0 = _lib.launch_count()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            step += 1
+            af.step(step)
+        ev1.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches = _lib.launch_count() - launches0
+    t_local = ev0.elapsed_time(ev1) / 1e3
+    t = barrier_max(t_local, world)
+    value = W * args.steps * world / t
+    phases = timer.summary()
+    from ipie_b200.propagation import _NoTimer
+
+    af.propagator.timer = _NoTimer()
+    energy_ok = bool(np.all(np.isfinite(np.array(af.block_data))))
+
+    # roofline of the dominant kernel phase
+    fl, fl_energy = flops_per_walker(M, na, nb, X)
+    dom = max((k for k in phases if k in fl), key=lambda k: phases[k][1])
+    n_launch, tot_ms = phases[dom]
+    achieved = fl[dom] * W * n_launch / (tot_ms / 1e3) / 1e12
+    roofline = {
+        "kernel": dom,
+        "bound": "fp64-tensor",
+        "achieved": round(achieved, 3),
+        "peak": peaks["fp64_tflops"],
+        "unit": "TFLOP/s",
+        "frac": round(achieved / peaks["fp64_tflops"], 4),
+        "traffic": None,
+        "peak_source": "measured cuBLAS DGEMM 8192^3 on B200 (no FP64 entry in MEASURED_PEAKS.json)",
+        "phase_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(phases.items())},
+    }
+    step_flops = sum(fl.values()) * W + fl_energy * W / 25.0
+    del af
+    torch.cuda.empty_cache()
+
+    # ---------------- end to end through the public API ----------------
+    e2e_steps = min(args.steps, args.e2e_steps)
+    af2, _ = build_afqmc(wl, W, "host", 7 + rank)
+    rng = np.random.default_rng(1234 + rank)
+    fields = [torch.from_numpy(rng.standard_normal((W, X))).pin_memory() for _ in range(args.warmup + e2e_steps)]
+    af2.propagator.host_fields = iter(fields)
+    wback = torch.empty(W, dtype=torch.float64).pin_memory()
+    af2.setup_run()
+    step = 0
+    for _ in range(args.warmup):
+        step += 1
+        af2.step(step)
+        wback.copy_(af2.walkers.weight)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        step += 1
+        af2.step(step)
+        wback.copy_(af2.walkers.weight)  # the step's result back to the host
+    e1.record()
+    torch.cuda.synchronize()
+    t2 = barrier_max(e0.elapsed_time(e1) / 1e3, world)
+    e2e_value = W * e2e_steps * world / t2
+    del af2, fields
+    torch.cuda.empty_cache()
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            r, sample, _, _ = cpu_oracle_rate(wl, walkers_sample=args.ref_walkers, steps=2, energy_walkers=1)
+            cpu = {"value": r, "unit": "walker-steps/s", "cores": blas_threads(), "kind": "port", "sample": sample}
+        line = {
+            "metric": "walker-steps/s (plain FP64 phaseless AFQMC step)",
+            "value": value,
+            "unit": "walker-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": t / args.steps * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {
+                "workload": wl, "nbasis": M, "nalpha": na, "nbeta": nb, "nchol": X, "walkers_per_gpu": W,
+                "dt": 0.005, "form": "plain_fp64", "parallelism": f"replicas{world}",
+                "l2": "inputs larger than L2 (VHS 1.3 GB + walkers 0.4 GB per step)",
+                "step": "reortho/5, propagate, clip, pair-branch/5, energy/25 (ipie driver order)",
+            },
+            "e2e": {"value": e2e_value, "unit": "walker-steps/s", "h2d_bytes_per_step": W * X * 8,
+                    "d2h_bytes_per_step": W * 8, "steps": e2e_steps,
+                    "fields": "host-supplied N(0,1) draws in pinned memory, one (W, X) array per step"},
+            "roofline": roofline,
+            "step_tflops": round(step_flops / (t / args.steps) / 1e12, 3),
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+            "finite_energies": energy_ok,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c2_rhf_m200", choices=sorted(WORKLOADS))
+    ap.add_argument("--walkers", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=25)
+    ap.add_argument("--ref-walkers", type=int, default=32)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

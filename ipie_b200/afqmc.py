@@ -1,0 +1,149 @@
+"""AFQMC driver: ``AFQMC.build(...)`` and ``AFQMC.run()`` on one B200.
+
+Mirror of ipie's ``AFQMC`` (``qmc/afqmc.py:297-392`` build, ``:508-633`` run):
+same arguments, same step order (reortho every ``stabilize_freq`` steps,
+propagate, weight clip, pair branch every ``pop_control_freq`` steps,
+accumulate, energy every block, eshift update).  The block estimates are
+kept in ``self.block_data`` (ipie writes them to HDF5) as rows of
+``[Weight, WeightFactor, HybridEnergy, ENumer, EDenom, ETotal, E1Body, E2Body]``.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from ._lib import call, ptr, stream
+from .estimators import EnergyEstimator
+from .pop_control import PopController
+from .propagation import PhaselessGeneric
+from .walkers import UHFWalkers
+
+C128 = torch.complex128
+
+
+@dataclass
+class QMCParams:
+    num_walkers: int
+    total_num_walkers: int
+    num_blocks: int
+    num_steps_per_block: int
+    timestep: float
+    num_stblz: int
+    pop_control_freq: int
+    rng_seed: int | None
+
+
+class WalkerAccumulator:
+    """Block sums of weight, unscaled weight and weighted hybrid energy (ipie ``base_walkers.py:32-83``)."""
+
+    def __init__(self, nsteps, device):
+        self.nsteps_per_block = nsteps
+        self.buffer = torch.zeros(7, dtype=C128, device=device)
+        self._eshift = 0.0
+
+    def update(self, walkers):
+        call("ipie_b200_walker_sums", walkers.nwalkers, ptr(walkers.weight), ptr(walkers.unscaled_weight),
+             ptr(walkers.hybrid_energy), None, ptr(self.buffer), 1, stream())
+
+    def block_end(self, block):
+        """Post-reduce hook (``base_walkers.py:69-80``) and the eshift of ``handler.py:231-236``."""
+        v = self.buffer.cpu().numpy()
+        factor = 1 if block == 0 else self.nsteps_per_block
+        vals = np.array([v[0] / factor, v[1] / factor, v[2] / v[0]])
+        self._eshift = vals[2]
+        self.buffer.zero_()
+        return vals
+
+    @property
+    def eshift(self):
+        return np.real(self._eshift)
+
+
+class AFQMC:
+    def __init__(self, system, hamiltonian, trial, walkers, propagator, params, verbose=False):
+        self.system = system
+        self.hamiltonian = hamiltonian
+        self.trial = trial
+        self.walkers = walkers
+        self.propagator = propagator
+        self.params = params
+        self.verbose = verbose
+        if params.rng_seed is not None:
+            np.random.seed(params.rng_seed)  # ipie qmc/utils.py:24-40 (seed + rank, rank 0)
+        self.block_data = []
+        self.timers = {}
+
+    @staticmethod
+    def build(num_elec, hamiltonian, trial_wavefunction, walkers=None, num_walkers=100, seed=None,
+              num_steps_per_block=25, num_blocks=100, timestep=0.005, stabilize_freq=5, pop_control_freq=5,
+              verbose=True, mpi_handler=None, rng="numpy"):
+        params = QMCParams(num_walkers, num_walkers, num_blocks, num_steps_per_block, timestep, stabilize_freq,
+                           pop_control_freq, seed)
+        if not trial_wavefunction.half_rotated:
+            trial_wavefunction.half_rotate(hamiltonian)
+        if walkers is None:
+            init = np.asarray(trial_wavefunction.psi).copy()  # walkers_dispatch.py:42-58
+            walkers = UHFWalkers(init, num_elec[0], num_elec[1], hamiltonian.nbasis, num_walkers,
+                                 device=trial_wavefunction.device)
+            walkers.build(trial_wavefunction)
+        prop = PhaselessGeneric(timestep, rng=rng, seed=seed if seed is not None else 7)
+        prop.build(hamiltonian, trial_wavefunction, walkers)
+        return AFQMC(num_elec, hamiltonian, trial_wavefunction, walkers, prop, params, verbose=verbose)
+
+    def _block(self, block, est, acc_vals):
+        d = est.data.copy()
+        est.post_reduce_hook(d)
+        row = [acc_vals[0].real, acc_vals[1].real, acc_vals[2].real, d[0].real, d[1].real, d[2].real, d[3].real,
+               d[4].real]
+        self.block_data.append(row)
+        if self.verbose:
+            print(f"{block:>17d} " + " ".join(f"{v: .16e}" for v in row))
+
+    def setup_run(self, walkers=None):
+        """Everything ``run`` does before its step loop (``afqmc.py:526-559``)."""
+        if walkers is not None:
+            self.walkers = walkers
+        w, ham, trial, p = self.walkers, self.hamiltonian, self.trial, self.params
+        self.eshift = 0.0
+        w.orthogonalise()
+        self.pcontrol = PopController(p.num_walkers, p.num_steps_per_block)
+        self.accumulators = WalkerAccumulator(p.num_steps_per_block, w.device)
+        self.estimator = EnergyEstimator()
+        self.estimator.compute_estimator(self.system, w, ham, trial)
+        self.accumulators.update(w)
+        self._block(0, self.estimator, self.accumulators.block_end(0))
+        self.num_eqlb_steps = 2.0 / p.timestep
+
+    def step(self, step):
+        """Body of ``run``'s loop for step number ``step`` (1-based; ``afqmc.py:561-633``)."""
+        w, ham, trial, prop, p = self.walkers, self.hamiltonian, self.trial, self.propagator, self.params
+        if step % p.num_stblz == 0:
+            w.orthogonalise()
+        prop.propagate_walkers(w, ham, trial, self.eshift)
+        if step > 1:
+            prop.clip_weights(w, self.pcontrol.total_weight * 0.10)
+        if step % p.pop_control_freq == 0:
+            self.pcontrol.pop_control(w)
+        self.accumulators.update(w)
+        if step % p.num_steps_per_block == 0:
+            block = step // p.num_steps_per_block
+            self.estimator.compute_estimator(self.system, w, ham, trial)
+            self._block(block, self.estimator, self.accumulators.block_end(block))
+            w.check_status()
+        if step < self.num_eqlb_steps:
+            self.eshift = self.accumulators.eshift
+        else:
+            self.eshift += self.accumulators.eshift - self.eshift
+
+    def run(self, walkers=None, estimator_filename=None, verbose=True, additional_estimators=None):
+        self.setup_run(walkers)
+        total_steps = self.params.num_steps_per_block * self.params.num_blocks
+        t0 = time.time()
+        for step in range(1, total_steps + 1):
+            self.step(step)
+        torch.cuda.synchronize()
+        self.timers["run"] = time.time() - t0
+        return np.array(self.block_data)

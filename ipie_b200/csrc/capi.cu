@@ -1,0 +1,145 @@
+// C ABI of the walker step (declared in include/ipie_b200.h).
+#include "../../include/ipie_b200.h"
+#include "kernels.h"
+
+#include <atomic>
+
+namespace ipie_b200 {
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace ipie_b200
+
+using namespace ipie_b200;
+
+#define ST(s) reinterpret_cast<cudaStream_t>(s)
+#define C2(p) reinterpret_cast<double2*>(p)
+#define CC2(p) reinterpret_cast<const double2*>(p)
+
+extern "C" {
+
+const char* ipie_b200_version(void) { return "ipie_b200 0.1 (sm_100a)"; }
+
+long long ipie_b200_launch_count(void) { return ipie_b200::g_launches.load(); }
+
+int ipie_b200_greens_function_single_det_batch(const void* phia, const void* phib, int W, int M, int na, int nb,
+                                               const void* psia_conj, const void* psib_conj, const double* log_shift,
+                                               void* ghalfa, void* ghalfb, void* ovlp, void* logdet,
+                                               unsigned int* status, void* stream) {
+  if (ghalfa == nullptr || (nb > 0 && ghalfb == nullptr)) return (int)cudaErrorInvalidValue;
+  return (int)launch_gf_overlap(CC2(phia), CC2(phib), W, M, na, nb, CC2(psia_conj), CC2(psib_conj), log_shift,
+                                C2(ghalfa), C2(ghalfb), C2(ovlp), C2(logdet), status, ST(stream));
+}
+
+int ipie_b200_calc_overlap_single_det_uhf(const void* phia, const void* phib, int W, int M, int na, int nb,
+                                          const void* psia_conj, const void* psib_conj, const double* log_shift,
+                                          void* ovlp, unsigned int* status, void* stream) {
+  return (int)launch_gf_overlap(CC2(phia), CC2(phib), W, M, na, nb, CC2(psia_conj), CC2(psib_conj), log_shift,
+                                nullptr, nullptr, C2(ovlp), nullptr, status, ST(stream));
+}
+
+int ipie_b200_construct_force_bias_batch_single_det(const double* rchola, const double* rcholb, const void* ghalfa,
+                                                    const void* ghalfb, int W, int X, int M, int na, int nb,
+                                                    void* vbias, void* stream) {
+  cudaError_t e = launch_force_bias(rchola, CC2(ghalfa), W, X, na * M, C2(vbias), 0, ST(stream));
+  if (e != cudaSuccess || nb == 0) return (int)e;
+  return (int)launch_force_bias(rcholb, CC2(ghalfb), W, X, nb * M, C2(vbias), 1, ST(stream));
+}
+
+int ipie_b200_field_shift(const void* vbias, const double* xi, const void* mf_shift, int W, int X, double sqrt_dt,
+                          double bound, void* xshifted, void* cmf, void* cfb, void* stream) {
+  return (int)launch_field_shift(CC2(vbias), xi, CC2(mf_shift), W, X, sqrt_dt, bound, C2(xshifted), C2(cmf), C2(cfb),
+                                 ST(stream));
+}
+
+int ipie_b200_construct_vhs(const double* chol_packed, const int* idx_i, const int* idx_j, int M, int X,
+                            const void* xshifted, int W, double sqrt_dt, void* vhs, void* stream) {
+  const int P = M * (M + 1) / 2;
+  return (int)launch_vhs(chol_packed, idx_i, idx_j, P, X, M, CC2(xshifted), W, sqrt_dt, C2(vhs), ST(stream));
+}
+
+int ipie_b200_apply_exponential_batch(const void* vhs, const void* phi_in, void* phi_out, void* work, int W, int M,
+                                      int N, int nmax, void* stream) {
+  if (phi_in == phi_out) return (int)cudaErrorInvalidValue;
+  double2* t0 = C2(work);
+  double2* t1 = t0 + (size_t)W * M * N;
+  return (int)launch_taylor(CC2(vhs), CC2(phi_in), C2(phi_out), t0, t1, W, M, N, nmax, ST(stream));
+}
+
+int ipie_b200_propagate_one_body(const void* expH1, int expH1_is_complex, const void* phi_in, void* phi_out, int W,
+                                 int M, int N, void* stream) {
+  if (phi_in == phi_out) return (int)cudaErrorInvalidValue;
+  return (int)launch_one_body(reinterpret_cast<const double*>(expH1), expH1_is_complex, CC2(phi_in), C2(phi_out), W, M,
+                              N, ST(stream));
+}
+
+int ipie_b200_update_weight(int W, const void* ovlp_new, const void* cfb, const void* cmf, const double* eshift,
+                            double dt, double ebound, const double* wbound, void* ovlp, void* hybrid_energy,
+                            double* weight, unsigned int* status, void* stream) {
+  return (int)launch_update_weight(W, CC2(ovlp_new), CC2(cfb), CC2(cmf), eshift, dt, ebound, wbound, C2(ovlp),
+                                   C2(hybrid_energy), weight, status, ST(stream));
+}
+
+int ipie_b200_clip_weight(int W, const double* wbound, double* weight, void* stream) {
+  return (int)launch_clip_weight(W, wbound, weight, ST(stream));
+}
+
+int ipie_b200_reortho(void* phia, void* phib, int W, int M, int na, int nb, const double* detR_shift, double* detR,
+                      double* log_detR, void* ovlp, unsigned int* status, void* stream) {
+  return (int)launch_reortho(C2(phia), C2(phib), W, M, na, nb, detR_shift, detR, log_detR, C2(ovlp), status,
+                             ST(stream));
+}
+
+int ipie_b200_walker_copy(const int* src, int W, int M, int na, int nb, void* phia, void* phib, double* weight,
+                          double* unscaled_weight, void* hybrid_energy, void* ovlp, void* phase, void* stream) {
+  return (int)launch_walker_copy(src, W, M, na, nb, C2(phia), C2(phib), weight, unscaled_weight, C2(hybrid_energy),
+                                 C2(ovlp), C2(phase), ST(stream));
+}
+
+int ipie_b200_exchange_rows(int W, int X, int M, int N) {
+  int rows = 0;
+  if (launch_exchange(nullptr, nullptr, W, X, M, N, nullptr, &rows, nullptr) != cudaSuccess) return -1;
+  return rows;
+}
+
+int ipie_b200_exchange(const double* rchol, const void* ghalf, int W, int X, int M, int N, void* part, void* stream) {
+  int rows = 0;
+  if (part == nullptr) return (int)cudaErrorInvalidValue;
+  return (int)launch_exchange(rchol, CC2(ghalf), W, X, M, N, C2(part), &rows, ST(stream));
+}
+
+int ipie_b200_local_energy_single_det_batch(int rhf, const double* rchola, const double* rcholb, const void* rH1a,
+                                            const void* rH1b, double ecore, const void* ghalfa, const void* ghalfb,
+                                            int W, int X, int M, int na, int nb, void* work, void* energy,
+                                            unsigned int* status, void* stream) {
+  cudaStream_t st = ST(stream);
+  double2* xv = C2(work);
+  double2* part = xv + (size_t)W * X;
+  const int use_b = (!rhf && nb > 0);
+  cudaError_t e = launch_force_bias(rchola, CC2(ghalfa), W, X, na * M, xv, 0, st);
+  if (e == cudaSuccess && use_b) e = launch_force_bias(rcholb, CC2(ghalfb), W, X, nb * M, xv, 1, st);
+  if (e != cudaSuccess) return (int)e;
+  int rows_a = 0, rows_b = 0;
+  e = launch_exchange(rchola, CC2(ghalfa), W, X, M, na, part, &rows_a, st);
+  if (e != cudaSuccess) return (int)e;
+  if (use_b) {
+    e = launch_exchange(rcholb, CC2(ghalfb), W, X, M, nb, part + (size_t)rows_a * W, &rows_b, st);
+    if (e != cudaSuccess) return (int)e;
+  }
+  // UHF: e1b = Ga.rH1a + Gb.rH1b + ecore; ecoul = (Xa+Xb)^2 / 2; exx = raw / 2.
+  // RHF: e1b = 2 Ga.rH1a + ecore;        ecoul = 2 Xa^2;         exx = raw.
+  const double f1 = rhf ? 2.0 : 1.0, fc = rhf ? 2.0 : 0.5, fx = rhf ? 1.0 : 0.5;
+  return (int)launch_energy_combine(W, X, na * M, nb * M, CC2(ghalfa), use_b ? CC2(ghalfb) : nullptr, CC2(rH1a),
+                                    CC2(rH1b), ecore, xv, part, rows_a + rows_b, f1, fc, fx, C2(energy), status, st);
+}
+
+int ipie_b200_walker_sums(int W, const double* weight, const double* unscaled_weight, const void* hybrid_energy,
+                          const void* energy, void* out, int accumulate, void* stream) {
+  return (int)launch_walker_sums(W, weight, unscaled_weight, CC2(hybrid_energy), CC2(energy), C2(out), accumulate,
+                                 ST(stream));
+}
+
+int ipie_b200_normal_fill(double* out, long long n, unsigned long long seed, unsigned long long offset, void* stream) {
+  return (int)launch_normal_fill(out, n, seed, offset, ST(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+// Internal launcher declarations (C++), wrapped by the C ABI in capi.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace ipie_b200 {
+
+size_t gf_smem_bytes(int M, int N);
+
+cudaError_t launch_gf_overlap(const double2* phia, const double2* phib, int W, int M, int na, int nb,
+                              const double2* psia_c, const double2* psib_c, const double* log_shift, double2* ghalfa,
+                              double2* ghalfb, double2* ovlp, double2* logdet, unsigned* status, cudaStream_t st);
+cudaError_t launch_field_shift(const double2* vbias, const double* xi, const double2* mf, int W, int X, double sqrt_dt,
+                               double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st);
+cudaError_t launch_update_weight(int W, const double2* ovlp_new, const double2* cfb, const double2* cmf,
+                                 const double* eshift, double dt, double ebound, const double* wbound, double2* ovlp,
+                                 double2* ehyb, double* weight, unsigned* status, cudaStream_t st);
+cudaError_t launch_clip_weight(int W, const double* wbound, double* weight, cudaStream_t st);
+cudaError_t launch_reortho(double2* phia, double2* phib, int W, int M, int na, int nb, const double* detR_shift,
+                           double* detR, double* log_detR, double2* ovlp, unsigned* status, cudaStream_t st);
+cudaError_t launch_walker_copy(const int* src, int W, int M, int na, int nb, double2* phia, double2* phib,
+                               double* weight, double* unscaled_weight, double2* ehyb, double2* ovlp, double2* phase,
+                               cudaStream_t st);
+cudaError_t launch_energy_combine(int W, int X, int Ka, int Kb, const double2* ga, const double2* gb,
+                                  const double2* rh1a, const double2* rh1b, double ecore, const double2* xv,
+                                  const double2* exx_part, int ntiles, double f1, double fc, double fx, double2* energy,
+                                  unsigned* status, cudaStream_t st);
+
+cudaError_t launch_force_bias(const double* rchol, const double2* ghalf, int W, int X, int K, double2* vbias,
+                              int accumulate, cudaStream_t st);
+cudaError_t launch_vhs(const double* chol_packed, const int* idx_i, const int* idx_j, int P, int X, int M,
+                       const double2* xshifted, int W, double sqrt_dt, double2* vhs, cudaStream_t st);
+cudaError_t launch_one_body(const double* expH1, int cplx, const double2* phi_in, double2* phi_out, int W, int M, int N,
+                            cudaStream_t st);
+cudaError_t launch_taylor(const double2* vhs, const double2* phi_in, double2* phi_out, double2* t0, double2* t1, int W,
+                          int M, int N, int nmax, cudaStream_t st);
+cudaError_t launch_exchange(const double* rchol, const double2* ghalf, int W, int X, int M, int N, double2* part,
+                            int* ntiles, cudaStream_t st);
+
+cudaError_t launch_normal_fill(double* out, long long n, unsigned long long seed, unsigned long long offset,
+                               cudaStream_t st);
+cudaError_t launch_walker_sums(int W, const double* weight, const double* unscaled, const double2* ehyb,
+                               const double2* energy, double2* out, int accumulate, cudaStream_t st);
+
+}  // namespace ipie_b200

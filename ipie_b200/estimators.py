@@ -1,0 +1,128 @@
+"""Local energy and the energy estimator on the device.
+
+Mirrors ipie's ``local_energy_single_det_uhf_batch`` / ``_rhf_batch`` /
+``local_energy_single_det_batch_gpu`` (``estimators/local_energy_sd.py``),
+``local_energy_batch`` (``estimators/local_energy_batch.py:36-75``) and
+``EnergyEstimator`` (``estimators/energy.py:133-181``).  The exchange term
+runs in the fused kernel (the intermediate T is never stored).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ._lib import call, lib, ptr, stream
+
+C128 = torch.complex128
+
+
+def _energy_work(walkers, hamiltonian, rhf):
+    W, X, M = walkers.nwalkers, hamiltonian.nchol, walkers.nbasis
+    rows = lib().ipie_b200_exchange_rows(W, X, M, walkers.nup)
+    if not rhf and walkers.ndown > 0:
+        rows += lib().ipie_b200_exchange_rows(W, X, M, walkers.ndown)
+    need = W * X + rows * W
+    buf = getattr(walkers, "_energy_work", None)
+    if buf is None or buf.numel() < need:
+        buf = torch.empty(need, dtype=C128, device=walkers.device)
+        walkers._energy_work = buf
+    return buf
+
+
+def _local_energy(hamiltonian, walkers, trial, rhf):
+    if not trial.half_rotated:
+        raise RuntimeError("trial.half_rotate(hamiltonian) must run before computing local energies")
+    W = walkers.nwalkers
+    work = _energy_work(walkers, hamiltonian, rhf)
+    energy = torch.empty(W, 3, dtype=C128, device=walkers.device)
+    call("ipie_b200_local_energy_single_det_batch", int(rhf), ptr(trial._rchola), ptr(trial._rcholb),
+         ptr(trial._rH1a), ptr(trial._rH1b), hamiltonian.ecore, ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), W,
+         hamiltonian.nchol, hamiltonian.nbasis, walkers.nup, walkers.ndown, ptr(work), ptr(energy),
+         ptr(walkers.status), stream())
+    return energy
+
+
+def local_energy_single_det_uhf_batch(system, hamiltonian, walkers, trial):
+    """(W, 3) complex ``[e1b + e2b, e1b, e2b]`` (ipie ``local_energy_sd.py:358-403``)."""
+    return _local_energy(hamiltonian, walkers, trial, rhf=False)
+
+
+def local_energy_single_det_batch_gpu(system, hamiltonian, walkers, trial, max_mem=2.0):
+    """ipie's GPU entry point (``local_energy_sd.py:987-1080``); same arithmetic as the UHF batch."""
+    return _local_energy(hamiltonian, walkers, trial, rhf=False)
+
+
+def local_energy_single_det_rhf_batch(system, hamiltonian, walkers, trial):
+    """RHF form: spin-alpha only, doubled (ipie ``local_energy_sd.py:106-155``)."""
+    return _local_energy(hamiltonian, walkers, trial, rhf=True)
+
+
+def local_energy_batch(system, hamiltonian, walkers, trial):
+    """Dispatch as ipie's ``local_energy_batch`` (``local_energy_batch.py:36-75``)."""
+    if walkers.rhf:
+        return local_energy_single_det_rhf_batch(system, hamiltonian, walkers, trial)
+    return local_energy_single_det_uhf_batch(system, hamiltonian, walkers, trial)
+
+
+local_energy = local_energy_batch
+
+
+class _OneWalker:
+    """A one-walker view holding given half-rotated densities (for trial energies)."""
+
+    def __init__(self, Ghalfa, Ghalfb, nbasis, device):
+        self.nwalkers = 1
+        self.nbasis = nbasis
+        self.nup = Ghalfa.shape[0]
+        self.ndown = Ghalfb.shape[0]
+        self.device = device
+        self.Ghalfa = torch.from_numpy(np.ascontiguousarray(Ghalfa[None].astype(np.complex128))).to(device)
+        self.Ghalfb = torch.from_numpy(np.ascontiguousarray(Ghalfb[None].astype(np.complex128))).to(device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self.rhf = False
+
+
+def local_energy_of_density(hamiltonian, trial, Ghalfa, Ghalfb):
+    """Local energy of one pair of half-rotated densities (e.g. the trial's own); complex (3,)."""
+    w = _OneWalker(np.asarray(Ghalfa), np.asarray(Ghalfb), hamiltonian.nbasis, trial.device)
+    return _local_energy(hamiltonian, w, trial, rhf=False)[0].cpu().numpy()
+
+
+class EnergyEstimator:
+    """Weighted energy sums of a block (ipie ``estimators/energy.py:133-181``)."""
+
+    names = ["ENumer", "EDenom", "ETotal", "E1Body", "E2Body"]
+
+    def __init__(self, system=None, ham=None, trial=None, filename=None):
+        self._data = {k: 0.0j for k in self.names}
+        self._sums = None
+        self.print_to_stdout = True
+        self.ascii_filename = filename
+
+    def compute_estimator(self, system=None, walkers=None, hamiltonian=None, trial=None):
+        trial.calc_greens_function(walkers)
+        energy = local_energy_batch(system, hamiltonian, walkers, trial)
+        if self._sums is None:
+            self._sums = torch.zeros(7, dtype=C128, device=walkers.device)
+        call("ipie_b200_walker_sums", walkers.nwalkers, ptr(walkers.weight), None, None, ptr(energy), ptr(self._sums),
+             0, stream())
+        s = self._sums.cpu().numpy()
+        self._data["ENumer"] = s[3].real
+        self._data["EDenom"] = s[4].real
+        self._data["E1Body"] = s[5].real
+        self._data["E2Body"] = s[6].real
+        self._data["ETotal"] = 0.0j
+        self.energies = energy
+        return self.data
+
+    @property
+    def data(self):
+        return np.array([self._data[k] for k in self.names], dtype=np.complex128)
+
+    def __getitem__(self, k):
+        return self._data[k]
+
+    def post_reduce_hook(self, data):
+        data[2] = data[0] / data[1]
+        data[3] = data[3] / data[1]
+        data[4] = data[4] / data[1]

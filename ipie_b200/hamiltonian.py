@@ -1,0 +1,54 @@
+"""Generic real-Cholesky Hamiltonian, device resident.
+
+Mirror of ipie's ``Generic`` factory / ``GenericRealChol``
+(``hamiltonians/generic.py:31-102,153-157``): same constructor arguments
+(``h1e`` (2, M, M), ``chol`` (M*M, X), ``ecore``), same attribute names.
+Set-up arithmetic (``h1e_mod``, packing) runs once on the host in numpy; the
+arrays the walker step reads are uploaded once and stay in HBM.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+
+class GenericRealChol:
+    def __init__(self, h1e, chol, ecore=0.0, device="cuda", verbose=False):
+        h1e = np.asarray(h1e)
+        chol = np.asarray(chol)
+        assert h1e.shape[0] == 2, "h1e must carry both spin components"
+        assert chol.dtype == np.float64, "GenericRealChol needs a float64 Cholesky tensor"
+        self.H1 = h1e
+        self.ecore = float(ecore)
+        self.nbasis = h1e.shape[-1]
+        self.nchol = chol.shape[-1]
+        self.nfields = self.nchol
+        assert self.nbasis ** 2 == chol.shape[0]
+        self.chunked = False
+        M, X = self.nbasis, self.nchol
+        self.chol = np.ascontiguousarray(chol)  # host copy (set-up only)
+        iu, ju = np.triu_indices(M)
+        self.sym_idx = (iu, ju)
+        packed = np.ascontiguousarray(self.chol.reshape(M, M, X)[iu, ju, :])
+        # h1e_mod = h1e - 1/2 sum_kn L_ik,n L_jk,n  (hamiltonians/generic.py:31-43)
+        view = self.chol.reshape(M, M * X)
+        v0 = 0.5 * view @ view.T
+        self.h1e_mod = np.array([h1e[0] - v0, h1e[1] - v0])
+        self.device = torch.device(device)
+        self.chol_packed = torch.from_numpy(packed).to(self.device)
+        self.sym_idx_i = torch.from_numpy(iu.astype(np.int32)).to(self.device)
+        self.sym_idx_j = torch.from_numpy(ju.astype(np.int32)).to(self.device)
+        if verbose:
+            print(f"# nbasis {M}  nchol {X}  packed Cholesky {packed.nbytes / 1e9:.3f} GB on {self.device}")
+
+    @property
+    def npacked(self):
+        return self.nbasis * (self.nbasis + 1) // 2
+
+
+def Generic(h1e, chol, ecore=0.0, shmem=False, chol_packed=None, verbose=False):
+    """Factory with ipie's signature (``hamiltonians/generic.py:153-157``); real Cholesky only."""
+    chol = np.asarray(chol)
+    if chol.dtype == np.complex128:
+        raise NotImplementedError("complex Cholesky Hamiltonians are not supported by the B200 walker step")
+    return GenericRealChol(h1e, chol, ecore, verbose=verbose)

@@ -1,0 +1,250 @@
+"""Phaseless propagator for generic real-Cholesky Hamiltonians on B200.
+
+Mirror of ipie's ``PhaselessGeneric`` / ``PhaselessBase``
+(``propagation/phaseless_generic.py:28-97``, ``propagation/phaseless_base.py:242-385``):
+``build``, ``propagate_walkers``, ``propagate_walkers_one_body``,
+``propagate_walkers_two_body``, ``construct_VHS``, ``apply_VHS`` and
+``update_weight`` keep ipie's names, arguments and order of operations.
+
+Auxiliary fields: ``rng="numpy"`` (default) draws them exactly as ipie does,
+``numpy.random.normal(0, 1, X*W).reshape(W, X)`` from numpy's global stream,
+so a run fed the same seed consumes the same draws; ``rng="device"`` draws
+them on the GPU (Philox4x32-10), which keeps a step free of host work;
+``rng="host"`` takes caller-supplied (W, X) host arrays from the iterator
+``propagator.host_fields`` and uploads one per step.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import scipy.linalg
+import torch
+
+from ._lib import call, ptr, stream
+from .trial import force_bias_into, greens_function_into, overlap_into
+
+C128 = torch.complex128
+F64 = torch.float64
+
+
+def construct_mean_field_shift(hamiltonian, trial):
+    """``mf = 1j L^T Re(G_a+G_b) - L^T Im(G_a+G_b)`` (ipie ``phaseless_base.py:153-172``)."""
+    g = (trial.G[0] + trial.G[1]).ravel()
+    return 1.0j * (hamiltonian.chol.T @ g.real) - hamiltonian.chol.T @ g.imag
+
+
+def construct_one_body_propagator(hamiltonian, mf_shift, dt):
+    """``expH1_s = expm(-dt/2 (h1e_mod_s - 1j L.mf))`` (ipie ``phaseless_base.py:27-74``)."""
+    M = hamiltonian.nbasis
+    shift = 1.0j * np.einsum("mx,x->m", hamiltonian.chol, mf_shift).reshape(M, M)
+    H1 = hamiltonian.h1e_mod - np.array([shift, shift])
+    return np.array([scipy.linalg.expm(-0.5 * dt * H1[0]), scipy.linalg.expm(-0.5 * dt * H1[1])])
+
+
+class PhaseTimer:
+    """CUDA-event timing of named step phases on the launching (current) stream."""
+
+    def __init__(self):
+        self.events = {}
+
+    def start(self, name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.events.setdefault(name, []).append([e, None])
+
+    def stop(self, name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.events[name][-1][1] = e
+
+    def summary(self):
+        """{phase: (launch groups, total ms)} after a device synchronize."""
+        out = {}
+        for k, v in self.events.items():
+            out[k] = (len(v), sum(a.elapsed_time(b) for a, b in v))
+        return out
+
+
+class _NoTimer:
+    def start(self, name):
+        pass
+
+    def stop(self, name):
+        pass
+
+
+class Workspace:
+    """Scratch buffers of one walker batch, allocated once."""
+
+    def __init__(self, W, M, na, nb, X, device):
+        self.W, self.M, self.na, self.nb, self.X = W, M, na, nb, X
+        dev = device
+        self.phia_tmp = torch.empty(W, M, na, dtype=C128, device=dev)
+        self.phib_tmp = torch.empty(W, M, nb, dtype=C128, device=dev)
+        nmax = max(na, nb)
+        self.taylor = torch.empty(2 * W * M * nmax, dtype=C128, device=dev)
+        self.vbias = torch.empty(W, X, dtype=C128, device=dev)
+        self.xi = torch.empty(W, X, dtype=F64, device=dev)
+        self.xshifted = torch.empty(X, W, dtype=C128, device=dev)
+        self.cmf = torch.empty(W, dtype=C128, device=dev)
+        self.cfb = torch.empty(W, dtype=C128, device=dev)
+        self.vhs = torch.empty(W, M, M, dtype=C128, device=dev)
+        self.ovlp_new = torch.empty(W, dtype=C128, device=dev)
+        self.eshift = torch.zeros(1, dtype=F64, device=dev)
+        self.wbound = torch.full((1,), -1.0, dtype=F64, device=dev)
+        self.xi_host = torch.empty(W, X, dtype=F64).pin_memory() if torch.cuda.is_available() else None
+        self.xi_copied = torch.cuda.Event() if torch.cuda.is_available() else None
+
+
+class PhaselessGeneric:
+    def __init__(self, time_step, exp_nmax=6, verbose=False, rng="numpy", seed=7):
+        self.dt = time_step
+        self.sqrt_dt = self.dt ** 0.5
+        self.isqrt_dt = 1j * self.sqrt_dt
+        self.exp_nmax = exp_nmax
+        self.ebound = (2.0 / self.dt) ** 0.5
+        self.fbbound = 1.0
+        self.verbose = verbose
+        self.rng = rng
+        self.rng_seed = seed
+        self.rng_counter = 0
+        self.vbias = None
+        self.ws = None
+        self.timer = _NoTimer()
+
+    # ------------------------------------------------------------------ set-up
+    def build(self, hamiltonian, trial=None, walkers=None, mpi_handler=None, verbose=False):
+        """Mean-field shift and one-body propagator (ipie ``phaseless_base.py:256-272``)."""
+        self.mf_shift = construct_mean_field_shift(hamiltonian, trial)
+        self.expH1 = construct_one_body_propagator(hamiltonian, self.mf_shift, self.dt)
+        dev = trial.device
+        self.device = dev
+        self.mf_shift_dev = torch.from_numpy(np.ascontiguousarray(self.mf_shift.astype(np.complex128))).to(dev)
+        self.expH1_complex = bool(np.iscomplexobj(self.expH1) and np.abs(self.expH1.imag).max() > 0)
+        e = self.expH1.astype(np.complex128) if self.expH1_complex else self.expH1.real.astype(np.float64)
+        self.expH1_dev = torch.from_numpy(np.ascontiguousarray(e)).to(dev)
+        if walkers is not None:
+            self._workspace(walkers, hamiltonian)
+
+    def _workspace(self, walkers, hamiltonian):
+        W, M, X = walkers.nwalkers, walkers.nbasis, hamiltonian.nchol
+        ws = self.ws
+        if ws is None or (ws.W, ws.M, ws.na, ws.nb, ws.X) != (W, M, walkers.nup, walkers.ndown, X):
+            self.ws = Workspace(W, M, walkers.nup, walkers.ndown, X, walkers.device)
+        return self.ws
+
+    # ------------------------------------------------------------- the step
+    def propagate_walkers_one_body(self, walkers):
+        """``phi_s <- expH1_s phi_s`` (ipie ``phaseless_base.py:274-280``)."""
+        ws = self.ws
+        self.timer.start("one_body")
+        for s, (phi, tmp, n) in enumerate(((walkers.phia, ws.phia_tmp, walkers.nup), (walkers.phib, ws.phib_tmp, walkers.ndown))):
+            if n == 0:
+                continue
+            call("ipie_b200_propagate_one_body", ptr(self.expH1_dev[s]), int(self.expH1_complex), ptr(phi), ptr(tmp),
+                 walkers.nwalkers, walkers.nbasis, n, stream())
+        self.timer.stop("one_body")
+        walkers.phia, ws.phia_tmp = ws.phia_tmp, walkers.phia
+        if walkers.ndown > 0:
+            walkers.phib, ws.phib_tmp = ws.phib_tmp, walkers.phib
+
+    def draw_fields(self, walkers, hamiltonian):
+        """N(0,1) auxiliary fields (W, X) into the workspace (ipie ``phaseless_base.py:296-298``)."""
+        ws = self.ws
+        W, X = walkers.nwalkers, hamiltonian.nchol
+        if self.rng == "numpy":
+            xi = np.random.normal(0.0, 1.0, X * W).reshape(W, X)
+            ws.xi_copied.synchronize()  # the previous step's upload has left the pinned buffer
+            ws.xi_host.numpy()[...] = xi
+            ws.xi.copy_(ws.xi_host, non_blocking=True)
+            ws.xi_copied.record()
+        elif self.rng == "host":
+            src = next(self.host_fields)  # (W, X) float64, ideally pinned host memory
+            ws.xi.copy_(src, non_blocking=True)
+        else:
+            call("ipie_b200_normal_fill", ptr(ws.xi), W * X, self.rng_seed, self.rng_counter, stream())
+            self.rng_counter += 1
+        return ws.xi
+
+    def propagate_walkers_two_body(self, walkers, hamiltonian, trial):
+        """Force bias, shifted fields, VHS and exp(VHS) (ipie ``phaseless_base.py:282-310``)."""
+        ws = self.ws
+        W, X = walkers.nwalkers, hamiltonian.nchol
+        self.timer.start("force_bias")
+        force_bias_into(hamiltonian, walkers, trial, ws.vbias)
+        self.timer.stop("force_bias")
+        self.vbias = ws.vbias
+        self.timer.start("rng")
+        xi = self.draw_fields(walkers, hamiltonian)
+        self.timer.stop("rng")
+        self.timer.start("field_shift")
+        call("ipie_b200_field_shift", ptr(ws.vbias), ptr(xi), ptr(self.mf_shift_dev), W, X, self.sqrt_dt, self.fbbound,
+             ptr(ws.xshifted), ptr(ws.cmf), ptr(ws.cfb), stream())
+        self.timer.stop("field_shift")
+        self.apply_VHS(walkers, hamiltonian, ws.xshifted)
+        return ws.cmf, ws.cfb
+
+    def construct_VHS(self, hamiltonian, xshifted, out=None):
+        """``VHS = i sqrt(dt) L . xshifted`` unpacked to (W, M, M) (ipie ``phaseless_generic.py:66-97``)."""
+        W = xshifted.shape[-1]
+        M = hamiltonian.nbasis
+        if out is None:
+            out = torch.empty(W, M, M, dtype=C128, device=xshifted.device)
+        call("ipie_b200_construct_vhs", ptr(hamiltonian.chol_packed), ptr(hamiltonian.sym_idx_i),
+             ptr(hamiltonian.sym_idx_j), M, hamiltonian.nchol, ptr(xshifted.contiguous()), W, self.sqrt_dt, ptr(out),
+             stream())
+        return out
+
+    def apply_VHS(self, walkers, hamiltonian, xshifted):
+        """Build VHS and apply exp(VHS) to both spin blocks (ipie ``phaseless_generic.py:35-58``)."""
+        assert walkers.nwalkers == xshifted.shape[-1]
+        ws = self.ws
+        self.timer.start("vhs")
+        vhs = self.construct_VHS(hamiltonian, xshifted, out=ws.vhs)
+        self.timer.stop("vhs")
+        self.timer.start("taylor")
+        for phi_name, tmp_name, n in (("phia", "phia_tmp", walkers.nup), ("phib", "phib_tmp", walkers.ndown)):
+            if n == 0:
+                continue
+            phi, tmp = getattr(walkers, phi_name), getattr(ws, tmp_name)
+            call("ipie_b200_apply_exponential_batch", ptr(vhs), ptr(phi), ptr(tmp), ptr(ws.taylor), walkers.nwalkers,
+                 walkers.nbasis, n, self.exp_nmax, stream())
+            setattr(walkers, phi_name, tmp)
+            setattr(ws, tmp_name, phi)
+        self.timer.stop("taylor")
+
+    def propagate_walkers(self, walkers, hamiltonian, trial, eshift):
+        """One phaseless step (ipie ``phaseless_base.py:312-338``)."""
+        ws = self._workspace(walkers, hamiltonian)
+        # the step's starting overlap goes into walkers.ovlp, which update_weight overwrites with ovlp_new
+        self.timer.start("greens_function")
+        greens_function_into(walkers, trial, walkers.ovlp)
+        self.timer.stop("greens_function")
+        self.propagate_walkers_one_body(walkers)
+        cmf, cfb = self.propagate_walkers_two_body(walkers, hamiltonian, trial)
+        self.propagate_walkers_one_body(walkers)
+        self.timer.start("overlap")
+        overlap_into(walkers, trial, ws.ovlp_new)
+        self.timer.stop("overlap")
+        self.update_weight(walkers, walkers.ovlp, ws.ovlp_new, cfb, cmf, eshift)
+
+    def update_weight(self, walkers, ovlp, ovlp_new, cfb, cmf, eshift):
+        """Hybrid energy, bound, importance function and cosine projection (ipie ``phaseless_base.py:340-358``).
+
+        ``ovlp`` is overwritten with ``ovlp_new`` and becomes ``walkers.ovlp``.
+        """
+        ws = self.ws
+        if isinstance(eshift, torch.Tensor):
+            ws.eshift.copy_(eshift.reshape(1).to(F64))
+        else:
+            ws.eshift.fill_(float(np.real(eshift)))
+        call("ipie_b200_update_weight", walkers.nwalkers, ptr(ovlp_new), ptr(cfb), ptr(cmf), ptr(ws.eshift), self.dt,
+             self.ebound, None, ptr(ovlp), ptr(walkers.hybrid_energy), ptr(walkers.weight), ptr(walkers.status),
+             stream())
+        walkers.ovlp = ovlp
+
+    def clip_weights(self, walkers, wbound):
+        """Driver weight clip to ``+-wbound`` (ipie ``qmc/afqmc.py:581-585``)."""
+        self.ws.wbound.fill_(float(wbound))
+        call("ipie_b200_clip_weight", walkers.nwalkers, ptr(self.ws.wbound), ptr(walkers.weight), stream())

@@ -1,0 +1,79 @@
+"""UHF walker batch, device resident.
+
+Mirror of ipie's ``UHFWalkers`` (``walkers/uhf_walkers.py:27-161``) and the
+parts of ``BaseWalkers`` (``walkers/base_walkers.py:86-179``) the walker step
+uses.  Every per-walker array is a torch CUDA tensor with ipie's name, shape
+and dtype; ``reortho`` runs the modified Gram-Schmidt kernel.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ._lib import call, ptr, stream
+
+C128 = torch.complex128
+F64 = torch.float64
+
+
+class UHFWalkers:
+    def __init__(self, initial_walker, nup, ndown, nbasis, nwalkers, mpi_handler=None, verbose=False, device="cuda"):
+        init = np.asarray(initial_walker)
+        assert init.ndim == 2
+        self.nup, self.ndown, self.nbasis, self.nwalkers = nup, ndown, nbasis, nwalkers
+        self.mpi_handler = mpi_handler
+        self.device = dev = torch.device(device)
+        W, M = nwalkers, nbasis
+        ia = torch.from_numpy(np.ascontiguousarray(init[:, :nup].astype(np.complex128)))
+        ib = torch.from_numpy(np.ascontiguousarray(init[:, nup:].astype(np.complex128)))
+        self.phia = ia.to(dev).unsqueeze(0).repeat(W, 1, 1).contiguous()
+        self.phib = ib.to(dev).unsqueeze(0).repeat(W, 1, 1).contiguous()
+        self.weight = torch.ones(W, dtype=F64, device=dev)
+        self.unscaled_weight = torch.ones(W, dtype=F64, device=dev)
+        self.phase = torch.ones(W, dtype=C128, device=dev)
+        self.ovlp = torch.ones(W, dtype=C128, device=dev)
+        self.sgn_ovlp = torch.ones(W, dtype=F64, device=dev)
+        self.log_ovlp = torch.zeros(W, dtype=F64, device=dev)
+        self.hybrid_energy = torch.zeros(W, dtype=C128, device=dev)
+        self.detR = torch.ones(W, dtype=F64, device=dev)
+        self.detR_shift = torch.zeros(W, dtype=F64, device=dev)
+        self.log_detR = torch.zeros(W, dtype=F64, device=dev)
+        self.log_shift = torch.zeros(W, dtype=F64, device=dev)
+        self.Ghalfa = torch.zeros(W, nup, M, dtype=C128, device=dev)
+        self.Ghalfb = torch.zeros(W, ndown, M, dtype=C128, device=dev)
+        # device status word: numerical trouble bits written by the kernels
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.rhf = False  # ipie propagates both spin blocks in production (uhf_walkers.py:99)
+        self.buff_names = ["weight", "unscaled_weight", "phase", "hybrid_energy", "ovlp", "sgn_ovlp", "log_ovlp",
+                           "phia", "phib"]
+
+    def build(self, trial):
+        """``walkers.build``: initial overlaps and Green's functions (``uhf_walkers.py:101-102``)."""
+        self.ovlp = trial.calc_greens_function(self)
+
+    def reortho(self):
+        """Thin QR per spin block with positive diag(R); returns detR (``uhf_walkers.py:108-161``)."""
+        call(
+            "ipie_b200_reortho",
+            ptr(self.phia), ptr(self.phib), self.nwalkers, self.nbasis, self.nup, self.ndown,
+            ptr(self.detR_shift), ptr(self.detR), ptr(self.log_detR), ptr(self.ovlp), ptr(self.status), stream(),
+        )
+        return self.detR
+
+    def orthogonalise(self, free_projection=False):
+        """``BaseWalkers.orthogonalise`` (``base_walkers.py:166-179``), phaseless branch."""
+        if free_projection:
+            raise NotImplementedError("free projection is not part of the B200 walker step")
+        return self.reortho()
+
+    def check_status(self):
+        """Raise if a kernel flagged non-finite values or a singular overlap since the last check."""
+        s = int(self.status.item())
+        if s:
+            self.status.zero_()
+            names = []
+            for bit, name in ((1, "non-finite weight/overlap/energy"), (2, "singular overlap matrix"),
+                              (4, "unsupported shape"), (8, "zero column in Gram-Schmidt")):
+                if s & bit:
+                    names.append(name)
+            raise FloatingPointError("walker step reported: " + ", ".join(names))

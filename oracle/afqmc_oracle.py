@@ -522,11 +522,14 @@ def exx_kernel(rchol: np.ndarray, Ghalf: np.ndarray) -> np.ndarray:
     """
     W, N, M = Ghalf.shape
     X = rchol.shape[0]
-    r = rchol.reshape(X, N, M)
+    r = rchol.reshape(X * N, M)
     exx = np.zeros(W, dtype=np.complex128)
     for iw in range(W):
-        T = np.einsum("xin,jn->xij", r, Ghalf[iw], optimize=True)
-        exx[iw] = np.einsum("xij,xji->", T, T, optimize=True)
+        if np.iscomplexobj(r):
+            T = (r @ Ghalf[iw].T).reshape(X, N, N)
+        else:  # real rchol: two real GEMMs, as ipie's numba kernel splits them
+            T = (r @ Ghalf[iw].real.T + 1.0j * (r @ Ghalf[iw].imag.T)).reshape(X, N, N)
+        exx[iw] = np.sum(T * np.transpose(T, (0, 2, 1)))
     return 0.5 * exx
 
 
