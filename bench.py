@@ -373,10 +373,45 @@ def run_ours(args):
     return 0
 
 
+def measure_peaks():
+    """torch/cuBLAS GEMM and copy peaks (the FP64/TF32 roofline denominators); prints JSON."""
+    import torch
+
+    def best(fn, iters=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        out = 1e9
+        for _ in range(iters):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            out = min(out, a.elapsed_time(b) / 1e3)
+        return out
+
+    res = {}
+    n = 8192
+    for name, dt, tf32 in (("f64", torch.float64, False), ("f32", torch.float32, False), ("tf32", torch.float32, True),
+                           ("bf16", torch.bfloat16, False)):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(n, n, device="cuda").to(dt)
+        b = torch.randn(n, n, device="cuda").to(dt)
+        res[f"{name}_tflops_8192"] = 2 * n ** 3 / best(lambda: a @ b) / 1e12
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
+    x = torch.empty(2 ** 28, device="cuda", dtype=torch.float64)
+    y = torch.empty_like(x)
+    res["copy_gbs"] = 2 * x.numel() * 8 / best(lambda: y.copy_(x)) / 1e9
+    print(json.dumps(res))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=50, help="timed steps; multiples of 25 include whole energy blocks")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c2_rhf_m200", choices=sorted(WORKLOADS))
@@ -384,7 +419,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=25)
     ap.add_argument("--ref-walkers", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--measure-peaks", action="store_true", help="print measured GEMM/copy peaks and exit")
     args = ap.parse_args()
+    if args.measure_peaks:
+        return measure_peaks()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
