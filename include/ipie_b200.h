@@ -121,6 +121,21 @@ int ipie_b200_reortho(void* phia, void* phib, int W, int M, int na, int nb, cons
 int ipie_b200_walker_copy(const int* src, int W, int M, int na, int nb, void* phia, void* phib, double* weight,
                           double* unscaled_weight, void* hybrid_energy, void* ovlp, void* phase, void* stream);
 
+/* Exchange energy for callers that cannot allocate device memory (their device
+ * memory is owned by their own pool allocator, or their loop cannot take the
+ * implicit synchronisation of cudaMalloc/cudaFree).  No counterpart in ipie:
+ * it is ipie_b200_exchange plus the sum over partial rows, with the partials in
+ * a fixed 16 MiB file-scope device array instead of a caller workspace.
+ * out: exx (W) complex = sum_x sum_ij T_ij T_ji.  Limit: ipie_b200_exchange_rows(W,X,M,N) * W
+ * <= 1048576 (e.g. W=2048, X=1600, M=200, N=32 fits); larger calls return
+ * cudaErrorInvalidValue (1) before any work.  The array is shared by all calls
+ * and keeps the last call's partials; calls overlapping on the GPU race.  The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress,
+ * that device current); make it before any stream capture on that device.
+ * Allocates nothing. */
+int ipie_b200_exchange_noalloc(const double* rchol, const void* ghalf, int W, int X, int M, int N, void* exx,
+                               void* stream);
+
 /* Number of partial rows the exchange kernel writes for one spin block
  * (the workspace for ipie_b200_exchange is rows * W complex). */
 int ipie_b200_exchange_rows(int W, int X, int M, int N);

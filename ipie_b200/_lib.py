@@ -34,6 +34,7 @@ SIGNATURES = {
     "ipie_b200_walker_copy": [P, I, I, I, I, P, P, P, P, P, P, P, P],
     "ipie_b200_exchange_rows": [I, I, I, I],
     "ipie_b200_exchange": [P, P, I, I, I, I, P, P],
+    "ipie_b200_exchange_noalloc": [P, P, I, I, I, I, P, P],
     "ipie_b200_local_energy_single_det_batch": [I, P, P, P, P, D, P, P, I, I, I, I, I, P, P, P, P],
     "ipie_b200_walker_sums": [I, P, P, P, P, P, I, P],
     "ipie_b200_normal_fill": [P, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_ulonglong, P],
