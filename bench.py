@@ -40,10 +40,16 @@ WORKLOADS = {
 }
 
 
-def flops_per_walker(M, na, nb, X):
-    """Algorithmic real FLOPs per walker (complex mult-add = 8, real x complex = 4)."""
+def flops_per_walker(M, na, nb, X, alias=False):
+    """Algorithmic real FLOPs per walker (complex mult-add = 8, real x complex = 4).
+
+    With ``alias`` (identical spin blocks computed once) the per-spin terms count
+    one block: the work executed.  Without it: both blocks, ipie's work.
+    """
     P = M * (M + 1) // 2
     spins = [n for n in (na, nb) if n > 0]
+    if alias:
+        spins = spins[:1]
     f = {
         "greens_function": sum(12 * M * n * n + 8 * n ** 3 for n in spins),
         "force_bias": sum(4 * X * n * M for n in spins),
@@ -52,6 +58,7 @@ def flops_per_walker(M, na, nb, X):
         "vhs": 4 * P * X,
         "overlap": sum(4 * M * n * n + 8 * n ** 3 for n in spins),
     }
+    f["orbitals"] = f["one_body"] + f["taylor"]  # fused launch: one-body + exp(VHS) + one-body
     energy = sum(4 * X * n * n * M + 8 * X * n * n + 4 * X * n * M for n in spins)
     return f, energy
 
@@ -64,8 +71,9 @@ def load_peaks():
             d = json.load(fh)
         peaks.update({k: d[k] for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained") if k in d})
         peaks["source"] = "measured"
-    # FP64 peak: cuBLAS DGEMM 8192^3 measured on this pool's B200 (profiles/peaks_fp64.md)
+    # FP64 and TF32 peaks: cuBLAS 8192^3 GEMMs measured on this pool's B200 (python bench.py --measure-peaks)
     peaks["fp64_tflops"] = 35.47
+    peaks["tf32_tflops"] = 755.8
     return peaks
 
 
@@ -147,7 +155,7 @@ def barrier_max(value, world):
     return float(t.item())
 
 
-def build_afqmc(wl, walkers, rng, seed):
+def build_afqmc(wl, walkers, rng, seed, precision="fp64"):
     from ipie_b200 import AFQMC, Generic, SingleDet, synthetic
 
     p = WORKLOADS[wl]
@@ -156,7 +164,8 @@ def build_afqmc(wl, walkers, rng, seed):
     trial = SingleDet(s.psi, (s.nup, s.ndown), s.nbasis)
     trial.half_rotate(ham)
     af = AFQMC.build((s.nup, s.ndown), ham, trial, num_walkers=walkers, seed=seed, num_steps_per_block=25,
-                     num_blocks=10 ** 6, timestep=0.005, stabilize_freq=5, pop_control_freq=5, verbose=False, rng=rng)
+                     num_blocks=10 ** 6, timestep=0.005, stabilize_freq=5, pop_control_freq=5, verbose=False, rng=rng,
+                     precision=precision)
     return af, s
 
 
@@ -235,21 +244,14 @@ def run_reference(args):
     return 0
 
 
-def run_ours(args):
+def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clock=False):
+    """Build, warm up and time ``args.steps`` driver steps of one form; returns a result dict."""
     import torch
 
     from ipie_b200 import _lib
-    from ipie_b200.propagation import PhaseTimer
+    from ipie_b200.propagation import PhaseTimer, _NoTimer
 
-    rank, world, local = dist_setup(args.gpus)
-    wl = args.workload
-    p = WORKLOADS[wl]
-    W = args.walkers or p["walkers"]
-    M, na, nb, X = p["nbasis"], p["nocc"], p["nocc"], p["nchol"]
-    peaks = load_peaks()
-
-    # ---------------- device-resident run (value) ----------------
-    af, s = build_afqmc(wl, W, "device", 7 + rank)
+    af, _ = build_afqmc(wl, W, rng, 7 + rank, precision=precision)
     af.setup_run()
     step = 0
     for _ in range(args.warmup):
@@ -258,53 +260,97 @@ def run_ours(args):
     torch.cuda.synchronize()
     timer = PhaseTimer()
     af.propagator.timer = timer
+    nblocks0 = len(af.block_data)
     launches0 = _lib.launch_count()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        ev0.record()
-        for _ in range(args.steps):
-            step += 1
-            af.step(step)
-        ev1.record()
-        torch.cuda.synchronize()
+    clk = ClockSampler(local) if with_clock else None
+    if clk:
+        clk.__enter__()
+    ev0.record()
+    for _ in range(args.steps):
+        step += 1
+        af.step(step)
+    ev1.record()
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
     if world > 1:
         torch.distributed.barrier()
-    launches = _lib.launch_count() - launches0
-    t_local = ev0.elapsed_time(ev1) / 1e3
-    t = barrier_max(t_local, world)
-    value = W * args.steps * world / t
-    phases = timer.summary()
-    from ipie_b200.propagation import _NoTimer
-
-    af.propagator.timer = _NoTimer()
-    energy_ok = bool(np.all(np.isfinite(np.array(af.block_data))))
-
-    # roofline of the dominant kernel phase
-    fl, fl_energy = flops_per_walker(M, na, nb, X)
-    dom = max((k for k in phases if k in fl), key=lambda k: phases[k][1])
-    n_launch, tot_ms = phases[dom]
-    achieved = fl[dom] * W * n_launch / (tot_ms / 1e3) / 1e12
-    roofline = {
-        "kernel": dom,
-        "bound": "fp64-tensor",
-        "achieved": round(achieved, 3),
-        "peak": peaks["fp64_tflops"],
-        "unit": "TFLOP/s",
-        "frac": round(achieved / peaks["fp64_tflops"], 4),
-        "traffic": None,
-        "peak_source": "measured cuBLAS DGEMM 8192^3 on B200 (no FP64 entry in MEASURED_PEAKS.json)",
-        "phase_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(phases.items())},
+    res = {
+        "t": barrier_max(ev0.elapsed_time(ev1) / 1e3, world),
+        "phases": timer.summary(),
+        "launches": _lib.launch_count() - launches0,
+        "blocks": np.array(af.block_data),
+        "timed_blocks": np.array(af.block_data[nblocks0:]),
+        "alias": bool(af.walkers.spin_alias),
+        "clocks": clk.summary() if clk else None,
     }
-    step_flops = sum(fl.values()) * W + fl_energy * W / 25.0
+    af.propagator.timer = _NoTimer()
     del af
     torch.cuda.empty_cache()
+    return res
 
-    # ---------------- end to end through the public API ----------------
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    wl = args.workload
+    p = WORKLOADS[wl]
+    W = args.walkers or p["walkers"]
+    M, na, nb, X = p["nbasis"], p["nocc"], p["nocc"], p["nchol"]
+    peaks = load_peaks()
+    forms = ["fp64", "mixed"] if args.form == "both" else [args.form]
+
+    runs = {}
+    for form in forms:
+        runs[form] = timed_run(wl, W, form, args, rank, world, local, with_clock=(form == forms[-1]))
+    head = "mixed" if "mixed" in runs else "fp64"
+    r = runs[head]
+    t = r["t"]
+    value = W * args.steps * world / t
+
+    # roofline of the dominant kernel phase of the headline form (work executed)
+    alias = r["alias"]
+    fl, fl_energy = flops_per_walker(M, na, nb, X, alias=alias)
+    fl_ipie, fl_energy_ipie = flops_per_walker(M, na, nb, X, alias=False)
+    phases = r["phases"]
+    dom = max((k for k in phases if k in fl), key=lambda k: phases[k][1])
+    n_launch, tot_ms = phases[dom]
+    if head == "mixed":
+        # tensor-core passes: force bias 1, VHS/orbitals 3 (hi/lo split); peak = measured TF32
+        passes = {"force_bias": 1}.get(dom, 3)
+        achieved = passes * fl[dom] * W * n_launch / (tot_ms / 1e3) / 1e12
+        peak, bound, src = peaks["tf32_tflops"], "tf32-tensor", "measured cuBLAS TF32 8192^3 on B200 (tcgen05)"
+    else:
+        achieved = fl[dom] * W * n_launch / (tot_ms / 1e3) / 1e12
+        peak, bound, src = peaks["fp64_tflops"], "fp64-tensor", "measured cuBLAS DGEMM 8192^3 on B200"
+    roofline = {
+        "kernel": dom, "bound": bound, "achieved": round(achieved, 3), "peak": peak, "unit": "TFLOP/s",
+        "frac": round(achieved / peak, 4), "traffic": None, "peak_source": src,
+        "phase_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(phases.items())},
+    }
+    step_flops = (sum(v for k, v in fl.items() if k != "orbitals") * W + fl_energy * W / 25.0)
+    step_flops_ipie = (sum(v for k, v in fl_ipie.items() if k != "orbitals") * W + fl_energy_ipie * W / 25.0)
+
+    forms_out = {}
+    for form, rr in runs.items():
+        forms_out[form] = {"walker_steps_per_s": W * args.steps * world / rr["t"], "ms_per_step": rr["t"] / args.steps * 1e3,
+                           "gpu_launches": int(rr["launches"]),
+                           "block_etotal": [round(float(x), 9) for x in rr["blocks"][:, 5]]}
+    shift = None
+    if "mixed" in runs and "fp64" in runs:
+        a, b = runs["mixed"]["blocks"][:, 5], runs["fp64"]["blocks"][:, 5]
+        n = min(len(a), len(b))
+        shift = float(np.max(np.abs(a[:n] - b[:n]))) * 1e3  # mEh, same draws and seed
+        forms_out["mixed_over_fp64"] = forms_out["mixed"]["walker_steps_per_s"] / forms_out["fp64"]["walker_steps_per_s"]
+
+    # ---------------- end to end through the public API (headline form) ----------------
     e2e_steps = min(args.steps, args.e2e_steps)
-    af2, _ = build_afqmc(wl, W, "host", 7 + rank)
+    af2, _ = build_afqmc(wl, W, "host", 7 + rank, precision=head)
     rng = np.random.default_rng(1234 + rank)
     fields = [torch.from_numpy(rng.standard_normal((W, X))).pin_memory() for _ in range(args.warmup + e2e_steps)]
     af2.propagator.host_fields = iter(fields)
@@ -331,14 +377,13 @@ def run_ours(args):
     del af2, fields
     torch.cuda.empty_cache()
 
-    line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            r, sample, _, _ = cpu_oracle_rate(wl, walkers_sample=args.ref_walkers, steps=2, energy_walkers=1)
-            cpu = {"value": r, "unit": "walker-steps/s", "cores": blas_threads(), "kind": "port", "sample": sample}
+            rcpu, sample, _, _ = cpu_oracle_rate(wl, walkers_sample=args.ref_walkers, steps=2, energy_walkers=1)
+            cpu = {"value": rcpu, "unit": "walker-steps/s", "cores": blas_threads(), "kind": "port", "sample": sample}
         line = {
-            "metric": "walker-steps/s (plain FP64 phaseless AFQMC step)",
+            "metric": "walker-steps/s at <=0.1 mEh energy shift (mixed vs plain FP64 phaseless AFQMC step)",
             "value": value,
             "unit": "walker-steps/s",
             "n_gpus": world,
@@ -348,23 +393,27 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64",
+            "dtype": "tf32+f64" if head == "mixed" else "f64",
             "data": "synthetic",
             "config": {
                 "workload": wl, "nbasis": M, "nalpha": na, "nbeta": nb, "nchol": X, "walkers_per_gpu": W,
-                "dt": 0.005, "form": "plain_fp64", "parallelism": f"replicas{world}",
-                "l2": "inputs larger than L2 (VHS 1.3 GB + walkers 0.4 GB per step)",
+                "dt": 0.005, "form": head, "parallelism": f"replicas{world}",
+                "l2": "inputs larger than L2 (VHS 1.3 GB fp64 / 1.3 GB split fp32, walkers 0.2-0.4 GB)",
                 "step": "reortho/5, propagate, clip, pair-branch/5, energy/25 (ipie driver order)",
             },
+            "forms": forms_out,
+            "energy_shift_mEh": shift,
             "e2e": {"value": e2e_value, "unit": "walker-steps/s", "h2d_bytes_per_step": W * X * 8,
                     "d2h_bytes_per_step": W * 8, "steps": e2e_steps,
                     "fields": "host-supplied N(0,1) draws in pinned memory, one (W, X) array per step"},
             "roofline": roofline,
             "step_tflops": round(step_flops / (t / args.steps) / 1e12, 3),
+            "work": {"spin_alias": alias, "executed_gflop_per_step": round(step_flops / 1e9, 1),
+                     "ipie_equivalent_gflop_per_step": round(step_flops_ipie / 1e9, 1)},
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
-            "gpu_launches": int(launches),
-            "finite_energies": energy_ok,
+            "clocks": r["clocks"],
+            "gpu_launches": int(r["launches"]),
+            "finite_energies": bool(all(np.all(np.isfinite(rr["blocks"])) for rr in runs.values())),
         }
         print(json.dumps(line))
     if world > 1:
@@ -419,6 +468,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=25)
     ap.add_argument("--ref-walkers", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", choices=["fp64", "mixed", "both"], default="both",
+                    help="which forms to time; with both, the mixed form is the headline and the FP64 form its reference")
     ap.add_argument("--measure-peaks", action="store_true", help="print measured GEMM/copy peaks and exit")
     args = ap.parse_args()
     if args.measure_peaks:

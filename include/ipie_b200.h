@@ -12,6 +12,11 @@
  *     vectors, P = M(M+1)/2 packed pairs;
  *   - return value: 0 on success, otherwise the cudaError_t of the failed
  *     launch (cudaErrorInvalidValue = 1 for unsupported sizes);
+ *   - spin aliasing: passing the same pointer for the alpha and beta arrays
+ *     (phib == phia, ghalfb == ghalfa, rcholb == rchola, with nb == na)
+ *     declares the beta block an exact copy of the alpha block (an RHF trial
+ *     and walkers started from it); such blocks are computed once and counted
+ *     twice, with the same results as two identical blocks;
  *   - `status` (optional, device unsigned int) collects numerical trouble
  *     bits: 1 non-finite value, 2 singular overlap pivot, 4 bad shape,
  *     8 zero column in Gram-Schmidt.  Kernels never trap; the caller reads
@@ -93,6 +98,18 @@ int ipie_b200_apply_exponential_batch(const void* vhs, const void* phi_in, void*
 int ipie_b200_propagate_one_body(const void* expH1, int expH1_is_complex, const void* phi_in, void* phi_out, int W,
                                  int M, int N, void* stream);
 
+/* One launch for the orbital update of a step: phi_out = B exp(VHS) B phi_in per
+ * walker, B = expH1 (each one-body factor optional), exp by the order-nmax
+ * Taylor recurrence.  replaces the sequence ipie applies in
+ * propagation/phaseless_base.py:321-327: propagate_walkers_one_body
+ * (operations.py:26-55), apply_exponential_batch (operations.py:85-117),
+ * propagate_walkers_one_body.
+ * vhs (W,M,M) complex; expH1 real (M, lda_e) row-major with lda_e even >= M
+ * (NULL when both flags are 0); phi_in/phi_out (W,M,N) complex, distinct.
+ * Supports M <= 256, N <= 32 (cudaErrorInvalidValue otherwise). */
+int ipie_b200_propagate_orbitals(const void* vhs, const double* expH1, int lda_e, const void* phi_in, void* phi_out,
+                                 int W, int M, int N, int nmax, int pre_one_body, int post_one_body, void* stream);
+
 /* Hybrid energy, importance function, cosine projection, then the driver's
  * weight clip when *wbound >= 0 (wbound may be NULL).
  * replaces: propagation/phaseless_base.py:340-358 (update_weight),
@@ -161,6 +178,16 @@ int ipie_b200_local_energy_single_det_batch(int rhf, const double* rchola, const
                                             int W, int X, int M, int na, int nb, void* work, void* energy,
                                             unsigned int* status, void* stream);
 
+/* Energy from its parts: energy[w] = (e1b + e2b, e1b, e2b) with
+ * e1b = f1 (Ghalfa.rH1a + Ghalfb.rH1b) + ecore (ghalfb NULL: alpha only),
+ * e2b = fc sum_x xv[w,x]^2 - fx sum_t part[t,w] (nrows = 0: no exchange term).
+ * The local-energy entry points are this combine after their GEMMs; the
+ * control variate uses it without the exchange. */
+int ipie_b200_energy_combine(int W, int X, int M, int na, int nb, const void* ghalfa, const void* ghalfb,
+                             const void* rH1a, const void* rH1b, double ecore, const void* xv, const void* part,
+                             int nrows, double f1, double fc, double fx, void* energy, unsigned int* status,
+                             void* stream);
+
 /* Per-walker block sums (complex[7], accumulated into out when accumulate=1):
  * [sum w, sum w_unscaled, sum w*E_hyb, sum w*Re E0, sum w, sum w*Re E1, sum w*Re E2].
  * replaces: walkers/base_walkers.py:43-50 (WalkerAccumulator.update) and
@@ -174,6 +201,114 @@ int ipie_b200_walker_sums(int W, const double* weight, const double* unscaled_we
  * propagation/phaseless_base.py:296-298 (xp.random.normal).  The sequence
  * differs from numpy's MT19937 by construction. */
 int ipie_b200_normal_fill(double* out, long long n, unsigned long long seed, unsigned long long offset, void* stream);
+
+/* ---- mixed-precision form: TF32 tensor cores (tcgen05), FP32 accumulation ----
+ * FP64 stays in the overlap LU/determinant, the Green's function solve,
+ * Gram-Schmidt, the weights/phases and the orbital accumulation. */
+
+/* Force bias as a 3-pass TF32 product (FP32 accumulation, FP64 output), from the
+ * padded half-rotated Cholesky split (ipie_b200_rchol_pad_split).  Same contract
+ * and spin-alias convention as ipie_b200_construct_force_bias_batch_single_det;
+ * gwork: 2*W*2*32*M floats; M % 4 == 0. */
+int ipie_b200_construct_force_bias_mixed(const float* ra_hi, const float* ra_lo, const float* rb_hi,
+                                         const float* rb_lo, const void* ghalfa, const void* ghalfb, float* gwork,
+                                         int W, int X, int M, int na, int nb, void* vbias, unsigned int* status,
+                                         void* stream);
+
+/* ipie_b200_field_shift that also (or only: xshifted may be NULL) writes the
+ * shifted fields as planar (W, 2, X) fp32 TF32 head/remainder pairs. */
+int ipie_b200_field_shift_mixed(const void* vbias, const double* xi, const void* mf_shift, int W, int X,
+                                double sqrt_dt, double bound, void* xshifted, float* xs_hi, float* xs_lo, void* cmf,
+                                void* cfb, void* stream);
+
+/* VHS = i sqrt(dt) L . xshifted as a 3-pass TF32 product (~2^-22 relative),
+ * written as four planar (W, M, M) fp32 arrays: Re/Im x TF32 head/remainder.
+ * cp_hi/cp_lo: packed Cholesky (P, X) split; xs_hi/xs_lo from
+ * ipie_b200_field_shift_mixed; X % 4 == 0.  replaces (mixed form):
+ * propagation/phaseless_generic.py:66-97. */
+int ipie_b200_construct_vhs_mixed(const float* cp_hi, const float* cp_lo, const int* idx_i, const int* idx_j, int M,
+                                  int X, const float* xs_hi, const float* xs_lo, int W, double sqrt_dt, float* v_re_hi,
+                                  float* v_re_lo, float* v_im_hi, float* v_im_lo, unsigned int* status, void* stream);
+
+/* phi_out = E exp(V) E phi_in per walker with every product a 3-pass TF32
+ * tensor-core GEMM (E = expH1 hi/lo (M, lde) fp32, lde % 4 == 0; V planar from
+ * ipie_b200_construct_vhs_mixed); phi accumulates in FP64.  work: 4*W*2N*M
+ * floats.  M % 4 == 0, 2N <= 64.  replaces (mixed form):
+ * propagation/phaseless_base.py:321-327. */
+int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float* e_lo, int lde, const float* v_re_hi,
+                                       const float* v_re_lo, const float* v_im_hi, const float* v_im_lo,
+                                       const void* phi_in, void* phi_out, float* work, int W, int M, int N, int nmax,
+                                       unsigned int* status, void* stream);
+
+/* Half-rotated Cholesky rows (x, i) padded to NP = 8/16/32 >= N, as fp32
+ * TF32 head/remainder (X*NP, M) arrays: the left operand of the mixed energy. */
+int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, float* hi, float* lo, void* stream);
+
+/* Local energy of the mixed form: the exchange as 3-pass TF32 tensor-core
+ * products (T never stored, bilinear sums in FP64); Coulomb vector and e1b in
+ * FP64.  Same contract and spin-alias convention as
+ * ipie_b200_local_energy_single_det_batch; rchola/rcholb FP64, r*_hi/lo from
+ * ipie_b200_rchol_pad_split; gwork: 2*W*2*32*M floats; work: W*X + rows*W
+ * complex with rows = sum over spin blocks of ceil(X*NP/128); M % 4 == 0.
+ * replaces (mixed form): estimators/local_energy_sd.py:987-1080. */
+int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const float* ra_hi,
+                                 const float* ra_lo, const float* rb_hi, const float* rb_lo, const void* rH1a,
+                                 const void* rH1b, double ecore, const void* ghalfa, const void* ghalfb, int W, int X,
+                                 int M, int na, int nb, float* gwork, void* work, void* energy, unsigned int* status,
+                                 void* stream);
+
+/* ---- learned control variate for the exchange energy (no counterpart in ipie) ----
+ * MLP 16 -> H -> H -> 1 (SiLU), bf16 weights `wbf`, fp32 master copy/biases,
+ * FP32 accumulation; parameter layout W1 (16,H), b1, W2 (H,H), b2, W3 (H,1), b3. */
+/* out (B) = MLP(x (B,16)); acts: 4*B*H floats (pre/post activations kept for backward). */
+int ipie_b200_mlp_forward(const float* x, int B, int F, int H, const void* wbf, const float* master, float* acts,
+                          float* out, void* stream);
+/* grad = d/dtheta mean((out - target)^2); work: B + 2*B*H floats; loss (+)= the batch loss. */
+int ipie_b200_mlp_backward(const float* x, const float* target, int B, int F, int H, const void* wbf,
+                           const float* acts, const float* out, float* grad, float* work, float* loss, void* stream);
+/* One Adam step (beta 0.9/0.999) on the fp32 master weights; refreshes the bf16 copy. */
+int ipie_b200_mlp_adam(float* master, void* wbf, const float* grad, float* m, float* v, long long n, float lr, int t,
+                       void* stream);
+/* (x - mu) / sigma per feature column, in place. */
+int ipie_b200_normalize_features(float* x, long long rows, int F, const float* mu, const float* sigma, void* stream);
+/* 16 per-walker features (fp32, row-major (W,16)) from the exchange-free energy (W,3), the Coulomb
+ * vector xv (W,X), overlaps, hybrid energies, Ghalf (W,N,M), conj trial (M,N), trial Ghalf (N,M), weights. */
+int ipie_b200_cv_features(int W, int X, int N, int M, const void* energy, const void* xv, const void* ovlp,
+                          const void* hybrid_energy, const void* ghalf, const void* psi_conj, const void* ghalf_trial,
+                          const double* weight, float* feat, void* stream);
+/* dst[s] = src[idx[s]] for rows of `row` complex values. */
+int ipie_b200_gather_walkers(const void* src, const int* idx, int S, long long row, void* dst, void* stream);
+/* out[0..4] = [sum w (A - c), (W/S) sum_S w (y - c), sum w, sum w A, (W/S) sum_S w y]: the control-variate
+ * estimate of the weighted energy numerator is out[0] - out[1] (A: exchange-free energy, c: prediction,
+ * y: exact exchange term on the random subsample idx). */
+int ipie_b200_cv_sums(int W, const double* weight, const void* energy_noexx, const float* pred, int S, const int* idx,
+                      const double* y_s, double* out, void* stream);
+
+/* ---- adjoint of the local energy w.r.t. the one-body Hamiltonian (no counterpart in ipie;
+ * ipie's AD-AFQMC addon differentiates the same energy with torch autograd,
+ * addons/adafqmc/estimators/estimator.py:4-23) ----
+ * rdm[s] (M, M) complex = sum_w coeff[w] psi_s^* Ghalf_s^w, i.e. dL/dh1_s for upstream
+ * gradients coeff of the per-walker e1b; with coeff = w / sum w, the mixed-estimator
+ * one-body density matrix.  work: max(na,nb)*M complex. */
+int ipie_b200_onebody_adjoint(int W, int M, int na, int nb, const void* ghalfa, const void* ghalfb,
+                              const void* psia_conj, const void* psib_conj, const double* coeff, void* work, void* rdm,
+                              void* stream);
+/* rH1 (N, M) complex = psi^H h1: the half-rotated one-body matrix for a given h1 (M, M) real
+ * (trial_wavefunction/half_rotate.py:55-56). */
+int ipie_b200_rotate_onebody(const void* psi_conj, const double* h1, int M, int N, void* rh1, void* stream);
+
+/* Split FP64 values into a TF32 head (round to nearest) and an FP32 remainder:
+ * x ~= hi + lo, the operands of the 3-pass TF32 tensor-core products of the
+ * mixed-precision form (lo may be NULL).  No counterpart in ipie. */
+int ipie_b200_split_tf32(const double* x, float* hi, float* lo, long long n, void* stream);
+
+/* Validation entry of the tcgen05 TF32 GEMM core: c[row][a][col] =
+ * sum_k A_a[row][k] B[col][k] for a < na (na = 1 or 2), A_a (M,K) and B (N,K)
+ * row-major fp32 with K % 4 == 0; nsplit = 1 (TF32) or 3 (hi/lo split, the
+ * *_lo operands used).  No counterpart in ipie. */
+int ipie_b200_umma_gemm_test(const float* a0_hi, const float* a0_lo, const float* a1_hi, const float* a1_lo,
+                             const float* b_hi, const float* b_lo, float* c, int M, int N, int K, int na, int nsplit,
+                             unsigned int* status, void* stream);
 
 #ifdef __cplusplus
 }

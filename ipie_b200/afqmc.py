@@ -79,7 +79,7 @@ class AFQMC:
     @staticmethod
     def build(num_elec, hamiltonian, trial_wavefunction, walkers=None, num_walkers=100, seed=None,
               num_steps_per_block=25, num_blocks=100, timestep=0.005, stabilize_freq=5, pop_control_freq=5,
-              verbose=True, mpi_handler=None, rng="numpy"):
+              verbose=True, mpi_handler=None, rng="numpy", spin_alias="auto", precision="fp64"):
         params = QMCParams(num_walkers, num_walkers, num_blocks, num_steps_per_block, timestep, stabilize_freq,
                            pop_control_freq, seed)
         if not trial_wavefunction.half_rotated:
@@ -89,8 +89,13 @@ class AFQMC:
             walkers = UHFWalkers(init, num_elec[0], num_elec[1], hamiltonian.nbasis, num_walkers,
                                  device=trial_wavefunction.device)
             walkers.build(trial_wavefunction)
-        prop = PhaselessGeneric(timestep, rng=rng, seed=seed if seed is not None else 7)
+        prop = PhaselessGeneric(timestep, rng=rng, seed=seed if seed is not None else 7, precision=precision)
         prop.build(hamiltonian, trial_wavefunction, walkers)
+        # identical spin blocks (RHF trial, walkers started from it, equal one-body operators):
+        # compute each block once (results equal propagating both, ipie's production mode)
+        if spin_alias and getattr(trial_wavefunction, "spin_symmetric", False) and prop.spin_symmetric:
+            if walkers.nup == walkers.ndown and torch.equal(walkers.phia, walkers.phib):
+                walkers.enable_spin_alias()
         return AFQMC(num_elec, hamiltonian, trial_wavefunction, walkers, prop, params, verbose=verbose)
 
     def _block(self, block, est, acc_vals):
@@ -111,7 +116,7 @@ class AFQMC:
         w.orthogonalise()
         self.pcontrol = PopController(p.num_walkers, p.num_steps_per_block)
         self.accumulators = WalkerAccumulator(p.num_steps_per_block, w.device)
-        self.estimator = EnergyEstimator()
+        self.estimator = EnergyEstimator(precision=self.propagator.precision)
         self.estimator.compute_estimator(self.system, w, ham, trial)
         self.accumulators.update(w)
         self._block(0, self.estimator, self.accumulators.block_end(0))

@@ -1,0 +1,272 @@
+"""Learned control variate for the exchange energy (no counterpart in ipie).
+
+The exchange term dominates the cost of a local-energy evaluation
+(O(W X N^2 M)).  A small MLP (16 -> 256 -> 256 -> 1, SiLU, bf16 weights, FP32
+accumulation) predicts each walker's exchange term from cheap per-walker
+features (one-body and Coulomb energies, force-bias norms, overlap phase and
+magnitude, hybrid energy, Green's-function norms; see
+``ipie_b200_cv_features``).  The block estimate stays unbiased: the exact
+exchange is evaluated on a uniform random subsample S of the walkers and
+
+    sum_w w_w E_w  ~=  sum_w w_w (A_w - c_w)  -  (W/|S|) sum_{s in S} w_s (y_s - c_s)
+
+with A_w the exchange-free energy, c_w the prediction and y_s the exact
+exchange term.  The expectation over S equals the exact sum for any c, so a
+poor network only costs variance; the exact kernel remains the reference.
+
+Training runs entirely on the GPU through the library's own forward,
+backward and Adam kernels (``ipie_b200_mlp_*``).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from ._lib import call, lib, ptr, stream
+
+F32, F64, C128 = torch.float32, torch.float64, torch.complex128
+NFEAT = 16
+
+
+def _param_count(F, H):
+    return F * H + H + H * H + H + H + 1
+
+
+class ExchangeControlVariate:
+    """MLP predictor of the per-walker exchange term, trained on the GPU."""
+
+    def __init__(self, hidden=256, device="cuda", seed=0):
+        self.F, self.H = NFEAT, hidden
+        self.device = torch.device(device)
+        n = _param_count(self.F, self.H)
+        self.n = n
+        rng = np.random.default_rng(seed)
+        theta = np.zeros(n, dtype=np.float32)
+        o = 0
+        for fan_in, fan_out in ((self.F, self.H), (self.H, self.H), (self.H, 1)):
+            lim = math.sqrt(6.0 / (fan_in + fan_out))
+            theta[o:o + fan_in * fan_out] = rng.uniform(-lim, lim, fan_in * fan_out)
+            o += fan_in * fan_out + fan_out  # biases start at zero
+        dev = self.device
+        self.master = torch.from_numpy(theta).to(dev)
+        self.wbf = self.master.to(torch.bfloat16)
+        self.grad = torch.zeros(n, dtype=F32, device=dev)
+        self.m = torch.zeros(n, dtype=F32, device=dev)
+        self.v = torch.zeros(n, dtype=F32, device=dev)
+        self.t = 0
+        self.mu = torch.zeros(self.F, dtype=F32, device=dev)
+        self.sigma = torch.ones(self.F, dtype=F32, device=dev)
+        self.y_mean = 0.0
+        self.y_scale = 1.0
+        self.trained = False
+
+    # ------------------------------------------------------------ training
+    def fit(self, feats, y, epochs=60, batch=4096, lr=2e-3, holdout=0.1, seed=0):
+        """Train on (features, exchange term) pairs; returns the train/holdout MSE history (normalised units).
+
+        ``feats``: (n, 16) float32 CUDA tensor of raw features; ``y``: (n,) float64/32 targets.
+        """
+        n = feats.shape[0]
+        fm = feats.double().mean(0)
+        fs = feats.double().std(0)
+        fs = torch.where(fs > 0, fs, torch.ones_like(fs))
+        self.mu.copy_(fm.float())
+        self.sigma.copy_(fs.float())
+        yd = y.double()
+        self.y_mean = float(yd.mean())
+        self.y_scale = float(yd.std()) or 1.0
+        x = feats.float().contiguous().clone()
+        call("ipie_b200_normalize_features", ptr(x), n, self.F, ptr(self.mu), ptr(self.sigma), stream())
+        yt = ((yd - self.y_mean) / self.y_scale).float().contiguous()
+        gen = torch.Generator(device="cpu").manual_seed(seed)
+        perm = torch.randperm(n, generator=gen).to(self.device)
+        nho = int(n * holdout)
+        ho, tr = perm[:nho], perm[nho:]
+        xh, yh = x[ho].contiguous(), yt[ho].contiguous()
+        acts = torch.empty(4 * batch * self.H, dtype=F32, device=self.device)
+        work = torch.empty(batch + 2 * batch * self.H, dtype=F32, device=self.device)
+        out = torch.empty(batch, dtype=F32, device=self.device)
+        loss = torch.zeros(1, dtype=F32, device=self.device)
+        history = []
+        for ep in range(epochs):
+            order = tr[torch.randperm(tr.numel(), generator=gen).to(self.device)]
+            loss.zero_()
+            nb = 0
+            for b0 in range(0, order.numel() - batch + 1, batch):
+                idx = order[b0:b0 + batch]
+                xb, yb = x[idx].contiguous(), yt[idx].contiguous()
+                self._step(xb, yb, batch, acts, work, out, loss, lr)
+                nb += 1
+            tr_loss = float(loss.item()) / max(nb, 1)
+            history.append((tr_loss, self.mse(xh, yh)))
+        self.trained = True
+        return history
+
+    def _step(self, xb, yb, B, acts, work, out, loss, lr):
+        call("ipie_b200_mlp_forward", ptr(xb), B, self.F, self.H, ptr(self.wbf), ptr(self.master), ptr(acts), ptr(out),
+             stream())
+        call("ipie_b200_mlp_backward", ptr(xb), ptr(yb), B, self.F, self.H, ptr(self.wbf), ptr(acts), ptr(out),
+             ptr(self.grad), ptr(work), ptr(loss), stream())
+        self.t += 1
+        call("ipie_b200_mlp_adam", ptr(self.master), ptr(self.wbf), ptr(self.grad), ptr(self.m), ptr(self.v), self.n,
+             float(lr), self.t, stream())
+
+    def mse(self, x_norm, y_norm):
+        pred = self.forward_normalised(x_norm)
+        return float(((pred - y_norm) ** 2).mean().item())
+
+    def forward_normalised(self, x_norm):
+        B = x_norm.shape[0]
+        acts = torch.empty(4 * B * self.H, dtype=F32, device=self.device)
+        out = torch.empty(B, dtype=F32, device=self.device)
+        call("ipie_b200_mlp_forward", ptr(x_norm.contiguous()), B, self.F, self.H, ptr(self.wbf), ptr(self.master),
+             ptr(acts), ptr(out), stream())
+        return out
+
+    def predict(self, feats):
+        """Exchange-term prediction (fp32, physical units) for raw features (W, 16)."""
+        x = feats.float().contiguous().clone()
+        call("ipie_b200_normalize_features", ptr(x), x.shape[0], self.F, ptr(self.mu), ptr(self.sigma), stream())
+        out = self.forward_normalised(x)
+        # physical units: y = mean + scale * out (a tiny elementwise map; kept as torch plumbing)
+        return (out.double() * self.y_scale + self.y_mean).float().contiguous()
+
+
+# ----------------------------------------------------------------------------
+# energy pieces used by the estimator and by training-data generation
+# ----------------------------------------------------------------------------
+class EnergyParts:
+    """Exchange-free energies, Coulomb vectors, exact exchange terms and features of a walker batch."""
+
+    def __init__(self, hamiltonian, trial, walkers):
+        self.ham, self.trial = hamiltonian, trial
+        W, X, M = walkers.nwalkers, hamiltonian.nchol, hamiltonian.nbasis
+        dev = walkers.device
+        self.xv = torch.empty(W, X, dtype=C128, device=dev)
+        self.energy_noexx = torch.empty(W, 3, dtype=C128, device=dev)
+        self.feat = torch.empty(W, NFEAT, dtype=F32, device=dev)
+        self.exx = torch.empty(W, dtype=C128, device=dev)
+        gh = trial.Ghalf[0]
+        self.ghalf_trial = torch.from_numpy(np.ascontiguousarray(gh.astype(np.complex128))).to(dev)
+
+    def compute(self, walkers, with_features=True):
+        """Green's functions, exchange-free energy and features for every walker."""
+        from .trial import force_bias_into
+
+        ham, trial = self.ham, self.trial
+        W, X, M = walkers.nwalkers, ham.nchol, ham.nbasis
+        trial.calc_greens_function(walkers)
+        force_bias_into(ham, walkers, trial, self.xv)  # Coulomb vector X_a + X_b
+        rhf = bool(walkers.rhf)
+        f1, fc = (2.0, 2.0) if rhf else (1.0, 0.5)
+        gb = None if (rhf or walkers.ndown == 0) else walkers.Ghalfb
+        call("ipie_b200_energy_combine", W, X, M, walkers.nup, walkers.ndown, ptr(walkers.Ghalfa), ptr(gb),
+             ptr(trial._rH1a), ptr(trial._rH1b), ham.ecore, ptr(self.xv), None, 0, f1, fc, 0.0,
+             ptr(self.energy_noexx), ptr(walkers.status), stream())
+        if with_features:
+            call("ipie_b200_cv_features", W, X, walkers.nup, M, ptr(self.energy_noexx), ptr(self.xv), ptr(walkers.ovlp),
+                 ptr(walkers.hybrid_energy), ptr(walkers.Ghalfa), ptr(trial.psia_conj), ptr(self.ghalf_trial),
+                 ptr(walkers.weight), ptr(self.feat), stream())
+
+    def exchange_term(self, walkers, idx=None):
+        """Exact exchange term y = 1/2 Re(raw_a + raw_b) (W,) or on the subsample ``idx``; float64."""
+        ham = self.ham
+        X, M = ham.nchol, ham.nbasis
+        S = walkers.nwalkers if idx is None else int(idx.numel())
+        total = torch.zeros(S, dtype=F64, device=walkers.device)
+        blocks = [(self.trial._rchola, walkers.Ghalfa, walkers.nup, 1.0 if walkers.spin_alias else 0.5)]
+        if walkers.ndown > 0 and not walkers.spin_alias:
+            blocks.append((self.trial._rcholb, walkers.Ghalfb, walkers.ndown, 0.5))
+        for rchol, gh, n, fac in blocks:
+            if idx is not None:
+                sub = torch.empty(S, n, M, dtype=C128, device=walkers.device)
+                call("ipie_b200_gather_walkers", ptr(gh), ptr(idx), S, n * M, ptr(sub), stream())
+            else:
+                sub = gh
+            rows = lib().ipie_b200_exchange_rows(S, X, M, n)
+            part = torch.empty(rows * S, dtype=C128, device=walkers.device)
+            call("ipie_b200_exchange", ptr(rchol), ptr(sub), S, X, M, n, ptr(part), stream())
+            total += fac * part.view(rows, S).sum(0).real
+        return total
+
+
+class ControlVariateEnergyEstimator:
+    """Block energy with the learned control variate and a uniform 1/``fraction`` exact subsample."""
+
+    names = ["ENumer", "EDenom", "ETotal", "E1Body", "E2Body"]
+
+    def __init__(self, cv, fraction=8, seed=11):
+        self.cv = cv
+        self.fraction = fraction
+        self.rng = np.random.default_rng(seed)
+        self.parts = None
+        self._out = None
+        self.last = {}
+
+    def compute_estimator(self, system=None, walkers=None, hamiltonian=None, trial=None):
+        if self.parts is None:
+            self.parts = EnergyParts(hamiltonian, trial, walkers)
+            self._out = torch.zeros(5, dtype=F64, device=walkers.device)
+        p = self.parts
+        p.compute(walkers)
+        pred = self.cv.predict(p.feat)
+        W = walkers.nwalkers
+        S = max(1, W // self.fraction)
+        idx = torch.from_numpy(np.sort(self.rng.choice(W, S, replace=False)).astype(np.int32)).to(walkers.device)
+        y_s = p.exchange_term(walkers, idx)
+        call("ipie_b200_cv_sums", W, ptr(walkers.weight), ptr(p.energy_noexx), ptr(pred), S, ptr(idx), ptr(y_s),
+             ptr(self._out), stream())
+        o = self._out.cpu().numpy()
+        numer = o[0] - o[1]
+        self.last = {"cv": numer, "plain_subsample": o[3] - o[4], "denom": o[2]}
+        self._data = np.array([numer, o[2], 0.0, 0.0, 0.0], dtype=np.complex128)
+        return self.data
+
+    @property
+    def data(self):
+        return self._data
+
+    def post_reduce_hook(self, data):
+        data[2] = data[0] / data[1]
+
+
+def generate_training_data(afqmc, steps=100, first_step=1):
+    """(features, exact exchange term) for every walker at each of ``steps`` driver steps.
+
+    Runs the walk forward with the plain method (the AFQMC object's own
+    propagator); returns float32 features (steps*W, 16) and float64 targets.
+    """
+    w = afqmc.walkers
+    parts = EnergyParts(afqmc.hamiltonian, afqmc.trial, w)
+    feats, ys = [], []
+    for step in range(first_step, first_step + steps):
+        afqmc.step(step)
+        parts.compute(w)
+        ys.append(parts.exchange_term(w))
+        feats.append(parts.feat.clone())
+    return torch.cat(feats), torch.cat(ys)
+
+
+def subsample_variances(cv, parts, walkers, fraction=8, trials=64, seed=3):
+    """Spread of the subsampled exchange estimate over random subsamples, with and without the network.
+
+    Returns (std_without, std_with, exact) for the weighted exchange sum of the current walkers.
+    """
+    parts.compute(walkers)
+    y = parts.exchange_term(walkers)
+    wt = walkers.weight.double()
+    exact = float((wt * y).sum().item())
+    pred = cv.predict(parts.feat).double()
+    full_c = float((wt * pred).sum().item())
+    rng = np.random.default_rng(seed)
+    W = walkers.nwalkers
+    S = max(1, W // fraction)
+    plain, with_cv = [], []
+    for _ in range(trials):
+        idx = torch.from_numpy(rng.choice(W, S, replace=False)).to(walkers.device)
+        f = W / S
+        plain.append(f * float((wt[idx] * y[idx]).sum().item()))
+        with_cv.append(full_c + f * float((wt[idx] * (y[idx] - pred[idx])).sum().item()))
+    return float(np.std(plain)), float(np.std(with_cv)), exact

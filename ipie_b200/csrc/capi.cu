@@ -40,8 +40,10 @@ int ipie_b200_calc_overlap_single_det_uhf(const void* phia, const void* phib, in
 int ipie_b200_construct_force_bias_batch_single_det(const double* rchola, const double* rcholb, const void* ghalfa,
                                                     const void* ghalfb, int W, int X, int M, int na, int nb,
                                                     void* vbias, void* stream) {
-  cudaError_t e = launch_force_bias(rchola, CC2(ghalfa), W, X, na * M, C2(vbias), 0, ST(stream));
-  if (e != cudaSuccess || nb == 0) return (int)e;
+  // Spin aliasing (rcholb == rchola, ghalfb == ghalfa, nb == na): one product, doubled (exactly t + t).
+  const bool alias = nb == na && nb > 0 && rcholb == rchola && ghalfb == ghalfa;
+  cudaError_t e = launch_force_bias(rchola, CC2(ghalfa), W, X, na * M, C2(vbias), 0, ST(stream), alias ? 2.0 : 1.0);
+  if (e != cudaSuccess || nb == 0 || alias) return (int)e;
   return (int)launch_force_bias(rcholb, CC2(ghalfb), W, X, nb * M, C2(vbias), 1, ST(stream));
 }
 
@@ -70,6 +72,12 @@ int ipie_b200_propagate_one_body(const void* expH1, int expH1_is_complex, const 
   if (phi_in == phi_out) return (int)cudaErrorInvalidValue;
   return (int)launch_one_body(reinterpret_cast<const double*>(expH1), expH1_is_complex, CC2(phi_in), C2(phi_out), W, M,
                               N, ST(stream));
+}
+
+int ipie_b200_propagate_orbitals(const void* vhs, const double* expH1, int lda_e, const void* phi_in, void* phi_out,
+                                 int W, int M, int N, int nmax, int pre_one_body, int post_one_body, void* stream) {
+  return (int)launch_propagate_fused(CC2(vhs), expH1, lda_e, CC2(phi_in), C2(phi_out), W, M, N, nmax, pre_one_body,
+                                     post_one_body, ST(stream));
 }
 
 int ipie_b200_update_weight(int W, const void* ovlp_new, const void* cfb, const void* cmf, const double* eshift,
@@ -114,8 +122,9 @@ int ipie_b200_local_energy_single_det_batch(int rhf, const double* rchola, const
   cudaStream_t st = ST(stream);
   double2* xv = C2(work);
   double2* part = xv + (size_t)W * X;
-  const int use_b = (!rhf && nb > 0);
-  cudaError_t e = launch_force_bias(rchola, CC2(ghalfa), W, X, na * M, xv, 0, st);
+  const bool alias = !rhf && nb == na && nb > 0 && rcholb == rchola && ghalfb == ghalfa;
+  const int use_b = (!rhf && nb > 0 && !alias);
+  cudaError_t e = launch_force_bias(rchola, CC2(ghalfa), W, X, na * M, xv, 0, st, alias ? 2.0 : 1.0);
   if (e == cudaSuccess && use_b) e = launch_force_bias(rcholb, CC2(ghalfb), W, X, nb * M, xv, 1, st);
   if (e != cudaSuccess) return (int)e;
   int rows_a = 0, rows_b = 0;
@@ -127,9 +136,19 @@ int ipie_b200_local_energy_single_det_batch(int rhf, const double* rchola, const
   }
   // UHF: e1b = Ga.rH1a + Gb.rH1b + ecore; ecoul = (Xa+Xb)^2 / 2; exx = raw / 2.
   // RHF: e1b = 2 Ga.rH1a + ecore;        ecoul = 2 Xa^2;         exx = raw.
-  const double f1 = rhf ? 2.0 : 1.0, fc = rhf ? 2.0 : 0.5, fx = rhf ? 1.0 : 0.5;
-  return (int)launch_energy_combine(W, X, na * M, nb * M, CC2(ghalfa), use_b ? CC2(ghalfb) : nullptr, CC2(rH1a),
+  // Spin aliasing: the beta exchange equals the alpha one (raw_a + raw_b = 2 raw_a).
+  const double f1 = rhf ? 2.0 : 1.0, fc = rhf ? 2.0 : 0.5, fx = (rhf || alias) ? 1.0 : 0.5;
+  const bool e1_b = !rhf && nb > 0;
+  return (int)launch_energy_combine(W, X, na * M, nb * M, CC2(ghalfa), e1_b ? CC2(ghalfb) : nullptr, CC2(rH1a),
                                     CC2(rH1b), ecore, xv, part, rows_a + rows_b, f1, fc, fx, C2(energy), status, st);
+}
+
+int ipie_b200_energy_combine(int W, int X, int M, int na, int nb, const void* ghalfa, const void* ghalfb,
+                             const void* rH1a, const void* rH1b, double ecore, const void* xv, const void* part,
+                             int nrows, double f1, double fc, double fx, void* energy, unsigned int* status,
+                             void* stream) {
+  return (int)launch_energy_combine(W, X, na * M, nb * M, CC2(ghalfa), CC2(ghalfb), CC2(rH1a), CC2(rH1b), ecore,
+                                    CC2(xv), CC2(part), nrows, f1, fc, fx, C2(energy), status, ST(stream));
 }
 
 int ipie_b200_walker_sums(int W, const double* weight, const double* unscaled_weight, const void* hybrid_energy,

@@ -21,20 +21,21 @@ struct EpiVbias {
   double2* v;
   int X;
   int accumulate;
+  double scale;  // 2 for spin-aliased walkers: exactly t + t
   __device__ __forceinline__ void operator()(int, int x, int col, double v0, double v1) const {
     const size_t idx = (size_t)(col >> 1) * X + x;
-    double2 r = make_double2(v0, v1);
+    double2 r = make_double2(scale * v0, scale * v1);
     if (accumulate) r = cadd(r, v[idx]);
     v[idx] = r;
   }
 };
 
 cudaError_t launch_force_bias(const double* rchol, const double2* ghalf, int W, int X, int K, double2* vbias,
-                              int accumulate, cudaStream_t st) {
+                              int accumulate, cudaStream_t st, double scale) {
   using C = CfgBig;
   LoadRowK<C, C::BM> la{rchol, 0, K};
   LoadWalkerCplx<C, C::BN> lb{reinterpret_cast<const double*>(ghalf), 2LL * K};
-  return launch_dmma_gemm<C>(X, 2 * W, K, 1, la, lb, EpiVbias{vbias, X, accumulate}, st);
+  return launch_dmma_gemm<C>(X, 2 * W, K, 1, la, lb, EpiVbias{vbias, X, accumulate, scale}, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -12,7 +12,8 @@ cudaError_t launch_gf_overlap(const double2* phia, const double2* phib, int W, i
                               const double2* psia_c, const double2* psib_c, const double* log_shift, double2* ghalfa,
                               double2* ghalfb, double2* ovlp, double2* logdet, unsigned* status, cudaStream_t st);
 cudaError_t launch_field_shift(const double2* vbias, const double* xi, const double2* mf, int W, int X, double sqrt_dt,
-                               double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st);
+                               double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st,
+                               float* xs_hi = nullptr, float* xs_lo = nullptr);
 cudaError_t launch_update_weight(int W, const double2* ovlp_new, const double2* cfb, const double2* cmf,
                                  const double* eshift, double dt, double ebound, const double* wbound, double2* ovlp,
                                  double2* ehyb, double* weight, unsigned* status, cudaStream_t st);
@@ -28,7 +29,7 @@ cudaError_t launch_energy_combine(int W, int X, int Ka, int Kb, const double2* g
                                   unsigned* status, cudaStream_t st);
 
 cudaError_t launch_force_bias(const double* rchol, const double2* ghalf, int W, int X, int K, double2* vbias,
-                              int accumulate, cudaStream_t st);
+                              int accumulate, cudaStream_t st, double scale = 1.0);
 cudaError_t launch_vhs(const double* chol_packed, const int* idx_i, const int* idx_j, int P, int X, int M,
                        const double2* xshifted, int W, double sqrt_dt, double2* vhs, cudaStream_t st);
 cudaError_t launch_one_body(const double* expH1, int cplx, const double2* phi_in, double2* phi_out, int W, int M, int N,
@@ -42,5 +43,18 @@ cudaError_t launch_normal_fill(double* out, long long n, unsigned long long seed
                                cudaStream_t st);
 cudaError_t launch_walker_sums(int W, const double* weight, const double* unscaled, const double2* ehyb,
                                const double2* energy, double2* out, int accumulate, cudaStream_t st);
+
+cudaError_t launch_propagate_fused(const double2* vhs, const double* expH1, int lda_e, const double2* phi_in,
+                                   double2* phi_out, int W, int M, int N, int nmax, int pre, int post, cudaStream_t st);
+
+namespace umma {
+cudaError_t mixed_vhs(const float* cp_hi, const float* cp_lo, const int* ii, const int* jj, int P, int X, int M,
+                      const float* xs_hi, const float* xs_lo, int W, double sqrt_dt, float* re_hi, float* re_lo,
+                      float* im_hi, float* im_lo, unsigned* status, cudaStream_t st);
+cudaError_t mixed_orbitals(const float* e_hi, const float* e_lo, int Mp, const float* v_re_hi, const float* v_re_lo,
+                           const float* v_im_hi, const float* v_im_lo, const double2* phi_in, double2* phi_out,
+                           float* b0_hi, float* b0_lo, float* b1_hi, float* b1_lo, int W, int M, int N, int nmax,
+                           unsigned* status, cudaStream_t st);
+}  // namespace umma
 
 }  // namespace ipie_b200

@@ -1,0 +1,604 @@
+// Mixed-precision (TF32 tensor-core) stages of the walker step and their
+// host-side plumbing: TMA tensor maps, hi/lo operand splits, launchers.
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "../../include/ipie_b200.h"
+#include "kernels.h"
+#include "umma_gemm.cuh"
+
+namespace ipie_b200 {
+namespace umma {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 2-D K-major fp32 operand: `rows` rows of `k` elements, row stride `ld` elements,
+// tiles of box_rows x 32 loaded 128B-swizzled; out-of-range elements read as 0.
+cudaError_t make_map(CUtensorMap* m, const float* base, long long rows, long long k, long long ld, int box_rows) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 4) || rows <= 0 || k <= 0) return cudaErrorInvalidValue;
+  cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+  cuuint32_t box[2] = {32, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// hi = TF32(x) (round to nearest), lo = float(x - hi): the split of the 3-pass product.
+__global__ void split_tf32_kernel(const double* __restrict__ x, float* __restrict__ hi, float* __restrict__ lo,
+                                  long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = x[i];
+    uint32_t h;
+    const float f = (float)v;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(f));
+    const float hf = __uint_as_float(h);
+    hi[i] = hf;
+    if (lo) lo[i] = (float)(v - (double)hf);
+  }
+}
+
+cudaError_t launch_split_tf32(const double* x, float* hi, float* lo, long long n, cudaStream_t st) {
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  split_tf32_kernel<<<(unsigned)blocks, 256, 0, st>>>(x, hi, lo, n);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- test epilogue
+// c[z][row][a][col] (row < M, col < N): the raw accumulators, for validation.
+template <int BN, int NA>
+struct EpiStoreF32 {
+  float* c;
+  int M, N;
+  __device__ __forceinline__ void operator()(int z, int row, int n0, const float* v, uint8_t*) const {
+    if (row >= M) return;
+    float* base = c + ((size_t)z * M + row) * (size_t)NA * N;
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int j = 0; j < BN; ++j)
+        if (n0 + j < N) base[(size_t)a * N + n0 + j] = v[a * BN + j];
+  }
+};
+
+template <int BN, int NA, int NSPLIT, int STAGES, class Epi>
+cudaError_t launch_umma(const GemmMaps& maps, int K, int a_rows_per_batch, int b_rows_per_batch, dim3 grid, Epi epi,
+                        unsigned* status, cudaStream_t st) {
+  using S = GemmShape<BN, NA, NSPLIT, STAGES>;
+  auto kern = umma_gemm_kernel<BN, NA, NSPLIT, STAGES, Epi>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, 128, S::SMEM_BYTES, st>>>(maps, K, a_rows_per_batch, b_rows_per_batch, epi, status);
+  note_launch();
+  return cudaGetLastError();
+}
+
+template <int NA, int NSPLIT, int STAGES>
+static cudaError_t gemm_test(const float* const* a_hi, const float* const* a_lo, const float* b_hi, const float* b_lo,
+                             float* c, int M, int N, int K, unsigned* status, cudaStream_t st) {
+  constexpr int BN = NA == 1 ? 128 : 64;
+  GemmMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  cudaError_t e;
+  for (int a = 0; a < NA; ++a) {
+    if ((e = make_map(&maps.a_hi[a], a_hi[a], M, K, K, kBM)) != cudaSuccess) return e;
+    if (NSPLIT == 3 && (e = make_map(&maps.a_lo[a], a_lo[a], M, K, K, kBM)) != cudaSuccess) return e;
+  }
+  if ((e = make_map(&maps.b_hi, b_hi, N, K, K, BN)) != cudaSuccess) return e;
+  if (NSPLIT == 3 && (e = make_map(&maps.b_lo, b_lo, N, K, K, BN)) != cudaSuccess) return e;
+  dim3 grid((N + BN - 1) / BN, (M + kBM - 1) / kBM, 1);
+  return launch_umma<BN, NA, NSPLIT, STAGES>(maps, K, 0, 0, grid, EpiStoreF32<BN, NA>{c, M, N}, status, st);
+}
+
+}  // namespace umma
+}  // namespace ipie_b200
+
+using namespace ipie_b200;
+
+extern "C" int ipie_b200_split_tf32(const double* x, float* hi, float* lo, long long n, void* stream) {
+  return (int)umma::launch_split_tf32(x, hi, lo, n, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ipie_b200_umma_gemm_test(const float* a0_hi, const float* a0_lo, const float* a1_hi,
+                                        const float* a1_lo, const float* b_hi, const float* b_lo, float* c, int M,
+                                        int N, int K, int na, int nsplit, unsigned int* status, void* stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (K % 4 || M <= 0 || N <= 0 || K <= 0) return (int)cudaErrorInvalidValue;
+  const float* ah[2] = {a0_hi, a1_hi};
+  const float* al[2] = {a0_lo, a1_lo};
+  if (na == 1 && nsplit == 1) return (int)umma::gemm_test<1, 1, 4>(ah, al, b_hi, b_lo, c, M, N, K, status, st);
+  if (na == 1 && nsplit == 3) return (int)umma::gemm_test<1, 3, 3>(ah, al, b_hi, b_lo, c, M, N, K, status, st);
+  if (na == 2 && nsplit == 3) return (int)umma::gemm_test<2, 3, 2>(ah, al, b_hi, b_lo, c, M, N, K, status, st);
+  return (int)cudaErrorInvalidValue;
+}
+
+// ============================================================================
+// Mixed-precision walker-step stages
+// ============================================================================
+namespace ipie_b200 {
+namespace umma {
+
+__device__ __forceinline__ void store_split(float* hi, float* lo, size_t i, float x) {
+  float h, l;
+  split_tf32(x, h, l);
+  hi[i] = h;
+  lo[i] = l;
+}
+
+// Force bias: rows x of rchol (X, K) fp32, B rows (w, c) of the planar Green's
+// function (W, 2, K) fp32 -> vbias[w][x] (complex double), scaled, optionally accumulated.
+template <int BN>
+struct EpiVbiasF {
+  double2* vbias;
+  int X, W;
+  double scale;
+  int accumulate;
+  __device__ __forceinline__ void operator()(int, int x, int n0, const float* v, uint8_t*) const {
+    if (x >= X) return;
+#pragma unroll
+    for (int q = 0; q < BN / 2; ++q) {
+      const int w = (n0 >> 1) + q;
+      if (w < W) {
+        const size_t i = (size_t)w * X + x;
+        double2 r = make_double2(scale * (double)v[2 * q], scale * (double)v[2 * q + 1]);
+        if (accumulate) r = cadd(r, vbias[i]);
+        vbias[i] = r;
+      }
+    }
+  }
+};
+
+// VHS: rows p of the packed Cholesky (P, X) hi/lo, B rows (w, c) of the shifted
+// fields (W, 2, X) hi/lo.  V = i sqrt(dt) (S_re + i S_im) is written to both
+// triangles of four planar (W, M, M) fp32 arrays: re/im x hi/lo (the left
+// operands of the exp(VHS) products).
+template <int BN>
+struct EpiVHSSplit {
+  float *re_hi, *re_lo, *im_hi, *im_lo;
+  const int* ii;
+  const int* jj;
+  int P, M, W;
+  float sdt;
+  __device__ __forceinline__ void operator()(int, int p, int n0, const float* v, uint8_t*) const {
+    if (p >= P) return;
+    const int i = ii[p], j = jj[p];
+#pragma unroll
+    for (int q = 0; q < BN / 2; ++q) {
+      const int w = (n0 >> 1) + q;
+      if (w < W) {
+        const float vre = -sdt * v[2 * q + 1], vim = sdt * v[2 * q];
+        const size_t a = ((size_t)w * M + i) * M + j, b = ((size_t)w * M + j) * M + i;
+        store_split(re_hi, re_lo, a, vre);
+        store_split(im_hi, im_lo, a, vim);
+        if (i != j) {
+          store_split(re_hi, re_lo, b, vre);
+          store_split(im_hi, im_lo, b, vim);
+        }
+      }
+    }
+  }
+};
+
+// One Taylor term / one-body factor on the orbitals of walker z (one spin):
+// accumulators (columns c*N + n, c = re/im of the right operand):
+//   one-body (NA = 1):  U = E . T
+//   Taylor   (NA = 2):  U = (V_re T_re - V_im T_im) + i (V_re T_im + V_im T_re)
+// then per mode
+//   PRE   : phi_acc = U;                 next B = U
+//   TERM  : T = U / n; phi_acc += T;     next B = T           (next B = phi_acc when last)
+//   POST  : phi_out = U
+enum OrbMode { ORB_PRE = 0, ORB_TERM = 1, ORB_TERM_LAST = 2, ORB_POST = 3 };
+
+template <int NA, int BN>
+struct EpiOrbital {
+  double2* phi_acc;   // (W, M, N) complex double
+  float* nb_hi;       // next right operand (W, 2N, M) fp32 hi/lo
+  float* nb_lo;
+  int M, N;
+  float inv_n;
+  int mode;
+  __device__ __forceinline__ void operator()(int w, int m, int, const float* v, uint8_t*) const {
+    if (m >= M) return;
+    for (int n = 0; n < N; ++n) {
+      float ur, ui;
+      if (NA == 2) {
+        ur = v[n] - v[BN + N + n];
+        ui = v[N + n] + v[BN + n];
+      } else {
+        ur = v[n];
+        ui = v[N + n];
+      }
+      const size_t pi = ((size_t)w * M + m) * N + n;
+      const size_t bre = ((size_t)w * 2 * N + n) * M + m, bim = ((size_t)w * 2 * N + N + n) * M + m;
+      if (mode == ORB_PRE) {
+        phi_acc[pi] = make_double2(ur, ui);
+        store_split(nb_hi, nb_lo, bre, ur);
+        store_split(nb_hi, nb_lo, bim, ui);
+      } else if (mode == ORB_POST) {
+        phi_acc[pi] = make_double2(ur, ui);
+      } else {
+        const float tr = ur * inv_n, ti = ui * inv_n;
+        double2 acc = phi_acc[pi];
+        acc.x += tr;
+        acc.y += ti;
+        phi_acc[pi] = acc;
+        if (mode == ORB_TERM) {
+          store_split(nb_hi, nb_lo, bre, tr);
+          store_split(nb_hi, nb_lo, bim, ti);
+        } else {
+          store_split(nb_hi, nb_lo, bre, (float)acc.x);
+          store_split(nb_hi, nb_lo, bim, (float)acc.y);
+        }
+      }
+    }
+  }
+};
+
+// phi (W, M, N) complex double -> planar right operand (W, 2N, M) fp32 hi/lo.
+__global__ void phi_to_planar_kernel(const double2* __restrict__ phi, int W, int M, int N, float* __restrict__ hi,
+                                     float* __restrict__ lo) {
+  const long long total = (long long)W * M * N;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    // e enumerates the output order (w, c-less n, m) so stores are coalesced
+    const int m = (int)(e % M);
+    const long long t = e / M;
+    const int n = (int)(t % N);
+    const int w = (int)(t / N);
+    const double2 z = phi[((size_t)w * M + m) * N + n];
+    store_split(hi, lo, ((size_t)w * 2 * N + n) * M + m, (float)z.x);
+    store_split(hi, lo, ((size_t)w * 2 * N + N + n) * M + m, (float)z.y);
+  }
+}
+
+// Ghalf (W, N*M) complex double -> planar (W, 2, N*M) fp32 (TF32-rounded).
+__global__ void ghalf_to_planar_kernel(const double2* __restrict__ g, long long W, long long K, float* __restrict__ out) {
+  const long long total = W * K;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const long long w = e / K, k = e % K;
+    const double2 z = g[e];
+    out[(w * 2) * K + k] = (float)z.x;
+    out[(w * 2 + 1) * K + k] = (float)z.y;
+  }
+}
+
+static unsigned grid_for(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 32) b = 148 * 32;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+// Exchange in 3-pass TF32: rows (x, i) of the padded half-rotated Cholesky
+// (X*NP, M), columns (w, c, j) of the padded planar Green's function
+// (W*2*NP, M); the epilogue parks the 128 x BN tile in shared memory and forms
+// sum_{i,j<N} T_ij T_ji per (x, w) block in FP64, one partial per (x tile, w).
+template <int NP, int BN>
+struct EpiExchange {
+  double2* part;
+  int X, W, N;
+  __device__ __forceinline__ void operator()(int, int, int n0, const float* v, uint8_t* smem) const {
+    constexpr int LD = BN + 1;
+    constexpr int XB = kBM / NP, WB = BN / (2 * NP);
+    float* sC = reinterpret_cast<float*>(smem);
+    double2* wpart = reinterpret_cast<double2*>(smem + ((kBM * LD * 4 + 15) / 16) * 16);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+#pragma unroll
+    for (int j = 0; j < BN; ++j) sC[tid * LD + j] = v[j];
+    __syncthreads();
+    for (int blk = warp; blk < XB * WB; blk += 4) {
+      const int xl = blk / WB, wl = blk % WB;
+      double2 s = make_double2(0.0, 0.0);
+      const bool valid = (blockIdx.y * XB + xl) < X && ((n0 / (2 * NP)) + wl) < W;
+      if (valid) {
+        const float* rows = sC + (xl * NP) * LD + wl * 2 * NP;
+        for (int e = lane; e < N * N; e += 32) {
+          const int i = e / N, j = e % N;
+          const double ar = rows[i * LD + j], ai = rows[i * LD + NP + j];
+          const double br = rows[j * LD + i], bi = rows[j * LD + NP + i];
+          s.x += ar * br - ai * bi;
+          s.y += ar * bi + ai * br;
+        }
+      }
+      s = warp_sum2(s);
+      if (lane == 0) wpart[blk] = s;
+    }
+    __syncthreads();
+    if (tid < WB) {
+      const int w = n0 / (2 * NP) + tid;
+      if (w < W) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int xl = 0; xl < XB; ++xl) s = cadd(s, wpart[xl * WB + tid]);
+        part[(size_t)blockIdx.y * W + w] = s;
+      }
+    }
+  }
+};
+
+// rchol (X, N*M) double -> rows (x, i) padded to NP: (X*NP, M) fp32 hi/lo, zero rows for i >= N.
+__global__ void rchol_pad_split_kernel(const double* __restrict__ r, int X, int N, int M, int NP, float* __restrict__ hi,
+                                       float* __restrict__ lo) {
+  const long long total = (long long)X * NP * M;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(e % M);
+    const long long t = e / M;
+    const int i = (int)(t % NP);
+    const long long x = t / NP;
+    const double val = i < N ? r[(x * N + i) * M + m] : 0.0;
+    uint32_t h;
+    const float f = (float)val;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(f));
+    hi[e] = __uint_as_float(h);
+    lo[e] = (float)(val - (double)__uint_as_float(h));
+  }
+}
+
+// Ghalf (W, N, M) complex double -> planar padded (W, 2, NP, M) fp32 hi/lo, zero rows j >= N.
+__global__ void ghalf_pad_split_kernel(const double2* __restrict__ g, int W, int N, int M, int NP, float* __restrict__ hi,
+                                       float* __restrict__ lo) {
+  const long long total = (long long)W * 2 * NP * M;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(e % M);
+    long long t = e / M;
+    const int j = (int)(t % NP);
+    t /= NP;
+    const int c = (int)(t % 2);
+    const long long w = t / 2;
+    double val = 0.0;
+    if (j < N) {
+      const double2 z = g[(w * N + j) * M + m];
+      val = c ? z.y : z.x;
+    }
+    uint32_t h;
+    const float f = (float)val;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(f));
+    hi[e] = __uint_as_float(h);
+    lo[e] = (float)(val - (double)__uint_as_float(h));
+  }
+}
+
+int exchange_np(int N) { return N <= 8 ? 8 : N <= 16 ? 16 : N <= 32 ? 32 : -1; }
+
+cudaError_t mixed_rchol_pad(const double* rchol, int X, int N, int M, float* hi, float* lo, cudaStream_t st) {
+  const int NP = exchange_np(N);
+  if (NP < 0) return cudaErrorInvalidValue;
+  rchol_pad_split_kernel<<<grid_for((long long)X * NP * M), 256, 0, st>>>(rchol, X, N, M, NP, hi, lo);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// Padded planar Green's function (TF32 head/remainder) of one spin block.
+static cudaError_t pad_ghalf(const double2* ghalf, int W, int M, int N, int NP, float* g_hi, float* g_lo,
+                             cudaStream_t st) {
+  ghalf_pad_split_kernel<<<grid_for((long long)W * 2 * NP * M), 256, 0, st>>>(ghalf, W, N, M, NP, g_hi, g_lo);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// X[w][x] (scale, accumulate as the force bias) = sum_k rchol[x][k] Ghalf[w][k] as a 3-pass TF32
+// product of the padded operands (rows (x) of (X, NP*M), rows (w, c) of (2W, NP*M)).
+static cudaError_t coulomb3(const float* r_hi, const float* r_lo, const float* g_hi, const float* g_lo, int W, int X,
+                            int M, int NP, double2* xv, int accumulate, double scale, unsigned* status,
+                            cudaStream_t st) {
+  constexpr int BN = 128;
+  const long long K = (long long)NP * M;
+  if (K % 4) return cudaErrorInvalidValue;
+  GemmMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  cudaError_t e;
+  if ((e = make_map(&maps.a_hi[0], r_hi, X, K, K, kBM)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.a_lo[0], r_lo, X, K, K, kBM)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.b_hi, g_hi, 2LL * W, K, K, BN)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.b_lo, g_lo, 2LL * W, K, K, BN)) != cudaSuccess) return e;
+  dim3 grid((2 * W + BN - 1) / BN, (X + kBM - 1) / kBM, 1);
+  return launch_umma<BN, 1, 3, 3>(maps, (int)K, 0, 0, grid, EpiVbiasF<BN>{xv, X, W, scale, accumulate}, status, st);
+}
+
+// Exchange partials of one spin block as a 3-pass TF32 product: (X*NP, M) x (W*2*NP, M)^T.
+template <int NP>
+static cudaError_t exchange3_np(const float* r_hi, const float* r_lo, const float* g_hi, const float* g_lo, int W,
+                                int X, int M, int N, double2* part, unsigned* status, cudaStream_t st) {
+  constexpr int BN = 128;
+  GemmMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  cudaError_t e;
+  if ((e = make_map(&maps.a_hi[0], r_hi, (long long)X * NP, M, M, kBM)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.a_lo[0], r_lo, (long long)X * NP, M, M, kBM)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.b_hi, g_hi, (long long)W * 2 * NP, M, M, BN)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.b_lo, g_lo, (long long)W * 2 * NP, M, M, BN)) != cudaSuccess) return e;
+  dim3 grid((W * 2 * NP + BN - 1) / BN, (X * NP + kBM - 1) / kBM, 1);
+  return launch_umma<BN, 1, 3, 3>(maps, M, 0, 0, grid, EpiExchange<NP, BN>{part, X, W, N}, status, st);
+}
+
+static cudaError_t exchange3(const float* r_hi, const float* r_lo, const float* g_hi, const float* g_lo, int W, int X,
+                             int M, int N, double2* part, unsigned* status, cudaStream_t st) {
+  switch (exchange_np(N)) {
+    case 8: return exchange3_np<8>(r_hi, r_lo, g_hi, g_lo, W, X, M, N, part, status, st);
+    case 16: return exchange3_np<16>(r_hi, r_lo, g_hi, g_lo, W, X, M, N, part, status, st);
+    case 32: return exchange3_np<32>(r_hi, r_lo, g_hi, g_lo, W, X, M, N, part, status, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int exchange3_rows(int X, int N) { return (X * exchange_np(N) + kBM - 1) / kBM; }
+
+cudaError_t mixed_vhs(const float* cp_hi, const float* cp_lo, const int* ii, const int* jj, int P, int X, int M,
+                      const float* xs_hi, const float* xs_lo, int W, double sqrt_dt, float* re_hi, float* re_lo,
+                      float* im_hi, float* im_lo, unsigned* status, cudaStream_t st) {
+  constexpr int BN = 128;
+  GemmMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  cudaError_t e;
+  if ((e = make_map(&maps.a_hi[0], cp_hi, P, X, X, kBM)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.a_lo[0], cp_lo, P, X, X, kBM)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.b_hi, xs_hi, 2LL * W, X, X, BN)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.b_lo, xs_lo, 2LL * W, X, X, BN)) != cudaSuccess) return e;
+  dim3 grid((2 * W + BN - 1) / BN, (P + kBM - 1) / kBM, 1);
+  EpiVHSSplit<BN> epi{re_hi, re_lo, im_hi, im_lo, ii, jj, P, M, W, (float)sqrt_dt};
+  return launch_umma<BN, 1, 3, 3>(maps, X, 0, 0, grid, epi, status, st);
+}
+
+// Orbital update of one spin block: phi_out = E exp(V) E phi_in (Taylor order nmax),
+// every product on the tensor cores as 3-pass TF32; phi accumulates in FP64.
+// E: expH1 hi/lo (M, Mp) fp32 with Mp % 4 == 0; V: planar (W, M, M) hi/lo;
+// b0/b1: two (W, 2N, M) fp32 hi/lo ping-pong buffers (4 arrays).
+cudaError_t mixed_orbitals(const float* e_hi, const float* e_lo, int Mp, const float* v_re_hi, const float* v_re_lo,
+                           const float* v_im_hi, const float* v_im_lo, const double2* phi_in, double2* phi_out,
+                           float* b0_hi, float* b0_lo, float* b1_hi, float* b1_lo, int W, int M, int N, int nmax,
+                           unsigned* status, cudaStream_t st) {
+  constexpr int BN = 64;
+  if (2 * N > BN || M % 4) return cudaErrorInvalidValue;
+  phi_to_planar_kernel<<<grid_for((long long)W * M * N), 256, 0, st>>>(phi_in, W, M, N, b0_hi, b0_lo);
+  note_launch();
+  float* bh[2] = {b0_hi, b1_hi};
+  float* bl[2] = {b0_lo, b1_lo};
+  int cur = 0;
+  cudaError_t e;
+  const dim3 grid(1, (M + kBM - 1) / kBM, W);
+  const int brows = 2 * N;
+  // one-body (pre, post): A = E shared by all walkers (rows per batch 0)
+  auto one_body = [&](int mode) -> cudaError_t {
+    GemmMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    cudaError_t r;
+    if ((r = make_map(&maps.a_hi[0], e_hi, M, M, Mp, kBM)) != cudaSuccess) return r;
+    if ((r = make_map(&maps.a_lo[0], e_lo, M, M, Mp, kBM)) != cudaSuccess) return r;
+    if ((r = make_map(&maps.b_hi, bh[cur], (long long)W * brows, M, M, BN)) != cudaSuccess) return r;
+    if ((r = make_map(&maps.b_lo, bl[cur], (long long)W * brows, M, M, BN)) != cudaSuccess) return r;
+    EpiOrbital<1, BN> epi{phi_out, bh[cur ^ 1], bl[cur ^ 1], M, N, 1.0f, mode};
+    r = launch_umma<BN, 1, 3, 3>(maps, M, 0, brows, grid, epi, status, st);
+    cur ^= 1;
+    return r;
+  };
+  if ((e = one_body(ORB_PRE)) != cudaSuccess) return e;
+  for (int n = 1; n <= nmax; ++n) {
+    GemmMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    if ((e = make_map(&maps.a_hi[0], v_re_hi, (long long)W * M, M, M, kBM)) != cudaSuccess) return e;
+    if ((e = make_map(&maps.a_lo[0], v_re_lo, (long long)W * M, M, M, kBM)) != cudaSuccess) return e;
+    if ((e = make_map(&maps.a_hi[1], v_im_hi, (long long)W * M, M, M, kBM)) != cudaSuccess) return e;
+    if ((e = make_map(&maps.a_lo[1], v_im_lo, (long long)W * M, M, M, kBM)) != cudaSuccess) return e;
+    if ((e = make_map(&maps.b_hi, bh[cur], (long long)W * brows, M, M, BN)) != cudaSuccess) return e;
+    if ((e = make_map(&maps.b_lo, bl[cur], (long long)W * brows, M, M, BN)) != cudaSuccess) return e;
+    EpiOrbital<2, BN> epi{phi_out, bh[cur ^ 1], bl[cur ^ 1], M, N, 1.0f / n, n == nmax ? ORB_TERM_LAST : ORB_TERM};
+    if ((e = launch_umma<BN, 2, 3, 2>(maps, M, M, brows, grid, epi, status, st)) != cudaSuccess) return e;
+    cur ^= 1;
+  }
+  return one_body(ORB_POST);
+}
+
+}  // namespace umma
+}  // namespace ipie_b200
+
+extern "C" int ipie_b200_construct_force_bias_mixed(const float* ra_hi, const float* ra_lo, const float* rb_hi,
+                                                    const float* rb_lo, const void* ghalfa, const void* ghalfb,
+                                                    float* gwork, int W, int X, int M, int na, int nb, void* vbias,
+                                                    unsigned int* status, void* stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const bool alias = nb == na && nb > 0 && rb_hi == ra_hi && ghalfb == ghalfa;
+  const int NPa = umma::exchange_np(na), NPb = nb > 0 ? umma::exchange_np(nb) : 8;
+  if (NPa < 0 || NPb < 0 || M % 4) return (int)cudaErrorInvalidValue;
+  float* g_hi = gwork;
+  float* g_lo = gwork + (size_t)W * 2 * 32 * M;
+  double2* v = reinterpret_cast<double2*>(vbias);
+  cudaError_t e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfa), W, M, na, NPa, g_hi, g_lo, st);
+  if (e == cudaSuccess) e = umma::coulomb3(ra_hi, ra_lo, g_hi, g_lo, W, X, M, NPa, v, 0, alias ? 2.0 : 1.0, status, st);
+  if (e != cudaSuccess || nb == 0 || alias) return (int)e;
+  e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfb), W, M, nb, NPb, g_hi, g_lo, st);
+  if (e == cudaSuccess) e = umma::coulomb3(rb_hi, rb_lo, g_hi, g_lo, W, X, M, NPb, v, 1, 1.0, status, st);
+  return (int)e;
+}
+
+extern "C" int ipie_b200_field_shift_mixed(const void* vbias, const double* xi, const void* mf_shift, int W, int X,
+                                           double sqrt_dt, double bound, void* xshifted, float* xs_hi, float* xs_lo,
+                                           void* cmf, void* cfb, void* stream) {
+  return (int)launch_field_shift(reinterpret_cast<const double2*>(vbias), xi, reinterpret_cast<const double2*>(mf_shift),
+                                 W, X, sqrt_dt, bound, reinterpret_cast<double2*>(xshifted),
+                                 reinterpret_cast<double2*>(cmf), reinterpret_cast<double2*>(cfb),
+                                 reinterpret_cast<cudaStream_t>(stream), xs_hi, xs_lo);
+}
+
+extern "C" int ipie_b200_construct_vhs_mixed(const float* cp_hi, const float* cp_lo, const int* idx_i,
+                                             const int* idx_j, int M, int X, const float* xs_hi, const float* xs_lo,
+                                             int W, double sqrt_dt, float* v_re_hi, float* v_re_lo, float* v_im_hi,
+                                             float* v_im_lo, unsigned int* status, void* stream) {
+  if (X % 4) return (int)cudaErrorInvalidValue;
+  return (int)umma::mixed_vhs(cp_hi, cp_lo, idx_i, idx_j, M * (M + 1) / 2, X, M, xs_hi, xs_lo, W, sqrt_dt, v_re_hi,
+                              v_re_lo, v_im_hi, v_im_lo, status, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float* e_lo, int lde, const float* v_re_hi,
+                                                  const float* v_re_lo, const float* v_im_hi, const float* v_im_lo,
+                                                  const void* phi_in, void* phi_out, float* work, int W, int M, int N,
+                                                  int nmax, unsigned int* status, void* stream) {
+  if (phi_in == phi_out || lde % 4 || lde < M) return (int)cudaErrorInvalidValue;
+  const size_t plane = (size_t)W * 2 * N * M;
+  return (int)umma::mixed_orbitals(e_hi, e_lo, lde, v_re_hi, v_re_lo, v_im_hi, v_im_lo,
+                                   reinterpret_cast<const double2*>(phi_in), reinterpret_cast<double2*>(phi_out), work,
+                                   work + plane, work + 2 * plane, work + 3 * plane, W, M, N, nmax, status,
+                                   reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, float* hi, float* lo, void* stream) {
+  return (int)umma::mixed_rchol_pad(rchol, X, N, M, hi, lo, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const float* ra_hi,
+                                            const float* ra_lo, const float* rb_hi, const float* rb_lo,
+                                            const void* rH1a, const void* rH1b, double ecore, const void* ghalfa,
+                                            const void* ghalfb, int W, int X, int M, int na, int nb, float* gwork,
+                                            void* work, void* energy, unsigned int* status, void* stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const bool alias = !rhf && nb == na && nb > 0 && rb_hi == ra_hi && ghalfb == ghalfa;
+  const int use_b = (!rhf && nb > 0 && !alias);
+  double2* xv = reinterpret_cast<double2*>(work);
+  double2* part = xv + (size_t)W * X;
+  const int NPa = umma::exchange_np(na), NPb = nb > 0 ? umma::exchange_np(nb) : 8;
+  if (NPa < 0 || NPb < 0 || M % 4) return (int)cudaErrorInvalidValue;
+  float* g_hi = gwork;
+  float* g_lo = gwork + (size_t)W * 2 * 32 * M;
+  // Coulomb vector in FP64 (DMMA): the Coulomb energy is the large, cancellation-free term
+  cudaError_t e = launch_force_bias(rchola, reinterpret_cast<const double2*>(ghalfa), W, X, na * M, xv, 0, st,
+                                    alias ? 2.0 : 1.0);
+  if (e == cudaSuccess && use_b)
+    e = launch_force_bias(rcholb, reinterpret_cast<const double2*>(ghalfb), W, X, nb * M, xv, 1, st);
+  if (e != cudaSuccess) return (int)e;
+  // exchange: 3-pass TF32 tensor-core products, bilinear sums in FP64
+  e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfa), W, M, na, NPa, g_hi, g_lo, st);
+  if (e == cudaSuccess) e = umma::exchange3(ra_hi, ra_lo, g_hi, g_lo, W, X, M, na, part, status, st);
+  if (e != cudaSuccess) return (int)e;
+  const int rows_a = umma::exchange3_rows(X, na);
+  int rows_b = 0;
+  if (use_b) {
+    rows_b = umma::exchange3_rows(X, nb);
+    e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfb), W, M, nb, NPb, g_hi, g_lo, st);
+    if (e == cudaSuccess)
+      e = umma::exchange3(rb_hi, rb_lo, g_hi, g_lo, W, X, M, nb, part + (size_t)rows_a * W, status, st);
+    if (e != cudaSuccess) return (int)e;
+  }
+  const double f1 = rhf ? 2.0 : 1.0, fc = rhf ? 2.0 : 0.5, fx = (rhf || alias) ? 1.0 : 0.5;
+  const bool e1_b = !rhf && nb > 0;
+  return (int)launch_energy_combine(W, X, na * M, nb * M, reinterpret_cast<const double2*>(ghalfa),
+                                    e1_b ? reinterpret_cast<const double2*>(ghalfb) : nullptr,
+                                    reinterpret_cast<const double2*>(rH1a), reinterpret_cast<const double2*>(rH1b),
+                                    ecore, xv, part, rows_a + rows_b, f1, fc, fx, reinterpret_cast<double2*>(energy),
+                                    status, st);
+}

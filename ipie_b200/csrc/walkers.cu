@@ -122,8 +122,9 @@ __device__ SpinLU overlap_lu(const double2* __restrict__ psic, int M, int N, dou
 }
 
 // Ghalf = O^{-1} phi^T from the LU in sO; thread m solves for column m.
+// ghalf2 (may be null) receives a second copy (spin-aliased walkers).
 __device__ void solve_ghalf(int M, int N, double2* sY, const double2* sO, const int* sPiv, const double2* sInvDiag,
-                            double2* __restrict__ ghalf) {
+                            double2* __restrict__ ghalf, double2* __restrict__ ghalf2) {
   const int NP = pad_n(N);
   for (int m = threadIdx.x; m < M; m += blockDim.x) {
     double2* y = sY + m * NP;
@@ -146,6 +147,8 @@ __device__ void solve_ghalf(int M, int N, double2* sY, const double2* sO, const 
       y[i] = cmul(s, sInvDiag[i]);
     }
     for (int i = 0; i < N; ++i) ghalf[(size_t)i * M + m] = y[i];
+    if (ghalf2 != nullptr)
+      for (int i = 0; i < N; ++i) ghalf2[(size_t)i * M + m] = y[i];
   }
 }
 
@@ -165,11 +168,20 @@ __global__ void __launch_bounds__(256) gf_overlap_kernel(const double2* __restri
   double2* sInvDiag = sPsi + 32 * Nmax;
   double2* red = sInvDiag + Nmax;
   int* sPiv = reinterpret_cast<int*>(red + 64);
+  // Spin aliasing: phib == phia (with nb == na) means the beta block is an exact
+  // copy of the alpha block; it is factored once and counted twice.
+  const bool alias = (phib == phia) && (nb == na);
   double logsum = 0.0;
   double2 phase = make_double2(1.0, 0.0);
   for (int s = 0; s < 2; ++s) {
     const int N = s == 0 ? na : nb;
     if (N == 0) continue;
+    if (s == 1 && alias) {
+      logsum += red[2].x;
+      phase = cmul(phase, red[3]);
+      if (logdet != nullptr && threadIdx.x == 0) logdet[(size_t)w * 2 + 1] = logdet[(size_t)w * 2];
+      continue;
+    }
     const double2* phi = (s == 0 ? phia : phib) + (size_t)w * M * N;
     const int np = pad_n(N);
     __syncthreads();
@@ -178,9 +190,15 @@ __global__ void __launch_bounds__(256) gf_overlap_kernel(const double2* __restri
     SpinLU lu = overlap_lu(s == 0 ? psia_c : psib_c, M, N, sY, sO, sPsi, sPiv, sInvDiag, red, status);
     logsum += lu.logabs;
     phase = cmul(phase, lu.phase);
+    if (threadIdx.x == 0) {
+      red[2] = make_double2(lu.logabs, 0.0);
+      red[3] = lu.phase;
+    }
     if (logdet != nullptr && threadIdx.x == 0) logdet[(size_t)w * 2 + s] = make_double2(lu.logabs, atan2(lu.phase.y, lu.phase.x));
     if (WITH_GHALF) {
-      solve_ghalf(M, N, sY, sO, sPiv, sInvDiag, (s == 0 ? ghalfa : ghalfb) + (size_t)w * N * M);
+      double2* g1 = (s == 0 ? ghalfa : ghalfb) + (size_t)w * N * M;
+      double2* g2 = (s == 0 && alias && nb > 0 && ghalfb != ghalfa) ? ghalfb + (size_t)w * N * M : nullptr;
+      solve_ghalf(M, N, sY, sO, sPiv, sInvDiag, g1, g2);
     }
   }
   if (threadIdx.x == 0) {
@@ -217,10 +235,22 @@ cudaError_t launch_gf_overlap(const double2* phia, const double2* phib, int W, i
 //   xs = xi - xbar;  cmf = -sqrt(dt) sum_x xs mf;  cfb = sum_x xi xbar - xbar^2/2
 // One CTA per 32 walkers; the (X, W) transposed store goes through smem.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void split_store_tf32(float* hi, float* lo, size_t i, double x) {
+  uint32_t h;
+  const float f = (float)x;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(f));
+  const float hf = __uint_as_float(h);
+  hi[i] = hf;
+  lo[i] = (float)(x - (double)hf);
+}
+
+// xs_hi/xs_lo (optional): the shifted fields as planar (W, 2, X) fp32 TF32 head/remainder,
+// the right operand of the mixed-precision VHS product.
 __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restrict__ vbias, const double* __restrict__ xi,
                                                           const double2* __restrict__ mf, int W, int X, double sqrt_dt,
                                                           double bound, double2* __restrict__ xshifted,
-                                                          double2* __restrict__ cmf, double2* __restrict__ cfb) {
+                                                          double2* __restrict__ cmf, double2* __restrict__ cfb,
+                                                          float* __restrict__ xs_hi, float* __restrict__ xs_lo) {
   __shared__ double2 tile[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int w0 = blockIdx.x * 32;
@@ -241,6 +271,10 @@ __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restr
         if (a > bound && a > 1e-13) xb = make_double2(xb.x / a, xb.y / a);
         const double r = xi[(size_t)w * X + x];
         xs = make_double2(r - xb.x, -xb.y);
+        if (xs_hi != nullptr) {
+          split_store_tf32(xs_hi, xs_lo, ((size_t)w * 2) * X + x, xs.x);
+          split_store_tf32(xs_hi, xs_lo, ((size_t)w * 2 + 1) * X + x, xs.y);
+        }
         acc_mf[q] = cadd(acc_mf[q], cmul(xs, m));
         double2 xb2 = cmul(xb, xb);
         acc_fb[q] = cadd(acc_fb[q], make_double2(r * xb.x - 0.5 * xb2.x, r * xb.y - 0.5 * xb2.y));
@@ -249,10 +283,11 @@ __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restr
     }
     __syncthreads();
     // transposed store: row x, 32 consecutive walkers
-    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
-      const int xl = e / 32, wl = e % 32;
-      if (x0 + xl < X && w0 + wl < W) xshifted[(size_t)(x0 + xl) * W + w0 + wl] = tile[xl][wl];
-    }
+    if (xshifted != nullptr)
+      for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
+        const int xl = e / 32, wl = e % 32;
+        if (x0 + xl < X && w0 + wl < W) xshifted[(size_t)(x0 + xl) * W + w0 + wl] = tile[xl][wl];
+      }
     __syncthreads();
   }
 #pragma unroll
@@ -267,8 +302,10 @@ __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restr
 }
 
 cudaError_t launch_field_shift(const double2* vbias, const double* xi, const double2* mf, int W, int X, double sqrt_dt,
-                               double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st) {
-  field_shift_kernel<<<(W + 31) / 32, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, xshifted, cmf, cfb);
+                               double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st,
+                               float* xs_hi, float* xs_lo) {
+  field_shift_kernel<<<(W + 31) / 32, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, xshifted, cmf, cfb, xs_hi,
+                                                    xs_lo);
   note_launch();
   return cudaGetLastError();
 }
@@ -366,16 +403,23 @@ __global__ void __launch_bounds__(256) reortho_kernel(double2* __restrict__ phia
   const int w = blockIdx.x;
   double2* red = sm;
   double2* sY = sm + 64;
-  double logsum = 0.0;
+  const bool alias = (phib == phia) && (nb == na);  // beta block is the alpha block: orthogonalise once
+  double logsum = 0.0, log_a = 0.0;
   for (int s = 0; s < 2; ++s) {
     const int N = s == 0 ? na : nb;
     if (N == 0) continue;
+    if (s == 1 && alias) {
+      logsum += log_a;
+      continue;
+    }
     double2* phi = (s == 0 ? phia : phib) + (size_t)w * M * N;
     const int np = pad_n(N);
     __syncthreads();
     for (int e = threadIdx.x; e < M * N; e += blockDim.x) sY[(e / N) * np + e % N] = phi[e];
     __syncthreads();
-    logsum += mgs_block(sY, M, N, red, status);
+    const double l = mgs_block(sY, M, N, red, status);
+    logsum += l;
+    if (s == 0) log_a = l;
     for (int e = threadIdx.x; e < M * N; e += blockDim.x) phi[e] = sY[(e / N) * np + e % N];
   }
   if (threadIdx.x == 0) {
@@ -409,7 +453,8 @@ __global__ void walker_copy_kernel(const int* __restrict__ src, int W, int M, in
   if (s < 0 || s == dst) return;
   const size_t sa = (size_t)M * na, sb = (size_t)M * nb;
   for (size_t e = threadIdx.x; e < sa; e += blockDim.x) phia[dst * sa + e] = phia[s * sa + e];
-  for (size_t e = threadIdx.x; e < sb; e += blockDim.x) phib[dst * sb + e] = phib[s * sb + e];
+  if (phib != phia)
+    for (size_t e = threadIdx.x; e < sb; e += blockDim.x) phib[dst * sb + e] = phib[s * sb + e];
   if (threadIdx.x == 0) {
     weight[dst] = weight[s];
     unscaled_weight[dst] = unscaled_weight[s];

@@ -42,6 +42,48 @@ def _local_energy(hamiltonian, walkers, trial, rhf):
     return energy
 
 
+def _mixed_energy_operands(trial, hamiltonian):
+    """Padded TF32 head/remainder copies of the half-rotated Cholesky (built once per trial)."""
+    if getattr(trial, "_rpad", None) is not None:
+        return trial._rpad
+    X, M = hamiltonian.nchol, hamiltonian.nbasis
+    out = []
+    for r, n in ((trial._rchola, trial.nalpha), (trial._rcholb, trial.nbeta)):
+        if out and r is trial._rchola:
+            out.append(out[0])
+            continue
+        NP = 8 if n <= 8 else 16 if n <= 16 else 32
+        hi = torch.empty(X * NP * M, dtype=torch.float32, device=trial.device)
+        lo = torch.empty_like(hi)
+        if n > 0:
+            call("ipie_b200_rchol_pad_split", ptr(r), X, n, M, ptr(hi), ptr(lo), stream())
+        out.append((hi, lo))
+    trial._rpad = out
+    return out
+
+
+def local_energy_mixed(system, hamiltonian, walkers, trial, rhf=False):
+    """Mixed-precision local energy: Coulomb and exchange as 3-pass TF32 tensor-core products."""
+    W, X, M = walkers.nwalkers, hamiltonian.nchol, hamiltonian.nbasis
+    (ra_hi, ra_lo), (rb_hi, rb_lo) = _mixed_energy_operands(trial, hamiltonian)
+    rows = 0
+    for n in (walkers.nup, walkers.ndown):
+        NP = 8 if n <= 8 else 16 if n <= 16 else 32
+        rows += (X * NP + 127) // 128
+    need = W * X + rows * W
+    buf = getattr(walkers, "_energy_work_mixed", None)
+    if buf is None or buf.numel() < need:
+        buf = torch.empty(need, dtype=C128, device=walkers.device)
+        walkers._energy_work_mixed = buf
+        walkers._energy_gwork = torch.empty(2 * W * 2 * 32 * M, dtype=torch.float32, device=walkers.device)
+    energy = torch.empty(W, 3, dtype=C128, device=walkers.device)
+    call("ipie_b200_local_energy_mixed", int(rhf), ptr(trial._rchola), ptr(trial._rcholb), ptr(ra_hi), ptr(ra_lo),
+         ptr(rb_hi), ptr(rb_lo), ptr(trial._rH1a),
+         ptr(trial._rH1b), hamiltonian.ecore, ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), W, X, M, walkers.nup,
+         walkers.ndown, ptr(walkers._energy_gwork), ptr(buf), ptr(energy), ptr(walkers.status), stream())
+    return energy
+
+
 def local_energy_single_det_uhf_batch(system, hamiltonian, walkers, trial):
     """(W, 3) complex ``[e1b + e2b, e1b, e2b]`` (ipie ``local_energy_sd.py:358-403``)."""
     return _local_energy(hamiltonian, walkers, trial, rhf=False)
@@ -93,7 +135,8 @@ class EnergyEstimator:
 
     names = ["ENumer", "EDenom", "ETotal", "E1Body", "E2Body"]
 
-    def __init__(self, system=None, ham=None, trial=None, filename=None):
+    def __init__(self, system=None, ham=None, trial=None, filename=None, precision="fp64"):
+        self.precision = precision
         self._data = {k: 0.0j for k in self.names}
         self._sums = None
         self.print_to_stdout = True
@@ -101,7 +144,10 @@ class EnergyEstimator:
 
     def compute_estimator(self, system=None, walkers=None, hamiltonian=None, trial=None):
         trial.calc_greens_function(walkers)
-        energy = local_energy_batch(system, hamiltonian, walkers, trial)
+        if self.precision == "mixed":
+            energy = local_energy_mixed(system, hamiltonian, walkers, trial, rhf=walkers.rhf)
+        else:
+            energy = local_energy_batch(system, hamiltonian, walkers, trial)
         if self._sums is None:
             self._sums = torch.zeros(7, dtype=C128, device=walkers.device)
         call("ipie_b200_walker_sums", walkers.nwalkers, ptr(walkers.weight), None, None, ptr(energy), ptr(self._sums),

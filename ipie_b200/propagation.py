@@ -95,10 +95,21 @@ class Workspace:
         self.wbound = torch.full((1,), -1.0, dtype=F64, device=dev)
         self.xi_host = torch.empty(W, X, dtype=F64).pin_memory() if torch.cuda.is_available() else None
         self.xi_copied = torch.cuda.Event() if torch.cuda.is_available() else None
+        self.dev = dev
+
+    def add_mixed(self):
+        """fp32 buffers of the mixed form."""
+        W, M, X, N = self.W, self.M, self.X, max(self.na, self.nb)
+        f32, dev = torch.float32, self.dev
+        self.gwork = torch.empty(2 * W * 2 * 32 * M, dtype=f32, device=dev)
+        self.xs_hi = torch.empty(W, 2, X, dtype=f32, device=dev)
+        self.xs_lo = torch.empty(W, 2, X, dtype=f32, device=dev)
+        self.v_planar = [torch.empty(W, M, M, dtype=f32, device=dev) for _ in range(4)]  # re_hi, re_lo, im_hi, im_lo
+        self.orb_work = torch.empty(4 * W * 2 * N * M, dtype=f32, device=dev)
 
 
 class PhaselessGeneric:
-    def __init__(self, time_step, exp_nmax=6, verbose=False, rng="numpy", seed=7):
+    def __init__(self, time_step, exp_nmax=6, verbose=False, rng="numpy", seed=7, precision="fp64"):
         self.dt = time_step
         self.sqrt_dt = self.dt ** 0.5
         self.isqrt_dt = 1j * self.sqrt_dt
@@ -112,6 +123,12 @@ class PhaselessGeneric:
         self.vbias = None
         self.ws = None
         self.timer = _NoTimer()
+        self.fused = True  # one launch per spin for one-body + exp(VHS) + one-body
+        # "fp64": the plain form (ipie's arithmetic); "mixed": force bias in TF32, VHS and the
+        # orbital update as 3-pass TF32 tensor-core products, FP64 everywhere else
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
+        self.precision = precision
 
     # ------------------------------------------------------------------ set-up
     def build(self, hamiltonian, trial=None, walkers=None, mpi_handler=None, verbose=False):
@@ -124,6 +141,16 @@ class PhaselessGeneric:
         self.expH1_complex = bool(np.iscomplexobj(self.expH1) and np.abs(self.expH1.imag).max() > 0)
         e = self.expH1.astype(np.complex128) if self.expH1_complex else self.expH1.real.astype(np.float64)
         self.expH1_dev = torch.from_numpy(np.ascontiguousarray(e)).to(dev)
+        # rows padded to an even length (16-byte aligned) for the fused orbital kernel
+        M = hamiltonian.nbasis
+        self.lda_e = M + (M & 1)
+        if not self.expH1_complex:
+            ep = np.zeros((2, M, self.lda_e))
+            ep[:, :, :M] = self.expH1.real
+            self.expH1_pad = torch.from_numpy(ep).to(dev)
+        self.spin_symmetric = bool(np.array_equal(self.expH1[0], self.expH1[1]))
+        if self.precision == "mixed":
+            self._mixed_setup(hamiltonian, trial)
         if walkers is not None:
             self._workspace(walkers, hamiltonian)
 
@@ -132,7 +159,31 @@ class PhaselessGeneric:
         ws = self.ws
         if ws is None or (ws.W, ws.M, ws.na, ws.nb, ws.X) != (W, M, walkers.nup, walkers.ndown, X):
             self.ws = Workspace(W, M, walkers.nup, walkers.ndown, X, walkers.device)
+            if self.precision == "mixed":
+                self.ws.add_mixed()
         return self.ws
+
+    def _mixed_setup(self, hamiltonian, trial):
+        """TF32 operands of the mixed form, prepared once: packed Cholesky hi/lo,
+        half-rotated Cholesky (TF32), expH1 hi/lo with rows padded to a multiple of 4."""
+        M, X = hamiltonian.nbasis, hamiltonian.nchol
+        if M % 4 or X % 4 or self.expH1_complex:
+            raise NotImplementedError("the mixed form needs nbasis and nchol multiples of 4 and a real expH1")
+        dev = self.device
+        P = hamiltonian.npacked
+        f32 = torch.float32
+        self.cp_hi = torch.empty(P, X, dtype=f32, device=dev)
+        self.cp_lo = torch.empty(P, X, dtype=f32, device=dev)
+        call("ipie_b200_split_tf32", ptr(hamiltonian.chol_packed), ptr(self.cp_hi), ptr(self.cp_lo), P * X, stream())
+        from .estimators import _mixed_energy_operands
+
+        # padded half-rotated Cholesky TF32 head/remainder: force bias and energy share it
+        self.rpad = _mixed_energy_operands(trial, hamiltonian)
+        self.lde = M
+        e = torch.from_numpy(np.ascontiguousarray(self.expH1.real)).to(dev)
+        self.e_hi = torch.empty(2, M, M, dtype=f32, device=dev)
+        self.e_lo = torch.empty(2, M, M, dtype=f32, device=dev)
+        call("ipie_b200_split_tf32", ptr(e), ptr(self.e_hi), ptr(self.e_lo), e.numel(), stream())
 
     # ------------------------------------------------------------- the step
     def propagate_walkers_one_body(self, walkers):
@@ -140,14 +191,15 @@ class PhaselessGeneric:
         ws = self.ws
         self.timer.start("one_body")
         for s, (phi, tmp, n) in enumerate(((walkers.phia, ws.phia_tmp, walkers.nup), (walkers.phib, ws.phib_tmp, walkers.ndown))):
-            if n == 0:
+            if n == 0 or (s == 1 and walkers.spin_alias):
                 continue
             call("ipie_b200_propagate_one_body", ptr(self.expH1_dev[s]), int(self.expH1_complex), ptr(phi), ptr(tmp),
                  walkers.nwalkers, walkers.nbasis, n, stream())
         self.timer.stop("one_body")
         walkers.phia, ws.phia_tmp = ws.phia_tmp, walkers.phia
-        if walkers.ndown > 0:
+        if walkers.ndown > 0 and not walkers.spin_alias:
             walkers.phib, ws.phib_tmp = ws.phib_tmp, walkers.phib
+        walkers.sync_alias()
 
     def draw_fields(self, walkers, hamiltonian):
         """N(0,1) auxiliary fields (W, X) into the workspace (ipie ``phaseless_base.py:296-298``)."""
@@ -205,29 +257,112 @@ class PhaselessGeneric:
         self.timer.stop("vhs")
         self.timer.start("taylor")
         for phi_name, tmp_name, n in (("phia", "phia_tmp", walkers.nup), ("phib", "phib_tmp", walkers.ndown)):
-            if n == 0:
+            if n == 0 or (phi_name == "phib" and walkers.spin_alias):
                 continue
             phi, tmp = getattr(walkers, phi_name), getattr(ws, tmp_name)
             call("ipie_b200_apply_exponential_batch", ptr(vhs), ptr(phi), ptr(tmp), ptr(ws.taylor), walkers.nwalkers,
                  walkers.nbasis, n, self.exp_nmax, stream())
             setattr(walkers, phi_name, tmp)
             setattr(ws, tmp_name, phi)
+        walkers.sync_alias()
         self.timer.stop("taylor")
 
     def propagate_walkers(self, walkers, hamiltonian, trial, eshift):
-        """One phaseless step (ipie ``phaseless_base.py:312-338``)."""
+        """One phaseless step (ipie ``phaseless_base.py:312-338``).
+
+        The two one-body half steps and exp(VHS) run as one fused launch per spin
+        block (``ipie_b200_propagate_orbitals``); the force bias reads the Green's
+        function of the step's starting orbitals, as in ipie, so moving the first
+        one-body factor after it changes nothing.
+        """
         ws = self._workspace(walkers, hamiltonian)
         # the step's starting overlap goes into walkers.ovlp, which update_weight overwrites with ovlp_new
         self.timer.start("greens_function")
         greens_function_into(walkers, trial, walkers.ovlp)
         self.timer.stop("greens_function")
-        self.propagate_walkers_one_body(walkers)
-        cmf, cfb = self.propagate_walkers_two_body(walkers, hamiltonian, trial)
-        self.propagate_walkers_one_body(walkers)
+        if self.precision == "mixed":
+            cmf, cfb = self._mixed_two_body(walkers, hamiltonian, trial)
+        elif not self.fused_ok(walkers):
+            self.propagate_walkers_one_body(walkers)
+            cmf, cfb = self.propagate_walkers_two_body(walkers, hamiltonian, trial)
+            self.propagate_walkers_one_body(walkers)
+        else:
+            W, X = walkers.nwalkers, hamiltonian.nchol
+            self.timer.start("force_bias")
+            force_bias_into(hamiltonian, walkers, trial, ws.vbias)
+            self.timer.stop("force_bias")
+            self.vbias = ws.vbias
+            self.timer.start("rng")
+            xi = self.draw_fields(walkers, hamiltonian)
+            self.timer.stop("rng")
+            self.timer.start("field_shift")
+            call("ipie_b200_field_shift", ptr(ws.vbias), ptr(xi), ptr(self.mf_shift_dev), W, X, self.sqrt_dt,
+                 self.fbbound, ptr(ws.xshifted), ptr(ws.cmf), ptr(ws.cfb), stream())
+            self.timer.stop("field_shift")
+            self.timer.start("vhs")
+            self.construct_VHS(hamiltonian, ws.xshifted, out=ws.vhs)
+            self.timer.stop("vhs")
+            self.timer.start("orbitals")
+            for s_, (phi_name, tmp_name, n) in enumerate((("phia", "phia_tmp", walkers.nup),
+                                                           ("phib", "phib_tmp", walkers.ndown))):
+                if n == 0 or (s_ == 1 and walkers.spin_alias):
+                    continue
+                phi, tmp = getattr(walkers, phi_name), getattr(ws, tmp_name)
+                call("ipie_b200_propagate_orbitals", ptr(ws.vhs), ptr(self.expH1_pad[s_]), self.lda_e, ptr(phi),
+                     ptr(tmp), W, walkers.nbasis, n, self.exp_nmax, 1, 1, stream())
+                setattr(walkers, phi_name, tmp)
+                setattr(ws, tmp_name, phi)
+            walkers.sync_alias()
+            self.timer.stop("orbitals")
+            cmf, cfb = ws.cmf, ws.cfb
         self.timer.start("overlap")
         overlap_into(walkers, trial, ws.ovlp_new)
         self.timer.stop("overlap")
         self.update_weight(walkers, walkers.ovlp, ws.ovlp_new, cfb, cmf, eshift)
+
+    def _mixed_two_body(self, walkers, hamiltonian, trial):
+        """Force bias (TF32), shifted fields, VHS and the orbital update (3-pass TF32) of the mixed form."""
+        ws = self.ws
+        W, X, M = walkers.nwalkers, hamiltonian.nchol, walkers.nbasis
+        self.timer.start("force_bias")
+        (ra_hi, ra_lo), (rb_hi, rb_lo) = self.rpad
+        call("ipie_b200_construct_force_bias_mixed", ptr(ra_hi), ptr(ra_lo), ptr(rb_hi), ptr(rb_lo),
+             ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), ptr(ws.gwork), W, X, M, walkers.nup, walkers.ndown,
+             ptr(ws.vbias), ptr(walkers.status), stream())
+        self.timer.stop("force_bias")
+        self.vbias = ws.vbias
+        self.timer.start("rng")
+        xi = self.draw_fields(walkers, hamiltonian)
+        self.timer.stop("rng")
+        self.timer.start("field_shift")
+        call("ipie_b200_field_shift_mixed", ptr(ws.vbias), ptr(xi), ptr(self.mf_shift_dev), W, X, self.sqrt_dt,
+             self.fbbound, None, ptr(ws.xs_hi), ptr(ws.xs_lo), ptr(ws.cmf), ptr(ws.cfb), stream())
+        self.timer.stop("field_shift")
+        self.timer.start("vhs")
+        v = ws.v_planar
+        call("ipie_b200_construct_vhs_mixed", ptr(self.cp_hi), ptr(self.cp_lo), ptr(hamiltonian.sym_idx_i),
+             ptr(hamiltonian.sym_idx_j), M, X, ptr(ws.xs_hi), ptr(ws.xs_lo), W, self.sqrt_dt, ptr(v[0]), ptr(v[1]),
+             ptr(v[2]), ptr(v[3]), ptr(walkers.status), stream())
+        self.timer.stop("vhs")
+        self.timer.start("orbitals")
+        for s_, (phi_name, tmp_name, n) in enumerate((("phia", "phia_tmp", walkers.nup),
+                                                       ("phib", "phib_tmp", walkers.ndown))):
+            if n == 0 or (s_ == 1 and walkers.spin_alias):
+                continue
+            phi, tmp = getattr(walkers, phi_name), getattr(ws, tmp_name)
+            call("ipie_b200_propagate_orbitals_mixed", ptr(self.e_hi[s_]), ptr(self.e_lo[s_]), self.lde, ptr(v[0]),
+                 ptr(v[1]), ptr(v[2]), ptr(v[3]), ptr(phi), ptr(tmp), ptr(ws.orb_work), W, M, n, self.exp_nmax,
+                 ptr(walkers.status), stream())
+            setattr(walkers, phi_name, tmp)
+            setattr(ws, tmp_name, phi)
+        walkers.sync_alias()
+        self.timer.stop("orbitals")
+        return ws.cmf, ws.cfb
+
+    def fused_ok(self, walkers):
+        """The fused orbital kernel covers real expH1, M <= 256 and N <= 32."""
+        return (self.fused and not self.expH1_complex and walkers.nbasis <= 256
+                and max(walkers.nup, walkers.ndown) <= 32)
 
     def update_weight(self, walkers, ovlp, ovlp_new, cfb, cmf, eshift):
         """Hybrid energy, bound, importance function and cosine projection (ipie ``phaseless_base.py:340-358``).

@@ -65,9 +65,16 @@ class SingleDet:
         rcholb = np.einsum("mi,mnx->xin", self.psi0b, L, optimize=True).reshape(X, -1)
         dev = self.device
         self._rH1a = torch.from_numpy(np.ascontiguousarray(rH1a.astype(np.complex128))).to(dev)
-        self._rH1b = torch.from_numpy(np.ascontiguousarray(rH1b.astype(np.complex128))).to(dev)
         self._rchola = torch.from_numpy(np.ascontiguousarray(rchola)).to(dev)
-        self._rcholb = torch.from_numpy(np.ascontiguousarray(rcholb)).to(dev)
+        # identical spin blocks share one copy (the kernels then compute the block once)
+        self.spin_symmetric = bool(self.nalpha == self.nbeta and np.array_equal(self.psi0a, self.psi0b)
+                                   and np.array_equal(hamiltonian.H1[0], hamiltonian.H1[1]))
+        if self.spin_symmetric:
+            self._rH1b, self._rcholb = self._rH1a, self._rchola
+            self.psib_conj = self.psia_conj
+        else:
+            self._rH1b = torch.from_numpy(np.ascontiguousarray(rH1b.astype(np.complex128))).to(dev)
+            self._rcholb = torch.from_numpy(np.ascontiguousarray(rcholb)).to(dev)
         self.half_rotated = True
 
     def calculate_energy(self, system, hamiltonian):

@@ -44,8 +44,29 @@ class UHFWalkers:
         # device status word: numerical trouble bits written by the kernels
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.rhf = False  # ipie propagates both spin blocks in production (uhf_walkers.py:99)
+        # spin_alias: phib is phia (same tensor) -- both blocks identical, computed once
+        self.spin_alias = False
         self.buff_names = ["weight", "unscaled_weight", "phase", "hybrid_energy", "ovlp", "sgn_ovlp", "log_ovlp",
                            "phia", "phib"]
+
+    def enable_spin_alias(self):
+        """Share one tensor for identical alpha and beta blocks (RHF trial, walkers started from it).
+
+        Every kernel then computes the block once and counts it twice; results equal
+        propagating both blocks (ipie's production mode), which stay identical because
+        they see the same operators and fields.
+        """
+        if self.nup != self.ndown or not torch.equal(self.phia, self.phib):
+            raise ValueError("spin aliasing needs identical alpha and beta blocks")
+        self.phib = self.phia
+        self.Ghalfb = self.Ghalfa
+        self.spin_alias = True
+
+    def sync_alias(self):
+        """Re-point the beta views after the alpha tensors were replaced."""
+        if self.spin_alias:
+            self.phib = self.phia
+            self.Ghalfb = self.Ghalfa
 
     def build(self, trial):
         """``walkers.build``: initial overlaps and Green's functions (``uhf_walkers.py:101-102``)."""

@@ -212,7 +212,58 @@ def known_answer_inputs(name):
     print("wrote", name)
 
 
+def ad_fixture(name):
+    """Derivative of RHF local energies w.r.t. a one-body coupling, by ipie's AD-AFQMC addon.
+
+    ``addons/adafqmc/estimators/estimator.py:4-23`` (get_local_energy) and
+    ``addons/adafqmc/trial_wavefunction/sdtrial.py`` (half rotation, Ghalf), with
+    torch autograd through h1 -> h1 + lambda V at lambda = 0 and fixed walkers.
+    """
+    import torch
+    from types import SimpleNamespace
+
+    from ipie.addons.adafqmc.estimators.estimator import get_local_energy
+    from ipie.addons.adafqmc.trial_wavefunction.sdtrial import SDTrial
+
+    sysw = synthetic.generate(30, (6, 6), 90, decay=30.0, seed=13, uhf=False, chol_scale="stable")
+    M, N, X = sysw.nbasis, sysw.nup, sysw.nchol
+    rng = np.random.default_rng(14)
+    V = rng.normal(0.0, 0.1, size=(M, M))
+    V = np.triu(V) + np.triu(V, 1).T
+    W = 8
+    phi = sysw.psi[:, :N][None] + 0.15 * (rng.normal(size=(W, M, N)) + 1j * rng.normal(size=(W, M, N)))
+    weights = rng.uniform(0.5, 1.5, size=W)
+    chol = torch.from_numpy(sysw.chol.T.reshape(X, M, M).copy())
+    lam = torch.zeros((), dtype=torch.float64, requires_grad=True)
+    h1 = torch.from_numpy(sysw.h1e[0].copy()) + lam * torch.from_numpy(V)
+    trial = SDTrial(torch.from_numpy(sysw.psi[:, :N].copy()), N)
+    trial.half_rot(SimpleNamespace(h1e=h1, chol=chol))
+    ghalf = trial.get_ghalf(SimpleNamespace(walker_states=torch.from_numpy(phi)))
+    e = get_local_energy(trial.rh1, ghalf, trial.rchol, sysw.ecore)
+    wt = torch.from_numpy(weights)
+    E = (wt * e.real).sum() / wt.sum()
+    E.backward()
+    dE_total = float(lam.grad)
+    dE_walker = []
+    for iw in range(W):
+        lam2 = torch.zeros((), dtype=torch.float64, requires_grad=True)
+        h1w = torch.from_numpy(sysw.h1e[0].copy()) + lam2 * torch.from_numpy(V)
+        t2 = SDTrial(torch.from_numpy(sysw.psi[:, :N].copy()), N)
+        t2.half_rot(SimpleNamespace(h1e=h1w, chol=chol))
+        ew = get_local_energy(t2.rh1, ghalf.detach(), t2.rchol, sysw.ecore)[iw].real
+        ew.backward()
+        dE_walker.append(float(lam2.grad))
+    out = dict(V=V, phi=phi, weights=weights, energy=e.detach().numpy(), dE_dlambda=np.array(dE_total),
+               dE_walker=np.array(dE_walker), E=np.array(float(E)), chol_checksum=checksum(sysw.chol),
+               psi_checksum=checksum(sysw.psi))
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name, "dE/dlambda", dE_total)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "ad":
+        ad_fixture("ad_onebody_m30.npz")
+        sys.exit(0)
     c0 = synthetic.workload("c0_rhf_m26")
     kernels_fixture("kernels_rhf_m26.npz", c0, nwalkers=8, seed=11)
     uhf = synthetic.generate(30, (6, 4), 90, decay=30.0, seed=5, uhf=True)
@@ -222,3 +273,4 @@ if __name__ == "__main__":
     gentle = synthetic.generate(30, (6, 4), 90, decay=30.0, seed=5, uhf=True, chol_scale=0.1)
     run_fixture("run_uhf_m30.npz", gentle, nwalkers=12, num_blocks=3, seed=9)
     known_answer_inputs("known_answers.npz")
+    ad_fixture("ad_onebody_m30.npz")

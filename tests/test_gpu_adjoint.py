@@ -1,0 +1,79 @@
+"""Hand-written adjoint of the local energy w.r.t. the one-body Hamiltonian.
+
+Checked against central finite differences (lambda = +-1e-4, same walkers)
+and against ipie's AD-AFQMC addon (torch autograd through its local energy),
+whose derivatives are stored in ``tests/golden/ad_onebody_m30.npz``.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from tests._systems import checksum, load  # noqa: E402
+from tests.test_gpu_parity import _walker_pert, dev, gpu_objects  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _ad_system():
+    from ipie_b200 import synthetic
+
+    return synthetic.generate(30, (6, 6), 90, decay=30.0, seed=13, uhf=False, chol_scale="stable")
+
+
+def test_adjoint_matches_central_differences():
+    from ipie_b200.adjoint import OneBodyLocalEnergy, energy_response, local_energy_state
+    from ipie_b200 import synthetic
+
+    s = synthetic.generate(40, (7, 5), 120, decay=30.0, seed=8, uhf=True, chol_scale="stable")
+    ham, trial, walkers, prop = gpu_objects(s, 12)
+    pa, pb = _walker_pert(s, 12, 9)
+    walkers.phia, walkers.phib = dev(pa), dev(pb)
+    walkers.weight = dev(np.random.default_rng(1).uniform(0.5, 1.5, 12))
+    V = np.random.default_rng(2).normal(0, 0.1, (40, 40))
+    V = V + V.T
+    dE, E0 = energy_response(ham, trial, walkers, V)
+    state = local_energy_state(ham, trial, walkers)
+    h1 = torch.from_numpy(ham.H1.copy()).cuda()
+    Vd = torch.from_numpy(np.stack([V, V])).cuda()
+    wt = walkers.weight
+    eps = 1e-4
+    ep = (OneBodyLocalEnergy.apply(h1 + eps * Vd, state) * wt).sum() / wt.sum()
+    em = (OneBodyLocalEnergy.apply(h1 - eps * Vd, state) * wt).sum() / wt.sum()
+    fd = float((ep - em).item()) / (2 * eps)
+    assert abs(dE - fd) < 1e-7 * max(1.0, abs(fd))
+
+
+def test_adjoint_matches_ipie_ad_afqmc():
+    from ipie_b200.adjoint import OneBodyLocalEnergy, energy_response, local_energy_state
+
+    f = load("ad_onebody_m30.npz")
+    s = _ad_system()
+    np.testing.assert_allclose(checksum(s.chol), f["chol_checksum"], rtol=1e-13)
+    phi = f["phi"]
+    W = phi.shape[0]
+    ham, trial, walkers, prop = gpu_objects(s, W)
+    walkers.phia = dev(phi)
+    walkers.phib = dev(phi.copy())
+    walkers.weight = dev(f["weights"])
+    dE, E = energy_response(ham, trial, walkers, f["V"])
+    assert abs(E - float(f["E"])) < 1e-10 * abs(float(f["E"]))
+    assert abs(dE - float(f["dE_dlambda"])) < 1e-10 * max(1.0, abs(float(f["dE_dlambda"])))
+    # per-walker derivatives: unit upstream gradient on each walker
+    state = local_energy_state(ham, trial, walkers)
+    for iw in range(W):
+        lam = torch.zeros((), dtype=torch.float64, device="cuda", requires_grad=True)
+        h1 = torch.from_numpy(ham.H1.copy()).cuda() + lam * torch.from_numpy(np.stack([f["V"], f["V"]])).cuda()
+        OneBodyLocalEnergy.apply(h1, state)[iw].backward()
+        assert abs(float(lam.grad) - f["dE_walker"][iw]) < 1e-10 * max(1.0, abs(f["dE_walker"][iw]))
+
+
+def test_mixed_one_rdm_properties():
+    """The mixed 1-RDM from the adjoint: trace = electrons per spin; equals the trial density for trial walkers."""
+    from ipie_b200.adjoint import mixed_one_rdm
+
+    s = _ad_system()
+    ham, trial, walkers, prop = gpu_objects(s, 5)
+    rdm = mixed_one_rdm(ham, trial, walkers).cpu().numpy()
+    assert abs(np.trace(rdm[0]) - 6) < 1e-10 and abs(np.trace(rdm[1]) - 6) < 1e-10
+    np.testing.assert_allclose(rdm[0], trial.G[0].real, atol=1e-10)

@@ -1,0 +1,147 @@
+"""The mixed-precision form (TF32 tensor cores) against the FP64 form.
+
+Tolerances follow the arithmetic: the force bias is one TF32 pass (~2^-11
+relative), the VHS and orbital products are 3-pass TF32 (~2^-22); walker
+weights and overlaps after a few steps stay within 1e-5 of the FP64 path.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from tests.test_gpu_parity import _walker_pert, dev, gpu_objects, rel  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(M=64, N=8, X=128, uhf=True):
+    from ipie_b200 import synthetic
+
+    return synthetic.generate(M, (N, N), X, decay=30.0, seed=21, uhf=uhf, chol_scale="stable")
+
+
+def _mixed_objects(s, W):
+    from ipie_b200.propagation import PhaselessGeneric
+
+    ham, trial, walkers, prop = gpu_objects(s, W)
+    pm = PhaselessGeneric(0.005, precision="mixed")
+    pm.build(ham, trial, walkers)
+    return ham, trial, walkers, prop, pm
+
+
+def test_mixed_force_bias_3pass():
+    s = _system()
+    ham, trial, walkers, prop, pm = _mixed_objects(s, 40)
+    pa, pb = _walker_pert(s, 40, 3)
+    walkers.phia, walkers.phib = dev(pa), dev(pb)
+    trial.calc_greens_function(walkers)
+    ref = trial.calc_force_bias(ham, walkers)
+    from ipie_b200._lib import call, ptr, stream
+
+    ws = pm._workspace(walkers, ham)
+    out = torch.empty_like(ref)
+    (ra_hi, ra_lo), (rb_hi, rb_lo) = pm.rpad
+    call("ipie_b200_construct_force_bias_mixed", ptr(ra_hi), ptr(ra_lo), ptr(rb_hi), ptr(rb_lo), ptr(walkers.Ghalfa),
+         ptr(walkers.Ghalfb), ptr(ws.gwork), 40, s.nchol, s.nbasis, s.nup, s.ndown, ptr(out), ptr(walkers.status),
+         stream())
+    assert rel(out, ref) < 1e-5
+    walkers.check_status()
+
+
+def test_mixed_vhs_3pass():
+    s = _system()
+    W = 24
+    ham, trial, walkers, prop, pm = _mixed_objects(s, W)
+    ws = pm._workspace(walkers, ham)
+    rng = np.random.default_rng(5)
+    vb = dev(0.3 * (rng.normal(size=(W, s.nchol)) + 1j * rng.normal(size=(W, s.nchol))))
+    xi = dev(rng.normal(size=(W, s.nchol)))
+    from ipie_b200._lib import call, ptr, stream
+
+    xs = torch.empty(s.nchol, W, dtype=torch.complex128, device="cuda")
+    call("ipie_b200_field_shift_mixed", ptr(vb), ptr(xi), ptr(pm.mf_shift_dev), W, s.nchol, pm.sqrt_dt, 1.0, ptr(xs),
+         ptr(ws.xs_hi), ptr(ws.xs_lo), ptr(ws.cmf), ptr(ws.cfb), stream())
+    ref = prop.construct_VHS(ham, xs)
+    v = ws.v_planar
+    call("ipie_b200_construct_vhs_mixed", ptr(pm.cp_hi), ptr(pm.cp_lo), ptr(ham.sym_idx_i), ptr(ham.sym_idx_j),
+         s.nbasis, s.nchol, ptr(ws.xs_hi), ptr(ws.xs_lo), W, pm.sqrt_dt, ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]),
+         ptr(walkers.status), stream())
+    got = (v[0].double() + v[1].double()) + 1j * (v[2].double() + v[3].double())
+    assert rel(got, ref) < 1e-5
+    walkers.check_status()
+
+
+@pytest.mark.parametrize("M,N", [(64, 8), (200, 32), (108, 15)])
+def test_mixed_orbital_update_3pass(M, N):
+    from ipie_b200 import synthetic
+    from ipie_b200._lib import call, ptr, stream
+
+    s = synthetic.generate(M, (N, N), 2 * M, decay=30.0, seed=9, uhf=True, chol_scale="stable")
+    W = 6
+    ham, trial, walkers, prop, pm = _mixed_objects(s, W)
+    pa, _ = _walker_pert(s, W, 4)
+    rng = np.random.default_rng(2)
+    xs = dev(rng.normal(size=(s.nchol, W)) + 0.2j * rng.normal(size=(s.nchol, W)))
+    vhs = prop.construct_VHS(ham, xs)
+    ref = torch.empty(W, M, N, dtype=torch.complex128, device="cuda")
+    pa_d = dev(pa)  # keep the input alive until the kernels have run
+    call("ipie_b200_propagate_orbitals", ptr(vhs), ptr(prop.expH1_pad[0]), prop.lda_e, ptr(pa_d), ptr(ref), W, M, N,
+         6, 1, 1, stream())
+    planes = []
+    for part in (vhs.real.contiguous(), vhs.imag.contiguous()):
+        hi = torch.empty(part.shape, dtype=torch.float32, device="cuda")
+        lo = torch.empty_like(hi)
+        call("ipie_b200_split_tf32", ptr(part), ptr(hi), ptr(lo), part.numel(), stream())
+        planes += [hi, lo]
+    out = torch.empty_like(ref)
+    work = torch.empty(4 * W * 2 * N * M, dtype=torch.float32, device="cuda")
+    call("ipie_b200_propagate_orbitals_mixed", ptr(pm.e_hi[0]), ptr(pm.e_lo[0]), pm.lde, ptr(planes[0]), ptr(planes[1]),
+         ptr(planes[2]), ptr(planes[3]), ptr(pa_d), ptr(out), ptr(work), W, M, N, 6, ptr(walkers.status), stream())
+    assert rel(out, ref) < 1e-5
+    walkers.check_status()
+
+
+def test_mixed_steps_track_fp64():
+    """Three steps with identical draws: the mixed form stays within 1e-5 of the FP64 form."""
+    s = _system(M=76, N=10, X=200, uhf=False)
+    W = 32
+    runs = {}
+    for precision in ("fp64", "mixed"):
+        from ipie_b200 import Generic, SingleDet, UHFWalkers
+        from ipie_b200.propagation import PhaselessGeneric
+
+        ham = Generic(s.h1e, s.chol, s.ecore)
+        trial = SingleDet(s.psi, (s.nup, s.ndown), s.nbasis)
+        trial.half_rotate(ham)
+        walkers = UHFWalkers(s.init, s.nup, s.ndown, s.nbasis, W)
+        walkers.build(trial)
+        walkers.enable_spin_alias()
+        prop = PhaselessGeneric(0.005, precision=precision)
+        prop.build(ham, trial, walkers)
+        for step in range(3):
+            np.random.seed(70 + step)
+            prop.propagate_walkers(walkers, ham, trial, -1.0 if step else 0.0)
+        walkers.check_status()
+        runs[precision] = (walkers.weight.cpu().numpy(), walkers.ovlp.cpu().numpy(), walkers.phia.cpu().numpy())
+    a, b = runs["mixed"], runs["fp64"]
+    assert rel(a[0], b[0]) < 1e-5
+    assert rel(a[1], b[1]) < 1e-5
+    assert rel(a[2], b[2]) < 1e-5
+
+
+@pytest.mark.parametrize("uhf,N", [(False, 10), (True, 15), (False, 32)])
+def test_mixed_local_energy(uhf, N):
+    """Exchange in 3-pass TF32 (Coulomb in FP64) against the FP64 local energy."""
+    from ipie_b200 import synthetic
+    from ipie_b200.estimators import local_energy_mixed, local_energy_single_det_uhf_batch
+
+    s = synthetic.generate(76, (N, N), 200, decay=30.0, seed=17, uhf=uhf, chol_scale="stable")
+    W = 40
+    ham, trial, walkers, prop = gpu_objects(s, W)
+    pa, pb = _walker_pert(s, W, 6)
+    walkers.phia, walkers.phib = dev(pa), dev(pb)
+    trial.calc_greens_function(walkers)
+    ref = local_energy_single_det_uhf_batch(None, ham, walkers, trial)
+    got = local_energy_mixed(None, ham, walkers, trial)
+    assert rel(got, ref) < 2e-6
+    walkers.check_status()

@@ -70,7 +70,8 @@ def test_kernels_match_ipie(name):
     work = torch.empty(2 * walkers.phia.numel(), dtype=torch.complex128, device="cuda")
     from ipie_b200._lib import call, ptr, stream
 
-    call("ipie_b200_apply_exponential_batch", ptr(dev(f["VHS"])), ptr(walkers.phia), ptr(out), ptr(work), W,
+    vhs_d = dev(f["VHS"])
+    call("ipie_b200_apply_exponential_batch", ptr(vhs_d), ptr(walkers.phia), ptr(out), ptr(work), W,
          s.nbasis, s.nup, 6, stream())
     assert rel(out, f["phia_exp"]) < 1e-13
     call("ipie_b200_propagate_one_body", ptr(prop.expH1_dev[0]), int(prop.expH1_complex), ptr(walkers.phia), ptr(out),
@@ -260,3 +261,79 @@ def test_device_rng_moments():
     assert abs(x.var() - 1.0) < 5.0 * np.sqrt(2.0 / n)
     assert abs(np.mean(x ** 4) - 3.0) < 0.02
     assert not np.allclose(x[:100], b.cpu().numpy()[:100])
+
+
+@pytest.mark.parametrize("M,N,pre,post", [(26, 5, 1, 1), (21, 4, 1, 0), (33, 7, 0, 1), (64, 16, 0, 0), (200, 32, 1, 1)])
+def test_fused_orbital_update_matches_oracle(M, N, pre, post):
+    """``ipie_b200_propagate_orbitals`` = one-body, exp(VHS) (order 6), one-body; odd M exercises padding."""
+    from ipie_b200 import synthetic
+    from ipie_b200._lib import call, ptr, stream
+
+    s = synthetic.generate(M, (N, N), 3 * M, decay=30.0, seed=4, uhf=True, chol_scale="stable")
+    S = oracle_system(s)
+    ham, trial, walkers, prop = gpu_objects(s, 3)
+    W = 3
+    pa, _ = _walker_pert(s, W, 8)
+    xs = np.random.default_rng(2).normal(size=(s.nchol, W)) + 0.2j * np.random.default_rng(3).normal(size=(s.nchol, W))
+    vhs = O.construct_vhs(S, xs)
+    ref = pa.copy()
+    if pre:
+        ref = O.propagate_one_body(ref, S.expH1[0])
+    ref = O.apply_exponential(ref, vhs, 6)
+    if post:
+        ref = O.propagate_one_body(ref, S.expH1[0])
+    out = torch.empty(W, M, N, dtype=torch.complex128, device="cuda")
+    vhs_d, pa_d = dev(vhs), dev(pa)  # keep the inputs alive until the kernel has run
+    call("ipie_b200_propagate_orbitals", ptr(vhs_d), ptr(prop.expH1_pad[0]), prop.lda_e, ptr(pa_d), ptr(out),
+         W, M, N, 6, pre, post, stream())
+    assert rel(out, ref) < 1e-13
+
+
+def test_spin_alias_equals_two_blocks_and_oracle():
+    """RHF walkers computed once per block (aliased) vs both blocks propagated, vs the oracle."""
+    from ipie_b200 import AFQMC, Generic, SingleDet, synthetic
+
+    s = synthetic.generate(30, (6, 6), 90, decay=30.0, seed=11, uhf=False, chol_scale="stable")
+    runs = {}
+    for alias in (True, False):
+        ham = Generic(s.h1e, s.chol, s.ecore)
+        trial = SingleDet(s.psi, (6, 6), 30)
+        trial.half_rotate(ham)
+        af = AFQMC.build((6, 6), ham, trial, num_walkers=10, seed=3, num_steps_per_block=25, num_blocks=2,
+                         verbose=False, spin_alias="auto" if alias else False)
+        assert af.walkers.spin_alias is alias
+        runs[alias] = (af.run(), af.walkers.weight.cpu().numpy(), af.walkers.phia.cpu().numpy(),
+                       af.walkers.phib.cpu().numpy())
+    a, b = runs[True], runs[False]
+    assert rel(a[0], b[0]) < 1e-12
+    assert rel(a[1], b[1]) < 1e-12
+    assert rel(a[2], b[2]) < 1e-12
+    assert rel(a[3], b[3]) < 1e-12
+    S = oracle_system(s)
+    ow = O.Walkers.from_initial(s.init, 6, 10)
+    ow.ovlp = O.greens_function(S, ow)
+    blocks = O.run_afqmc(S, ow, num_blocks=2, seed=3)
+    et = np.array([blk["ETotal"] for blk in blocks])
+    assert rel(a[0][:, 5], et) < TOL
+    assert rel(a[1], ow.weight) < TOL
+
+
+def test_unfused_step_path_matches_oracle():
+    """The per-stage launches (one-body, Taylor terms, one-body) used when the fused kernel does not apply."""
+    from ipie_b200 import synthetic
+
+    s = synthetic.generate(26, (5, 3), 60, decay=30.0, seed=6, uhf=True, chol_scale="stable")
+    S = oracle_system(s)
+    ham, trial, walkers, prop = gpu_objects(s, 4)
+    prop.fused = False
+    ow = O.Walkers.from_initial(s.init, s.nup, 4)
+    ow.ovlp = O.greens_function(S, ow)
+    walkers.ovlp = trial.calc_greens_function(walkers)
+    for step in range(2):
+        np.random.seed(31 + step)
+        prop.propagate_walkers(walkers, ham, trial, 0.0)
+        np.random.seed(31 + step)
+        O.propagate_walkers(S, ow, 0.0)
+    assert rel(walkers.weight, ow.weight) < TOL
+    assert rel(walkers.phia, ow.phia) < TOL
+    assert rel(walkers.phib, ow.phib) < TOL
