@@ -244,7 +244,28 @@ def run_reference(args):
     return 0
 
 
-def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clock=False):
+def train_control_variate(wl, W, rank, steps=100, epochs=60):
+    """Exchange control variate trained on (features, exchange) pairs of `steps` plain FP64 steps."""
+    import time as _t
+
+    from ipie_b200.control_variate import ExchangeControlVariate, generate_training_data
+
+    t0 = _t.perf_counter()
+    af, _ = build_afqmc(wl, W, "device", 1000 + rank, precision="fp64")
+    af.setup_run()
+    feats, ys, bases = generate_training_data(af, steps=steps)
+    del af
+    cv = ExchangeControlVariate(hidden=256, seed=rank)
+    hist = cv.fit(feats, ys, bases, epochs=epochs, batch=4096, lr=2e-3)
+    resid = (ys - bases)
+    info = {"pairs": int(feats.shape[0]), "epochs": epochs,
+            "var_y": float(ys.var().item()), "var_y_minus_linear": float(resid.var().item()),
+            "holdout_mse_first": hist[0][1], "holdout_mse_last": hist[-1][1],
+            "mse_units": "var(y - linear term)", "seconds": _t.perf_counter() - t0}
+    return cv, info
+
+
+def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clock=False, cv=None):
     """Build, warm up and time ``args.steps`` driver steps of one form; returns a result dict."""
     import torch
 
@@ -253,6 +274,10 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
 
     af, _ = build_afqmc(wl, W, rng, 7 + rank, precision=precision)
     af.setup_run()
+    if cv is not None:
+        from ipie_b200.control_variate import ControlVariateEnergyEstimator
+
+        af.estimator = ControlVariateEnergyEstimator(cv, fraction=8, seed=7 + rank)
     step = 0
     for _ in range(args.warmup):
         step += 1
@@ -289,6 +314,18 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
         "clocks": clk.summary() if clk else None,
     }
     af.propagator.timer = _NoTimer()
+    # untimed checks on the final walkers
+    w, ham, trial = af.walkers, af.hamiltonian, af.trial
+    if precision == "mixed" and cv is None:
+        from ipie_b200.estimators import EnergyEstimator
+
+        d64 = EnergyEstimator(precision="fp64").compute_estimator(None, w, ham, trial)
+        dmx = EnergyEstimator(precision="mixed").compute_estimator(None, w, ham, trial)
+        res["estimator_shift_mEh"] = abs(float((dmx[0] / dmx[1]).real - (d64[0] / d64[1]).real)) * 1e3
+    if cv is not None:
+        from ipie_b200.control_variate import EnergyParts, cv_estimator_error
+
+        res["cv_error"] = cv_estimator_error(cv, EnergyParts(ham, trial, w), w, fraction=8, trials=64)
     del af
     torch.cuda.empty_cache()
     return res
@@ -308,6 +345,12 @@ def run_ours(args):
     runs = {}
     for form in forms:
         runs[form] = timed_run(wl, W, form, args, rank, world, local, with_clock=(form == forms[-1]))
+    cv_info = None
+    if args.form == "both" and not args.no_cv:
+        cv, cv_info = train_control_variate(wl, W, rank, steps=args.cv_steps)
+        runs["mixed_cv"] = timed_run(wl, W, "mixed", args, rank, world, local, cv=cv)
+        cv_info["estimator_error"] = runs["mixed_cv"].pop("cv_error", None)
+        del cv
     head = "mixed" if "mixed" in runs else "fp64"
     r = runs[head]
     t = r["t"]
@@ -347,6 +390,14 @@ def run_ours(args):
         n = min(len(a), len(b))
         shift = float(np.max(np.abs(a[:n] - b[:n]))) * 1e3  # mEh, same draws and seed
         forms_out["mixed_over_fp64"] = forms_out["mixed"]["walker_steps_per_s"] / forms_out["fp64"]["walker_steps_per_s"]
+        forms_out["mixed"]["estimator_shift_mEh"] = runs["mixed"].get("estimator_shift_mEh")
+    if "mixed_cv" in runs and "fp64" in runs:
+        a, b = runs["mixed_cv"]["blocks"][1:, 5], runs["fp64"]["blocks"][1:, 5]
+        n = min(len(a), len(b))
+        forms_out["mixed_cv"]["energy_shift_vs_fp64_mEh"] = float(np.max(np.abs(a[:n] - b[:n]))) * 1e3
+        forms_out["mixed_cv_over_fp64"] = (forms_out["mixed_cv"]["walker_steps_per_s"]
+                                          / forms_out["fp64"]["walker_steps_per_s"])
+        forms_out["mixed_cv"]["training"] = cv_info
 
     # ---------------- end to end through the public API (headline form) ----------------
     e2e_steps = min(args.steps, args.e2e_steps)
@@ -468,6 +519,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=25)
     ap.add_argument("--ref-walkers", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cv", action="store_true", help="skip the learned control-variate form")
+    ap.add_argument("--cv-steps", type=int, default=100, help="plain-method steps generating control-variate training data")
     ap.add_argument("--form", choices=["fp64", "mixed", "both"], default="both",
                     help="which forms to time; with both, the mixed form is the headline and the FP64 form its reference")
     ap.add_argument("--measure-peaks", action="store_true", help="print measured GEMM/copy peaks and exit")

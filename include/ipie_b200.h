@@ -132,11 +132,25 @@ int ipie_b200_reortho(void* phia, void* phib, int W, int M, int na, int nb, cons
 
 /* Population-control walker copies: walker d receives walker src[d]
  * (src[d] < 0 keeps it): orbitals, weight, unscaled weight, hybrid energy,
- * overlap and phase (phase may be NULL).
+ * overlap, phase and the half-rotated Green's functions (phase, ghalfa,
+ * ghalfb may be NULL).
  * replaces: walkers/pop_controller.py:128-196 (get_buffer/set_buffer) and
  *           the send/receive loop :403-429 */
 int ipie_b200_walker_copy(const int* src, int W, int M, int na, int nb, void* phia, void* phib, double* weight,
-                          double* unscaled_weight, void* hybrid_energy, void* ovlp, void* phase, void* stream);
+                          double* unscaled_weight, void* hybrid_energy, void* ovlp, void* phase, void* ghalfa,
+                          void* ghalfb, void* stream);
+/* Out-of-place resampling: walker d of the *_out arrays becomes walker src[d]
+ * of the inputs (orbitals, half-rotated Green's functions, hybrid energy,
+ * overlap, phase, unscaled weight; sources may repeat).  ghalf*, phase may be
+ * NULL; phib == phia / ghalfb == ghalfa (spin-aliased blocks) copy once.
+ * Inputs and outputs must not overlap.
+ * replaces: the gather/scatter of stochastic_reconfiguration,
+ *           walkers/pop_controller.py:432-475 */
+int ipie_b200_walker_gather(const int* src, int W, int M, int na, int nb, const void* phia, const void* phib,
+                            const void* ghalfa, const void* ghalfb, const void* hybrid_energy, const void* ovlp,
+                            const void* phase, const double* unscaled_weight, void* phia_out, void* phib_out,
+                            void* ghalfa_out, void* ghalfb_out, void* hybrid_energy_out, void* ovlp_out,
+                            void* phase_out, double* unscaled_weight_out, void* stream);
 
 /* Exchange energy for callers that cannot allocate device memory (their device
  * memory is owned by their own pool allocator, or their loop cannot take the
@@ -249,13 +263,20 @@ int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, float* h
  * FP64.  Same contract and spin-alias convention as
  * ipie_b200_local_energy_single_det_batch; rchola/rcholb FP64, r*_hi/lo from
  * ipie_b200_rchol_pad_split; gwork: 2*W*2*32*M floats; work: W*X + rows*W
- * complex with rows = sum over spin blocks of ceil(X*NP/128); M % 4 == 0.
+ * complex with rows = sum over spin blocks of ceil(X*NP/128) (+1 per spin
+ * block with the trial reference); M % 4 == 0.
+ * Trial reference (optional; ghalf_trial_a NULL disables it): the trial's
+ * Ghalf_s (N_s, M), the exchange gradient there K_s (N_s, M) and raw_trial[s]
+ * = sum_x tr(T_s T_s) at the trial (complex); the tensor cores then only see
+ * G - G_T and raw(G_T) + K.(G - G_T) is added in FP64, so the exchange error
+ * scales with the walker's distance from the trial.
  * replaces (mixed form): estimators/local_energy_sd.py:987-1080. */
 int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const float* ra_hi,
                                  const float* ra_lo, const float* rb_hi, const float* rb_lo, const void* rH1a,
-                                 const void* rH1b, double ecore, const void* ghalfa, const void* ghalfb, int W, int X,
-                                 int M, int na, int nb, float* gwork, void* work, void* energy, unsigned int* status,
-                                 void* stream);
+                                 const void* rH1b, double ecore, const void* ghalfa, const void* ghalfb,
+                                 const void* ghalf_trial_a, const void* ghalf_trial_b, const void* kmat_a,
+                                 const void* kmat_b, const void* raw_trial, int W, int X, int M, int na, int nb,
+                                 float* gwork, void* work, void* energy, unsigned int* status, void* stream);
 
 /* ---- learned control variate for the exchange energy (no counterpart in ipie) ----
  * MLP 16 -> H -> H -> 1 (SiLU), bf16 weights `wbf`, fp32 master copy/biases,
@@ -272,10 +293,15 @@ int ipie_b200_mlp_adam(float* master, void* wbf, const float* grad, float* m, fl
 /* (x - mu) / sigma per feature column, in place. */
 int ipie_b200_normalize_features(float* x, long long rows, int F, const float* mu, const float* sigma, void* stream);
 /* 16 per-walker features (fp32, row-major (W,16)) from the exchange-free energy (W,3), the Coulomb
- * vector xv (W,X), overlaps, hybrid energies, Ghalf (W,N,M), conj trial (M,N), trial Ghalf (N,M), weights. */
-int ipie_b200_cv_features(int W, int X, int N, int M, const void* energy, const void* xv, const void* ovlp,
-                          const void* hybrid_energy, const void* ghalf, const void* psi_conj, const void* ghalf_trial,
-                          const double* weight, float* feat, void* stream);
+ * vector xv (W,X), overlaps, hybrid energies, Ghalf per spin (W,N_s,M), the trial's Ghalf (N_s,M),
+ * the exchange gradient at the trial K_s (N_s,M) complex and, in the last column, lead[w] (e.g. the
+ * exchange term over the leading Cholesky vectors; NULL: the weights); base (W,) f64 receives
+ * the first-order change of the exchange term from its trial value, Re sum_s f_s K_s.(G_s - G_T,s)
+ * (f_s = 1/2, or 1 for spin-aliased blocks: ghalfb == ghalfa, nb == na). */
+int ipie_b200_cv_features(int W, int X, int na, int nb, int M, const void* energy, const void* xv, const void* ovlp,
+                          const void* hybrid_energy, const void* ghalfa, const void* ghalfb, const void* ghalf_trial_a,
+                          const void* ghalf_trial_b, const void* kmat_a, const void* kmat_b, const double* weight,
+                          const double* lead, float* feat, double* base, void* stream);
 /* dst[s] = src[idx[s]] for rows of `row` complex values. */
 int ipie_b200_gather_walkers(const void* src, const int* idx, int S, long long row, void* dst, void* stream);
 /* out[0..4] = [sum w (A - c), (W/S) sum_S w (y - c), sum w, sum w A, (W/S) sum_S w y]: the control-variate

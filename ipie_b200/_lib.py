@@ -32,7 +32,8 @@ SIGNATURES = {
     "ipie_b200_update_weight": [I, P, P, P, P, D, D, P, P, P, P, P, P],
     "ipie_b200_clip_weight": [I, P, P, P],
     "ipie_b200_reortho": [P, P, I, I, I, I, P, P, P, P, P, P],
-    "ipie_b200_walker_copy": [P, I, I, I, I, P, P, P, P, P, P, P, P],
+    "ipie_b200_walker_copy": [P, I, I, I, I, P, P, P, P, P, P, P, P, P, P],
+    "ipie_b200_walker_gather": [P, I, I, I, I] + [P] * 17,
     "ipie_b200_exchange_rows": [I, I, I, I],
     "ipie_b200_exchange": [P, P, I, I, I, I, P, P],
     "ipie_b200_exchange_noalloc": [P, P, I, I, I, I, P, P],
@@ -43,13 +44,13 @@ SIGNATURES = {
     "ipie_b200_construct_vhs_mixed": [P, P, P, P, I, I, P, P, I, D, P, P, P, P, P, P],
     "ipie_b200_propagate_orbitals_mixed": [P, P, I, P, P, P, P, P, P, P, I, I, I, I, P, P],
     "ipie_b200_rchol_pad_split": [P, I, I, I, P, P, P],
-    "ipie_b200_local_energy_mixed": [I, P, P, P, P, P, P, P, P, D, P, P, I, I, I, I, I, P, P, P, P, P],
+    "ipie_b200_local_energy_mixed": [I, P, P, P, P, P, P, P, P, D, P, P, P, P, P, P, P, I, I, I, I, I, P, P, P, P, P],
     "ipie_b200_energy_combine": [I, I, I, I, I, P, P, P, P, D, P, P, I, D, D, D, P, P, P],
     "ipie_b200_mlp_forward": [P, I, I, I, P, P, P, P, P],
     "ipie_b200_mlp_backward": [P, P, I, I, I, P, P, P, P, P, P, P],
     "ipie_b200_mlp_adam": [P, P, P, P, P, ctypes.c_longlong, ctypes.c_float, I, P],
     "ipie_b200_normalize_features": [P, ctypes.c_longlong, I, P, P, P],
-    "ipie_b200_cv_features": [I, I, I, I, P, P, P, P, P, P, P, P, P, P],
+    "ipie_b200_cv_features": [I, I, I, I, I, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "ipie_b200_gather_walkers": [P, P, I, ctypes.c_longlong, P, P],
     "ipie_b200_cv_sums": [I, P, P, P, I, P, P, P, P],
     "ipie_b200_onebody_adjoint": [I, I, I, I, P, P, P, P, P, P, P, P],

@@ -1,12 +1,20 @@
 """Learned control variate for the exchange energy (no counterpart in ipie).
 
 The exchange term dominates the cost of a local-energy evaluation
-(O(W X N^2 M)).  A small MLP (16 -> 256 -> 256 -> 1, SiLU, bf16 weights, FP32
-accumulation) predicts each walker's exchange term from cheap per-walker
-features (one-body and Coulomb energies, force-bias norms, overlap phase and
-magnitude, hybrid energy, Green's-function norms; see
-``ipie_b200_cv_features``).  The block estimate stays unbiased: the exact
-exchange is evaluated on a uniform random subsample S of the walkers and
+(O(W X N^2 M)).  Each walker's exchange term is predicted as
+
+    c_w = b_w + MLP(f_w),
+
+b_w the exact exchange term over the leading X/``lead_fraction`` Cholesky
+vectors (the half-rotated vectors are ordered by decreasing weight, so these
+carry most of it, at 1/``lead_fraction`` of the exact cost), and a small MLP
+(16 -> 256 -> 256 -> 1, SiLU, bf16 weights, FP32 accumulation) learning the
+remaining tail from cheap per-walker features (one-body and Coulomb energies,
+Coulomb vector norms, overlap phase and magnitude, hybrid energy,
+Green's-function norms, the first-order change of the exchange from its trial
+value K_s.(G_s - G_T,s), b_w itself; see ``ipie_b200_cv_features``).  The
+block estimate stays unbiased: the exact exchange is evaluated on a uniform
+random subsample S of the walkers and
 
     sum_w w_w E_w  ~=  sum_w w_w (A_w - c_w)  -  (W/|S|) sum_{s in S} w_s (y_s - c_s)
 
@@ -63,12 +71,15 @@ class ExchangeControlVariate:
         self.trained = False
 
     # ------------------------------------------------------------ training
-    def fit(self, feats, y, epochs=60, batch=4096, lr=2e-3, holdout=0.1, seed=0):
+    def fit(self, feats, y, base=None, epochs=60, batch=4096, lr=2e-3, holdout=0.1, seed=0):
         """Train on (features, exchange term) pairs; returns the train/holdout MSE history (normalised units).
 
-        ``feats``: (n, 16) float32 CUDA tensor of raw features; ``y``: (n,) float64/32 targets.
+        ``feats``: (n, 16) float32 CUDA tensor of raw features; ``y``: (n,) float64/32 targets;
+        ``base``: (n,) float64 linear term the network is added to (the network learns y - base).
         """
         n = feats.shape[0]
+        if base is not None:
+            y = y.double() - base.double()
         fm = feats.double().mean(0)
         fs = feats.double().std(0)
         fs = torch.where(fs > 0, fs, torch.ones_like(fs))
@@ -125,31 +136,52 @@ class ExchangeControlVariate:
              ptr(acts), ptr(out), stream())
         return out
 
-    def predict(self, feats):
-        """Exchange-term prediction (fp32, physical units) for raw features (W, 16)."""
+    def predict(self, feats, base=None):
+        """Exchange-term prediction (fp32, physical units) for raw features (W, 16) and the linear term."""
         x = feats.float().contiguous().clone()
         call("ipie_b200_normalize_features", ptr(x), x.shape[0], self.F, ptr(self.mu), ptr(self.sigma), stream())
         out = self.forward_normalised(x)
-        # physical units: y = mean + scale * out (a tiny elementwise map; kept as torch plumbing)
-        return (out.double() * self.y_scale + self.y_mean).float().contiguous()
+        # physical units: c = base + mean + scale * out (a tiny elementwise map; kept as torch plumbing)
+        c = out.double() * self.y_scale + self.y_mean
+        if base is not None:
+            c = c + base
+        return c.float().contiguous()
 
 
 # ----------------------------------------------------------------------------
 # energy pieces used by the estimator and by training-data generation
 # ----------------------------------------------------------------------------
+def exchange_gradient(rchol, ghalf_trial):
+    """K = d raw / d Ghalf at the trial, (N, M) complex, for raw = sum_x sum_ij T^x_ij T^x_ji.
+
+    T^x_ij = sum_m L_x[i, m] G[j, m] with L_x the half-rotated Cholesky vector
+    (rows of ``rchol`` (X, N*M)); dT^x_ab/dG[j, m] = delta_bj L_x[a, m] gives
+    K[j, m] = 2 sum_x sum_a T^x_ja L_x[a, m] (holomorphic, no conjugation).  Done once per
+    trial with two library GEMMs (torch plumbing; the per-walker contraction is a kernel).
+    """
+    N, M = ghalf_trial.shape
+    L = rchol.reshape(-1, N, M).to(torch.complex128)
+    T = torch.einsum("xim,jm->xij", L, ghalf_trial.to(torch.complex128))
+    return (2.0 * torch.einsum("xja,xam->jm", T, L)).contiguous()
+
+
 class EnergyParts:
     """Exchange-free energies, Coulomb vectors, exact exchange terms and features of a walker batch."""
 
-    def __init__(self, hamiltonian, trial, walkers):
+    def __init__(self, hamiltonian, trial, walkers, lead_fraction=8):
         self.ham, self.trial = hamiltonian, trial
+        self.n_lead = max(1, hamiltonian.nchol // lead_fraction)
         W, X, M = walkers.nwalkers, hamiltonian.nchol, hamiltonian.nbasis
         dev = walkers.device
         self.xv = torch.empty(W, X, dtype=C128, device=dev)
         self.energy_noexx = torch.empty(W, 3, dtype=C128, device=dev)
         self.feat = torch.empty(W, NFEAT, dtype=F32, device=dev)
+        self.base = torch.empty(W, dtype=F64, device=dev)  # exchange term over the leading vectors
+        self.linear = torch.empty(W, dtype=F64, device=dev)  # first-order change from the trial value
         self.exx = torch.empty(W, dtype=C128, device=dev)
-        gh = trial.Ghalf[0]
-        self.ghalf_trial = torch.from_numpy(np.ascontiguousarray(gh.astype(np.complex128))).to(dev)
+        from .estimators import exchange_reference
+
+        self.ghalf_trial, self.kmat, _ = exchange_reference(trial, hamiltonian)
 
     def compute(self, walkers, with_features=True):
         """Green's functions, exchange-free energy and features for every walker."""
@@ -157,7 +189,8 @@ class EnergyParts:
 
         ham, trial = self.ham, self.trial
         W, X, M = walkers.nwalkers, ham.nchol, ham.nbasis
-        trial.calc_greens_function(walkers)
+        if not walkers.gf_current(trial):
+            trial.calc_greens_function(walkers)
         force_bias_into(ham, walkers, trial, self.xv)  # Coulomb vector X_a + X_b
         rhf = bool(walkers.rhf)
         f1, fc = (2.0, 2.0) if rhf else (1.0, 0.5)
@@ -166,14 +199,19 @@ class EnergyParts:
              ptr(trial._rH1a), ptr(trial._rH1b), ham.ecore, ptr(self.xv), None, 0, f1, fc, 0.0,
              ptr(self.energy_noexx), ptr(walkers.status), stream())
         if with_features:
-            call("ipie_b200_cv_features", W, X, walkers.nup, M, ptr(self.energy_noexx), ptr(self.xv), ptr(walkers.ovlp),
-                 ptr(walkers.hybrid_energy), ptr(walkers.Ghalfa), ptr(trial.psia_conj), ptr(self.ghalf_trial),
-                 ptr(walkers.weight), ptr(self.feat), stream())
+            self.base.copy_(self.exchange_term(walkers, nchol=self.n_lead))
+            call("ipie_b200_cv_features", W, X, walkers.nup, walkers.ndown, M, ptr(self.energy_noexx), ptr(self.xv),
+                 ptr(walkers.ovlp), ptr(walkers.hybrid_energy), ptr(walkers.Ghalfa), ptr(walkers.Ghalfb),
+                 ptr(self.ghalf_trial[0]), ptr(self.ghalf_trial[1]), ptr(self.kmat[0]), ptr(self.kmat[1]),
+                 ptr(walkers.weight), ptr(self.base), ptr(self.feat), ptr(self.linear), stream())
 
-    def exchange_term(self, walkers, idx=None):
-        """Exact exchange term y = 1/2 Re(raw_a + raw_b) (W,) or on the subsample ``idx``; float64."""
+    def exchange_term(self, walkers, idx=None, nchol=None):
+        """Exact exchange term y = 1/2 Re(raw_a + raw_b) (W,) or on the subsample ``idx``; float64.
+
+        ``nchol`` restricts the sum to the leading Cholesky vectors (rows of the half-rotated
+        Cholesky are contiguous per vector, so the leading block is a prefix)."""
         ham = self.ham
-        X, M = ham.nchol, ham.nbasis
+        X, M = (nchol or ham.nchol), ham.nbasis
         S = walkers.nwalkers if idx is None else int(idx.numel())
         total = torch.zeros(S, dtype=F64, device=walkers.device)
         blocks = [(self.trial._rchola, walkers.Ghalfa, walkers.nup, 1.0 if walkers.spin_alias else 0.5)]
@@ -211,7 +249,7 @@ class ControlVariateEnergyEstimator:
             self._out = torch.zeros(5, dtype=F64, device=walkers.device)
         p = self.parts
         p.compute(walkers)
-        pred = self.cv.predict(p.feat)
+        pred = self.cv.predict(p.feat, p.base)
         W = walkers.nwalkers
         S = max(1, W // self.fraction)
         idx = torch.from_numpy(np.sort(self.rng.choice(W, S, replace=False)).astype(np.int32)).to(walkers.device)
@@ -233,20 +271,22 @@ class ControlVariateEnergyEstimator:
 
 
 def generate_training_data(afqmc, steps=100, first_step=1):
-    """(features, exact exchange term) for every walker at each of ``steps`` driver steps.
+    """(features, exact exchange term, linear term) for every walker at each of ``steps`` driver steps.
 
     Runs the walk forward with the plain method (the AFQMC object's own
-    propagator); returns float32 features (steps*W, 16) and float64 targets.
+    propagator); returns float32 features (steps*W, 16), float64 targets and
+    float64 linear terms.
     """
     w = afqmc.walkers
     parts = EnergyParts(afqmc.hamiltonian, afqmc.trial, w)
-    feats, ys = [], []
+    feats, ys, bases = [], [], []
     for step in range(first_step, first_step + steps):
         afqmc.step(step)
         parts.compute(w)
         ys.append(parts.exchange_term(w))
         feats.append(parts.feat.clone())
-    return torch.cat(feats), torch.cat(ys)
+        bases.append(parts.base.clone())
+    return torch.cat(feats), torch.cat(ys), torch.cat(bases)
 
 
 def subsample_variances(cv, parts, walkers, fraction=8, trials=64, seed=3):
@@ -258,7 +298,7 @@ def subsample_variances(cv, parts, walkers, fraction=8, trials=64, seed=3):
     y = parts.exchange_term(walkers)
     wt = walkers.weight.double()
     exact = float((wt * y).sum().item())
-    pred = cv.predict(parts.feat).double()
+    pred = cv.predict(parts.feat, parts.base).double()
     full_c = float((wt * pred).sum().item())
     rng = np.random.default_rng(seed)
     W = walkers.nwalkers
@@ -270,3 +310,30 @@ def subsample_variances(cv, parts, walkers, fraction=8, trials=64, seed=3):
         plain.append(f * float((wt[idx] * y[idx]).sum().item()))
         with_cv.append(full_c + f * float((wt[idx] * (y[idx] - pred[idx])).sum().item()))
     return float(np.std(plain)), float(np.std(with_cv)), exact
+
+
+def cv_estimator_error(cv, parts, walkers, fraction=8, trials=64, seed=5):
+    """Error the subsampled estimate adds to the block energy of the current walkers, in mEh.
+
+    Over ``trials`` random subsamples: the spread of (estimate - exact) / sum w with the
+    control variate and without it (plain subsample), and the mean difference with its
+    standard error (zero within it: the estimator is unbiased).
+    """
+    sd_plain, sd_cv, exact = subsample_variances(cv, parts, walkers, fraction=fraction, trials=trials, seed=seed)
+    y = parts.exchange_term(walkers)
+    wt = walkers.weight.double()
+    pred = cv.predict(parts.feat, parts.base).double()
+    full_c = float((wt * pred).sum().item())
+    rng = np.random.default_rng(seed + 1)
+    W = walkers.nwalkers
+    S = max(1, W // fraction)
+    diffs = []
+    for _ in range(trials):
+        idx = torch.from_numpy(rng.choice(W, S, replace=False)).to(walkers.device)
+        est = full_c + (W / S) * float((wt[idx] * (y[idx] - pred[idx])).sum().item())
+        diffs.append(est - exact)
+    wsum = float(wt.sum().item())
+    d = np.asarray(diffs) / wsum * 1e3
+    return {"noise_mEh": float(d.std()), "plain_subsample_noise_mEh": sd_plain / wsum * 1e3,
+            "mean_diff_mEh": float(d.mean()), "mean_diff_stderr_mEh": float(d.std() / np.sqrt(trials)),
+            "fraction": fraction, "trials": trials}

@@ -98,9 +98,29 @@ int ipie_b200_reortho(void* phia, void* phib, int W, int M, int na, int nb, cons
 }
 
 int ipie_b200_walker_copy(const int* src, int W, int M, int na, int nb, void* phia, void* phib, double* weight,
-                          double* unscaled_weight, void* hybrid_energy, void* ovlp, void* phase, void* stream) {
+                          double* unscaled_weight, void* hybrid_energy, void* ovlp, void* phase, void* ghalfa,
+                          void* ghalfb, void* stream) {
   return (int)launch_walker_copy(src, W, M, na, nb, C2(phia), C2(phib), weight, unscaled_weight, C2(hybrid_energy),
-                                 C2(ovlp), C2(phase), ST(stream));
+                                 C2(ovlp), C2(phase), C2(ghalfa), C2(ghalfb), ST(stream));
+}
+
+int ipie_b200_walker_gather(const int* src, int W, int M, int na, int nb, const void* phia, const void* phib,
+                            const void* ghalfa, const void* ghalfb, const void* hybrid_energy, const void* ovlp,
+                            const void* phase, const double* unscaled_weight, void* phia_out, void* phib_out,
+                            void* ghalfa_out, void* ghalfb_out, void* hybrid_energy_out, void* ovlp_out,
+                            void* phase_out, double* unscaled_weight_out, void* stream) {
+  const bool alias_phi = phib == phia, alias_g = ghalfb == ghalfa;
+  if ((nb > 0 && !alias_phi && (phib == nullptr || phib_out == nullptr)) || phia == phia_out ||
+      (!alias_phi && phib != nullptr && phib == phib_out) || (ghalfa != nullptr && ghalfa == ghalfa_out) ||
+      (phase != nullptr && phase_out == nullptr) || (ghalfa != nullptr && ghalfa_out == nullptr) ||
+      (ghalfb != nullptr && !alias_g && ghalfb_out == nullptr))
+    return (int)cudaErrorInvalidValue;
+  using D = double2*;
+  WalkerArrays in{(D)phia, (D)phib, (D)ghalfa, (D)ghalfb, (D)hybrid_energy, (D)ovlp, (D)phase,
+                  const_cast<double*>(unscaled_weight)};
+  WalkerArrays out{(D)phia_out, (D)phib_out, (D)ghalfa_out, (D)ghalfb_out, (D)hybrid_energy_out, (D)ovlp_out,
+                   (D)phase_out, unscaled_weight_out};
+  return (int)launch_walker_gather(src, W, M, na, nb, in, out, ST(stream));
 }
 
 int ipie_b200_exchange_rows(int W, int X, int M, int N) {

@@ -22,7 +22,14 @@ cudaError_t launch_reortho(double2* phia, double2* phib, int W, int M, int na, i
                            double* detR, double* log_detR, double2* ovlp, unsigned* status, cudaStream_t st);
 cudaError_t launch_walker_copy(const int* src, int W, int M, int na, int nb, double2* phia, double2* phib,
                                double* weight, double* unscaled_weight, double2* ehyb, double2* ovlp, double2* phase,
-                               cudaStream_t st);
+                               double2* ghalfa, double2* ghalfb, cudaStream_t st);
+// per-walker arrays moved by the out-of-place resampling gather
+struct WalkerArrays {
+  double2 *phia, *phib, *ghalfa, *ghalfb, *ehyb, *ovlp, *phase;
+  double* unscaled_weight;
+};
+cudaError_t launch_walker_gather(const int* src, int W, int M, int na, int nb, const WalkerArrays& in,
+                                 const WalkerArrays& out, cudaStream_t st);
 cudaError_t launch_energy_combine(int W, int X, int Ka, int Kb, const double2* ga, const double2* gb,
                                   const double2* rh1a, const double2* rh1b, double ecore, const double2* xv,
                                   const double2* exx_part, int ntiles, double f1, double fc, double fx, double2* energy,

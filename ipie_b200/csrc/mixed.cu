@@ -41,17 +41,14 @@ cudaError_t make_map(CUtensorMap* m, const float* base, long long rows, long lon
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-// hi = TF32(x) (round to nearest), lo = float(x - hi): the split of the 3-pass product.
+// hi = TF32(x), lo = TF32(x - hi) (both rounded to nearest): the split of the 3-pass product.
 __global__ void split_tf32_kernel(const double* __restrict__ x, float* __restrict__ hi, float* __restrict__ lo,
                                   long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const double v = x[i];
-    uint32_t h;
-    const float f = (float)v;
-    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(f));
-    const float hf = __uint_as_float(h);
-    hi[i] = hf;
-    if (lo) lo[i] = (float)(v - (double)hf);
+    float h, l;
+    split_tf32(x[i], h, l);
+    hi[i] = h;
+    if (lo) lo[i] = l;
   }
 }
 
@@ -138,7 +135,8 @@ extern "C" int ipie_b200_umma_gemm_test(const float* a0_hi, const float* a0_lo, 
 namespace ipie_b200 {
 namespace umma {
 
-__device__ __forceinline__ void store_split(float* hi, float* lo, size_t i, float x) {
+template <typename T>
+__device__ __forceinline__ void store_split(float* hi, float* lo, size_t i, T x) {
   float h, l;
   split_tf32(x, h, l);
   hi[i] = h;
@@ -211,8 +209,9 @@ enum OrbMode { ORB_PRE = 0, ORB_TERM = 1, ORB_TERM_LAST = 2, ORB_POST = 3 };
 
 template <int NA, int BN>
 struct EpiOrbital {
-  double2* phi_acc;   // (W, M, N) complex double
-  float* nb_hi;       // next right operand (W, 2N, M) fp32 hi/lo
+  const double2* phi_base;  // one-body modes: phi_out = phi_base + (E - I) phi (FP64 add)
+  double2* phi_acc;         // (W, M, N) complex double
+  float* nb_hi;             // next right operand (W, 2N, M) fp32 hi/lo
   float* nb_lo;
   int M, N;
   float inv_n;
@@ -230,12 +229,16 @@ struct EpiOrbital {
       }
       const size_t pi = ((size_t)w * M + m) * N + n;
       const size_t bre = ((size_t)w * 2 * N + n) * M + m, bim = ((size_t)w * 2 * N + N + n) * M + m;
-      if (mode == ORB_PRE) {
-        phi_acc[pi] = make_double2(ur, ui);
-        store_split(nb_hi, nb_lo, bre, ur);
-        store_split(nb_hi, nb_lo, bim, ui);
-      } else if (mode == ORB_POST) {
-        phi_acc[pi] = make_double2(ur, ui);
+      if (mode == ORB_PRE || mode == ORB_POST) {
+        // the one-body factor is applied as phi + (E - I) phi: the identity part stays exact in
+        // FP64 and the TF32 product only carries the small correction
+        const double2 b = phi_base[pi];
+        const double2 out = make_double2(b.x + (double)ur, b.y + (double)ui);
+        phi_acc[pi] = out;
+        if (mode == ORB_PRE) {
+          store_split(nb_hi, nb_lo, bre, out.x);
+          store_split(nb_hi, nb_lo, bim, out.y);
+        }
       } else {
         const float tr = ur * inv_n, ti = ui * inv_n;
         double2 acc = phi_acc[pi];
@@ -246,8 +249,8 @@ struct EpiOrbital {
           store_split(nb_hi, nb_lo, bre, tr);
           store_split(nb_hi, nb_lo, bim, ti);
         } else {
-          store_split(nb_hi, nb_lo, bre, (float)acc.x);
-          store_split(nb_hi, nb_lo, bim, (float)acc.y);
+          store_split(nb_hi, nb_lo, bre, acc.x);
+          store_split(nb_hi, nb_lo, bim, acc.y);
         }
       }
     }
@@ -265,8 +268,8 @@ __global__ void phi_to_planar_kernel(const double2* __restrict__ phi, int W, int
     const int n = (int)(t % N);
     const int w = (int)(t / N);
     const double2 z = phi[((size_t)w * M + m) * N + n];
-    store_split(hi, lo, ((size_t)w * 2 * N + n) * M + m, (float)z.x);
-    store_split(hi, lo, ((size_t)w * 2 * N + N + n) * M + m, (float)z.y);
+    store_split(hi, lo, ((size_t)w * 2 * N + n) * M + m, z.x);
+    store_split(hi, lo, ((size_t)w * 2 * N + N + n) * M + m, z.y);
   }
 }
 
@@ -343,17 +346,17 @@ __global__ void rchol_pad_split_kernel(const double* __restrict__ r, int X, int 
     const int i = (int)(t % NP);
     const long long x = t / NP;
     const double val = i < N ? r[(x * N + i) * M + m] : 0.0;
-    uint32_t h;
-    const float f = (float)val;
-    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(f));
-    hi[e] = __uint_as_float(h);
-    lo[e] = (float)(val - (double)__uint_as_float(h));
+    float h, l;
+    split_tf32(val, h, l);
+    hi[e] = h;
+    lo[e] = l;
   }
 }
 
 // Ghalf (W, N, M) complex double -> planar padded (W, 2, NP, M) fp32 hi/lo, zero rows j >= N.
-__global__ void ghalf_pad_split_kernel(const double2* __restrict__ g, int W, int N, int M, int NP, float* __restrict__ hi,
-                                       float* __restrict__ lo) {
+// With gref (N, M) given, the split operand is Ghalf - gref (the deviation from the trial).
+__global__ void ghalf_pad_split_kernel(const double2* __restrict__ g, const double2* __restrict__ gref, int W, int N,
+                                       int M, int NP, float* __restrict__ hi, float* __restrict__ lo) {
   const long long total = (long long)W * 2 * NP * M;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
     const int m = (int)(e % M);
@@ -364,14 +367,18 @@ __global__ void ghalf_pad_split_kernel(const double2* __restrict__ g, int W, int
     const long long w = t / 2;
     double val = 0.0;
     if (j < N) {
-      const double2 z = g[(w * N + j) * M + m];
+      double2 z = g[(w * N + j) * M + m];
+      if (gref != nullptr) {
+        const double2 r = gref[(size_t)j * M + m];
+        z.x -= r.x;
+        z.y -= r.y;
+      }
       val = c ? z.y : z.x;
     }
-    uint32_t h;
-    const float f = (float)val;
-    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(f));
-    hi[e] = __uint_as_float(h);
-    lo[e] = (float)(val - (double)__uint_as_float(h));
+    float h, l;
+    split_tf32(val, h, l);
+    hi[e] = h;
+    lo[e] = l;
   }
 }
 
@@ -387,8 +394,35 @@ cudaError_t mixed_rchol_pad(const double* rchol, int X, int N, int M, float* hi,
 
 // Padded planar Green's function (TF32 head/remainder) of one spin block.
 static cudaError_t pad_ghalf(const double2* ghalf, int W, int M, int N, int NP, float* g_hi, float* g_lo,
-                             cudaStream_t st) {
-  ghalf_pad_split_kernel<<<grid_for((long long)W * 2 * NP * M), 256, 0, st>>>(ghalf, W, N, M, NP, g_hi, g_lo);
+                             cudaStream_t st, const double2* gref = nullptr) {
+  ghalf_pad_split_kernel<<<grid_for((long long)W * 2 * NP * M), 256, 0, st>>>(ghalf, gref, W, N, M, NP, g_hi, g_lo);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// Reference row of the exchange around the trial: with T linear in Ghalf,
+//   raw(G) = sum_x tr(T_G T_G) = raw(G_T) + K.(G - G_T) + raw(G - G_T),
+// K = d raw/dG at the trial.  out[w] = raw(G_T) + sum K (G_w - G_T) in FP64; the
+// quadratic remainder raw(G - G_T) is the tensor-core part.  One CTA per walker.
+__global__ void __launch_bounds__(256) exchange_ref_row_kernel(const double2* __restrict__ g,
+                                                               const double2* __restrict__ gref,
+                                                               const double2* __restrict__ kmat, int NM,
+                                                               const double2* __restrict__ raw_ref,
+                                                               double2* __restrict__ out) {
+  __shared__ double2 red[32];
+  const int w = blockIdx.x;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int e = threadIdx.x; e < NM; e += blockDim.x) {
+    const double2 a = g[(size_t)w * NM + e], r = gref[e];
+    acc = cadd(acc, cmul(kmat[e], make_double2(a.x - r.x, a.y - r.y)));
+  }
+  acc = block_sum2(acc, red);
+  if (threadIdx.x == 0) out[w] = cadd(acc, raw_ref[0]);
+}
+
+static cudaError_t exchange_ref_row(const double2* g, const double2* gref, const double2* kmat, int W, int NM,
+                                    const double2* raw_ref, double2* out, cudaStream_t st) {
+  exchange_ref_row_kernel<<<W, 256, 0, st>>>(g, gref, kmat, NM, raw_ref, out);
   note_launch();
   return cudaGetLastError();
 }
@@ -458,7 +492,7 @@ cudaError_t mixed_vhs(const float* cp_hi, const float* cp_lo, const int* ii, con
 
 // Orbital update of one spin block: phi_out = E exp(V) E phi_in (Taylor order nmax),
 // every product on the tensor cores as 3-pass TF32; phi accumulates in FP64.
-// E: expH1 hi/lo (M, Mp) fp32 with Mp % 4 == 0; V: planar (W, M, M) hi/lo;
+// E enters as its difference from the identity: (E - I) hi/lo (M, Mp) fp32 with Mp % 4 == 0; V: planar (W, M, M) hi/lo;
 // b0/b1: two (W, 2N, M) fp32 hi/lo ping-pong buffers (4 arrays).
 cudaError_t mixed_orbitals(const float* e_hi, const float* e_lo, int Mp, const float* v_re_hi, const float* v_re_lo,
                            const float* v_im_hi, const float* v_im_lo, const double2* phi_in, double2* phi_out,
@@ -483,7 +517,7 @@ cudaError_t mixed_orbitals(const float* e_hi, const float* e_lo, int Mp, const f
     if ((r = make_map(&maps.a_lo[0], e_lo, M, M, Mp, kBM)) != cudaSuccess) return r;
     if ((r = make_map(&maps.b_hi, bh[cur], (long long)W * brows, M, M, BN)) != cudaSuccess) return r;
     if ((r = make_map(&maps.b_lo, bl[cur], (long long)W * brows, M, M, BN)) != cudaSuccess) return r;
-    EpiOrbital<1, BN> epi{phi_out, bh[cur ^ 1], bl[cur ^ 1], M, N, 1.0f, mode};
+    EpiOrbital<1, BN> epi{mode == ORB_PRE ? phi_in : phi_out, phi_out, bh[cur ^ 1], bl[cur ^ 1], M, N, 1.0f, mode};
     r = launch_umma<BN, 1, 3, 3>(maps, M, 0, brows, grid, epi, status, st);
     cur ^= 1;
     return r;
@@ -498,7 +532,8 @@ cudaError_t mixed_orbitals(const float* e_hi, const float* e_lo, int Mp, const f
     if ((e = make_map(&maps.a_lo[1], v_im_lo, (long long)W * M, M, M, kBM)) != cudaSuccess) return e;
     if ((e = make_map(&maps.b_hi, bh[cur], (long long)W * brows, M, M, BN)) != cudaSuccess) return e;
     if ((e = make_map(&maps.b_lo, bl[cur], (long long)W * brows, M, M, BN)) != cudaSuccess) return e;
-    EpiOrbital<2, BN> epi{phi_out, bh[cur ^ 1], bl[cur ^ 1], M, N, 1.0f / n, n == nmax ? ORB_TERM_LAST : ORB_TERM};
+    EpiOrbital<2, BN> epi{nullptr, phi_out, bh[cur ^ 1], bl[cur ^ 1], M, N, 1.0f / n,
+                          n == nmax ? ORB_TERM_LAST : ORB_TERM};
     if ((e = launch_umma<BN, 2, 3, 2>(maps, M, M, brows, grid, epi, status, st)) != cudaSuccess) return e;
     cur ^= 1;
   }
@@ -564,11 +599,17 @@ extern "C" int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int 
 extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const float* ra_hi,
                                             const float* ra_lo, const float* rb_hi, const float* rb_lo,
                                             const void* rH1a, const void* rH1b, double ecore, const void* ghalfa,
-                                            const void* ghalfb, int W, int X, int M, int na, int nb, float* gwork,
+                                            const void* ghalfb, const void* ghalf_trial_a,
+                                            const void* ghalf_trial_b, const void* kmat_a, const void* kmat_b,
+                                            const void* raw_trial, int W, int X, int M, int na, int nb, float* gwork,
                                             void* work, void* energy, unsigned int* status, void* stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const bool alias = !rhf && nb == na && nb > 0 && rb_hi == ra_hi && ghalfb == ghalfa;
   const int use_b = (!rhf && nb > 0 && !alias);
+  const bool delta = ghalf_trial_a != nullptr;
+  if (delta && (kmat_a == nullptr || raw_trial == nullptr || (use_b && (ghalf_trial_b == nullptr || kmat_b == nullptr))))
+    return (int)cudaErrorInvalidValue;
+  using CC = const double2*;
   double2* xv = reinterpret_cast<double2*>(work);
   double2* part = xv + (size_t)W * X;
   const int NPa = umma::exchange_np(na), NPb = nb > 0 ? umma::exchange_np(nb) : 8;
@@ -581,17 +622,27 @@ extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const
   if (e == cudaSuccess && use_b)
     e = launch_force_bias(rcholb, reinterpret_cast<const double2*>(ghalfb), W, X, nb * M, xv, 1, st);
   if (e != cudaSuccess) return (int)e;
-  // exchange: 3-pass TF32 tensor-core products, bilinear sums in FP64
-  e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfa), W, M, na, NPa, g_hi, g_lo, st);
+  // exchange: 3-pass TF32 tensor-core products (of G - G_T when the trial reference is given),
+  // bilinear sums in FP64; the reference row adds raw(G_T) + K.(G - G_T) in FP64
+  e = umma::pad_ghalf((CC)ghalfa, W, M, na, NPa, g_hi, g_lo, st, delta ? (CC)ghalf_trial_a : nullptr);
   if (e == cudaSuccess) e = umma::exchange3(ra_hi, ra_lo, g_hi, g_lo, W, X, M, na, part, status, st);
   if (e != cudaSuccess) return (int)e;
-  const int rows_a = umma::exchange3_rows(X, na);
-  int rows_b = 0;
+  int rows = umma::exchange3_rows(X, na);
   if (use_b) {
-    rows_b = umma::exchange3_rows(X, nb);
-    e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfb), W, M, nb, NPb, g_hi, g_lo, st);
-    if (e == cudaSuccess)
-      e = umma::exchange3(rb_hi, rb_lo, g_hi, g_lo, W, X, M, nb, part + (size_t)rows_a * W, status, st);
+    e = umma::pad_ghalf((CC)ghalfb, W, M, nb, NPb, g_hi, g_lo, st, delta ? (CC)ghalf_trial_b : nullptr);
+    if (e == cudaSuccess) e = umma::exchange3(rb_hi, rb_lo, g_hi, g_lo, W, X, M, nb, part + (size_t)rows * W, status, st);
+    if (e != cudaSuccess) return (int)e;
+    rows += umma::exchange3_rows(X, nb);
+  }
+  if (delta) {
+    e = umma::exchange_ref_row((CC)ghalfa, (CC)ghalf_trial_a, (CC)kmat_a, W, na * M, (CC)raw_trial,
+                               part + (size_t)rows * W, st);
+    rows += 1;
+    if (e == cudaSuccess && use_b) {
+      e = umma::exchange_ref_row((CC)ghalfb, (CC)ghalf_trial_b, (CC)kmat_b, W, nb * M, (CC)raw_trial + 1,
+                                 part + (size_t)rows * W, st);
+      rows += 1;
+    }
     if (e != cudaSuccess) return (int)e;
   }
   const double f1 = rhf ? 2.0 : 1.0, fc = rhf ? 2.0 : 0.5, fx = (rhf || alias) ? 1.0 : 0.5;
@@ -599,6 +650,5 @@ extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const
   return (int)launch_energy_combine(W, X, na * M, nb * M, reinterpret_cast<const double2*>(ghalfa),
                                     e1_b ? reinterpret_cast<const double2*>(ghalfb) : nullptr,
                                     reinterpret_cast<const double2*>(rH1a), reinterpret_cast<const double2*>(rH1b),
-                                    ecore, xv, part, rows_a + rows_b, f1, fc, fx, reinterpret_cast<double2*>(energy),
-                                    status, st);
+                                    ecore, xv, part, rows, f1, fc, fx, reinterpret_cast<double2*>(energy), status, st);
 }

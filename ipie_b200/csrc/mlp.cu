@@ -215,14 +215,36 @@ cudaError_t mlp_adam(float* master, __nv_bfloat16* wbf, const float* g, float* m
 // 11    sum |Ghalf|^2     12,13 Re/Im sum_i Ghalf[i, :] . psi*[:, i] (trial projection)
 // 14    sum |Ghalf - Ghalf_T|^2 (distance from the trial density)   15  weight
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) cv_features_kernel(int W, int X, int N, int M, const double2* __restrict__ energy,
+// Per-spin sums of one walker's half-rotated Green's function G against the
+// trial's G_T and the exchange gradient K at the trial:
+//   (|G|^2, |G - G_T|^2) and lin = sum K (G - G_T)  (complex, no conjugation).
+__device__ __forceinline__ void cv_spin_sums(const double2* __restrict__ g, const double2* __restrict__ gt,
+                                             const double2* __restrict__ kmat, int NM, double2& g2, double2& lin) {
+  for (int e = threadIdx.x; e < NM; e += blockDim.x) {
+    const double2 a = g[e], t = gt[e];
+    const double dx = a.x - t.x, dy = a.y - t.y;
+    g2.x += a.x * a.x + a.y * a.y;
+    g2.y += dx * dx + dy * dy;
+    lin = cadd(lin, cmul(kmat[e], make_double2(dx, dy)));
+  }
+}
+
+// One CTA per walker.  base[w] = Re(lin): the first-order change of the
+// exchange term y = 1/2 Re(raw_a + raw_b) away from its trial value.
+__global__ void __launch_bounds__(256) cv_features_kernel(int W, int X, int na, int nb, int M, bool alias,
+                                                          const double2* __restrict__ energy,
                                                           const double2* __restrict__ xv,
                                                           const double2* __restrict__ ovlp,
                                                           const double2* __restrict__ ehyb,
-                                                          const double2* __restrict__ ghalf,
-                                                          const double2* __restrict__ psi_c,
-                                                          const double2* __restrict__ ghalf_t,
-                                                          const double* __restrict__ weight, float* __restrict__ feat) {
+                                                          const double2* __restrict__ ghalfa,
+                                                          const double2* __restrict__ ghalfb,
+                                                          const double2* __restrict__ gta,
+                                                          const double2* __restrict__ gtb,
+                                                          const double2* __restrict__ ka,
+                                                          const double2* __restrict__ kb,
+                                                          const double* __restrict__ weight,
+                                                          const double* __restrict__ lead, float* __restrict__ feat,
+                                                          double* __restrict__ base) {
   __shared__ double2 red[32];
   const int w = blockIdx.x;
   double2 sx = make_double2(0.0, 0.0);  // (sum |X|^2, sum (Re X)^2)
@@ -231,20 +253,21 @@ __global__ void __launch_bounds__(256) cv_features_kernel(int W, int X, int N, i
     sx.x += v.x * v.x + v.y * v.y;
     sx.y += v.x * v.x;
   }
-  double2 g2 = make_double2(0.0, 0.0), pr = make_double2(0.0, 0.0);  // (|G|^2, |G - G_T|^2), projection
-  const double2* g = ghalf + (size_t)w * N * M;
-  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
-    const double2 a = g[e], t = ghalf_t[e];
-    g2.x += a.x * a.x + a.y * a.y;
-    const double dx = a.x - t.x, dy = a.y - t.y;
-    g2.y += dx * dx + dy * dy;
-    const int i = e / M, m = e % M;
-    pr = cadd(pr, cmul(a, psi_c[(size_t)m * N + i]));
-  }
+  double2 g2a = make_double2(0.0, 0.0), lina = make_double2(0.0, 0.0);
+  double2 g2b = make_double2(0.0, 0.0), linb = make_double2(0.0, 0.0);
+  cv_spin_sums(ghalfa + (size_t)w * na * M, gta, ka, na * M, g2a, lina);
+  if (nb > 0 && !alias) cv_spin_sums(ghalfb + (size_t)w * nb * M, gtb, kb, nb * M, g2b, linb);
   sx = block_sum2(sx, red);
-  g2 = block_sum2(g2, red);
-  pr = block_sum2(pr, red);
+  g2a = block_sum2(g2a, red);
+  lina = block_sum2(lina, red);
+  g2b = block_sum2(g2b, red);
+  linb = block_sum2(linb, red);
   if (threadIdx.x == 0) {
+    // alias: both blocks are spin a (y = raw_a); otherwise y = (raw_a + raw_b) / 2
+    const double fa = alias ? 1.0 : 0.5;
+    const double2 lin = make_double2(fa * lina.x + 0.5 * linb.x, fa * lina.y + 0.5 * linb.y);
+    const double g2 = alias ? 2.0 * g2a.x : g2a.x + g2b.x;
+    const double d2 = alias ? 2.0 * g2a.y : g2a.y + g2b.y;
     float* f = feat + (size_t)w * 16;
     const double2 e1 = energy[(size_t)w * 3 + 1], e2 = energy[(size_t)w * 3 + 2];
     const double2 o = ovlp[w], h = ehyb[w];
@@ -260,11 +283,12 @@ __global__ void __launch_bounds__(256) cv_features_kernel(int W, int X, int N, i
     f[8] = ao > 0 ? (float)log(ao) : 0.f;
     f[9] = (float)h.x;
     f[10] = (float)h.y;
-    f[11] = (float)g2.x;
-    f[12] = (float)pr.x;
-    f[13] = (float)pr.y;
-    f[14] = (float)g2.y;
-    f[15] = (float)weight[w];
+    f[11] = (float)g2;
+    f[12] = (float)lin.x;
+    f[13] = (float)lin.y;
+    f[14] = (float)d2;
+    f[15] = lead != nullptr ? (float)lead[w] : (float)weight[w];
+    base[w] = lin.x;
   }
 }
 
@@ -373,14 +397,19 @@ int ipie_b200_mlp_adam(float* master, void* wbf, const float* grad, float* m, fl
                        reinterpret_cast<cudaStream_t>(stream));
 }
 
-int ipie_b200_cv_features(int W, int X, int N, int M, const void* energy, const void* xv, const void* ovlp,
-                          const void* hybrid_energy, const void* ghalf, const void* psi_conj, const void* ghalf_trial,
-                          const double* weight, float* feat, void* stream) {
+int ipie_b200_cv_features(int W, int X, int na, int nb, int M, const void* energy, const void* xv, const void* ovlp,
+                          const void* hybrid_energy, const void* ghalfa, const void* ghalfb, const void* ghalf_trial_a,
+                          const void* ghalf_trial_b, const void* kmat_a, const void* kmat_b, const double* weight,
+                          const double* lead, float* feat, double* base, void* stream) {
+  const bool alias = nb == na && nb > 0 && ghalfb == ghalfa;
+  if (nb > 0 && !alias && (ghalfb == nullptr || ghalf_trial_b == nullptr || kmat_b == nullptr))
+    return (int)cudaErrorInvalidValue;
+  using C = const double2*;
   cv_features_kernel<<<W, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      W, X, N, M, reinterpret_cast<const double2*>(energy), reinterpret_cast<const double2*>(xv),
-      reinterpret_cast<const double2*>(ovlp), reinterpret_cast<const double2*>(hybrid_energy),
-      reinterpret_cast<const double2*>(ghalf), reinterpret_cast<const double2*>(psi_conj),
-      reinterpret_cast<const double2*>(ghalf_trial), weight, feat);
+      W, X, na, nb, M, alias, reinterpret_cast<C>(energy), reinterpret_cast<C>(xv), reinterpret_cast<C>(ovlp),
+      reinterpret_cast<C>(hybrid_energy), reinterpret_cast<C>(ghalfa), reinterpret_cast<C>(ghalfb),
+      reinterpret_cast<C>(ghalf_trial_a), reinterpret_cast<C>(ghalf_trial_b), reinterpret_cast<C>(kmat_a),
+      reinterpret_cast<C>(kmat_b), weight, lead, feat, base);
   note_launch();
   return (int)cudaGetLastError();
 }

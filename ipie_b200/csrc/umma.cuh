@@ -132,15 +132,27 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "memory");
 }
 
-// Split x into a TF32 head and the remainder: x ~= hi + lo with hi exactly
-// representable in TF32 (10 explicit mantissa bits, round to nearest) and lo
-// the rounding error, so hi*y_hi + hi*y_lo + lo*y_hi carries ~2^-22 relative
-// accuracy when the tensor core reads each operand as TF32.
-__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+// Round to the nearest TF32 value (10 explicit mantissa bits), kept in an FP32 register.
+__device__ __forceinline__ float round_tf32(float x) {
   uint32_t h;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(x));
-  hi = __uint_as_float(h);
-  lo = x - hi;
+  return __uint_as_float(h);
+}
+
+// Split x into a TF32 head and a TF32 remainder: x ~= hi + lo to ~2^-22
+// relative, so hi*y_hi + hi*y_lo + lo*y_hi carries ~2^-22 relative accuracy.
+// Both parts are rounded here rather than left to the tensor core, which is not
+// specified to round an FP32 operand it reads as TF32 (dropping the low 13
+// mantissa bits would bias every product toward zero by ~2^-22 relative).
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+  hi = round_tf32(x);
+  lo = round_tf32(x - hi);
+}
+
+// Split of a double: hi + lo carries ~2^-22 relative accuracy of x itself.
+__device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
+  hi = round_tf32((float)x);
+  lo = round_tf32((float)(x - (double)hi));
 }
 
 }  // namespace umma

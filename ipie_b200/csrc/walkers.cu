@@ -235,13 +235,16 @@ cudaError_t launch_gf_overlap(const double2* phia, const double2* phib, int W, i
 //   xs = xi - xbar;  cmf = -sqrt(dt) sum_x xs mf;  cfb = sum_x xi xbar - xbar^2/2
 // One CTA per 32 walkers; the (X, W) transposed store goes through smem.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void split_store_tf32(float* hi, float* lo, size_t i, double x) {
+// TF32 head and TF32 remainder of x, both rounded to nearest (the 3-pass operand split)
+__device__ __forceinline__ float round_to_tf32(float x) {
   uint32_t h;
-  const float f = (float)x;
-  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(f));
-  const float hf = __uint_as_float(h);
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(x));
+  return __uint_as_float(h);
+}
+__device__ __forceinline__ void split_store_tf32(float* hi, float* lo, size_t i, double x) {
+  const float hf = round_to_tf32((float)x);
   hi[i] = hf;
-  lo[i] = (float)(x - (double)hf);
+  lo[i] = round_to_tf32((float)(x - (double)hf));
 }
 
 // xs_hi/xs_lo (optional): the shifted fields as planar (W, 2, X) fp32 TF32 head/remainder,
@@ -447,7 +450,7 @@ cudaError_t launch_reortho(double2* phia, double2* phib, int W, int M, int na, i
 // ---------------------------------------------------------------------------
 __global__ void walker_copy_kernel(const int* __restrict__ src, int W, int M, int na, int nb, double2* phia,
                                    double2* phib, double* weight, double* unscaled_weight, double2* ehyb,
-                                   double2* ovlp, double2* phase) {
+                                   double2* ovlp, double2* phase, double2* ghalfa, double2* ghalfb) {
   const int dst = blockIdx.x;
   const int s = src[dst];
   if (s < 0 || s == dst) return;
@@ -455,6 +458,11 @@ __global__ void walker_copy_kernel(const int* __restrict__ src, int W, int M, in
   for (size_t e = threadIdx.x; e < sa; e += blockDim.x) phia[dst * sa + e] = phia[s * sa + e];
   if (phib != phia)
     for (size_t e = threadIdx.x; e < sb; e += blockDim.x) phib[dst * sb + e] = phib[s * sb + e];
+  // Green's functions travel with the orbitals (they are functions of them)
+  if (ghalfa != nullptr)
+    for (size_t e = threadIdx.x; e < sa; e += blockDim.x) ghalfa[dst * sa + e] = ghalfa[s * sa + e];
+  if (ghalfb != nullptr && ghalfb != ghalfa)
+    for (size_t e = threadIdx.x; e < sb; e += blockDim.x) ghalfb[dst * sb + e] = ghalfb[s * sb + e];
   if (threadIdx.x == 0) {
     weight[dst] = weight[s];
     unscaled_weight[dst] = unscaled_weight[s];
@@ -466,8 +474,40 @@ __global__ void walker_copy_kernel(const int* __restrict__ src, int W, int M, in
 
 cudaError_t launch_walker_copy(const int* src, int W, int M, int na, int nb, double2* phia, double2* phib,
                                double* weight, double* unscaled_weight, double2* ehyb, double2* ovlp, double2* phase,
-                               cudaStream_t st) {
-  walker_copy_kernel<<<W, 256, 0, st>>>(src, W, M, na, nb, phia, phib, weight, unscaled_weight, ehyb, ovlp, phase);
+                               double2* ghalfa, double2* ghalfb, cudaStream_t st) {
+  walker_copy_kernel<<<W, 256, 0, st>>>(src, W, M, na, nb, phia, phib, weight, unscaled_weight, ehyb, ovlp, phase,
+                                        ghalfa, ghalfb);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// Out-of-place resampling (stochastic reconfiguration): walker d of the output
+// arrays is walker src[d] of the input arrays, for every d; the weight is set by
+// the caller.  Sources may repeat, so the copy cannot run in place.
+
+__global__ void walker_gather_kernel(const int* __restrict__ src, int M, int na, int nb, WalkerArrays in,
+                                     WalkerArrays out) {
+  const int d = blockIdx.x;
+  const int s = src[d];
+  const size_t sa = (size_t)M * na, sb = (size_t)M * nb;
+  for (size_t e = threadIdx.x; e < sa; e += blockDim.x) out.phia[d * sa + e] = in.phia[s * sa + e];
+  if (in.phib != in.phia)
+    for (size_t e = threadIdx.x; e < sb; e += blockDim.x) out.phib[d * sb + e] = in.phib[s * sb + e];
+  if (in.ghalfa != nullptr)
+    for (size_t e = threadIdx.x; e < sa; e += blockDim.x) out.ghalfa[d * sa + e] = in.ghalfa[s * sa + e];
+  if (in.ghalfb != nullptr && in.ghalfb != in.ghalfa)
+    for (size_t e = threadIdx.x; e < sb; e += blockDim.x) out.ghalfb[d * sb + e] = in.ghalfb[s * sb + e];
+  if (threadIdx.x == 0) {
+    out.ehyb[d] = in.ehyb[s];
+    out.ovlp[d] = in.ovlp[s];
+    if (in.phase) out.phase[d] = in.phase[s];
+    out.unscaled_weight[d] = in.unscaled_weight[s];
+  }
+}
+
+cudaError_t launch_walker_gather(const int* src, int W, int M, int na, int nb, const WalkerArrays& in,
+                                 const WalkerArrays& out, cudaStream_t st) {
+  walker_gather_kernel<<<W, 256, 0, st>>>(src, M, na, nb, in, out);
   note_launch();
   return cudaGetLastError();
 }

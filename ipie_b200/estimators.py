@@ -62,11 +62,49 @@ def _mixed_energy_operands(trial, hamiltonian):
     return out
 
 
-def local_energy_mixed(system, hamiltonian, walkers, trial, rhf=False):
-    """Mixed-precision local energy: Coulomb and exchange as 3-pass TF32 tensor-core products."""
+def exchange_reference(trial, hamiltonian):
+    """Trial Ghalf_s, the exchange gradient K_s there and raw_s = sum_x tr(T_s T_s) (FP64, once per trial).
+
+    The mixed energy expands the exchange around the trial so that only the
+    deviation G - G_T passes through the tensor cores.
+    """
+    ref = getattr(trial, "_exchange_ref", None)
+    if ref is not None:
+        return ref
+    from .control_variate import exchange_gradient
+
+    dev = trial.device
+    X, M = hamiltonian.nchol, hamiltonian.nbasis
+    gts, ks = [], []
+    raw = torch.zeros(2, dtype=C128, device=dev)
+    for s_, (gh, rchol, n) in enumerate(((trial.Ghalf[0], trial._rchola, trial.nalpha),
+                                          (trial.Ghalf[1], trial._rcholb, trial.nbeta))):
+        if n == 0:
+            gts.append(None)
+            ks.append(None)
+            continue
+        if s_ == 1 and rchol is trial._rchola and np.array_equal(np.asarray(gh), np.asarray(trial.Ghalf[0])):
+            gts.append(gts[0])
+            ks.append(ks[0])
+            raw[1] = raw[0]
+            continue
+        g = torch.from_numpy(np.ascontiguousarray(np.asarray(gh).astype(np.complex128))).to(dev)
+        gts.append(g)
+        ks.append(exchange_gradient(rchol, g))
+        rows = lib().ipie_b200_exchange_rows(1, X, M, n)
+        part = torch.empty(rows, dtype=C128, device=dev)
+        call("ipie_b200_exchange", ptr(rchol), ptr(g), 1, X, M, n, ptr(part), stream())
+        raw[s_] = part.sum()
+    trial._exchange_ref = (gts, ks, raw)
+    return trial._exchange_ref
+
+
+def local_energy_mixed(system, hamiltonian, walkers, trial, rhf=False, reference=True):
+    """Mixed-precision local energy: the exchange as 3-pass TF32 tensor-core products
+    (around the trial when ``reference``), Coulomb and one-body in FP64."""
     W, X, M = walkers.nwalkers, hamiltonian.nchol, hamiltonian.nbasis
     (ra_hi, ra_lo), (rb_hi, rb_lo) = _mixed_energy_operands(trial, hamiltonian)
-    rows = 0
+    rows = 2
     for n in (walkers.nup, walkers.ndown):
         NP = 8 if n <= 8 else 16 if n <= 16 else 32
         rows += (X * NP + 127) // 128
@@ -77,9 +115,11 @@ def local_energy_mixed(system, hamiltonian, walkers, trial, rhf=False):
         walkers._energy_work_mixed = buf
         walkers._energy_gwork = torch.empty(2 * W * 2 * 32 * M, dtype=torch.float32, device=walkers.device)
     energy = torch.empty(W, 3, dtype=C128, device=walkers.device)
+    gts, ks, raw = exchange_reference(trial, hamiltonian) if reference else ((None, None), (None, None), None)
     call("ipie_b200_local_energy_mixed", int(rhf), ptr(trial._rchola), ptr(trial._rcholb), ptr(ra_hi), ptr(ra_lo),
          ptr(rb_hi), ptr(rb_lo), ptr(trial._rH1a),
-         ptr(trial._rH1b), hamiltonian.ecore, ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), W, X, M, walkers.nup,
+         ptr(trial._rH1b), hamiltonian.ecore, ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), ptr(gts[0]), ptr(gts[1]),
+         ptr(ks[0]), ptr(ks[1]), ptr(raw), W, X, M, walkers.nup,
          walkers.ndown, ptr(walkers._energy_gwork), ptr(buf), ptr(energy), ptr(walkers.status), stream())
     return energy
 
@@ -143,7 +183,9 @@ class EnergyEstimator:
         self.ascii_filename = filename
 
     def compute_estimator(self, system=None, walkers=None, hamiltonian=None, trial=None):
-        trial.calc_greens_function(walkers)
+        # ipie recomputes the Green's function here; it is skipped while the cached one is current
+        if not walkers.gf_current(trial):
+            trial.calc_greens_function(walkers)
         if self.precision == "mixed":
             energy = local_energy_mixed(system, hamiltonian, walkers, trial, rhf=walkers.rhf)
         else:

@@ -12,6 +12,21 @@ import numpy as np
 import torch
 
 
+def tiled_triu_indices(M, rows=8, cols=16):
+    """Upper-triangle (i <= j) pairs ordered by tiles of ``rows`` x ``cols``: consecutive packed
+    entries then cover a small square of the matrix, so the symmetric scatter of VHS writes
+    runs of ``cols`` (i, j) and ``rows`` (j, i) contiguous elements instead of single ones."""
+    ii, jj = [], []
+    for I in range(0, M, rows):
+        for J in range((I // cols) * cols, M, cols):
+            i = np.arange(I, min(I + rows, M))[:, None]
+            j = np.arange(J, min(J + cols, M))[None, :]
+            keep = j >= i
+            ii.append(np.broadcast_to(i, keep.shape)[keep])
+            jj.append(np.broadcast_to(j, keep.shape)[keep])
+    return np.concatenate(ii), np.concatenate(jj)
+
+
 class GenericRealChol:
     def __init__(self, h1e, chol, ecore=0.0, device="cuda", verbose=False):
         h1e = np.asarray(h1e)
@@ -28,16 +43,18 @@ class GenericRealChol:
         M, X = self.nbasis, self.nchol
         self.chol = np.ascontiguousarray(chol)  # host copy (set-up only)
         iu, ju = np.triu_indices(M)
-        self.sym_idx = (iu, ju)
-        packed = np.ascontiguousarray(self.chol.reshape(M, M, X)[iu, ju, :])
+        self.sym_idx = (iu, ju)  # ipie's packing order (host attribute)
+        # the device copy is packed in tiled order (same entries, see tiled_triu_indices)
+        ti, tj = tiled_triu_indices(M)
+        packed = np.ascontiguousarray(self.chol.reshape(M, M, X)[ti, tj, :])
         # h1e_mod = h1e - 1/2 sum_kn L_ik,n L_jk,n  (hamiltonians/generic.py:31-43)
         view = self.chol.reshape(M, M * X)
         v0 = 0.5 * view @ view.T
         self.h1e_mod = np.array([h1e[0] - v0, h1e[1] - v0])
         self.device = torch.device(device)
         self.chol_packed = torch.from_numpy(packed).to(self.device)
-        self.sym_idx_i = torch.from_numpy(iu.astype(np.int32)).to(self.device)
-        self.sym_idx_j = torch.from_numpy(ju.astype(np.int32)).to(self.device)
+        self.sym_idx_i = torch.from_numpy(ti.astype(np.int32)).to(self.device)
+        self.sym_idx_j = torch.from_numpy(tj.astype(np.int32)).to(self.device)
         if verbose:
             print(f"# nbasis {M}  nchol {X}  packed Cholesky {packed.nbytes / 1e9:.3f} GB on {self.device}")
 

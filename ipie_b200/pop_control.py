@@ -1,9 +1,12 @@
-"""Population control (pair branch) for a device-resident walker batch.
+"""Population control for a device-resident walker batch.
 
-Mirror of ipie's ``PopController`` (``walkers/pop_controller.py:33-125``) and
-``pair_branch`` (``:304-429``) on one process.  ipie runs the pairing on the
-host with one ``numpy.random.rand()`` per pair; that is kept so a run fed the
-same seed makes the same decisions.  The walker copies run on the device.
+Mirror of ipie's ``PopController`` (``walkers/pop_controller.py:33-125``) with
+its three methods on one process: ``pair_branch`` (``:304-429``), ``comb``
+(``:199-301``) and ``stochastic_reconfiguration`` (``:432-475``).  ipie
+decides on the host from the |w| vector with numpy's global generator (one
+``rand()`` per pair, one ``random()`` per comb, one ``rand()`` per
+reconfiguration); that is kept so a run fed the same seed makes the same
+decisions.  The walker copies run on the device.
 
 Single-process message semantics (``qmc/comm.py:61-71``): every send in
 ipie's pair branch carries the same tag (it is built from a rank index), and
@@ -53,12 +56,39 @@ def pair_branch_table(absw, max_weight, min_weight, rand=np.random.rand):
     return out_w, out_s
 
 
+def comb_parent_counts(weights, target_weight, r):
+    """Copies of each walker under the comb (``pop_controller.py:215-229``).
+
+    Teeth ``(i + r) * total / target`` for i < target; walker iw takes every tooth
+    in [cprobs[iw-1], cprobs[iw]), i.e. a right-sided search in the cumulative weights.
+    """
+    cprobs = np.cumsum(weights)
+    total = cprobs[-1]  # ipie's builtin sum: the same sequential sum
+    teeth = (np.arange(target_weight) + r) * (total / target_weight)
+    iw = np.minimum(np.searchsorted(cprobs, teeth, side="right"), len(weights) - 1)
+    return np.bincount(iw, minlength=len(weights)).astype(np.int64)
+
+
+def reconfiguration_sources(absw, zeta):
+    """Source walker of every slot under stochastic reconfiguration (``pop_controller.py:455-465``)."""
+    n = absw.size
+    cumulative = np.cumsum(absw)
+    total = cumulative[-1]
+    z = (np.arange(n) + zeta) / n / 1
+    return np.searchsorted(cumulative, z * total), total / n / 1
+
+
+METHODS = ("pair_branch", "comb", "stochastic_reconfiguration")
+
+
 class PopController:
     def __init__(self, num_walkers_local, num_steps, mpi_handler=None, pop_control_method="pair_branch",
                  min_weight=0.1, max_weight=4, reconfiguration_freq=50, verbose=False):
-        if pop_control_method != "pair_branch":
-            raise NotImplementedError(f"population control {pop_control_method!r}: only pair_branch is provided")
+        if pop_control_method not in METHODS:
+            raise NotImplementedError(f"population control {pop_control_method!r}: one of {METHODS}")
         self.method = pop_control_method
+        self.reconfiguration_counter = 0
+        self.reconfiguration_freq = reconfiguration_freq
         self.num_walkers_local = num_walkers_local
         self.num_steps = num_steps
         self.min_weight = min_weight
@@ -69,32 +99,78 @@ class PopController:
         self.total_weight = self.ntot_walkers
         self._src = None
 
-    def pop_control(self, walkers, comm=None, rand=np.random.rand):
-        """Rescale by total |w| / target, then pair branch (``pop_controller.py:78-125``)."""
+    def pop_control(self, walkers, comm=None, rand=None):
+        """Rescale by total |w| / target, then the configured method (``pop_controller.py:78-125``).
+
+        ``rand`` replaces numpy's global ``rand``/``random`` (tests replay draws with it).
+        """
         if self.ntot_walkers == 1:
             return
         w = walkers.weight.cpu().numpy()
-        total_weight = float(np.sum(np.abs(w)))
+        absw = np.abs(w)
+        if self.method == "comb":
+            total_weight = float(np.cumsum(absw)[-1])  # ipie: builtin sum of the gathered |w|
+        else:
+            total_weight = float(np.sum(absw))
         scale = total_weight / self.target_weight
         if total_weight < 1e-8:
             raise ValueError(f"Total weight is {total_weight:13.8e}: something is seriously wrong")
         self.total_weight = total_weight
         unscaled = w.copy()
         w = w / scale
+        walkers.unscaled_weight.copy_(torch.from_numpy(unscaled))
+        if self.method == "pair_branch":
+            return self._pair_branch(walkers, w, rand or np.random.rand)
+        if self.method == "comb":
+            return self._comb(walkers, w, absw / scale, rand or np.random.random)
+        walkers.weight.copy_(torch.from_numpy(w))
+        self.reconfiguration_counter += 1
+        if self.reconfiguration_counter % self.reconfiguration_freq == 0:
+            self.reconfiguration_counter = 0
+            return self._reconfigure(walkers, np.abs(w), rand or np.random.rand)
+
+    def _copy(self, walkers, src):
+        if self._src is None or self._src.numel() != walkers.nwalkers:
+            self._src = torch.empty(walkers.nwalkers, dtype=torch.int32, device=walkers.device)
+        self._src.copy_(torch.from_numpy(src.astype(np.int32)))
+        call("ipie_b200_walker_copy", ptr(self._src), walkers.nwalkers, walkers.nbasis, walkers.nup, walkers.ndown,
+             ptr(walkers.phia), ptr(walkers.phib), ptr(walkers.weight), ptr(walkers.unscaled_weight),
+             ptr(walkers.hybrid_energy), ptr(walkers.ovlp), ptr(walkers.phase), ptr(walkers.Ghalfa),
+             ptr(walkers.Ghalfb), stream())
+
+    def _pair_branch(self, walkers, w, rand):
         neww, status = pair_branch_table(np.abs(w), self.max_weight, self.min_weight, rand)
         cloned = np.nonzero(status == 2)[0]
         killed = np.nonzero(status == 0)[0]
         w[cloned] = neww[cloned]
-        src = np.full(walkers.nwalkers, -1, dtype=np.int32)
-        if cloned.size:
-            src[killed] = cloned.max()
-        walkers.unscaled_weight.copy_(torch.from_numpy(unscaled))
         walkers.weight.copy_(torch.from_numpy(w))
         if killed.size:
-            if self._src is None or self._src.numel() != walkers.nwalkers:
-                self._src = torch.empty(walkers.nwalkers, dtype=torch.int32, device=walkers.device)
-            self._src.copy_(torch.from_numpy(src))
-            call("ipie_b200_walker_copy", ptr(self._src), walkers.nwalkers, walkers.nbasis, walkers.nup, walkers.ndown,
-                 ptr(walkers.phia), ptr(walkers.phib), ptr(walkers.weight), ptr(walkers.unscaled_weight),
-                 ptr(walkers.hybrid_energy), ptr(walkers.ovlp), ptr(walkers.phase), stream())
+            src = np.full(walkers.nwalkers, -1, dtype=np.int32)
+            if cloned.size:
+                src[killed] = cloned.max()
+            self._copy(walkers, src)
         return neww, status
+
+    def _comb(self, walkers, w, global_weights, rand):
+        """Walker kill[i] <- clone[i] (pairs zipped in index order), then every weight is 1."""
+        parent = comb_parent_counts(global_weights, self.target_weight, rand())
+        kill = np.where(parent == 0)[0]
+        clone = np.where(parent > 1)[0]
+        walkers.weight.copy_(torch.from_numpy(w))
+        src = np.full(walkers.nwalkers, -1, dtype=np.int32)
+        for c, k in zip(clone, kill):
+            src[k] = c
+        if (src >= 0).any():
+            self._copy(walkers, src)
+        walkers.weight.fill_(1.0)
+        return parent
+
+    def _reconfigure(self, walkers, absw, rand):
+        """Resample every slot from the cumulative |w|; all weights become the mean."""
+        src, mean_weight = reconfiguration_sources(absw, rand())
+        if self._src is None or self._src.numel() != walkers.nwalkers:
+            self._src = torch.empty(walkers.nwalkers, dtype=torch.int32, device=walkers.device)
+        self._src.copy_(torch.from_numpy(src.astype(np.int32)))
+        walkers.resample(self._src)
+        walkers.weight.fill_(mean_weight)
+        return src

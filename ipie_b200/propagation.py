@@ -165,7 +165,7 @@ class PhaselessGeneric:
 
     def _mixed_setup(self, hamiltonian, trial):
         """TF32 operands of the mixed form, prepared once: packed Cholesky hi/lo,
-        half-rotated Cholesky (TF32), expH1 hi/lo with rows padded to a multiple of 4."""
+        half-rotated Cholesky hi/lo (padded), expH1 - I hi/lo."""
         M, X = hamiltonian.nbasis, hamiltonian.nchol
         if M % 4 or X % 4 or self.expH1_complex:
             raise NotImplementedError("the mixed form needs nbasis and nchol multiples of 4 and a real expH1")
@@ -180,7 +180,8 @@ class PhaselessGeneric:
         # padded half-rotated Cholesky TF32 head/remainder: force bias and energy share it
         self.rpad = _mixed_energy_operands(trial, hamiltonian)
         self.lde = M
-        e = torch.from_numpy(np.ascontiguousarray(self.expH1.real)).to(dev)
+        # the one-body factor enters the mixed orbital update as E - I (the identity is added in FP64)
+        e = torch.from_numpy(np.ascontiguousarray(self.expH1.real - np.eye(M)[None])).to(dev)
         self.e_hi = torch.empty(2, M, M, dtype=f32, device=dev)
         self.e_lo = torch.empty(2, M, M, dtype=f32, device=dev)
         call("ipie_b200_split_tf32", ptr(e), ptr(self.e_hi), ptr(self.e_lo), e.numel(), stream())
@@ -276,10 +277,14 @@ class PhaselessGeneric:
         one-body factor after it changes nothing.
         """
         ws = self._workspace(walkers, hamiltonian)
-        # the step's starting overlap goes into walkers.ovlp, which update_weight overwrites with ovlp_new
-        self.timer.start("greens_function")
-        greens_function_into(walkers, trial, walkers.ovlp)
-        self.timer.stop("greens_function")
+        # The step's starting Green's function and overlap: the previous step ended with those of
+        # the current orbitals (reortho and pair branch keep them consistent), so they are only
+        # recomputed when the orbitals were replaced.  walkers.ovlp is overwritten by update_weight.
+        if not walkers.gf_current(trial):
+            self.timer.start("greens_function")
+            greens_function_into(walkers, trial, walkers.ovlp)
+            self.timer.stop("greens_function")
+        walkers.invalidate_gf()  # the orbitals change below
         if self.precision == "mixed":
             cmf, cfb = self._mixed_two_body(walkers, hamiltonian, trial)
         elif not self.fused_ok(walkers):
@@ -315,9 +320,12 @@ class PhaselessGeneric:
             walkers.sync_alias()
             self.timer.stop("orbitals")
             cmf, cfb = ws.cmf, ws.cfb
-        self.timer.start("overlap")
-        overlap_into(walkers, trial, ws.ovlp_new)
-        self.timer.stop("overlap")
+        # Green's function of the new orbitals: its overlap is ovlp_new (ipie's calc_overlap) and its
+        # Ghalf is the next step's (ipie recomputes it at the next step's start)
+        self.timer.start("greens_function")
+        greens_function_into(walkers, trial, ws.ovlp_new)
+        self.timer.stop("greens_function")
+        walkers.mark_gf_current(trial)
         self.update_weight(walkers, walkers.ovlp, ws.ovlp_new, cfb, cmf, eshift)
 
     def _mixed_two_body(self, walkers, hamiltonian, trial):

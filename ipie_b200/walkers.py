@@ -17,6 +17,25 @@ F64 = torch.float64
 
 
 class UHFWalkers:
+    # phia/phib are properties: replacing either drops the cached Green's function
+    @property
+    def phia(self):
+        return self._phia
+
+    @phia.setter
+    def phia(self, value):
+        self._phia = value
+        self._gf_key = None
+
+    @property
+    def phib(self):
+        return self._phib
+
+    @phib.setter
+    def phib(self, value):
+        self._phib = value
+        self._gf_key = None
+
     def __init__(self, initial_walker, nup, ndown, nbasis, nwalkers, mpi_handler=None, verbose=False, device="cuda"):
         init = np.asarray(initial_walker)
         assert init.ndim == 2
@@ -24,6 +43,8 @@ class UHFWalkers:
         self.mpi_handler = mpi_handler
         self.device = dev = torch.device(device)
         W, M = nwalkers, nbasis
+        # orbitals Ghalfa/b and ovlp were last computed from (see gf_current)
+        self._gf_key = None
         ia = torch.from_numpy(np.ascontiguousarray(init[:, :nup].astype(np.complex128)))
         ib = torch.from_numpy(np.ascontiguousarray(init[:, nup:].astype(np.complex128)))
         self.phia = ia.to(dev).unsqueeze(0).repeat(W, 1, 1).contiguous()
@@ -68,9 +89,59 @@ class UHFWalkers:
             self.phib = self.phia
             self.Ghalfb = self.Ghalfa
 
+    def _orbital_key(self, trial):
+        return (self._phia._version, self._phib._version, id(trial))
+
+    def mark_gf_current(self, trial):
+        """Ghalfa/b and ovlp now belong to the current orbitals."""
+        self._gf_key = self._orbital_key(trial)
+
+    def gf_current(self, trial):
+        """True while Ghalfa/b and ovlp are those of the current orbitals.
+
+        Kept valid by the library's own updates (a propagation step ends with the
+        Green's function of its new orbitals; reorthogonalisation leaves Ghalf
+        unchanged and rescales ovlp; population control copies Ghalf with the
+        orbitals).  Assigning ``phia``/``phib`` or changing them with in-place torch
+        operations invalidates it; after writing them through raw device pointers
+        call :meth:`invalidate_gf`.
+        """
+        return self._gf_key is not None and self._gf_key == self._orbital_key(trial)
+
+    def invalidate_gf(self):
+        self._gf_key = None
+
+    def resample(self, src):
+        """Walker d becomes walker ``src[d]`` (int32 device tensor; sources may repeat).
+
+        Orbitals, Green's functions, overlaps, hybrid energies, phases and unscaled
+        weights move together (out of place); the Green's-function cache stays valid.
+        """
+        was_current = self._gf_key is not None and self._gf_key[:2] == (self._phia._version, self._phib._version)
+        key_trial = self._gf_key[2] if was_current else None
+        alias = self.spin_alias
+        new = {n: torch.empty_like(getattr(self, n)) for n in ("phia", "Ghalfa", "hybrid_energy", "ovlp", "phase",
+                                                                 "unscaled_weight")}
+        if not alias:
+            new["phib"] = torch.empty_like(self.phib)
+            new["Ghalfb"] = torch.empty_like(self.Ghalfb)
+        call("ipie_b200_walker_gather", ptr(src), self.nwalkers, self.nbasis, self.nup, self.ndown,
+             ptr(self.phia), ptr(self.phib), ptr(self.Ghalfa), ptr(self.Ghalfb), ptr(self.hybrid_energy),
+             ptr(self.ovlp), ptr(self.phase), ptr(self.unscaled_weight), ptr(new["phia"]),
+             ptr(new.get("phib", new["phia"])), ptr(new["Ghalfa"]), ptr(new.get("Ghalfb", new["Ghalfa"])),
+             ptr(new["hybrid_energy"]), ptr(new["ovlp"]), ptr(new["phase"]), ptr(new["unscaled_weight"]), stream())
+        for n, t in new.items():
+            setattr(self, n, t)
+        if alias:
+            self.phib = self.phia
+            self.Ghalfb = self.Ghalfa
+        if was_current:
+            self._gf_key = (self._phia._version, self._phib._version, key_trial)
+
     def build(self, trial):
         """``walkers.build``: initial overlaps and Green's functions (``uhf_walkers.py:101-102``)."""
         self.ovlp = trial.calc_greens_function(self)
+        self.mark_gf_current(trial)
 
     def reortho(self):
         """Thin QR per spin block with positive diag(R); returns detR (``uhf_walkers.py:108-161``)."""

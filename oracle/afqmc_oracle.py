@@ -489,27 +489,98 @@ def pair_branch(w: Walkers, max_weight: float = 4.0, min_weight: float = 0.1, ra
     return neww, status
 
 
-class PopController:
-    """Weight rescaling + pair branch; ipie ``walkers/pop_controller.py:33-125``."""
+def comb_parent_counts(weights: np.ndarray, target_weight: int, r: float) -> np.ndarray:
+    """Copies of each walker under the comb (Booth & Gubernatis, PRE 80, 046704 (2009)).
 
-    def __init__(self, num_walkers: int, min_weight: float = 0.1, max_weight: float = 4.0):
+    ipie: ``walkers/pop_controller.py:199-243``.  The comb teeth are
+    ``(i + r) * total / target`` for i < target; walker iw receives every tooth in
+    [cprobs[iw-1], cprobs[iw]).  ipie walks the teeth with a while loop; the
+    same assignment is a right-sided search in the cumulative weights.
+    """
+    cprobs = np.cumsum(weights)
+    total_weight = cprobs[-1]  # ipie's builtin sum(weights): the same sequential sum
+    teeth = (np.arange(target_weight) + r) * (total_weight / target_weight)
+    iw = np.searchsorted(cprobs, teeth, side="right")
+    return np.bincount(iw, minlength=len(weights))[: len(weights)].astype(np.int64)
+
+
+def comb(w: Walkers, weights: np.ndarray, target_weight: int, rand=np.random.random):
+    """Comb pop control on one process: walker ``kill[i]`` becomes a copy of ``clone[i]``
+    (pairs in index order, as ipie zips them), then every weight is reset to 1.
+
+    ipie: ``walkers/pop_controller.py:199-301``; each send carries its own tag
+    ``i`` there, so single-process copies are exact.
+    """
+    parent_ix = comb_parent_counts(weights, target_weight, rand())
+    kill = np.where(parent_ix == 0)[0]
+    clone = np.where(parent_ix > 1)[0]
+    buffers = [get_buffer(w, c) for c, _ in zip(clone, kill)]
+    for (c, k), buff in zip(zip(clone, kill), buffers):
+        set_buffer(w, k, buff)
+    w.weight.fill(1.0)
+    return parent_ix
+
+
+def stochastic_reconfiguration(w: Walkers, rand=np.random.rand):
+    """Resample W walkers with a uniform comb on the cumulative |w|; all get the mean weight.
+
+    ipie: ``walkers/pop_controller.py:432-475`` on one process.
+    """
+    nwalkers = w.nwalkers
+    buffers = np.array([get_buffer(w, i) for i in range(nwalkers)])
+    cumulative_weights = np.cumsum(np.abs(buffers[:, 0]))
+    total_weight = cumulative_weights[-1]
+    new_average_weight = total_weight / nwalkers / 1
+    zeta = rand()
+    new_ix = np.empty(nwalkers, dtype=np.int64)
+    for i in range(nwalkers):
+        z = (i + zeta) / nwalkers / 1
+        new_ix[i] = np.searchsorted(cumulative_weights, z * total_weight)
+    for i in range(nwalkers):
+        b = buffers[new_ix[i]].copy()
+        b[0] = new_average_weight
+        set_buffer(w, i, b)
+    return new_ix
+
+
+class PopController:
+    """Weight rescaling + pair branch / comb / stochastic reconfiguration;
+    ipie ``walkers/pop_controller.py:33-125``."""
+
+    def __init__(self, num_walkers: int, min_weight: float = 0.1, max_weight: float = 4.0,
+                 method: str = "pair_branch", reconfiguration_freq: int = 50):
         self.ntot_walkers = num_walkers
         self.target_weight = num_walkers
         self.total_weight = num_walkers
         self.min_weight = min_weight
         self.max_weight = max_weight
+        self.method = method
+        self.reconfiguration_counter = 0
+        self.reconfiguration_freq = reconfiguration_freq
 
     def pop_control(self, w: Walkers, rand=np.random.rand):
         if self.ntot_walkers == 1:
             return
-        total_weight = float(np.sum(np.abs(w.weight)))
+        absw = np.abs(w.weight)
+        if self.method == "comb":
+            total_weight = float(np.cumsum(absw)[-1])  # builtin sum over the gathered weights
+        else:
+            total_weight = float(np.sum(absw))
         scale = total_weight / self.target_weight
         if total_weight < 1e-8:
             raise ValueError(f"Total weight is {total_weight:13.8e}")
         self.total_weight = total_weight
         w.unscaled_weight = w.weight
         w.weight = w.weight / scale
-        pair_branch(w, self.max_weight, self.min_weight, rand)
+        if self.method == "comb":
+            comb(w, absw / scale, self.target_weight, rand)
+        elif self.method == "pair_branch":
+            pair_branch(w, self.max_weight, self.min_weight, rand)
+        elif self.method == "stochastic_reconfiguration":
+            self.reconfiguration_counter += 1
+            if self.reconfiguration_counter % self.reconfiguration_freq == 0:
+                stochastic_reconfiguration(w, rand)
+                self.reconfiguration_counter = 0
 
 
 # --------------------------------------------------------------------------

@@ -2,7 +2,7 @@
 
 Run from the repository root with ipie's source tree available:
 
-    python tests/golden/make_golden.py /path/to/ipie-checkout
+    python tests/golden/make_golden.py /path/to/ipie-checkout [ad|pop]
 
 ipie needs ``plum`` and ``h5py``, which are absent here; the small stand-ins in
 ``_ref_shims/`` are put first on ``sys.path``.  mpi4py is absent, so ipie
@@ -260,9 +260,35 @@ def ad_fixture(name):
     print("wrote", name, "dE/dlambda", dE_total)
 
 
+def pop_control_fixture(name):
+    """ipie's comb (``walkers/tests/test_population_control.py:84-142``) and stochastic
+    reconfiguration (no ipie test; reconfiguration every 3rd call) on the known-answer
+    builder's system (the pair-branch inputs of ``known_answers.npz``)."""
+    from ipie.utils.misc import dotdict
+    from ipie.utils.testing import build_test_case_handlers_mpi
+
+    out = {}
+    for key, method in (("comb", "comb"), ("sr", "stochastic_reconfiguration")):
+        qmc = dotdict({"dt": 0.005, "nstblz": 5, "nwalkers": 10, "batched": True, "hybrid": True,
+                       "num_steps": 10, "population_control": method, "reconfiguration_freq": 3})
+        d = build_test_case_handlers_mpi((5, 5), 10, MPIHandler(), num_dets=1, complex_trial=True, options=qmc,
+                                         seed=7)
+        out[f"{key}_weight"] = np.array(d.walkers.weight)
+        out[f"{key}_unscaled_weight"] = np.array(d.walkers.unscaled_weight)
+        out[f"{key}_phia"] = np.array(d.walkers.phia)
+        out[f"{key}_phib"] = np.array(d.walkers.phib)
+        out[f"{key}_ovlp"] = np.array(d.walkers.ovlp)
+    print("comb phia[9][0,0]", out["comb_phia"][9][0, 0])
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 2 and sys.argv[2] == "ad":
         ad_fixture("ad_onebody_m30.npz")
+        sys.exit(0)
+    if len(sys.argv) > 2 and sys.argv[2] == "pop":
+        pop_control_fixture("pop_control.npz")
         sys.exit(0)
     c0 = synthetic.workload("c0_rhf_m26")
     kernels_fixture("kernels_rhf_m26.npz", c0, nwalkers=8, seed=11)
@@ -273,4 +299,5 @@ if __name__ == "__main__":
     gentle = synthetic.generate(30, (6, 4), 90, decay=30.0, seed=5, uhf=True, chol_scale=0.1)
     run_fixture("run_uhf_m30.npz", gentle, nwalkers=12, num_blocks=3, seed=9)
     known_answer_inputs("known_answers.npz")
+    pop_control_fixture("pop_control.npz")
     ad_fixture("ad_onebody_m30.npz")

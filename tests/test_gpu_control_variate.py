@@ -47,10 +47,14 @@ def test_trained_control_variate_reduces_subsample_variance():
     trial.half_rotate(ham)
     af = AFQMC.build((8, 8), ham, trial, num_walkers=256, seed=5, num_blocks=100, verbose=False, rng="device")
     af.setup_run()
-    feats, ys = generate_training_data(af, steps=40)
+    feats, ys, bases = generate_training_data(af, steps=40)
+    # the exchange over the leading eighth of the Cholesky vectors already carries most of the spread
+    assert (ys - bases).var().item() < 0.5 * ys.var().item()
     cv = ExchangeControlVariate(hidden=128, seed=1)
-    hist = cv.fit(feats, ys, epochs=40, batch=1024, lr=2e-3)
-    assert hist[-1][1] < 0.2 * hist[0][1] + 1e-3  # holdout MSE fell
+    hist = cv.fit(feats, ys, bases, epochs=40, batch=1024, lr=2e-3)
+    # holdout MSE (units of var(y - base)) fell during training and beats the leading-vector term alone
+    assert hist[-1][1] < hist[0][1]
+    assert hist[-1][1] < 0.8
     for step in range(41, 51):
         af.step(step)
     parts = EnergyParts(ham, trial, af.walkers)

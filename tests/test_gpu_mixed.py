@@ -143,5 +143,20 @@ def test_mixed_local_energy(uhf, N):
     trial.calc_greens_function(walkers)
     ref = local_energy_single_det_uhf_batch(None, ham, walkers, trial)
     got = local_energy_mixed(None, ham, walkers, trial)
-    assert rel(got, ref) < 2e-6
+    assert rel(got, ref) < 2e-7
+    plain = local_energy_mixed(None, ham, walkers, trial, reference=False)
+    assert rel(plain, ref) < 2e-6
     walkers.check_status()
+
+
+def test_mixed_local_energy_is_exact_at_the_trial():
+    """Expanded around the trial, the tensor cores see G - G_T = 0 there: FP64 energies result."""
+    from ipie_b200 import synthetic
+    from ipie_b200.estimators import local_energy_mixed, local_energy_single_det_uhf_batch
+
+    s = synthetic.generate(76, (10, 10), 200, decay=30.0, seed=17, uhf=False, chol_scale="stable")
+    ham, trial, walkers, prop = gpu_objects(s, 8)
+    trial.calc_greens_function(walkers)
+    ref = local_energy_single_det_uhf_batch(None, ham, walkers, trial)
+    got = local_energy_mixed(None, ham, walkers, trial)
+    assert rel(got, ref) < 1e-12

@@ -152,6 +152,57 @@ def test_known_answer_pair_branch():
                                                                  rel=1e-9)
 
 
+def _known_answer_walk_gpu(method):
+    """ipie's ``build_test_case_handlers_mpi`` loop (``utils/testing.py:465-528``) on the CUDA path."""
+    from ipie_b200 import Generic, PopController, SingleDet, UHFWalkers
+    from ipie_b200.propagation import PhaselessGeneric
+
+    f = load("known_answers.npz")
+    M = f["pb_h1e"].shape[-1]
+    ham = Generic(f["pb_h1e"], f["pb_chol"], 0.0)
+    trial = SingleDet(f["pb_psi"], (5, 5), M)
+    trial.half_rotate(ham)
+    walkers = UHFWalkers(f["pb_init"], 5, 5, M, 10)
+    walkers.build(trial)
+    np.random.seed(7)
+    prop = PhaselessGeneric(0.005)
+    prop.build(ham, trial, walkers)
+    pc = PopController(10, 10, pop_control_method=method, reconfiguration_freq=3)
+    eshift = complex(f["pb_eshift"]).real
+    for _ in range(10):
+        prop.propagate_walkers(walkers, ham, trial, eshift)
+        walkers.reortho()
+        pc.pop_control(walkers)
+        trial.calc_greens_function(walkers)
+    walkers.check_status()
+    return walkers
+
+
+def test_known_answer_comb():
+    """ipie ``walkers/tests/test_population_control.py:84-142`` (comb) on the CUDA path."""
+    walkers = _known_answer_walk_gpu("comb")
+    assert complex(walkers.phia[9, 0, 0].item()) == pytest.approx(-0.0597200851442905 - 0.002353281222663805j,
+                                                                 rel=1e-9)
+    f = load("pop_control.npz")
+    assert rel(walkers.weight, f["comb_weight"]) < 1e-12
+    assert rel(walkers.unscaled_weight, f["comb_unscaled_weight"]) < 1e-9
+    assert rel(walkers.phia, f["comb_phia"]) < 1e-9
+    assert rel(walkers.phib, f["comb_phib"]) < 1e-9
+
+
+def test_stochastic_reconfiguration_matches_ipie():
+    """ipie's stochastic reconfiguration every 3rd call (``walkers/pop_controller.py:432-475``)."""
+    walkers = _known_answer_walk_gpu("stochastic_reconfiguration")
+    f = load("pop_control.npz")
+    assert rel(walkers.weight, f["sr_weight"]) < 1e-9
+    assert rel(walkers.unscaled_weight, f["sr_unscaled_weight"]) < 1e-9
+    assert rel(walkers.phia, f["sr_phia"]) < 1e-9
+    assert rel(walkers.phib, f["sr_phib"]) < 1e-9
+    # the particle-hole trial of ipie's builder scales every overlap by its determinant coefficient
+    ratio = walkers.ovlp.cpu().numpy() / f["sr_ovlp"]
+    assert np.max(np.abs(ratio - ratio[0])) < 1e-9 * abs(ratio[0])
+
+
 def test_known_answer_local_energy():
     """ipie ``estimators/tests/test_generic.py:51-69`` on the CUDA path."""
     from ipie_b200 import Generic, SingleDet
@@ -337,3 +388,27 @@ def test_unfused_step_path_matches_oracle():
     assert rel(walkers.weight, ow.weight) < TOL
     assert rel(walkers.phia, ow.phia) < TOL
     assert rel(walkers.phib, ow.phib) < TOL
+
+
+def test_cached_green_function_stays_current():
+    """The step reuses the Green's function computed at the end of the previous one; after
+    propagation, reortho and pair branch it must equal a fresh computation."""
+    from ipie_b200 import AFQMC, Generic, SingleDet, synthetic
+
+    s = synthetic.generate(30, (6, 4), 90, decay=30.0, seed=12, uhf=True, chol_scale="stable")
+    ham = Generic(s.h1e, s.chol, s.ecore)
+    trial = SingleDet(s.psi, (6, 4), 30)
+    trial.half_rotate(ham)
+    af = AFQMC.build((6, 4), ham, trial, num_walkers=12, seed=4, num_steps_per_block=25, num_blocks=1, verbose=False)
+    af.setup_run()
+    for step in range(1, 11):  # includes reortho (every 5) and pair branch (every 5)
+        af.step(step)
+        w = af.walkers
+        assert w.gf_current(trial)
+        ga, gb, ov = w.Ghalfa.clone(), w.Ghalfb.clone(), w.ovlp.clone()
+        fresh = trial.calc_greens_function(w)
+        assert rel(ga, w.Ghalfa) < 1e-12
+        assert rel(gb, w.Ghalfb) < 1e-12
+        assert rel(ov, fresh) < 1e-12
+    w.phia = w.phia.clone()
+    assert not w.gf_current(trial)

@@ -48,3 +48,51 @@ def test_stable_scale_pins_field_operator_norm():
         xs = np.random.default_rng(0).normal(size=(X, 3)).astype(complex)
         norms.append(np.mean([np.linalg.norm(v, 2) for v in O.construct_vhs(S, xs)]))
     assert 0.15 < norms[0] < 0.35 and 0.15 < norms[1] < 0.35
+
+
+def test_exchange_gradient_is_the_derivative_of_the_oracle_exchange():
+    """K = d raw / d Ghalf (raw = 2 * oracle exx): central differences are exact for the quadratic."""
+    torch = pytest.importorskip("torch")
+    from ipie_b200.control_variate import exchange_gradient
+
+    rng = np.random.default_rng(4)
+    X, N, M = 12, 3, 7
+    rchol = rng.normal(size=(X, N * M))
+    g = rng.normal(size=(N, M)) + 1j * rng.normal(size=(N, M))
+    d = rng.normal(size=(N, M)) + 1j * rng.normal(size=(N, M))
+    K = exchange_gradient(torch.from_numpy(rchol), torch.from_numpy(g)).numpy()
+    eps = 0.37
+    raw = lambda G: 2.0 * O.exx_kernel(rchol.reshape(X, N, M), G[None])[0]  # noqa: E731
+    fd = (raw(g + eps * d) - raw(g - eps * d)) / (2 * eps)
+    assert abs(fd - np.sum(K * d)) < 1e-10 * abs(fd)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_comb_and_reconfiguration_tables_match_oracle(seed):
+    """Host decisions of comb and stochastic reconfiguration equal the oracle's ipie restatement."""
+    from ipie_b200.pop_control import comb_parent_counts, reconfiguration_sources
+
+    rng = np.random.default_rng(seed)
+    w = rng.exponential(size=37) * (rng.random(37) < 0.9)
+    r = rng.random()
+    assert np.array_equal(comb_parent_counts(w, 37, r), O.comb_parent_counts(w, 37, r))
+    # the oracle's walker-level restatement on dummy walkers carrying their index
+    ow = O.Walkers.from_initial(np.eye(4, 2), 1, 37)
+    ow.weight = w.copy()
+    ow.phia = np.arange(37, dtype=np.complex128)[:, None, None] * np.ones((37, 4, 1))
+    ix = O.stochastic_reconfiguration(ow, rand=lambda: r)
+    src, mean_w = reconfiguration_sources(np.abs(w), r)
+    assert np.array_equal(src, ix)
+    assert np.allclose(ow.phia[:, 0, 0].real, src)
+    assert np.all(ow.weight == mean_w)
+
+
+@pytest.mark.parametrize("M", [1, 7, 26, 30, 108, 200])
+def test_tiled_packing_covers_the_upper_triangle_once(M):
+    from ipie_b200.hamiltonian import tiled_triu_indices
+
+    i, j = tiled_triu_indices(M)
+    assert len(i) == M * (M + 1) // 2
+    pairs = set(zip(i.tolist(), j.tolist()))
+    assert len(pairs) == len(i)
+    assert all(a <= b < M for a, b in pairs)

@@ -126,6 +126,49 @@ def test_known_answer_pair_branch():
     assert rel(w.unscaled_weight, f["pb_unscaled_weight"]) < 1e-9
 
 
+def _known_answer_walk(method):
+    """ipie's ``build_test_case_handlers_mpi`` loop (``utils/testing.py:465-528``) on the oracle."""
+    f = load("known_answers.npz")
+    M = f["pb_h1e"].shape[-1]
+    S = O.System(M, 5, 5, f["pb_h1e"], f["pb_chol"], 0.0, f["pb_psi"]).build()
+    w = O.Walkers.from_initial(f["pb_init"], 5, 10)
+    w.ovlp = O.greens_function(S, w)
+    np.random.seed(7)
+    pc = O.PopController(10, method=method, reconfiguration_freq=3)
+    eshift = complex(f["pb_eshift"])
+    for _ in range(10):
+        O.propagate_walkers(S, w, eshift)
+        O.reortho(S, w)
+        pc.pop_control(w)
+        O.greens_function(S, w)
+    return w
+
+
+def test_known_answer_comb():
+    """ipie ``walkers/tests/test_population_control.py:84-142``: comb pop control."""
+    w = _known_answer_walk("comb")
+    assert w.phia[9][0, 0] == pytest.approx(-0.0597200851442905 - 0.002353281222663805j, rel=1e-9)
+    f = load("pop_control.npz")
+    assert rel(w.weight, f["comb_weight"]) < 1e-12
+    assert rel(w.unscaled_weight, f["comb_unscaled_weight"]) < 1e-9
+    assert rel(w.phia, f["comb_phia"]) < 1e-9
+    assert rel(w.phib, f["comb_phib"]) < 1e-9
+
+
+def test_stochastic_reconfiguration_matches_ipie():
+    """ipie's stochastic reconfiguration (``walkers/pop_controller.py:432-475``), every 3rd call."""
+    w = _known_answer_walk("stochastic_reconfiguration")
+    f = load("pop_control.npz")
+    assert rel(w.weight, f["sr_weight"]) < 1e-9
+    assert rel(w.unscaled_weight, f["sr_unscaled_weight"]) < 1e-9
+    assert rel(w.phia, f["sr_phia"]) < 1e-9
+    assert rel(w.phib, f["sr_phib"]) < 1e-9
+    # ipie's builder uses a one-determinant particle-hole trial whose overlaps carry its
+    # (complex) determinant coefficient: equal up to one global factor
+    ratio = w.ovlp / f["sr_ovlp"]
+    assert np.max(np.abs(ratio - ratio[0])) < 1e-9 * abs(ratio[0])
+
+
 def test_known_answer_local_energy():
     """ipie ``estimators/tests/test_generic.py:51-69``: energy of a random real determinant."""
     f = load("known_answers.npz")
