@@ -155,7 +155,7 @@ def barrier_max(value, world):
     return float(t.item())
 
 
-def build_afqmc(wl, walkers, rng, seed, precision="fp64"):
+def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5):
     from ipie_b200 import AFQMC, Generic, SingleDet, synthetic
 
     p = WORKLOADS[wl]
@@ -164,7 +164,8 @@ def build_afqmc(wl, walkers, rng, seed, precision="fp64"):
     trial = SingleDet(s.psi, (s.nup, s.ndown), s.nbasis)
     trial.half_rotate(ham)
     af = AFQMC.build((s.nup, s.ndown), ham, trial, num_walkers=walkers, seed=seed, num_steps_per_block=25,
-                     num_blocks=10 ** 6, timestep=0.005, stabilize_freq=5, pop_control_freq=5, verbose=False, rng=rng,
+                     num_blocks=10 ** 6, timestep=0.005, stabilize_freq=5, pop_control_freq=pop_control_freq,
+                     verbose=False, rng=rng,
                      precision=precision)
     return af, s
 
@@ -265,6 +266,22 @@ def train_control_variate(wl, W, rank, steps=100, epochs=60):
     return cv, info
 
 
+def precision_shift(wl, W, rank, steps=50):
+    """Block energies of the FP64 and mixed forms over ``steps`` steps with identical draws and no
+    population control (a flipped branching decision would swap whole walkers between the runs and
+    hide the precision effect); returns the largest difference in mEh and both series."""
+    out = {}
+    for form in ("fp64", "mixed"):
+        af, _ = build_afqmc(wl, W, "device", 4242 + rank, precision=form, pop_control_freq=10 ** 9)
+        af.setup_run()
+        for step in range(1, steps + 1):
+            af.step(step)
+        out[form] = np.array(af.block_data)[:, 5].real
+        del af
+    n = min(len(out["fp64"]), len(out["mixed"]))
+    return float(np.max(np.abs(out["mixed"][:n] - out["fp64"][:n]))) * 1e3, out
+
+
 def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clock=False, cv=None):
     """Build, warm up and time ``args.steps`` driver steps of one form; returns a result dict."""
     import torch
@@ -277,7 +294,7 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
     if cv is not None:
         from ipie_b200.control_variate import ControlVariateEnergyEstimator
 
-        af.estimator = ControlVariateEnergyEstimator(cv, fraction=8, seed=7 + rank)
+        af.estimator = ControlVariateEnergyEstimator(cv, fraction=8, seed=7 + rank, precision="mixed")
     step = 0
     for _ in range(args.warmup):
         step += 1
@@ -388,7 +405,10 @@ def run_ours(args):
     if "mixed" in runs and "fp64" in runs:
         a, b = runs["mixed"]["blocks"][:, 5], runs["fp64"]["blocks"][:, 5]
         n = min(len(a), len(b))
-        shift = float(np.max(np.abs(a[:n] - b[:n]))) * 1e3  # mEh, same draws and seed
+        # with population control a single flipped branching decision moves whole walkers
+        forms_out["trajectory_shift_with_branching_mEh"] = float(np.max(np.abs(a[:n] - b[:n]))) * 1e3
+        shift, series = precision_shift(wl, W, rank)
+        forms_out["precision_shift_runs"] = {k: [round(float(x), 9) for x in v] for k, v in series.items()}
         forms_out["mixed_over_fp64"] = forms_out["mixed"]["walker_steps_per_s"] / forms_out["fp64"]["walker_steps_per_s"]
         forms_out["mixed"]["estimator_shift_mEh"] = runs["mixed"].get("estimator_shift_mEh")
     if "mixed_cv" in runs and "fp64" in runs:
@@ -454,6 +474,9 @@ def run_ours(args):
             },
             "forms": forms_out,
             "energy_shift_mEh": shift,
+            "energy_shift_method": ("max |block E(mixed) - block E(fp64)| over 50 steps (2 blocks) of 2 runs with "
+                                    "identical draws and no population control; estimator-only shift on identical "
+                                    "walkers in forms.mixed.estimator_shift_mEh"),
             "e2e": {"value": e2e_value, "unit": "walker-steps/s", "h2d_bytes_per_step": W * X * 8,
                     "d2h_bytes_per_step": W * 8, "steps": e2e_steps,
                     "fields": "host-supplied N(0,1) draws in pinned memory, one (W, X) array per step"},

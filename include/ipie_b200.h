@@ -258,6 +258,18 @@ int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float* e_lo, int
  * TF32 head/remainder (X*NP, M) arrays: the left operand of the mixed energy. */
 int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, float* hi, float* lo, void* stream);
 
+/* Exchange of one spin block in the mixed form: exx[w] (complex) = sum_x sum_ij T_ij T_ji,
+ * T = rchol_x (N x M) . Ghalf_w^T, as 3-pass TF32 tensor-core products with FP64 bilinear
+ * sums.  r_hi/r_lo: the padded split rows of ipie_b200_rchol_pad_split (the first X
+ * Cholesky vectors of a larger array may be passed with a smaller X); gwork: 2*W*2*32*M
+ * floats; part: (ceil(X*NP/128) + 1) * W complex.  With the trial reference (ghalf_trial,
+ * kmat, raw_trial[1]; see ipie_b200_local_energy_mixed) only G - G_T passes through the
+ * tensor cores; ghalf_trial NULL disables it.
+ * replaces (mixed form): estimators/local_energy_sd.py:263-303 (exx_kernel_batch_real_rchol). */
+int ipie_b200_exchange_mixed(const float* r_hi, const float* r_lo, const void* ghalf, const void* ghalf_trial,
+                             const void* kmat, const void* raw_trial, int W, int X, int M, int N, float* gwork,
+                             void* part, void* exx, unsigned int* status, void* stream);
+
 /* Local energy of the mixed form: the exchange as 3-pass TF32 tensor-core
  * products (T never stored, bilinear sums in FP64); Coulomb vector and e1b in
  * FP64.  Same contract and spin-alias convention as

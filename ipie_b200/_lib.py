@@ -44,6 +44,7 @@ SIGNATURES = {
     "ipie_b200_construct_vhs_mixed": [P, P, P, P, I, I, P, P, I, D, P, P, P, P, P, P],
     "ipie_b200_propagate_orbitals_mixed": [P, P, I, P, P, P, P, P, P, P, I, I, I, I, P, P],
     "ipie_b200_rchol_pad_split": [P, I, I, I, P, P, P],
+    "ipie_b200_exchange_mixed": [P, P, P, P, P, P, I, I, I, I, P, P, P, P, P],
     "ipie_b200_local_energy_mixed": [I, P, P, P, P, P, P, P, P, D, P, P, P, P, P, P, P, I, I, I, I, I, P, P, P, P, P],
     "ipie_b200_energy_combine": [I, I, I, I, I, P, P, P, P, D, P, P, I, D, D, D, P, P, P],
     "ipie_b200_mlp_forward": [P, I, I, I, P, P, P, P, P],

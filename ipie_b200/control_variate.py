@@ -168,8 +168,13 @@ def exchange_gradient(rchol, ghalf_trial):
 class EnergyParts:
     """Exchange-free energies, Coulomb vectors, exact exchange terms and features of a walker batch."""
 
-    def __init__(self, hamiltonian, trial, walkers, lead_fraction=8):
+    def __init__(self, hamiltonian, trial, walkers, lead_fraction=8, precision="fp64"):
+        """``precision="mixed"``: exchange terms as 3-pass TF32 tensor-core products (the exact
+        subsample expanded around the trial, as the mixed local energy does)."""
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision {precision!r}: 'fp64' or 'mixed'")
         self.ham, self.trial = hamiltonian, trial
+        self.precision = precision
         self.n_lead = max(1, hamiltonian.nchol // lead_fraction)
         W, X, M = walkers.nwalkers, hamiltonian.nchol, hamiltonian.nbasis
         dev = walkers.device
@@ -181,7 +186,7 @@ class EnergyParts:
         self.exx = torch.empty(W, dtype=C128, device=dev)
         from .estimators import exchange_reference
 
-        self.ghalf_trial, self.kmat, _ = exchange_reference(trial, hamiltonian)
+        self.ghalf_trial, self.kmat, self.raw_trial = exchange_reference(trial, hamiltonian)
 
     def compute(self, walkers, with_features=True):
         """Green's functions, exchange-free energy and features for every walker."""
@@ -217,16 +222,34 @@ class EnergyParts:
         blocks = [(self.trial._rchola, walkers.Ghalfa, walkers.nup, 1.0 if walkers.spin_alias else 0.5)]
         if walkers.ndown > 0 and not walkers.spin_alias:
             blocks.append((self.trial._rcholb, walkers.Ghalfb, walkers.ndown, 0.5))
-        for rchol, gh, n, fac in blocks:
+        if self.precision == "mixed":
+            from .estimators import _mixed_energy_operands
+
+            ops = _mixed_energy_operands(self.trial, ham)
+        for s_, (rchol, gh, n, fac) in enumerate(blocks):
             if idx is not None:
                 sub = torch.empty(S, n, M, dtype=C128, device=walkers.device)
                 call("ipie_b200_gather_walkers", ptr(gh), ptr(idx), S, n * M, ptr(sub), stream())
             else:
                 sub = gh
-            rows = lib().ipie_b200_exchange_rows(S, X, M, n)
-            part = torch.empty(rows * S, dtype=C128, device=walkers.device)
-            call("ipie_b200_exchange", ptr(rchol), ptr(sub), S, X, M, n, ptr(part), stream())
-            total += fac * part.view(rows, S).sum(0).real
+            if self.precision == "mixed":
+                hi, lo = ops[s_]
+                NP = 8 if n <= 8 else 16 if n <= 16 else 32
+                rows = (X * NP + 127) // 128 + 1
+                part = torch.empty(rows * S, dtype=C128, device=walkers.device)
+                gwork = torch.empty(2 * S * 2 * 32 * M, dtype=F32, device=walkers.device)
+                exx = torch.empty(S, dtype=C128, device=walkers.device)
+                ref = nchol is None  # the trial reference belongs to the full Cholesky sum
+                call("ipie_b200_exchange_mixed", ptr(hi), ptr(lo), ptr(sub),
+                     ptr(self.ghalf_trial[s_]) if ref else None, ptr(self.kmat[s_]) if ref else None,
+                     ptr(self.raw_trial[s_:s_ + 1]) if ref else None, S, X, M, n, ptr(gwork), ptr(part), ptr(exx),
+                     ptr(walkers.status), stream())
+                total += fac * exx.real
+            else:
+                rows = lib().ipie_b200_exchange_rows(S, X, M, n)
+                part = torch.empty(rows * S, dtype=C128, device=walkers.device)
+                call("ipie_b200_exchange", ptr(rchol), ptr(sub), S, X, M, n, ptr(part), stream())
+                total += fac * part.view(rows, S).sum(0).real
         return total
 
 
@@ -235,9 +258,10 @@ class ControlVariateEnergyEstimator:
 
     names = ["ENumer", "EDenom", "ETotal", "E1Body", "E2Body"]
 
-    def __init__(self, cv, fraction=8, seed=11):
+    def __init__(self, cv, fraction=8, seed=11, precision="fp64"):
         self.cv = cv
         self.fraction = fraction
+        self.precision = precision
         self.rng = np.random.default_rng(seed)
         self.parts = None
         self._out = None
@@ -245,7 +269,7 @@ class ControlVariateEnergyEstimator:
 
     def compute_estimator(self, system=None, walkers=None, hamiltonian=None, trial=None):
         if self.parts is None:
-            self.parts = EnergyParts(hamiltonian, trial, walkers)
+            self.parts = EnergyParts(hamiltonian, trial, walkers, precision=self.precision)
             self._out = torch.zeros(5, dtype=F64, device=walkers.device)
         p = self.parts
         p.compute(walkers)

@@ -8,6 +8,10 @@ namespace ipie_b200 {
 
 size_t gf_smem_bytes(int M, int N);
 
+bool gf_lu32_fits(int na, int nb);
+cudaError_t launch_gf_lu32(const double2* phia, const double2* phib, int W, int M, int na, int nb,
+                           const double2* psia_c, const double2* psib_c, const double* log_shift, double2* ghalfa,
+                           double2* ghalfb, double2* ovlp, double2* logdet, unsigned* status, cudaStream_t st);
 cudaError_t launch_gf_overlap(const double2* phia, const double2* phib, int W, int M, int na, int nb,
                               const double2* psia_c, const double2* psib_c, const double* log_shift, double2* ghalfa,
                               double2* ghalfb, double2* ovlp, double2* logdet, unsigned* status, cudaStream_t st);
@@ -55,6 +59,11 @@ cudaError_t launch_propagate_fused(const double2* vhs, const double* expH1, int 
                                    double2* phi_out, int W, int M, int N, int nmax, int pre, int post, cudaStream_t st);
 
 namespace umma {
+bool orbital_chain_fits(int M, int N);
+cudaError_t mixed_orbital_chain(const float* e_hi, const float* e_lo, int lde, const float* v_re_hi,
+                                const float* v_re_lo, const float* v_im_hi, const float* v_im_lo,
+                                const double2* phi_in, double2* phi_out, int W, int M, int N, int nmax,
+                                unsigned* status, cudaStream_t st);
 cudaError_t mixed_vhs(const float* cp_hi, const float* cp_lo, const int* ii, const int* jj, int P, int X, int M,
                       const float* xs_hi, const float* xs_lo, int W, double sqrt_dt, float* re_hi, float* re_lo,
                       float* im_hi, float* im_lo, unsigned* status, cudaStream_t st);

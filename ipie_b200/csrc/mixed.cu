@@ -25,6 +25,24 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
+// 3-D batched K-major fp32 operand: `batch` matrices of `rows` x `k` (row stride k, matrix stride
+// rows * k elements), tiles of box_rows x 32 of one matrix; rows past `rows` read as 0 (no traffic).
+cudaError_t make_map_batched(CUtensorMap* m, const float* base, long long batch, long long rows, long long k,
+                             int box_rows) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (k % 4) || rows <= 0 || k <= 0 || batch <= 0)
+    return cudaErrorInvalidValue;
+  cuuint64_t dims[3] = {(cuuint64_t)k, (cuuint64_t)rows, (cuuint64_t)batch};
+  cuuint64_t strides[2] = {(cuuint64_t)k * 4, (cuuint64_t)rows * k * 4};
+  cuuint32_t box[3] = {32, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 // 2-D K-major fp32 operand: `rows` rows of `k` elements, row stride `ld` elements,
 // tiles of box_rows x 32 loaded 128B-swizzled; out-of-range elements read as 0.
 cudaError_t make_map(CUtensorMap* m, const float* base, long long rows, long long k, long long ld, int box_rows) {
@@ -585,6 +603,10 @@ extern "C" int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float
                                                   const void* phi_in, void* phi_out, float* work, int W, int M, int N,
                                                   int nmax, unsigned int* status, void* stream) {
   if (phi_in == phi_out || lde % 4 || lde < M) return (int)cudaErrorInvalidValue;
+  if (umma::orbital_chain_fits(M, N))
+    return (int)umma::mixed_orbital_chain(e_hi, e_lo, lde, v_re_hi, v_re_lo, v_im_hi, v_im_lo,
+                                          reinterpret_cast<const double2*>(phi_in), reinterpret_cast<double2*>(phi_out),
+                                          W, M, N, nmax, status, reinterpret_cast<cudaStream_t>(stream));
   const size_t plane = (size_t)W * 2 * N * M;
   return (int)umma::mixed_orbitals(e_hi, e_lo, lde, v_re_hi, v_re_lo, v_im_hi, v_im_lo,
                                    reinterpret_cast<const double2*>(phi_in), reinterpret_cast<double2*>(phi_out), work,
@@ -594,6 +616,42 @@ extern "C" int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float
 
 extern "C" int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, float* hi, float* lo, void* stream) {
   return (int)umma::mixed_rchol_pad(rchol, X, N, M, hi, lo, reinterpret_cast<cudaStream_t>(stream));
+}
+
+// Per-walker sum of the exchange partial rows: out[w] = sum_t part[t * W + w].
+__global__ void row_sum_kernel(const double2* __restrict__ part, int rows, int W, double2* __restrict__ out) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int t = 0; t < rows; ++t) acc = cadd(acc, part[(size_t)t * W + w]);
+  out[w] = acc;
+}
+
+extern "C" int ipie_b200_exchange_mixed(const float* r_hi, const float* r_lo, const void* ghalf,
+                                        const void* ghalf_trial, const void* kmat, const void* raw_trial, int W, int X,
+                                        int M, int N, float* gwork, void* part, void* exx, unsigned int* status,
+                                        void* stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  using CC = const double2*;
+  const int NP = umma::exchange_np(N);
+  if (NP < 0 || M % 4 || W <= 0 || X <= 0) return (int)cudaErrorInvalidValue;
+  const bool delta = ghalf_trial != nullptr;
+  if (delta && (kmat == nullptr || raw_trial == nullptr)) return (int)cudaErrorInvalidValue;
+  float* g_hi = gwork;
+  float* g_lo = gwork + (size_t)W * 2 * 32 * M;
+  double2* p = reinterpret_cast<double2*>(part);
+  cudaError_t e = umma::pad_ghalf((CC)ghalf, W, M, N, NP, g_hi, g_lo, st, delta ? (CC)ghalf_trial : nullptr);
+  if (e == cudaSuccess) e = umma::exchange3(r_hi, r_lo, g_hi, g_lo, W, X, M, N, p, status, st);
+  if (e != cudaSuccess) return (int)e;
+  int rows = umma::exchange3_rows(X, N);
+  if (delta) {
+    e = umma::exchange_ref_row((CC)ghalf, (CC)ghalf_trial, (CC)kmat, W, N * M, (CC)raw_trial, p + (size_t)rows * W, st);
+    if (e != cudaSuccess) return (int)e;
+    rows += 1;
+  }
+  row_sum_kernel<<<(W + 127) / 128, 128, 0, st>>>(p, rows, W, reinterpret_cast<double2*>(exx));
+  note_launch();
+  return (int)cudaGetLastError();
 }
 
 extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const float* ra_hi,

@@ -1,0 +1,361 @@
+// Fused mixed-precision orbital update of one spin block, one walker per CTA
+// at a time (persistent CTAs):
+//
+//     phi <- phi + (E - I) phi                  (one-body, FP64 add of a TF32 correction)
+//     T_0 = phi;  T_k = V T_{k-1} / k;  phi += T_k   (k = 1 .. nmax, Taylor series of exp(V))
+//     phi <- phi + (E - I) phi                  (one-body)
+//
+// Every product is a 3-pass TF32 tcgen05 GEMM (A_hi B_hi + A_hi B_lo + A_lo B_hi,
+// ~2^-22 relative) with FP32 accumulators in TMEM; phi accumulates in FP64.
+//
+// What stays on chip: the right operand B (the walker's current T_k or phi as
+// planar rows -- Re of orbital n at row n, Im at row BN/2 + n -- TF32 head and
+// remainder) lives in shared memory for the whole chain -- each term's
+// epilogue writes the next term's operand straight into the 128B-swizzled
+// K-major layout the MMA reads, so T_k never goes to global memory.  Only the
+// left operands stream through TMA: the walker's VHS planes (re/im, hi/lo,
+// read through a 3-D tensor map so rows past M are zero-filled without
+// traffic; the same ~0.6 MB for every term, so after the first term they come
+// from L2) and the shared E - I.
+//
+// Roles (192 threads): warps 0-3 epilogue (TMEM lanes 0-127, one output row per
+// thread), warp 4 lane 0 TMA producer, warp 5 lane 0 MMA issuer.  Barriers:
+// full/empty per stage (TMA <-> MMA), accb (MMA -> epilogue, once per term),
+// bready (epilogue -> MMA, 128 arrivals once per term: B written and TMEM read).
+// Every wait is bounded (umma.cuh); a timeout raises the status bit and all
+// roles leave their loops, then TMEM is released.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include "../../include/ipie_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+#include "umma.cuh"
+
+namespace ipie_b200 {
+namespace umma {
+
+cudaError_t make_map(CUtensorMap* m, const float* base, long long rows, long long k, long long ld, int box_rows);
+cudaError_t make_map_batched(CUtensorMap* m, const float* base, long long batch, long long rows, long long k,
+                             int box_rows);
+
+namespace {
+
+struct ChainMaps {
+  CUtensorMap e_hi, e_lo;  // E - I (M x M), box 128 x 32
+  CUtensorMap v[4];        // VHS planes re_hi, im_hi, re_lo, im_lo (W, M, M), box 1 x 128 x 32
+};
+
+constexpr int kATile = 128 * 128;        // 128 rows x 32 fp32
+constexpr int kStages = 3;
+constexpr int kStageBytes = 2 * kATile;  // re and im planes of one part (hi or lo)
+constexpr int kThreads = 192;
+constexpr int kMaxM = 256;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+// byte offset of B element (row n, k) inside one B region (hi or lo): k-block tiles of
+// BN rows x 128 bytes, 16-byte chunks XOR-swizzled with the row (TMA's 128B pattern)
+template <int BN>
+__device__ __forceinline__ uint32_t b_offset(int n, int k) {
+  const int kb = k >> 5, kc = k & 31;
+  return (uint32_t)(kb * BN * 128 + n * 128 + ((((kc >> 2) ^ (n & 7)) << 4) | ((kc & 3) << 2)));
+}
+
+template <int BN>
+__device__ __forceinline__ void put_b(uint8_t* bhi, uint8_t* blo, int n, int k, float h, float l) {
+  const uint32_t o = b_offset<BN>(n, k);
+  *reinterpret_cast<float*>(bhi + o) = h;
+  *reinterpret_cast<float*>(blo + o) = l;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads, 1)
+    orbital_chain_kernel(const __grid_constant__ ChainMaps maps, const double2* __restrict__ phi_in,
+                         double2* __restrict__ phi_out, int W, int M, int N, int nmax, unsigned* status) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int KB = (M + 31) / 32, MT = (M + 127) / 128;
+  constexpr int kBTile = BN * 128;
+  constexpr int kH = BN / 2;  // Im rows start here
+  uint8_t* b_hi = smem;
+  uint8_t* b_lo = smem + KB * kBTile;
+  uint8_t* stg = smem + 2 * KB * kBTile;
+  uint64_t* full = reinterpret_cast<uint64_t*>(stg + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* accb = empty + kStages;
+  uint64_t* bready = accb + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bready + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  constexpr uint32_t kTmemCols = 4 * BN;  // 2 m-tiles x 2 left operands x BN
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accb, 1);
+    mbar_init(bready, 128);
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  // rows n >= N (and kH + n >= kH + N) and k >= M of B stay zero for the whole kernel
+  for (int i = threadIdx.x; i < 2 * KB * kBTile / 16; i += kThreads)
+    reinterpret_cast<int4*>(smem)[i] = make_int4(0, 0, 0, 0);
+  fence_proxy_async_smem();
+  if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int nterms = nmax + 2;
+
+  if (warp == 4) {
+    // ------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      tma_prefetch_desc(&maps.e_hi);
+      tma_prefetch_desc(&maps.e_lo);
+      for (int i = 0; i < 4; ++i) tma_prefetch_desc(&maps.v[i]);
+      uint32_t g = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < W && ok; w += gridDim.x)
+        for (int t = 0; t < nterms && ok; ++t) {
+          const bool onebody = (t == 0 || t == nterms - 1);
+          for (int mt = 0; mt < MT && ok; ++mt)
+            for (int kb = 0; kb < KB && ok; ++kb)
+              for (int part = 0; part < 2; ++part, ++g) {
+                const uint32_t s = g % kStages, r = g / kStages;
+                if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) {
+                  ok = false;
+                  break;
+                }
+                uint8_t* st = stg + s * kStageBytes;
+                if (onebody) {
+                  mbar_expect_tx(&full[s], kATile);
+                  tma_load_2d(st, part ? &maps.e_lo : &maps.e_hi, kb * 32, mt * 128, &full[s]);
+                } else {
+                  // rows past M of the walker's matrix are zero-filled by TMA (no traffic)
+                  mbar_expect_tx(&full[s], 2 * kATile);
+                  tma_load_3d(st, &maps.v[2 * part], kb * 32, mt * 128, w, &full[s]);
+                  tma_load_3d(st + kATile, &maps.v[2 * part + 1], kb * 32, mt * 128, w, &full[s]);
+                }
+              }
+        }
+    }
+    __syncwarp();
+  } else if (warp == 5) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_tf32(128, BN);
+      uint32_t g = 0, term = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < W && ok; w += gridDim.x)
+        for (int t = 0; t < nterms && ok; ++t, ++term) {
+          const bool onebody = (t == 0 || t == nterms - 1);
+          if (!mbar_wait(bready, term & 1, abort_flag, status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          for (int mt = 0; mt < MT && ok; ++mt)
+            for (int kb = 0; kb < KB && ok; ++kb)
+              for (int part = 0; part < 2; ++part, ++g) {
+                const uint32_t s = g % kStages, r = g / kStages;
+                if (!mbar_wait(&full[s], r & 1, abort_flag, status)) {
+                  ok = false;
+                  break;
+                }
+                tc_fence_after();
+                uint8_t* st = stg + s * kStageBytes;
+                const uint64_t a0 = desc_kmajor_sw128(st), a1 = desc_kmajor_sw128(st + kATile);
+                const uint64_t bh = desc_kmajor_sw128(b_hi + kb * kBTile), bl = desc_kmajor_sw128(b_lo + kb * kBTile);
+                const uint32_t d0 = tmem + (uint32_t)((mt * 2 + 0) * BN), d1 = tmem + (uint32_t)((mt * 2 + 1) * BN);
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                  const uint32_t acc = (kb > 0 || kk > 0 || part > 0) ? 1u : 0u;
+                  if (part == 0) {
+                    mma_tf32(d0, a0 + 2 * kk, bh + 2 * kk, idesc, acc);
+                    mma_tf32(d0, a0 + 2 * kk, bl + 2 * kk, idesc, 1u);
+                    if (!onebody) {
+                      mma_tf32(d1, a1 + 2 * kk, bh + 2 * kk, idesc, acc);
+                      mma_tf32(d1, a1 + 2 * kk, bl + 2 * kk, idesc, 1u);
+                    }
+                  } else {
+                    mma_tf32(d0, a0 + 2 * kk, bh + 2 * kk, idesc, 1u);
+                    if (!onebody) mma_tf32(d1, a1 + 2 * kk, bh + 2 * kk, idesc, 1u);
+                  }
+                }
+                mma_commit(&empty[s]);
+              }
+          if (ok) mma_commit(accb);
+        }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue (warps 0-3)
+    uint32_t term = 0;
+    bool ok = true;
+    for (int w = blockIdx.x; w < W && ok; w += gridDim.x) {
+      const double2* pin = phi_in + (size_t)w * M * N;
+      double2* pout = phi_out + (size_t)w * M * N;
+      // prologue: B = planar split of the walker's starting orbitals (8 loads in flight per thread)
+      for (int m = threadIdx.x; m < M; m += 128)
+        for (int n0 = 0; n0 < N; n0 += 8) {
+          double2 z[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (n0 + q < N) z[q] = pin[(size_t)m * N + n0 + q];
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (n0 + q < N) {
+              float h, l;
+              split_tf32(z[q].x, h, l);
+              put_b<BN>(b_hi, b_lo, n0 + q, m, h, l);
+              split_tf32(z[q].y, h, l);
+              put_b<BN>(b_hi, b_lo, kH + n0 + q, m, h, l);
+            }
+        }
+      fence_proxy_async_smem();
+      mbar_arrive(bready);
+      for (int t = 0; t < nterms; ++t, ++term) {
+        if (!mbar_wait(accb, term & 1, abort_flag, status)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const bool onebody = (t == 0 || t == nterms - 1);
+        const float inv_k = onebody ? 1.0f : 1.0f / (float)t;
+        for (int mt = 0; mt < MT; ++mt) {
+          // warp-collective TMEM reads: every lane takes part, rows past M are dropped after
+          float d0[BN], d1[BN];
+          const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+#pragma unroll
+          for (int c = 0; c < BN / 32; ++c) {
+            float tmp[32];
+            tmem_ld32(tmem + lane_base + (uint32_t)((mt * 2 + 0) * BN + c * 32), tmp);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) d0[c * 32 + i] = tmp[i];
+            if (!onebody) {
+              tmem_ld32(tmem + lane_base + (uint32_t)((mt * 2 + 1) * BN + c * 32), tmp);
+#pragma unroll
+              for (int i = 0; i < 32; ++i) d1[c * 32 + i] = tmp[i];
+            }
+          }
+          const int m = mt * 128 + warp * 32 + lane;
+          if (m < M) {
+            // orbitals in chunks of 8: the chunk's FP64 loads are issued together so their
+            // latency is paid once per chunk; compile-time indices keep d0/d1 in registers
+#pragma unroll
+            for (int n0 = 0; n0 < kH; n0 += 8) {
+              if (n0 >= N) break;
+              double2 base[8];
+              const double2* src = (t == 0) ? pin : pout;
+#pragma unroll
+              for (int q = 0; q < 8; ++q)
+                if (n0 + q < N) base[q] = src[(size_t)m * N + n0 + q];
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                const int n = n0 + q;
+                if (n >= N) continue;
+                float ur, ui;
+                if (onebody) {
+                  ur = d0[n];
+                  ui = d0[kH + n];
+                } else {
+                  ur = d0[n] - d1[kH + n];
+                  ui = d0[kH + n] + d1[n];
+                }
+                const size_t idx = (size_t)m * N + n;
+                float h, l;
+                if (t == 0 || t == nterms - 1) {
+                  const double2 out = make_double2(base[q].x + (double)ur, base[q].y + (double)ui);
+                  pout[idx] = out;
+                  if (t == 0) {
+                    split_tf32(out.x, h, l);
+                    put_b<BN>(b_hi, b_lo, n, m, h, l);
+                    split_tf32(out.y, h, l);
+                    put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
+                  }
+                } else {
+                  const float tr = ur * inv_k, ti = ui * inv_k;
+                  const double2 acc = make_double2(base[q].x + tr, base[q].y + ti);
+                  pout[idx] = acc;
+                  if (t < nmax) {
+                    split_tf32(tr, h, l);
+                    put_b<BN>(b_hi, b_lo, n, m, h, l);
+                    split_tf32(ti, h, l);
+                    put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
+                  } else {
+                    split_tf32(acc.x, h, l);
+                    put_b<BN>(b_hi, b_lo, n, m, h, l);
+                    split_tf32(acc.y, h, l);
+                    put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
+                  }
+                }
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        if (t < nterms - 1) {
+          fence_proxy_async_smem();
+          mbar_arrive(bready);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+}
+
+template <int BN>
+cudaError_t launch_chain(const ChainMaps& maps, const double2* phi_in, double2* phi_out, int W, int M, int N, int nmax,
+                         unsigned* status, cudaStream_t st) {
+  const int KB = (M + 31) / 32;
+  const size_t smem = 1024 + 2 * (size_t)KB * BN * 128 + kStages * kStageBytes + 256;
+  auto kern = orbital_chain_kernel<BN>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  const int grid = W < sms ? W : sms;
+  kern<<<grid, kThreads, smem, st>>>(maps, phi_in, phi_out, W, M, N, nmax, status);
+  note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+bool orbital_chain_fits(int M, int N) { return M % 4 == 0 && M <= kMaxM && N >= 1 && N <= 32; }
+
+// One launch for the whole mixed orbital update of one spin block (see the file comment).
+// e_hi/e_lo: (E - I) (M, lde) fp32; v_*: VHS planes (W, M, M) fp32.
+cudaError_t mixed_orbital_chain(const float* e_hi, const float* e_lo, int lde, const float* v_re_hi,
+                                const float* v_re_lo, const float* v_im_hi, const float* v_im_lo,
+                                const double2* phi_in, double2* phi_out, int W, int M, int N, int nmax,
+                                unsigned* status, cudaStream_t st) {
+  if (!orbital_chain_fits(M, N) || nmax < 1 || phi_in == phi_out) return cudaErrorInvalidValue;
+  ChainMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  cudaError_t e;
+  if ((e = make_map(&maps.e_hi, e_hi, M, M, lde, 128)) != cudaSuccess) return e;
+  if ((e = make_map(&maps.e_lo, e_lo, M, M, lde, 128)) != cudaSuccess) return e;
+  const float* planes[4] = {v_re_hi, v_im_hi, v_re_lo, v_im_lo};
+  for (int i = 0; i < 4; ++i)
+    if ((e = make_map_batched(&maps.v[i], planes[i], W, M, M, 128)) != cudaSuccess) return e;
+  if (2 * N <= 32) return launch_chain<32>(maps, phi_in, phi_out, W, M, N, nmax, status, st);
+  return launch_chain<64>(maps, phi_in, phi_out, W, M, N, nmax, status, st);
+}
+
+}  // namespace umma
+}  // namespace ipie_b200

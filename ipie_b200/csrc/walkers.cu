@@ -213,6 +213,10 @@ cudaError_t launch_gf_overlap(const double2* phia, const double2* phib, int W, i
                               double2* ghalfb, double2* ovlp, double2* logdet, unsigned* status, cudaStream_t st) {
   const int Nmax = max(na, nb);
   if (Nmax <= 0 || M <= 0 || W <= 0) return cudaErrorInvalidValue;
+  // N <= 32: small-footprint kernel (greens.cu), several walkers per SM; larger blocks below
+  if (gf_lu32_fits(na, nb))
+    return launch_gf_lu32(phia, phib, W, M, na, nb, psia_c, psib_c, log_shift, ghalfa, ghalfb, ovlp, logdet, status,
+                          st);
   size_t smem = gf_smem_bytes(M, Nmax);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   if (ghalfa != nullptr) {

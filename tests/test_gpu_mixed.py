@@ -1,14 +1,16 @@
 """The mixed-precision form (TF32 tensor cores) against the FP64 form.
 
-Tolerances follow the arithmetic: the force bias is one TF32 pass (~2^-11
-relative), the VHS and orbital products are 3-pass TF32 (~2^-22); walker
-weights and overlaps after a few steps stay within 1e-5 of the FP64 path.
+Tolerances follow the arithmetic: the force bias, VHS, orbital and exchange
+products are 3-pass TF32 (~2^-22 relative per product); walker weights and
+overlaps after a few steps stay within 1e-5 of the FP64 path; the local energy,
+expanded around the trial, within 1e-6 (exact at the trial itself).
 """
 import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
 
+from oracle import afqmc_oracle as O  # noqa: E402
 from tests.test_gpu_parity import _walker_pert, dev, gpu_objects, rel  # noqa: E402
 
 pytestmark = pytest.mark.gpu
@@ -71,29 +73,30 @@ def test_mixed_vhs_3pass():
     walkers.check_status()
 
 
-@pytest.mark.parametrize("M,N", [(64, 8), (200, 32), (108, 15)])
-def test_mixed_orbital_update_3pass(M, N):
+@pytest.mark.parametrize("M,N,W", [(64, 8, 6), (200, 32, 6), (108, 15, 6), (128, 16, 5), (64, 4, 300),
+                                   (260, 4, 3)])
+def test_mixed_orbital_update_3pass(M, N, W):
+    """One-launch chain (M <= 256; W = 300 > SM count exercises the persistent walker loop) and the
+    per-term launches (M = 260) against the oracle's one-body, Taylor-6, one-body."""
     from ipie_b200 import synthetic
     from ipie_b200._lib import call, ptr, stream
 
     s = synthetic.generate(M, (N, N), 2 * M, decay=30.0, seed=9, uhf=True, chol_scale="stable")
-    W = 6
     ham, trial, walkers, prop, pm = _mixed_objects(s, W)
     pa, _ = _walker_pert(s, W, 4)
     rng = np.random.default_rng(2)
     xs = dev(rng.normal(size=(s.nchol, W)) + 0.2j * rng.normal(size=(s.nchol, W)))
     vhs = prop.construct_VHS(ham, xs)
-    ref = torch.empty(W, M, N, dtype=torch.complex128, device="cuda")
     pa_d = dev(pa)  # keep the input alive until the kernels have run
-    call("ipie_b200_propagate_orbitals", ptr(vhs), ptr(prop.expH1_pad[0]), prop.lda_e, ptr(pa_d), ptr(ref), W, M, N,
-         6, 1, 1, stream())
+    E = prop.expH1[0].real
+    ref = np.einsum("pq,wqn->wpn", E, O.apply_exponential(np.einsum("pq,wqn->wpn", E, pa), vhs.cpu().numpy(), 6))
     planes = []
     for part in (vhs.real.contiguous(), vhs.imag.contiguous()):
         hi = torch.empty(part.shape, dtype=torch.float32, device="cuda")
         lo = torch.empty_like(hi)
         call("ipie_b200_split_tf32", ptr(part), ptr(hi), ptr(lo), part.numel(), stream())
         planes += [hi, lo]
-    out = torch.empty_like(ref)
+    out = torch.empty_like(pa_d)
     work = torch.empty(4 * W * 2 * N * M, dtype=torch.float32, device="cuda")
     call("ipie_b200_propagate_orbitals_mixed", ptr(pm.e_hi[0]), ptr(pm.e_lo[0]), pm.lde, ptr(planes[0]), ptr(planes[1]),
          ptr(planes[2]), ptr(planes[3]), ptr(pa_d), ptr(out), ptr(work), W, M, N, 6, ptr(walkers.status), stream())
@@ -142,8 +145,9 @@ def test_mixed_local_energy(uhf, N):
     walkers.phia, walkers.phib = dev(pa), dev(pb)
     trial.calc_greens_function(walkers)
     ref = local_energy_single_det_uhf_batch(None, ham, walkers, trial)
+    # these walkers are random perturbations far from the trial: the expansion gains little here
     got = local_energy_mixed(None, ham, walkers, trial)
-    assert rel(got, ref) < 2e-7
+    assert rel(got, ref) < 1e-6
     plain = local_energy_mixed(None, ham, walkers, trial, reference=False)
     assert rel(plain, ref) < 2e-6
     walkers.check_status()
@@ -160,3 +164,26 @@ def test_mixed_local_energy_is_exact_at_the_trial():
     ref = local_energy_single_det_uhf_batch(None, ham, walkers, trial)
     got = local_energy_mixed(None, ham, walkers, trial)
     assert rel(got, ref) < 1e-12
+
+
+@pytest.mark.parametrize("uhf,N", [(False, 10), (True, 15)])
+def test_mixed_exchange_terms_match_fp64(uhf, N):
+    """ipie_b200_exchange_mixed (with and without the trial expansion, full and leading-vector
+    sums, on a walker subsample) against the FP64 exchange kernel."""
+    from ipie_b200 import synthetic
+    from ipie_b200.control_variate import EnergyParts
+
+    s = synthetic.generate(76, (N, N), 200, decay=30.0, seed=21, uhf=uhf, chol_scale="stable")
+    W = 24
+    ham, trial, walkers, prop = gpu_objects(s, W)
+    pa, pb = _walker_pert(s, W, 8)
+    walkers.phia, walkers.phib = dev(0.3 * pa + 0.7 * s.init[:, :N][None]), dev(0.3 * pb + 0.7 * s.init[:, N:][None])
+    trial.calc_greens_function(walkers)
+    p64 = EnergyParts(ham, trial, walkers)
+    pmx = EnergyParts(ham, trial, walkers, precision="mixed")
+    idx = torch.tensor([1, 4, 5, 17, 23], dtype=torch.int32, device="cuda")
+    for kw in ({}, {"nchol": 25}, {"idx": idx}):
+        ref = p64.exchange_term(walkers, **kw)
+        got = pmx.exchange_term(walkers, **kw)
+        assert rel(got, ref) < 1e-6, kw
+    walkers.check_status()
