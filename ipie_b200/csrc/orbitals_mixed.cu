@@ -6,7 +6,9 @@
 //     phi <- phi + (E - I) phi                  (one-body)
 //
 // Every product is a 3-pass TF32 tcgen05 GEMM (A_hi B_hi + A_hi B_lo + A_lo B_hi,
-// ~2^-22 relative) with FP32 accumulators in TMEM; phi accumulates in FP64.
+// ~2^-22 relative) with FP32 accumulators in TMEM.  phi accumulates in TMEM as
+// head/tail float pairs (~2^-47 relative) between the first one-body factor, read
+// from FP64 global memory, and the last, written to it in FP64.
 //
 // What stays on chip: the right operand B (the walker's current T_k or phi as
 // planar rows -- Re of orbital n at row n, Im at row BN/2 + n -- TF32 head and
@@ -19,7 +21,7 @@
 // from L2) and the shared E - I.
 //
 // Roles (192 threads): warps 0-3 epilogue (TMEM lanes 0-127, one output row per
-// thread), warp 4 lane 0 TMA producer, warp 5 lane 0 MMA issuer.  Barriers:
+// thread; between the two one-body factors it touches no global memory), warp 4 lane 0 TMA producer, warp 5 lane 0 MMA issuer.  Barriers:
 // full/empty per stage (TMA <-> MMA), accb (MMA -> epilogue, once per term),
 // bready (epilogue -> MMA, 128 arrivals once per term: B written and TMEM read).
 // Every wait is bounded (umma.cuh); a timeout raises the status bit and all
@@ -68,6 +70,18 @@ __device__ __forceinline__ uint32_t b_offset(int n, int k) {
   return (uint32_t)(kb * BN * 128 + n * 128 + ((((kc >> 2) ^ (n & 7)) << 4) | ((kc & 3) << 2)));
 }
 
+// (a, b) += x for a head/tail float pair a + b (|b| <= ulp(a)/2): Knuth's two-sum of a and x,
+// then the tail folded back; ~2^-47 relative, enough to accumulate the FP32 Taylor terms
+// of phi without a round trip through FP64 global memory.
+__device__ __forceinline__ void ff_add(float& a, float& b, float x) {
+  const float s = a + x;
+  const float v = s - a;
+  const float e = (a - (s - v)) + (x - v);
+  const float t = b + e;
+  a = s + t;
+  b = t - (a - s);
+}
+
 template <int BN>
 __device__ __forceinline__ void put_b(uint8_t* bhi, uint8_t* blo, int n, int k, float h, float l) {
   const uint32_t o = b_offset<BN>(n, k);
@@ -93,7 +107,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* bready = accb + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bready + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  constexpr uint32_t kTmemCols = 4 * BN;  // 2 m-tiles x 2 left operands x BN
+  // columns: accumulators 2 m-tiles x 2 left operands x BN, then phi as head/tail float pairs
+  // (2 m-tiles x [head BN | tail BN])
+  constexpr uint32_t kTmemCols = 8 * BN;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -232,77 +248,117 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_after();
         const bool onebody = (t == 0 || t == nterms - 1);
         const float inv_k = onebody ? 1.0f : 1.0f / (float)t;
+        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
         for (int mt = 0; mt < MT; ++mt) {
-          // warp-collective TMEM reads: every lane takes part, rows past M are dropped after
-          float d0[BN], d1[BN];
-          const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-#pragma unroll
-          for (int c = 0; c < BN / 32; ++c) {
-            float tmp[32];
-            tmem_ld32(tmem + lane_base + (uint32_t)((mt * 2 + 0) * BN + c * 32), tmp);
-#pragma unroll
-            for (int i = 0; i < 32; ++i) d0[c * 32 + i] = tmp[i];
-            if (!onebody) {
-              tmem_ld32(tmem + lane_base + (uint32_t)((mt * 2 + 1) * BN + c * 32), tmp);
-#pragma unroll
-              for (int i = 0; i < 32; ++i) d1[c * 32 + i] = tmp[i];
-            }
-          }
           const int m = mt * 128 + warp * 32 + lane;
-          if (m < M) {
-            // orbitals in chunks of 8: the chunk's FP64 loads are issued together so their
-            // latency is paid once per chunk; compile-time indices keep d0/d1 in registers
+          const bool row_ok = m < M;
+          const uint32_t dc0 = lane_base + (uint32_t)((mt * 2 + 0) * BN);
+          const uint32_t dc1 = lane_base + (uint32_t)((mt * 2 + 1) * BN);
+          const uint32_t ac = lane_base + (uint32_t)(4 * BN + mt * 2 * BN);  // acc: head [0, BN), tail [BN, 2BN)
+          // 16 orbitals at a time; TMEM reads/writes are warp-collective, so every lane takes
+          // part and rows past M only skip their global and shared-memory writes
 #pragma unroll
-            for (int n0 = 0; n0 < kH; n0 += 8) {
-              if (n0 >= N) break;
-              double2 base[8];
-              const double2* src = (t == 0) ? pin : pout;
+          for (int c0 = 0; c0 < kH; c0 += 16) {
+            if (c0 >= N) break;
+            uint32_t xr[16], xi[16], yr[16], yi[16], hr[16], hi_[16], lr[16], li[16];
+            tmem_ld16(tmem + dc0 + c0, xr);
+            tmem_ld16(tmem + dc0 + kH + c0, xi);
+            if (!onebody) {
+              tmem_ld16(tmem + dc1 + c0, yr);
+              tmem_ld16(tmem + dc1 + kH + c0, yi);
+            }
+            if (t > 0) {
+              tmem_ld16(tmem + ac + c0, hr);
+              tmem_ld16(tmem + ac + kH + c0, hi_);
+              tmem_ld16(tmem + ac + BN + c0, lr);
+              tmem_ld16(tmem + ac + BN + kH + c0, li);
+            }
+            tmem_wait_ld();
+            reg_after_wait(xr);
+            reg_after_wait(xi);
+            if (!onebody) {
+              reg_after_wait(yr);
+              reg_after_wait(yi);
+            }
+            if (t > 0) {
+              reg_after_wait(hr);
+              reg_after_wait(hi_);
+              reg_after_wait(lr);
+              reg_after_wait(li);
+            }
+            double2 base[16];
+            if (t == 0) {
 #pragma unroll
-              for (int q = 0; q < 8; ++q)
-                if (n0 + q < N) base[q] = src[(size_t)m * N + n0 + q];
+              for (int q = 0; q < 16; ++q)
+                base[q] = (row_ok && c0 + q < N) ? pin[(size_t)m * N + c0 + q] : make_double2(0.0, 0.0);
+            }
 #pragma unroll
-              for (int q = 0; q < 8; ++q) {
-                const int n = n0 + q;
-                if (n >= N) continue;
-                float ur, ui;
-                if (onebody) {
-                  ur = d0[n];
-                  ui = d0[kH + n];
-                } else {
-                  ur = d0[n] - d1[kH + n];
-                  ui = d0[kH + n] + d1[n];
+            for (int q = 0; q < 16; ++q) {
+              const int n = c0 + q;
+              float ur, ui;
+              if (onebody) {
+                ur = __uint_as_float(xr[q]);
+                ui = __uint_as_float(xi[q]);
+              } else {
+                ur = __uint_as_float(xr[q]) - __uint_as_float(yi[q]);
+                ui = __uint_as_float(xi[q]) + __uint_as_float(yr[q]);
+              }
+              const bool live = row_ok && n < N;
+              float h, l;
+              if (t == 0) {
+                // phi after the first one-body factor, kept as a head/tail float pair
+                const double oR = base[q].x + (double)ur, oI = base[q].y + (double)ui;
+                const float hR = (float)oR, hI = (float)oI;
+                hr[q] = __float_as_uint(hR);
+                hi_[q] = __float_as_uint(hI);
+                lr[q] = __float_as_uint((float)(oR - (double)hR));
+                li[q] = __float_as_uint((float)(oI - (double)hI));
+                if (live) {
+                  split_tf32(oR, h, l);
+                  put_b<BN>(b_hi, b_lo, n, m, h, l);
+                  split_tf32(oI, h, l);
+                  put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
                 }
-                const size_t idx = (size_t)m * N + n;
-                float h, l;
-                if (t == 0 || t == nterms - 1) {
-                  const double2 out = make_double2(base[q].x + (double)ur, base[q].y + (double)ui);
-                  pout[idx] = out;
-                  if (t == 0) {
-                    split_tf32(out.x, h, l);
-                    put_b<BN>(b_hi, b_lo, n, m, h, l);
-                    split_tf32(out.y, h, l);
-                    put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
-                  }
-                } else {
-                  const float tr = ur * inv_k, ti = ui * inv_k;
-                  const double2 acc = make_double2(base[q].x + tr, base[q].y + ti);
-                  pout[idx] = acc;
+              } else if (t == nterms - 1) {
+                if (live) {
+                  const double oR = (double)__uint_as_float(hr[q]) + (double)__uint_as_float(lr[q]) + (double)ur;
+                  const double oI = (double)__uint_as_float(hi_[q]) + (double)__uint_as_float(li[q]) + (double)ui;
+                  pout[(size_t)m * N + n] = make_double2(oR, oI);
+                }
+              } else {
+                const float tr = ur * inv_k, ti = ui * inv_k;
+                float aR = __uint_as_float(hr[q]), bR = __uint_as_float(lr[q]);
+                float aI = __uint_as_float(hi_[q]), bI = __uint_as_float(li[q]);
+                ff_add(aR, bR, tr);
+                ff_add(aI, bI, ti);
+                hr[q] = __float_as_uint(aR);
+                lr[q] = __float_as_uint(bR);
+                hi_[q] = __float_as_uint(aI);
+                li[q] = __float_as_uint(bI);
+                if (live) {
                   if (t < nmax) {
                     split_tf32(tr, h, l);
                     put_b<BN>(b_hi, b_lo, n, m, h, l);
                     split_tf32(ti, h, l);
                     put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
                   } else {
-                    split_tf32(acc.x, h, l);
+                    split_tf32((double)aR + (double)bR, h, l);
                     put_b<BN>(b_hi, b_lo, n, m, h, l);
-                    split_tf32(acc.y, h, l);
+                    split_tf32((double)aI + (double)bI, h, l);
                     put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
                   }
                 }
               }
             }
+            if (t < nterms - 1) {
+              tmem_st16(tmem + ac + c0, hr);
+              tmem_st16(tmem + ac + kH + c0, hi_);
+              tmem_st16(tmem + ac + BN + c0, lr);
+              tmem_st16(tmem + ac + BN + kH + c0, li);
+            }
           }
         }
+        tmem_wait_st();
         tc_fence_before();
         if (t < nterms - 1) {
           fence_proxy_async_smem();

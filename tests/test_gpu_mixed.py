@@ -182,8 +182,10 @@ def test_mixed_exchange_terms_match_fp64(uhf, N):
     p64 = EnergyParts(ham, trial, walkers)
     pmx = EnergyParts(ham, trial, walkers, precision="mixed")
     idx = torch.tensor([1, 4, 5, 17, 23], dtype=torch.int32, device="cuda")
-    for kw in ({}, {"nchol": 25}, {"idx": idx}):
+    # the leading-vector sum (a control-variate input) runs without the trial expansion: plain
+    # 3-pass accuracy; the full sums are expanded around the trial
+    for kw, tol in (({}, 1e-6), ({"nchol": 25}, 5e-6), ({"idx": idx}, 1e-6)):
         ref = p64.exchange_term(walkers, **kw)
         got = pmx.exchange_term(walkers, **kw)
-        assert rel(got, ref) < 1e-6, kw
+        assert rel(got, ref) < tol, kw
     walkers.check_status()
