@@ -40,6 +40,20 @@ WORKLOADS = {
 }
 
 
+METRIC = "walker-steps/s at <=0.1 mEh energy shift (mixed vs plain FP64 phaseless AFQMC step)"
+
+
+def line_config(wl, W, world, form="mixed"):
+    """The bench line's ``config`` (shared by both arms so the driver compares like with like)."""
+    p = WORKLOADS[wl]
+    return {
+        "workload": wl, "nbasis": p["nbasis"], "nalpha": p["nocc"], "nbeta": p["nocc"], "nchol": p["nchol"],
+        "walkers_per_gpu": W, "dt": 0.005, "form": form, "parallelism": f"replicas{world}",
+        "l2": "inputs larger than L2 (VHS 1.3 GB fp64 / 1.3 GB split fp32, walkers 0.2-0.4 GB)",
+        "step": "reortho/5, propagate, clip, pair-branch/5, energy/25 (ipie driver order)",
+    }
+
+
 def flops_per_walker(M, na, nb, X, alias=False):
     """Algorithmic real FLOPs per walker (complex mult-add = 8, real x complex = 4).
 
@@ -136,8 +150,13 @@ def dist_setup(ngpus):
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        # NCCL between GPUs; gloo when no GPU is visible (the CPU test of the multi-rank path)
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            backend = "nccl"
+        else:
+            backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return rank, world, local
@@ -150,7 +169,8 @@ def barrier_max(value, world):
         return value
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -158,7 +178,11 @@ def barrier_max(value, world):
 # DRAM bytes (read + write) per launch of a phase's kernel from one ncu capture, scaled to the
 # workload's walker count (the capture's traffic grows with the walkers it processes); the
 # capture and its command are summarised under profiles/.
-DRAM_TRAFFIC = {}
+DRAM_TRAFFIC = {
+    # orbital chain at 512 walkers: 740.2 MB read + 38.5 MB written per launch
+    # (profiles/orbital_chain_gf_vhs_fb_c2_w512.md), x4 for 2048 walkers
+    ("c2_rhf_m200", "mixed", "orbitals"): 4 * (740.2e6 + 38.5e6),
+}
 
 
 def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5):
@@ -231,19 +255,20 @@ def run_reference(args):
     cores = blas_threads()
     line = {
         "impl": "reference",
-        "metric": "walker-steps/s (plain FP64 phaseless AFQMC step)",
+        "metric": METRIC,
         "value": value,
         "unit": "walker-steps/s",
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": p["walkers"] / value * 1e3,
+        "ms_per_step": (args.walkers or p["walkers"]) / value * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": wl, **{k: p[k] for k in ("nbasis", "nocc", "nchol", "walkers")}, "dt": 0.005},
+        "config": line_config(wl, args.walkers or p["walkers"], int(os.environ.get("WORLD_SIZE", "1"))),
+        "reference_path": "ipie's numpy walker step (oracle restatement, pinned to ipie) on the host cores",
         "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -396,6 +421,7 @@ def run_ours(args):
     roofline = {
         "kernel": dom, "bound": "tensor", "pipe": pipe, "achieved": round(achieved, 3), "peak": peak,
         "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": DRAM_TRAFFIC.get((wl, head, dom)),
+        "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled by walkers)",
         "peak_source": src,
         "phase_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(phases.items())},
     }
@@ -460,7 +486,7 @@ def run_ours(args):
             rcpu, sample, _, _ = cpu_oracle_rate(wl, walkers_sample=args.ref_walkers, steps=2, energy_walkers=1)
             cpu = {"value": rcpu, "unit": "walker-steps/s", "cores": blas_threads(), "kind": "port", "sample": sample}
         line = {
-            "metric": "walker-steps/s at <=0.1 mEh energy shift (mixed vs plain FP64 phaseless AFQMC step)",
+            "metric": METRIC,
             "value": value,
             "unit": "walker-steps/s",
             "n_gpus": world,
@@ -472,12 +498,7 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "tf32+f64" if head == "mixed" else "f64",
             "data": "synthetic",
-            "config": {
-                "workload": wl, "nbasis": M, "nalpha": na, "nbeta": nb, "nchol": X, "walkers_per_gpu": W,
-                "dt": 0.005, "form": head, "parallelism": f"replicas{world}",
-                "l2": "inputs larger than L2 (VHS 1.3 GB fp64 / 1.3 GB split fp32, walkers 0.2-0.4 GB)",
-                "step": "reortho/5, propagate, clip, pair-branch/5, energy/25 (ipie driver order)",
-            },
+            "config": line_config(wl, W, world, head),
             "forms": forms_out,
             "energy_shift_mEh": shift,
             "energy_shift_method": ("max |block E(mixed) - block E(fp64)| over 50 steps (2 blocks) of 2 runs with "
