@@ -10,7 +10,9 @@ Default workload: nbasis 200, 32+32 electrons, 1600 Cholesky vectors,
 2048 walkers, dt 0.005 (synthetic Hamiltonian, seeded).
 
 ``value`` is walker-steps/s over the timed steps with all state resident in
-HBM (auxiliary fields drawn on the device).  ``e2e`` runs the same steps
+HBM (auxiliary fields drawn on the device); each step's propagation and weight
+clip replay from a captured CUDA graph (the phase breakdown comes from a few
+steps launched kernel by kernel).  ``e2e`` runs the same steps
 through the public API with the auxiliary fields supplied from pinned host
 memory each step and the weights read back each step.  ``--impl reference``
 times the CPU oracle (numpy restatement of ipie's path) on the host cores.
@@ -185,7 +187,7 @@ DRAM_TRAFFIC = {
 }
 
 
-def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5):
+def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5, graph=False):
     from ipie_b200 import AFQMC, Generic, SingleDet, synthetic
 
     p = WORKLOADS[wl]
@@ -196,7 +198,7 @@ def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5):
     af = AFQMC.build((s.nup, s.ndown), ham, trial, num_walkers=walkers, seed=seed, num_steps_per_block=25,
                      num_blocks=10 ** 6, timestep=0.005, stabilize_freq=5, pop_control_freq=pop_control_freq,
                      verbose=False, rng=rng,
-                     precision=precision)
+                     precision=precision, graph=graph)
     return af, s
 
 
@@ -320,7 +322,9 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
     from ipie_b200 import _lib
     from ipie_b200.propagation import PhaseTimer, _NoTimer
 
-    af, _ = build_afqmc(wl, W, rng, 7 + rank, precision=precision)
+    # each step's propagation and weight clip replay from a captured CUDA graph (device draws)
+    graph = rng == "device"
+    af, _ = build_afqmc(wl, W, rng, 7 + rank, precision=precision, graph=graph)
     af.setup_run()
     if cv is not None:
         from ipie_b200.control_variate import ControlVariateEnergyEstimator
@@ -330,11 +334,23 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
     for _ in range(args.warmup):
         step += 1
         af.step(step)
+    # phase breakdown: a few steps launched one kernel at a time with CUDA events between phases
     torch.cuda.synchronize()
     timer = PhaseTimer()
     af.propagator.timer = timer
+    af.use_graph = False
+    phase_steps = min(10, args.steps)
+    l0 = _lib.launch_count()
+    for _ in range(phase_steps):
+        step += 1
+        af.step(step)
+    torch.cuda.synchronize()
+    launches_per_step_eager = (_lib.launch_count() - l0) / phase_steps
+    af.propagator.timer = _NoTimer()
+    af.use_graph = graph
     nblocks0 = len(af.block_data)
     launches0 = _lib.launch_count()
+    replays0 = af.graphs.replays if af.graphs is not None else 0
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -352,10 +368,17 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
         clk.__exit__(None, None, None)
     if world > 1:
         torch.distributed.barrier()
+    # kernels launched in the timed region: ordinary launches plus the captured ones replayed
+    launches = _lib.launch_count() - launches0
+    if af.graphs is not None:
+        launches += (af.graphs.replays - replays0) * af.graphs.launches_per_step
     res = {
         "t": barrier_max(ev0.elapsed_time(ev1) / 1e3, world),
         "phases": timer.summary(),
-        "launches": _lib.launch_count() - launches0,
+        "phase_steps": phase_steps,
+        "launches": launches,
+        "launches_per_step_eager": launches_per_step_eager,
+        "graph": bool(graph),
         "blocks": np.array(af.block_data),
         "timed_blocks": np.array(af.block_data[nblocks0:]),
         "alias": bool(af.walkers.spin_alias),
@@ -423,7 +446,8 @@ def run_ours(args):
         "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": DRAM_TRAFFIC.get((wl, head, dom)),
         "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled by walkers)",
         "peak_source": src,
-        "phase_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(phases.items())},
+        "phase_ms_per_step": {k: round(v[1] / r["phase_steps"], 4) for k, v in sorted(phases.items())},
+        "phase_timing": f"{r['phase_steps']} steps launched kernel by kernel with CUDA events between phases",
     }
     step_flops = (sum(v for k, v in fl.items() if k != "orbitals") * W + fl_energy * W / 25.0)
     step_flops_ipie = (sum(v for k, v in fl_ipie.items() if k != "orbitals") * W + fl_energy_ipie * W / 25.0)
@@ -431,7 +455,7 @@ def run_ours(args):
     forms_out = {}
     for form, rr in runs.items():
         forms_out[form] = {"walker_steps_per_s": W * args.steps * world / rr["t"], "ms_per_step": rr["t"] / args.steps * 1e3,
-                           "gpu_launches": int(rr["launches"]),
+                           "gpu_launches": int(rr["launches"]), "cuda_graph_steps": rr["graph"],
                            "block_etotal": [round(float(x), 9) for x in rr["blocks"][:, 5]]}
     shift = None
     if "mixed" in runs and "fp64" in runs:

@@ -215,6 +215,11 @@ int ipie_b200_walker_sums(int W, const double* weight, const double* unscaled_we
  * propagation/phaseless_base.py:296-298 (xp.random.normal).  The sequence
  * differs from numpy's MT19937 by construction. */
 int ipie_b200_normal_fill(double* out, long long n, unsigned long long seed, unsigned long long offset, void* stream);
+/* The same draws with the counter block read from *counter (device memory), which is then
+ * advanced by one on the stream: a step captured in a CUDA graph draws a new block on
+ * every replay. */
+int ipie_b200_normal_fill_dev(double* out, long long n, unsigned long long seed, unsigned long long* counter,
+                              void* stream);
 
 /* ---- mixed-precision form: TF32 tensor cores (tcgen05), FP32 accumulation ----
  * FP64 stays in the overlap LU/determinant, the Green's function solve,

@@ -59,6 +59,7 @@ SIGNATURES = {
     "ipie_b200_split_tf32": [P, P, P, ctypes.c_longlong, P],
     "ipie_b200_umma_gemm_test": [P, P, P, P, P, P, P, I, I, I, I, I, P, P],
     "ipie_b200_normal_fill": [P, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_ulonglong, P],
+    "ipie_b200_normal_fill_dev": [P, ctypes.c_longlong, ctypes.c_ulonglong, P, P],
 }
 
 _lib = None

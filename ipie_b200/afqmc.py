@@ -75,11 +75,16 @@ class AFQMC:
             np.random.seed(params.rng_seed)  # ipie qmc/utils.py:24-40 (seed + rank, rank 0)
         self.block_data = []
         self.timers = {}
+        self.use_graph = False
+        self.graphs = None
 
     @staticmethod
     def build(num_elec, hamiltonian, trial_wavefunction, walkers=None, num_walkers=100, seed=None,
               num_steps_per_block=25, num_blocks=100, timestep=0.005, stabilize_freq=5, pop_control_freq=5,
-              verbose=True, mpi_handler=None, rng="numpy", spin_alias="auto", precision="fp64"):
+              verbose=True, mpi_handler=None, rng="numpy", spin_alias="auto", precision="fp64", graph=False):
+        """ipie's ``AFQMC.build`` (``qmc/afqmc.py:297-392``) plus the B200 options: ``rng`` ("numpy":
+        ipie's draws; "device": on-GPU draws), ``precision`` ("fp64" | "mixed"), ``spin_alias`` and
+        ``graph`` (replay each step's device work from a captured CUDA graph; needs rng="device")."""
         params = QMCParams(num_walkers, num_walkers, num_blocks, num_steps_per_block, timestep, stabilize_freq,
                            pop_control_freq, seed)
         if not trial_wavefunction.half_rotated:
@@ -96,7 +101,11 @@ class AFQMC:
         if spin_alias and getattr(trial_wavefunction, "spin_symmetric", False) and prop.spin_symmetric:
             if walkers.nup == walkers.ndown and torch.equal(walkers.phia, walkers.phib):
                 walkers.enable_spin_alias()
-        return AFQMC(num_elec, hamiltonian, trial_wavefunction, walkers, prop, params, verbose=verbose)
+        af = AFQMC(num_elec, hamiltonian, trial_wavefunction, walkers, prop, params, verbose=verbose)
+        af.use_graph = bool(graph)
+        if af.use_graph and rng != "device":
+            raise ValueError("graph=True needs rng='device'")
+        return af
 
     def _block(self, block, est, acc_vals):
         d = est.data.copy()
@@ -127,9 +136,16 @@ class AFQMC:
         w, ham, trial, prop, p = self.walkers, self.hamiltonian, self.trial, self.propagator, self.params
         if step % p.num_stblz == 0:
             w.orthogonalise()
-        prop.propagate_walkers(w, ham, trial, self.eshift)
-        if step > 1:
-            prop.clip_weights(w, self.pcontrol.total_weight * 0.10)
+        if self.use_graph and step > 1:
+            if self.graphs is None:
+                from .graphs import StepGraphs
+
+                self.graphs = StepGraphs(prop, w, ham, trial)
+            self.graphs.step(np.real(self.eshift), self.pcontrol.total_weight * 0.10)
+        else:
+            prop.propagate_walkers(w, ham, trial, self.eshift)
+            if step > 1:
+                prop.clip_weights(w, self.pcontrol.total_weight * 0.10)
         if step % p.pop_control_freq == 0:
             self.pcontrol.pop_control(w)
         self.accumulators.update(w)

@@ -181,4 +181,9 @@ int ipie_b200_normal_fill(double* out, long long n, unsigned long long seed, uns
   return (int)launch_normal_fill(out, n, seed, offset, ST(stream));
 }
 
+int ipie_b200_normal_fill_dev(double* out, long long n, unsigned long long seed, unsigned long long* counter,
+                              void* stream) {
+  return (int)launch_normal_fill_dev(out, n, seed, counter, ST(stream));
+}
+
 }  // extern "C"

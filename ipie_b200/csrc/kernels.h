@@ -50,6 +50,8 @@ cudaError_t launch_taylor(const double2* vhs, const double2* phi_in, double2* ph
 cudaError_t launch_exchange(const double* rchol, const double2* ghalf, int W, int X, int M, int N, double2* part,
                             int* ntiles, cudaStream_t st);
 
+cudaError_t launch_normal_fill_dev(double* out, long long n, unsigned long long seed, unsigned long long* counter,
+                                   cudaStream_t st);
 cudaError_t launch_normal_fill(double* out, long long n, unsigned long long seed, unsigned long long offset,
                                cudaStream_t st);
 cudaError_t launch_walker_sums(int W, const double* weight, const double* unscaled, const double2* ehyb,

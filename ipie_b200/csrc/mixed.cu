@@ -103,7 +103,7 @@ cudaError_t launch_umma(const GemmMaps& maps, int K, int a_rows_per_batch, int b
   auto kern = umma_gemm_kernel<BN, NA, NSPLIT, STAGES, Epi>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_BYTES);
   if (e != cudaSuccess) return e;
-  kern<<<grid, 128, S::SMEM_BYTES, st>>>(maps, K, a_rows_per_batch, b_rows_per_batch, epi, status);
+  kern<<<grid, kGemmThreads, S::SMEM_BYTES, st>>>(maps, K, a_rows_per_batch, b_rows_per_batch, epi, status);
   note_launch();
   return cudaGetLastError();
 }
@@ -324,7 +324,7 @@ struct EpiExchange {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 #pragma unroll
     for (int j = 0; j < BN; ++j) sC[tid * LD + j] = v[j];
-    __syncthreads();
+    epi_sync();
     for (int blk = warp; blk < XB * WB; blk += 4) {
       const int xl = blk / WB, wl = blk % WB;
       double2 s = make_double2(0.0, 0.0);
@@ -342,7 +342,7 @@ struct EpiExchange {
       s = warp_sum2(s);
       if (lane == 0) wpart[blk] = s;
     }
-    __syncthreads();
+    epi_sync();
     if (tid < WB) {
       const int w = n0 / (2 * NP) + tid;
       if (w < W) {

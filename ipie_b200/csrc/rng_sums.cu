@@ -59,6 +59,39 @@ cudaError_t launch_normal_fill(double* out, long long n, unsigned long long seed
   return cudaGetLastError();
 }
 
+// Same draws with the counter block read from device memory and advanced by one
+// afterwards (two launches): a captured CUDA graph then draws a new block per replay.
+__global__ void normal_fill_dev_kernel(double* __restrict__ out, long long n, unsigned long long seed,
+                                       const unsigned long long* __restrict__ counter) {
+  const unsigned long long offset = *counter;
+  const long long pairs = (n + 1) / 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < pairs; i += (long long)gridDim.x * blockDim.x) {
+    U4 c{(unsigned)i, (unsigned)(i >> 32), (unsigned)offset, (unsigned)(offset >> 32)};
+    U4 r = philox10(c, (unsigned)seed, (unsigned)(seed >> 32));
+    const double u1 = u53(r.x, r.y), u2 = u53(r.z, r.w);
+    const double rad = sqrt(-2.0 * log(u1));
+    double s, co;
+    sincospi(2.0 * u2, &s, &co);
+    out[2 * i] = rad * co;
+    if (2 * i + 1 < n) out[2 * i + 1] = rad * s;
+  }
+}
+
+__global__ void counter_add_kernel(unsigned long long* counter, unsigned long long inc) { *counter += inc; }
+
+cudaError_t launch_normal_fill_dev(double* out, long long n, unsigned long long seed, unsigned long long* counter,
+                                   cudaStream_t st) {
+  const long long pairs = (n + 1) / 2;
+  long long blocks = (pairs + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  normal_fill_dev_kernel<<<(unsigned)blocks, 256, 0, st>>>(out, n, seed, counter);
+  note_launch();
+  counter_add_kernel<<<1, 1, 0, st>>>(counter, 1ull);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // Uniform (0, 1] doubles from the same generator (pair-branch draws on device).
 __device__ double philox_uniform(unsigned long long seed, unsigned long long offset, unsigned long long i) {
   U4 c{(unsigned)i, (unsigned)(i >> 32), (unsigned)offset, (unsigned)(offset >> 32) ^ 0x5bd1e995u};

@@ -120,12 +120,13 @@ class PhaselessGeneric:
         self.rng = rng
         self.rng_seed = seed
         self.rng_counter = 0
+        self.rng_counter_dev = None  # device copy of the counter block of rng="device"
         self.vbias = None
         self.ws = None
         self.timer = _NoTimer()
         self.fused = True  # one launch per spin for one-body + exp(VHS) + one-body
-        # "fp64": the plain form (ipie's arithmetic); "mixed": force bias in TF32, VHS and the
-        # orbital update as 3-pass TF32 tensor-core products, FP64 everywhere else
+        # "fp64": the plain form (ipie's arithmetic); "mixed": force bias, VHS and the orbital
+        # update as 3-pass TF32 tensor-core products, FP64 everywhere else
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
         self.precision = precision
@@ -216,7 +217,11 @@ class PhaselessGeneric:
             src = next(self.host_fields)  # (W, X) float64, ideally pinned host memory
             ws.xi.copy_(src, non_blocking=True)
         else:
-            call("ipie_b200_normal_fill", ptr(ws.xi), W * X, self.rng_seed, self.rng_counter, stream())
+            # the counter lives on the device so that a step captured in a CUDA graph draws a
+            # new block on every replay (same sequence as counting on the host)
+            if self.rng_counter_dev is None:
+                self.rng_counter_dev = torch.full((1,), self.rng_counter, dtype=torch.int64, device=ws.xi.device)
+            call("ipie_b200_normal_fill_dev", ptr(ws.xi), W * X, self.rng_seed, ptr(self.rng_counter_dev), stream())
             self.rng_counter += 1
         return ws.xi
 
@@ -378,7 +383,9 @@ class PhaselessGeneric:
         ``ovlp`` is overwritten with ``ovlp_new`` and becomes ``walkers.ovlp``.
         """
         ws = self.ws
-        if isinstance(eshift, torch.Tensor):
+        if eshift is ws.eshift:
+            pass  # already on the device (set before a captured step is replayed)
+        elif isinstance(eshift, torch.Tensor):
             ws.eshift.copy_(eshift.reshape(1).to(F64))
         else:
             ws.eshift.fill_(float(np.real(eshift)))
@@ -387,7 +394,9 @@ class PhaselessGeneric:
              stream())
         walkers.ovlp = ovlp
 
-    def clip_weights(self, walkers, wbound):
-        """Driver weight clip to ``+-wbound`` (ipie ``qmc/afqmc.py:581-585``)."""
-        self.ws.wbound.fill_(float(wbound))
+    def clip_weights(self, walkers, wbound=None):
+        """Driver weight clip to ``+-wbound`` (ipie ``qmc/afqmc.py:581-585``); ``None`` keeps the bound
+        already in the workspace (set before a captured step is replayed)."""
+        if wbound is not None:
+            self.ws.wbound.fill_(float(wbound))
         call("ipie_b200_clip_weight", walkers.nwalkers, ptr(self.ws.wbound), ptr(walkers.weight), stream())
