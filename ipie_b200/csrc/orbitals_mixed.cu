@@ -20,10 +20,12 @@
 // traffic; the same ~0.6 MB for every term, so after the first term they come
 // from L2) and the shared E - I.
 //
-// Roles (192 threads): warps 0-3 epilogue (TMEM lanes 0-127, one output row per
-// thread; between the two one-body factors it touches no global memory), warp 4 lane 0 TMA producer, warp 5 lane 0 MMA issuer.  Barriers:
+// Roles (320 threads): warps 0-7 epilogue (warp w: TMEM lane quarter w % 4, i.e. one
+// output row per thread, and half w / 4 of the orbitals; between the two one-body
+// factors it touches no global memory), warp 8 lane 0 TMA producer, warp 9 lane 0
+// MMA issuer.  Barriers:
 // full/empty per stage (TMA <-> MMA), accb (MMA -> epilogue, once per term),
-// bready (epilogue -> MMA, 128 arrivals once per term: B written and TMEM read).
+// bready (epilogue -> MMA, 256 arrivals once per term: B written and TMEM read).
 // Every wait is bounded (umma.cuh); a timeout raises the status bit and all
 // roles leave their loops, then TMEM is released.
 #include <cuda.h>
@@ -52,7 +54,10 @@ struct ChainMaps {
 constexpr int kATile = 128 * 128;        // 128 rows x 32 fp32
 constexpr int kStages = 3;
 constexpr int kStageBytes = 2 * kATile;  // re and im planes of one part (hi or lo)
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;  // two per TMEM lane quarter, each taking half of the orbitals
+constexpr int kEpiThreads = 32 * kEpiWarps;
+constexpr int kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
+constexpr int kThreads = kEpiThreads + 64;
 constexpr int kMaxM = 256;
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -97,7 +102,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int KB = (M + 31) / 32, MT = (M + 127) / 128;
   constexpr int kBTile = BN * 128;
-  constexpr int kH = BN / 2;  // Im rows start here
+  constexpr int kH = BN / 2;     // Im rows start here
+  constexpr int kHalf = kH / 2;  // orbitals per epilogue warp group
   uint8_t* b_hi = smem;
   uint8_t* b_lo = smem + KB * kBTile;
   uint8_t* stg = smem + 2 * KB * kBTile;
@@ -118,7 +124,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&empty[s], 1);
     }
     mbar_init(accb, 1);
-    mbar_init(bready, 128);
+    mbar_init(bready, kEpiThreads);
     *abort_flag = 0;
     mbar_fence_init();
   }
@@ -133,7 +139,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
   const int nterms = nmax + 2;
 
-  if (warp == 4) {
+  if (warp == kProducerWarp) {
     // ------------------------------------------------------------ TMA producer
     if (lane == 0) {
       tma_prefetch_desc(&maps.e_hi);
@@ -166,7 +172,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     }
     __syncwarp();
-  } else if (warp == 5) {
+  } else if (warp == kMmaWarp) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_tf32(128, BN);
@@ -215,29 +221,34 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncwarp();
   } else {
-    // ------------------------------------------------------------ epilogue (warps 0-3)
+    // ------------------------------------------------------------ epilogue (warps 0-7)
     uint32_t term = 0;
     bool ok = true;
     for (int w = blockIdx.x; w < W && ok; w += gridDim.x) {
       const double2* pin = phi_in + (size_t)w * M * N;
       double2* pout = phi_out + (size_t)w * M * N;
-      // prologue: B = planar split of the walker's starting orbitals (8 loads in flight per thread)
-      for (int m = threadIdx.x; m < M; m += 128)
-        for (int n0 = 0; n0 < N; n0 += 8) {
-          double2 z[8];
+      // prologue: B = planar split of the walker's starting orbitals; thread e takes rows
+      // e % 128 (+128) and the orbital half e / 128 (8 loads in flight per thread)
+      {
+        const int e = threadIdx.x, half = e >> 7;
+        const int nlo = half * kHalf, nhi = min(N, nlo + kHalf);
+        for (int m = e & 127; m < M; m += 128)
+          for (int n0 = nlo; n0 < nhi; n0 += 8) {
+            double2 z[8];
 #pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (n0 + q < N) z[q] = pin[(size_t)m * N + n0 + q];
+            for (int q = 0; q < 8; ++q)
+              if (n0 + q < nhi) z[q] = pin[(size_t)m * N + n0 + q];
 #pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (n0 + q < N) {
-              float h, l;
-              split_tf32(z[q].x, h, l);
-              put_b<BN>(b_hi, b_lo, n0 + q, m, h, l);
-              split_tf32(z[q].y, h, l);
-              put_b<BN>(b_hi, b_lo, kH + n0 + q, m, h, l);
-            }
-        }
+            for (int q = 0; q < 8; ++q)
+              if (n0 + q < nhi) {
+                float h, l;
+                split_tf32(z[q].x, h, l);
+                put_b<BN>(b_hi, b_lo, n0 + q, m, h, l);
+                split_tf32(z[q].y, h, l);
+                put_b<BN>(b_hi, b_lo, kH + n0 + q, m, h, l);
+              }
+          }
+      }
       fence_proxy_async_smem();
       mbar_arrive(bready);
       for (int t = 0; t < nterms; ++t, ++term) {
@@ -248,30 +259,32 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_after();
         const bool onebody = (t == 0 || t == nterms - 1);
         const float inv_k = onebody ? 1.0f : 1.0f / (float)t;
-        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         for (int mt = 0; mt < MT; ++mt) {
-          const int m = mt * 128 + warp * 32 + lane;
+          const int m = mt * 128 + quarter * 32 + lane;
           const bool row_ok = m < M;
           const uint32_t dc0 = lane_base + (uint32_t)((mt * 2 + 0) * BN);
           const uint32_t dc1 = lane_base + (uint32_t)((mt * 2 + 1) * BN);
           const uint32_t ac = lane_base + (uint32_t)(4 * BN + mt * 2 * BN);  // acc: head [0, BN), tail [BN, 2BN)
-          // 16 orbitals at a time; TMEM reads/writes are warp-collective, so every lane takes
-          // part and rows past M only skip their global and shared-memory writes
+          // this warp's orbitals, 8 at a time; TMEM reads/writes are warp-collective, so every
+          // lane takes part and rows past M only skip their global and shared-memory writes
 #pragma unroll
-          for (int c0 = 0; c0 < kH; c0 += 16) {
+          for (int j = 0; j < kHalf; j += 8) {
+            const int c0 = half * kHalf + j;
             if (c0 >= N) break;
-            uint32_t xr[16], xi[16], yr[16], yi[16], hr[16], hi_[16], lr[16], li[16];
-            tmem_ld16(tmem + dc0 + c0, xr);
-            tmem_ld16(tmem + dc0 + kH + c0, xi);
+            uint32_t xr[8], xi[8], yr[8], yi[8], hr[8], hi_[8], lr[8], li[8];
+            tmem_ld8(tmem + dc0 + c0, xr);
+            tmem_ld8(tmem + dc0 + kH + c0, xi);
             if (!onebody) {
-              tmem_ld16(tmem + dc1 + c0, yr);
-              tmem_ld16(tmem + dc1 + kH + c0, yi);
+              tmem_ld8(tmem + dc1 + c0, yr);
+              tmem_ld8(tmem + dc1 + kH + c0, yi);
             }
             if (t > 0) {
-              tmem_ld16(tmem + ac + c0, hr);
-              tmem_ld16(tmem + ac + kH + c0, hi_);
-              tmem_ld16(tmem + ac + BN + c0, lr);
-              tmem_ld16(tmem + ac + BN + kH + c0, li);
+              tmem_ld8(tmem + ac + c0, hr);
+              tmem_ld8(tmem + ac + kH + c0, hi_);
+              tmem_ld8(tmem + ac + BN + c0, lr);
+              tmem_ld8(tmem + ac + BN + kH + c0, li);
             }
             tmem_wait_ld();
             reg_after_wait(xr);
@@ -286,14 +299,14 @@ __global__ void __launch_bounds__(kThreads, 1)
               reg_after_wait(lr);
               reg_after_wait(li);
             }
-            double2 base[16];
+            double2 base[8];
             if (t == 0) {
 #pragma unroll
-              for (int q = 0; q < 16; ++q)
+              for (int q = 0; q < 8; ++q)
                 base[q] = (row_ok && c0 + q < N) ? pin[(size_t)m * N + c0 + q] : make_double2(0.0, 0.0);
             }
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
+            for (int q = 0; q < 8; ++q) {
               const int n = c0 + q;
               float ur, ui;
               if (onebody) {
@@ -351,10 +364,10 @@ __global__ void __launch_bounds__(kThreads, 1)
               }
             }
             if (t < nterms - 1) {
-              tmem_st16(tmem + ac + c0, hr);
-              tmem_st16(tmem + ac + kH + c0, hi_);
-              tmem_st16(tmem + ac + BN + c0, lr);
-              tmem_st16(tmem + ac + BN + kH + c0, li);
+              tmem_st8(tmem + ac + c0, hr);
+              tmem_st8(tmem + ac + kH + c0, hi_);
+              tmem_st8(tmem + ac + BN + c0, lr);
+              tmem_st8(tmem + ac + BN + kH + c0, li);
             }
           }
         }

@@ -77,3 +77,40 @@ def test_mixed_one_rdm_properties():
     rdm = mixed_one_rdm(ham, trial, walkers).cpu().numpy()
     assert abs(np.trace(rdm[0]) - 6) < 1e-10 and abs(np.trace(rdm[1]) - 6) < 1e-10
     np.testing.assert_allclose(rdm[0], trial.G[0].real, atol=1e-10)
+
+
+def test_adjoint_response_on_walked_c4_walkers():
+    """The adjoint-property workload (M=76, 10+10 electrons, X=400, 512 walkers, V entries N(0, 0.1)):
+    after 25 steps of the walk, dE/dlambda from the adjoint equals the contraction of the mixed
+    1-RDM with V and central differences (lambda = +-1e-4) of the production energy estimator."""
+    from ipie_b200 import AFQMC, EnergyEstimator, Generic, SingleDet, synthetic
+    from ipie_b200.adjoint import energy_response, mixed_one_rdm
+
+    s = synthetic.workload("c4_rhf_m76", chol_scale="stable")
+    M = s.nbasis
+    A = np.random.default_rng(4).normal(0.0, 0.1, (M, M))
+    V = 0.5 * (A + A.T)
+    ham = Generic(s.h1e, s.chol, s.ecore)
+    trial = SingleDet(s.psi, (s.nup, s.ndown), M)
+    trial.half_rotate(ham)
+    af = AFQMC.build((s.nup, s.ndown), ham, trial, num_walkers=512, seed=3, num_steps_per_block=25, num_blocks=1,
+                     verbose=False, rng="device")
+    af.setup_run()
+    for step in range(1, 26):
+        af.step(step)
+    w = af.walkers
+    dE, E0 = energy_response(ham, trial, w, V)
+    rdm = mixed_one_rdm(ham, trial, w).cpu().numpy()
+    assert abs(np.sum(rdm[0] * V) + np.sum(rdm[1] * V) - dE) < 1e-10 * max(1.0, abs(dE))
+    eps = 1e-4
+    energies = []
+    for sign in (1.0, -1.0):
+        h1 = s.h1e + sign * eps * np.stack([V, V])
+        ham_s = Generic(h1, s.chol, s.ecore)
+        trial_s = SingleDet(s.psi, (s.nup, s.ndown), M)
+        trial_s.half_rotate(ham_s)
+        d = EnergyEstimator().compute_estimator(None, w, ham_s, trial_s)
+        energies.append((d[0] / d[1]).real)
+    fd = (energies[0] - energies[1]) / (2 * eps)
+    assert abs(fd - dE) < 1e-7 * max(1.0, abs(dE))
+    w.check_status()
