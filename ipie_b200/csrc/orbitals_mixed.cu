@@ -20,12 +20,12 @@
 // traffic; the same ~0.6 MB for every term, so after the first term they come
 // from L2) and the shared E - I.
 //
-// Roles (320 threads): warps 0-7 epilogue (warp w: TMEM lane quarter w % 4, i.e. one
-// output row per thread, and half w / 4 of the orbitals; between the two one-body
-// factors it touches no global memory), warp 8 lane 0 TMA producer, warp 9 lane 0
-// MMA issuer.  Barriers:
+// Roles (BN = 64: 576 threads): warps 0..4G-1 epilogue (warp w: TMEM lane quarter
+// w % 4, i.e. one output row per thread, and orbital group w / 4 of G = BN / 16 groups
+// of 8; between the two one-body factors it touches no global memory), then one warp
+// whose lane 0 is the TMA producer and one whose lane 0 issues the MMAs.  Barriers:
 // full/empty per stage (TMA <-> MMA), accb (MMA -> epilogue, once per term),
-// bready (epilogue -> MMA, 256 arrivals once per term: B written and TMEM read).
+// bready (epilogue -> MMA, one arrival per epilogue thread per term: B written and TMEM read).
 // Every wait is bounded (umma.cuh); a timeout raises the status bit and all
 // roles leave their loops, then TMEM is released.
 #include <cuda.h>
@@ -54,10 +54,15 @@ struct ChainMaps {
 constexpr int kATile = 128 * 128;        // 128 rows x 32 fp32
 constexpr int kStages = 3;
 constexpr int kStageBytes = 2 * kATile;  // re and im planes of one part (hi or lo)
-constexpr int kEpiWarps = 8;  // two per TMEM lane quarter, each taking half of the orbitals
-constexpr int kEpiThreads = 32 * kEpiWarps;
-constexpr int kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
-constexpr int kThreads = kEpiThreads + 64;
+// epilogue warps: kGroups per TMEM lane quarter, each taking 8 of the BN / 2 orbitals
+template <int BN>
+struct ChainRoles {
+  static constexpr int kGroups = BN / 16;
+  static constexpr int kEpiWarps = 4 * kGroups;
+  static constexpr int kEpiThreads = 32 * kEpiWarps;
+  static constexpr int kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
+  static constexpr int kThreads = kEpiThreads + 64;
+};
 constexpr int kMaxM = 256;
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -95,15 +100,18 @@ __device__ __forceinline__ void put_b(uint8_t* bhi, uint8_t* blo, int n, int k, 
 }
 
 template <int BN>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(ChainRoles<BN>::kThreads, 1)
     orbital_chain_kernel(const __grid_constant__ ChainMaps maps, const double2* __restrict__ phi_in,
                          double2* __restrict__ phi_out, int W, int M, int N, int nmax, unsigned* status) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int KB = (M + 31) / 32, MT = (M + 127) / 128;
   constexpr int kBTile = BN * 128;
-  constexpr int kH = BN / 2;     // Im rows start here
-  constexpr int kHalf = kH / 2;  // orbitals per epilogue warp group
+  constexpr int kH = BN / 2;  // Im rows start here
+  using R = ChainRoles<BN>;
+  constexpr int kEpiThreads = R::kEpiThreads, kThreads = R::kThreads;
+  constexpr int kProducerWarp = R::kProducerWarp, kMmaWarp = R::kMmaWarp;
+  constexpr int kHalf = kH / R::kGroups;  // orbitals per epilogue warp group (8)
   uint8_t* b_hi = smem;
   uint8_t* b_lo = smem + KB * kBTile;
   uint8_t* stg = smem + 2 * KB * kBTile;
@@ -221,14 +229,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncwarp();
   } else {
-    // ------------------------------------------------------------ epilogue (warps 0-7)
+    // ------------------------------------------------------------ epilogue warps
     uint32_t term = 0;
     bool ok = true;
     for (int w = blockIdx.x; w < W && ok; w += gridDim.x) {
       const double2* pin = phi_in + (size_t)w * M * N;
       double2* pout = phi_out + (size_t)w * M * N;
       // prologue: B = planar split of the walker's starting orbitals; thread e takes rows
-      // e % 128 (+128) and the orbital half e / 128 (8 loads in flight per thread)
+      // e % 128 (+128) and the orbital group e / 128 (8 loads in flight per thread)
       {
         const int e = threadIdx.x, half = e >> 7;
         const int nlo = half * kHalf, nhi = min(N, nlo + kHalf);
@@ -259,7 +267,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_after();
         const bool onebody = (t == 0 || t == nterms - 1);
         const float inv_k = onebody ? 1.0f : 1.0f / (float)t;
-        const int quarter = warp & 3, half = warp >> 2;
+        const int quarter = warp & 3, half = warp >> 2;  // lane quarter, orbital group
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         for (int mt = 0; mt < MT; ++mt) {
           const int m = mt * 128 + quarter * 32 + lane;
@@ -398,7 +406,7 @@ cudaError_t launch_chain(const ChainMaps& maps, const double2* phi_in, double2* 
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
   const int grid = W < sms ? W : sms;
-  kern<<<grid, kThreads, smem, st>>>(maps, phi_in, phi_out, W, M, N, nmax, status);
+  kern<<<grid, ChainRoles<BN>::kThreads, smem, st>>>(maps, phi_in, phi_out, W, M, N, nmax, status);
   note_launch();
   return cudaGetLastError();
 }
