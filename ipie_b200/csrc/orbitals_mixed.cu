@@ -24,7 +24,7 @@
 // w % 4, i.e. one output row per thread, and orbital group w / 4 of G = BN / 16 groups
 // of 8; between the two one-body factors it touches no global memory), then one warp
 // whose lane 0 is the TMA producer and one whose lane 0 issues the MMAs.  Barriers:
-// full/empty per stage (TMA <-> MMA), accb (MMA -> epilogue, once per term),
+// full/empty per stage (TMA <-> MMA), accb[mt] (MMA -> epilogue, once per 128-row tile and term),
 // bready (epilogue -> MMA, one arrival per epilogue thread per term: B written and TMEM read).
 // Every wait is bounded (umma.cuh); a timeout raises the status bit and all
 // roles leave their loops, then TMEM is released.
@@ -117,8 +117,8 @@ __global__ void __launch_bounds__(ChainRoles<BN>::kThreads, 1)
   uint8_t* stg = smem + 2 * KB * kBTile;
   uint64_t* full = reinterpret_cast<uint64_t*>(stg + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accb = empty + kStages;
-  uint64_t* bready = accb + 1;
+  uint64_t* accb = empty + kStages;  // one per 128-row tile (M <= 256)
+  uint64_t* bready = accb + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bready + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   // columns: accumulators 2 m-tiles x 2 left operands x BN, then phi as head/tail float pairs
@@ -131,7 +131,8 @@ __global__ void __launch_bounds__(ChainRoles<BN>::kThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accb, 1);
+    mbar_init(&accb[0], 1);
+    mbar_init(&accb[1], 1);
     mbar_init(bready, kEpiThreads);
     *abort_flag = 0;
     mbar_fence_init();
@@ -223,8 +224,8 @@ __global__ void __launch_bounds__(ChainRoles<BN>::kThreads, 1)
                   }
                 }
                 mma_commit(&empty[s]);
+                if (kb == KB - 1 && part == 1) mma_commit(&accb[mt]);
               }
-          if (ok) mma_commit(accb);
         }
     }
     __syncwarp();
@@ -235,150 +236,131 @@ __global__ void __launch_bounds__(ChainRoles<BN>::kThreads, 1)
     for (int w = blockIdx.x; w < W && ok; w += gridDim.x) {
       const double2* pin = phi_in + (size_t)w * M * N;
       double2* pout = phi_out + (size_t)w * M * N;
-      // prologue: B = planar split of the walker's starting orbitals; thread e takes rows
-      // e % 128 (+128) and the orbital group e / 128 (8 loads in flight per thread)
-      {
-        const int e = threadIdx.x, half = e >> 7;
-        const int nlo = half * kHalf, nhi = min(N, nlo + kHalf);
-        for (int m = e & 127; m < M; m += 128)
-          for (int n0 = nlo; n0 < nhi; n0 += 8) {
-            double2 z[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-              if (n0 + q < nhi) z[q] = pin[(size_t)m * N + n0 + q];
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-              if (n0 + q < nhi) {
-                float h, l;
-                split_tf32(z[q].x, h, l);
-                put_b<BN>(b_hi, b_lo, n0 + q, m, h, l);
-                split_tf32(z[q].y, h, l);
-                put_b<BN>(b_hi, b_lo, kH + n0 + q, m, h, l);
-              }
-          }
+      // prologue: B = planar split of the walker's starting orbitals, read coalesced (consecutive
+      // threads take consecutive elements of the row-major M x N block)
+      for (int i = threadIdx.x; i < M * N; i += kEpiThreads) {
+        const int m = i / N, n = i - m * N;
+        const double2 z = pin[i];
+        float h, l;
+        split_tf32(z.x, h, l);
+        put_b<BN>(b_hi, b_lo, n, m, h, l);
+        split_tf32(z.y, h, l);
+        put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
       }
       fence_proxy_async_smem();
       mbar_arrive(bready);
+      static_assert(kHalf == 8, "one group of 8 orbitals per epilogue warp");
+      const int quarter = warp & 3, half = warp >> 2;  // lane quarter, orbital group
+      const int c0 = half * kHalf;                     // this warp's first orbital
+      const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
       for (int t = 0; t < nterms; ++t, ++term) {
-        if (!mbar_wait(accb, term & 1, abort_flag, status)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
         const bool onebody = (t == 0 || t == nterms - 1);
         const float inv_k = onebody ? 1.0f : 1.0f / (float)t;
-        const int quarter = warp & 3, half = warp >> 2;  // lane quarter, orbital group
-        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-        for (int mt = 0; mt < MT; ++mt) {
+        // B values of the first 128-row tile, held back until every MMA of this term (which
+        // still reads the current B) has completed; [p][q], p = 0 real, 1 imaginary
+        float dh[2][8], dl[2][8];
+        bool held = false;
+        for (int mt = 0; mt < MT && ok; ++mt) {
+          // each 128-row tile has its own accumulator barrier, so the first tile's epilogue
+          // overlaps the second tile's MMAs
+          if (!mbar_wait(&accb[mt], term & 1, abort_flag, status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          if (held) {
+            const int mp = (mt - 1) * 128 + quarter * 32 + lane;
+            if (mp < M)
+#pragma unroll
+              for (int p = 0; p < 2; ++p)
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                  if (c0 + q < N) put_b<BN>(b_hi, b_lo, (p ? kH : 0) + c0 + q, mp, dh[p][q], dl[p][q]);
+            held = false;
+          }
+          // a warp whose 32 rows all lie past M, or whose orbitals all lie past N, has nothing to do
+          if (mt * 128 + quarter * 32 >= M || c0 >= N) continue;
+          const bool hold = mt + 1 < MT && t < nterms - 1;
           const int m = mt * 128 + quarter * 32 + lane;
           const bool row_ok = m < M;
           const uint32_t dc0 = lane_base + (uint32_t)((mt * 2 + 0) * BN);
           const uint32_t dc1 = lane_base + (uint32_t)((mt * 2 + 1) * BN);
           const uint32_t ac = lane_base + (uint32_t)(4 * BN + mt * 2 * BN);  // acc: head [0, BN), tail [BN, 2BN)
-          // this warp's orbitals, 8 at a time; TMEM reads/writes are warp-collective, so every
-          // lane takes part and rows past M only skip their global and shared-memory writes
+          // real parts, then imaginary parts (half the live registers of both at once); TMEM
+          // reads/writes are warp-collective, so every lane takes part and rows past M only
+          // skip their global and shared-memory writes
 #pragma unroll
-          for (int j = 0; j < kHalf; j += 8) {
-            const int c0 = half * kHalf + j;
-            if (c0 >= N) break;
-            uint32_t xr[8], xi[8], yr[8], yi[8], hr[8], hi_[8], lr[8], li[8];
-            tmem_ld8(tmem + dc0 + c0, xr);
-            tmem_ld8(tmem + dc0 + kH + c0, xi);
-            if (!onebody) {
-              tmem_ld8(tmem + dc1 + c0, yr);
-              tmem_ld8(tmem + dc1 + kH + c0, yi);
-            }
+          for (int p = 0; p < 2; ++p) {
+            // p = 0: Re = D0[n] - D1[kH + n]; p = 1: Im = D0[kH + n] + D1[n]
+            // (one-body: D0[n] and D0[kH + n] with the real left operand E - I)
+            const int cx = (p ? kH : 0) + c0, cy = (p ? 0 : kH) + c0;
+            uint32_t x[8], y[8], ha[8], ta[8];
+            tmem_ld8(tmem + dc0 + cx, x);
+            if (!onebody) tmem_ld8(tmem + dc1 + cy, y);
             if (t > 0) {
-              tmem_ld8(tmem + ac + c0, hr);
-              tmem_ld8(tmem + ac + kH + c0, hi_);
-              tmem_ld8(tmem + ac + BN + c0, lr);
-              tmem_ld8(tmem + ac + BN + kH + c0, li);
+              tmem_ld8(tmem + ac + cx, ha);
+              tmem_ld8(tmem + ac + BN + cx, ta);
             }
             tmem_wait_ld();
-            reg_after_wait(xr);
-            reg_after_wait(xi);
-            if (!onebody) {
-              reg_after_wait(yr);
-              reg_after_wait(yi);
-            }
+            reg_after_wait(x);
+            if (!onebody) reg_after_wait(y);
             if (t > 0) {
-              reg_after_wait(hr);
-              reg_after_wait(hi_);
-              reg_after_wait(lr);
-              reg_after_wait(li);
+              reg_after_wait(ha);
+              reg_after_wait(ta);
             }
-            double2 base[8];
+            double base[8];
             if (t == 0) {
 #pragma unroll
-              for (int q = 0; q < 8; ++q)
-                base[q] = (row_ok && c0 + q < N) ? pin[(size_t)m * N + c0 + q] : make_double2(0.0, 0.0);
+              for (int q = 0; q < 8; ++q) {
+                const double* src = reinterpret_cast<const double*>(pin + (size_t)m * N + c0 + q) + p;
+                base[q] = (row_ok && c0 + q < N) ? *src : 0.0;
+              }
             }
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
               const int n = c0 + q;
-              float ur, ui;
-              if (onebody) {
-                ur = __uint_as_float(xr[q]);
-                ui = __uint_as_float(xi[q]);
-              } else {
-                ur = __uint_as_float(xr[q]) - __uint_as_float(yi[q]);
-                ui = __uint_as_float(xi[q]) + __uint_as_float(yr[q]);
-              }
+              float u = __uint_as_float(x[q]);
+              if (!onebody) u = p ? u + __uint_as_float(y[q]) : u - __uint_as_float(y[q]);
               const bool live = row_ok && n < N;
-              float h, l;
+              float h = 0.0f, l = 0.0f;
               if (t == 0) {
                 // phi after the first one-body factor, kept as a head/tail float pair
-                const double oR = base[q].x + (double)ur, oI = base[q].y + (double)ui;
-                const float hR = (float)oR, hI = (float)oI;
-                hr[q] = __float_as_uint(hR);
-                hi_[q] = __float_as_uint(hI);
-                lr[q] = __float_as_uint((float)(oR - (double)hR));
-                li[q] = __float_as_uint((float)(oI - (double)hI));
-                if (live) {
-                  split_tf32(oR, h, l);
-                  put_b<BN>(b_hi, b_lo, n, m, h, l);
-                  split_tf32(oI, h, l);
-                  put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
-                }
+                const double o = base[q] + (double)u;
+                const float hh = (float)o;
+                ha[q] = __float_as_uint(hh);
+                ta[q] = __float_as_uint((float)(o - (double)hh));
+                split_tf32(o, h, l);
               } else if (t == nterms - 1) {
-                if (live) {
-                  const double oR = (double)__uint_as_float(hr[q]) + (double)__uint_as_float(lr[q]) + (double)ur;
-                  const double oI = (double)__uint_as_float(hi_[q]) + (double)__uint_as_float(li[q]) + (double)ui;
-                  pout[(size_t)m * N + n] = make_double2(oR, oI);
-                }
+                const double o = (double)__uint_as_float(ha[q]) + (double)__uint_as_float(ta[q]) + (double)u;
+                if (live) reinterpret_cast<double*>(pout + (size_t)m * N + n)[p] = o;
               } else {
-                const float tr = ur * inv_k, ti = ui * inv_k;
-                float aR = __uint_as_float(hr[q]), bR = __uint_as_float(lr[q]);
-                float aI = __uint_as_float(hi_[q]), bI = __uint_as_float(li[q]);
-                ff_add(aR, bR, tr);
-                ff_add(aI, bI, ti);
-                hr[q] = __float_as_uint(aR);
-                lr[q] = __float_as_uint(bR);
-                hi_[q] = __float_as_uint(aI);
-                li[q] = __float_as_uint(bI);
-                if (live) {
-                  if (t < nmax) {
-                    split_tf32(tr, h, l);
-                    put_b<BN>(b_hi, b_lo, n, m, h, l);
-                    split_tf32(ti, h, l);
-                    put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
-                  } else {
-                    split_tf32((double)aR + (double)bR, h, l);
-                    put_b<BN>(b_hi, b_lo, n, m, h, l);
-                    split_tf32((double)aI + (double)bI, h, l);
-                    put_b<BN>(b_hi, b_lo, kH + n, m, h, l);
-                  }
+                const float tk = u * inv_k;
+                float a = __uint_as_float(ha[q]), b = __uint_as_float(ta[q]);
+                ff_add(a, b, tk);
+                ha[q] = __float_as_uint(a);
+                ta[q] = __float_as_uint(b);
+                if (t < nmax)
+                  split_tf32(tk, h, l);
+                else
+                  split_tf32((double)a + (double)b, h, l);
+              }
+              if (t < nterms - 1) {
+                if (hold) {
+                  dh[p][q] = h;
+                  dl[p][q] = l;
+                } else if (live) {
+                  put_b<BN>(b_hi, b_lo, cx + q, m, h, l);
                 }
               }
             }
             if (t < nterms - 1) {
-              tmem_st8(tmem + ac + c0, hr);
-              tmem_st8(tmem + ac + kH + c0, hi_);
-              tmem_st8(tmem + ac + BN + c0, lr);
-              tmem_st8(tmem + ac + BN + kH + c0, li);
+              tmem_st8(tmem + ac + cx, ha);
+              tmem_st8(tmem + ac + BN + cx, ta);
             }
           }
+          held = hold;
         }
+        if (!ok) break;
         tmem_wait_st();
         tc_fence_before();
         if (t < nterms - 1) {

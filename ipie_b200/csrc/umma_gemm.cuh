@@ -16,17 +16,20 @@
 // finished chunk into FP32 registers (round-to-nearest adds) while the tensor
 // cores fill the other buffer, which bounds the shrink to that of one chunk.
 //
-// Roles (192 threads): warp 4 lane 0 issues TMA loads into a STAGES-deep ring
-// (full/empty mbarriers); warp 5 lane 0 issues tcgen05.mma; warps 0-3 (TMEM
-// lanes 0-127, one output row per thread) drain the chunks (chunk_full /
-// chunk_empty mbarriers) and run the epilogue on the summed row of NA*BN
-// values.  Epilogues synchronise with bar.sync 1, 128 (epi_sync), never with
-// __syncthreads.
+// Roles: 4 epilogue warps per 128 accumulator columns (warp w: TMEM lane
+// quarter w % 4, i.e. one output row per thread, and column group w / 4) drain
+// the chunks (chunk_full / chunk_empty mbarriers) and run the epilogue on their
+// group's summed 128 values (a tile of BN = 256 is handed to the epilogue as two
+// 128-column tiles); then one warp whose lane 0 issues TMA loads into a
+// STAGES-deep ring (full/empty mbarriers) and one whose lane 0 issues
+// tcgen05.mma.  One-group epilogues may synchronise with bar.sync 1, 128
+// (epi_sync), never with __syncthreads.
 //
-// Batching: grid.z indexes a batch; the tile's first A row is
-// z * a_rows_per_batch + blockIdx.y * 128 and its first B row
-// z * b_rows_per_batch + blockIdx.x * BN (rows past a batch's own extent read
-// the next batch or TMA's zero fill; the epilogue drops them).
+// Tiles: TileOrder numbers the 128 x BN output tiles of nz batches; a tile
+// (z, mt, nt) reads A rows from z * a_rows_per_batch + mt * 128 and B rows from
+// z * b_rows_per_batch + nt * BN (rows past a batch's own extent read the next
+// batch or TMA's zero fill; the epilogue drops them).  The CTAs are persistent:
+// one per SM, each walking the tile list with stride gridDim.x.
 #pragma once
 
 #include "umma.cuh"
@@ -46,18 +49,29 @@ constexpr int kBK = 32;  // fp32 per 128-byte row
 
 __host__ __device__ constexpr int tmem_cols_for(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : n <= 256 ? 256 : 512; }
 
-constexpr int kGemmThreads = 192;
 constexpr int kChunkKB = 2;  // k-blocks (of 32) accumulated in TMEM before a drain
 
-// named barrier of the 128 epilogue threads (warps 0-3)
+// Epilogue warps: one group of 4 (the four TMEM lane quarters) per 128 accumulator
+// columns; then a producer and an MMA warp.
+template <int NA, int BN>
+struct GemmRoles {
+  static constexpr int kGroups = (NA * BN + 127) / 128;
+  static constexpr int kGroupCols = NA * BN / kGroups;
+  static constexpr int kEpiThreads = 128 * kGroups;
+  static constexpr int kThreads = kEpiThreads + 64;
+  static constexpr int kProducerWarp = 4 * kGroups, kMmaWarp = 4 * kGroups + 1;
+  static_assert(NA * BN % kGroups == 0 && kGroupCols % 32 == 0, "column groups of whole 32-column loads");
+};
+
+// named barrier of the 128 epilogue threads of a one-group tile (warps 0-3)
 __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
-// AND of pred over the 128 epilogue threads (named barrier 1)
-__device__ __forceinline__ bool epi_all(bool pred) {
+// AND of pred over the nthreads epilogue threads (named barrier 2)
+__device__ __forceinline__ bool epi_all(bool pred, int nthreads) {
   uint32_t r;
   asm volatile(
-      "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.and.pred q, 1, 128, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+      "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.and.pred q, 2, %2, p;\nselp.u32 %0, 1, 0, q;\n}\n"
       : "=r"(r)
-      : "r"((uint32_t)pred)
+      : "r"((uint32_t)pred), "r"(nthreads)
       : "memory");
   return r != 0;
 }
@@ -65,7 +79,40 @@ __device__ __forceinline__ void mbar_arrive_cta(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
-template <int BN, int NA, int NSPLIT, int STAGES>
+// Order of the output tiles: tile l (of nm x nn x nz) has batch z = l / (nm * nn) and, inside the
+// batch, the row-tile index fastest (m_fast) or the column-tile index fastest.  The CTAs resident
+// at one time take consecutive tiles, so the operand that is swept along the fast index should
+// be the one that fits in L2.
+struct TileOrder {
+  int nm, nn, nz;
+  int m_fast;
+  __host__ __device__ int count() const { return nm * nn * nz; }
+  __device__ void decode(int l, int& z, int& mt, int& nt) const {
+    const int per = nm * nn;
+    z = l / per;
+    const int r = l - z * per;
+    if (m_fast) {
+      mt = r % nm;
+      nt = r / nm;
+    } else {
+      nt = r % nn;
+      mt = r / nn;
+    }
+  }
+};
+
+// Epilogues declare the shared memory they use (kSmemBytes): it is a region of its own, since in
+// a persistent CTA the TMA ring is already refilled for the next tile while an epilogue runs.
+template <class Epi, class = void>
+struct EpiSmem {
+  static constexpr int value = 0;
+};
+template <class Epi>
+struct EpiSmem<Epi, decltype((void)Epi::kSmemBytes)> {
+  static constexpr int value = Epi::kSmemBytes;
+};
+
+template <int BN, int NA, int NSPLIT, int STAGES, int EPI_SMEM = 0>
 struct GemmShape {
   static constexpr int A_TILE = kBM * kBK * 4;
   static constexpr int B_TILE = BN * kBK * 4;
@@ -74,23 +121,31 @@ struct GemmShape {
   static constexpr int STAGE_BYTES = NAT * A_TILE + NBT * B_TILE;
   static constexpr int BUF_COLS = tmem_cols_for(NA * BN);  // one accumulator buffer
   static constexpr int TMEM_COLS = 2 * BUF_COLS;
-  static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
+  static constexpr int EPI_OFFSET = STAGES * STAGE_BYTES;
+  static constexpr int BAR_OFFSET = EPI_OFFSET + ((EPI_SMEM + 15) / 16) * 16;
+  static constexpr int SMEM_BYTES = 1024 + BAR_OFFSET + 256;
   static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "BN must be a multiple of 32 in [32, 256]");
   static_assert(2 * NA * BN <= 512, "two accumulator buffers exceed TMEM");
   static_assert(STAGE_BYTES % 1024 == 0, "stage must keep 1024-byte alignment");
+  static_assert(SMEM_BYTES <= 232448, "shared memory per CTA exceeded");
 };
 
+// Persistent CTAs: CTA b computes tiles b, b + gridDim.x, ...; the stage ring, the chunk counter
+// and the two TMEM buffers run on across tiles, so one tile's epilogue overlaps the next tile's
+// loads and first MMAs.
 template <int BN, int NA, int NSPLIT, int STAGES, class Epi>
-__global__ void __launch_bounds__(kGemmThreads, 1)
-    umma_gemm_kernel(const __grid_constant__ GemmMaps maps, int K, int a_rows_per_batch, int b_rows_per_batch, Epi epi,
-                     unsigned* status) {
-  using S = GemmShape<BN, NA, NSPLIT, STAGES>;
+__global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
+    umma_gemm_kernel(const __grid_constant__ GemmMaps maps, int K, int a_rows_per_batch, int b_rows_per_batch,
+                     TileOrder order, Epi epi, unsigned* status) {
+  using S = GemmShape<BN, NA, NSPLIT, STAGES, EpiSmem<Epi>::value>;
+  using R = GemmRoles<NA, BN>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * S::STAGE_BYTES);
+  uint8_t* epi_smem = smem + S::EPI_OFFSET;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S::BAR_OFFSET);
   uint64_t* empty = full + STAGES;
   uint64_t* cfull = empty + STAGES;  // [2] chunk accumulated (MMA commit)
-  uint64_t* cempty = cfull + 2;      // [2] chunk drained (128 epilogue arrivals)
+  uint64_t* cempty = cfull + 2;      // [2] chunk drained (one arrival per epilogue thread)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -102,7 +157,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&cfull[b], 1);
-      mbar_init(&cempty[b], 128);
+      mbar_init(&cempty[b], R::kEpiThreads);
     }
     *abort_flag = 0;
     mbar_fence_init();
@@ -115,12 +170,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
   const int nk = (K + kBK - 1) / kBK;
   const int nchunks = (nk + kChunkKB - 1) / kChunkKB;
-  const int z = blockIdx.z;
-  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
-  const int arow = z * a_rows_per_batch + m0;
-  const int brow = z * b_rows_per_batch + n0;
+  const int ntiles = order.count();
 
-  if (warp == 4) {
+  if (warp == R::kProducerWarp) {
     if (lane == 0) {
       for (int a = 0; a < NA; ++a) {
         tma_prefetch_desc(&maps.a_hi[a]);
@@ -128,81 +180,116 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       }
       tma_prefetch_desc(&maps.b_hi);
       if (NSPLIT == 3) tma_prefetch_desc(&maps.b_lo);
-      for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % STAGES, r = kb / STAGES;
-        if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) break;
-        mbar_expect_tx(&full[s], S::STAGE_BYTES);
-        uint8_t* st = smem + s * S::STAGE_BYTES;
-        const int k = kb * kBK;
+      uint32_t g = 0;  // stage uses so far (all tiles)
+      bool ok = true;
+      for (int l = blockIdx.x; l < ntiles && ok; l += gridDim.x) {
+        int z, mt, nt;
+        order.decode(l, z, mt, nt);
+        const int arow = z * a_rows_per_batch + mt * kBM;
+        const int brow = z * b_rows_per_batch + nt * BN;
+        for (int kb = 0; kb < nk; ++kb, ++g) {
+          const uint32_t s = g % STAGES, r = g / STAGES;
+          if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&full[s], S::STAGE_BYTES);
+          uint8_t* st = smem + s * S::STAGE_BYTES;
+          const int k = kb * kBK;
 #pragma unroll
-        for (int a = 0; a < NA; ++a) {
-          tma_load_2d(st + (a * (S::NAT / NA)) * S::A_TILE, &maps.a_hi[a], k, arow, &full[s]);
-          if (NSPLIT == 3) tma_load_2d(st + (a * 2 + 1) * S::A_TILE, &maps.a_lo[a], k, arow, &full[s]);
+          for (int a = 0; a < NA; ++a) {
+            tma_load_2d(st + (a * (S::NAT / NA)) * S::A_TILE, &maps.a_hi[a], k, arow, &full[s]);
+            if (NSPLIT == 3) tma_load_2d(st + (a * 2 + 1) * S::A_TILE, &maps.a_lo[a], k, arow, &full[s]);
+          }
+          tma_load_2d(st + S::NAT * S::A_TILE, &maps.b_hi, k, brow, &full[s]);
+          if (NSPLIT == 3) tma_load_2d(st + S::NAT * S::A_TILE + S::B_TILE, &maps.b_lo, k, brow, &full[s]);
         }
-        tma_load_2d(st + S::NAT * S::A_TILE, &maps.b_hi, k, brow, &full[s]);
-        if (NSPLIT == 3) tma_load_2d(st + S::NAT * S::A_TILE + S::B_TILE, &maps.b_lo, k, brow, &full[s]);
       }
     }
     __syncwarp();
-  } else if (warp == 5) {
+  } else if (warp == R::kMmaWarp) {
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_tf32(kBM, BN);
+      uint32_t g = 0, c = 0;  // stage uses and chunks so far (all tiles)
       bool ok = true;
-      for (int kb = 0; kb < nk && ok; ++kb) {
-        const int c = kb / kChunkKB, buf = c & 1;
-        const bool first = (kb % kChunkKB) == 0;
-        if (first && c >= 2 && !mbar_wait(&cempty[buf], ((c >> 1) - 1) & 1, abort_flag, status)) break;
-        const int s = kb % STAGES, r = kb / STAGES;
-        if (!mbar_wait(&full[s], r & 1, abort_flag, status)) break;
-        tc_fence_after();
-        uint8_t* st = smem + s * S::STAGE_BYTES;
-        const uint64_t db_hi = desc_kmajor_sw128(st + S::NAT * S::A_TILE);
-        const uint64_t db_lo = desc_kmajor_sw128(st + S::NAT * S::A_TILE + S::B_TILE);
+      for (int l = blockIdx.x; l < ntiles && ok; l += gridDim.x) {
+        for (int kb = 0; kb < nk; ++kb, ++g) {
+          const bool first = (kb % kChunkKB) == 0;
+          const bool last = (kb % kChunkKB) == kChunkKB - 1 || kb == nk - 1;
+          const uint32_t buf = c & 1;
+          if (first && c >= 2 && !mbar_wait(&cempty[buf], ((c >> 1) - 1) & 1, abort_flag, status)) {
+            ok = false;
+            break;
+          }
+          const uint32_t s = g % STAGES, r = g / STAGES;
+          if (!mbar_wait(&full[s], r & 1, abort_flag, status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint8_t* st = smem + s * S::STAGE_BYTES;
+          const uint64_t db_hi = desc_kmajor_sw128(st + S::NAT * S::A_TILE);
+          const uint64_t db_lo = desc_kmajor_sw128(st + S::NAT * S::A_TILE + S::B_TILE);
 #pragma unroll
-        for (int a = 0; a < NA; ++a) {
-          const uint64_t da_hi = desc_kmajor_sw128(st + (a * (S::NAT / NA)) * S::A_TILE);
-          const uint64_t da_lo = desc_kmajor_sw128(st + (a * 2 + 1) * S::A_TILE);
-          const uint32_t d = tmem + (uint32_t)(buf * S::BUF_COLS + a * BN);
+          for (int a = 0; a < NA; ++a) {
+            const uint64_t da_hi = desc_kmajor_sw128(st + (a * (S::NAT / NA)) * S::A_TILE);
+            const uint64_t da_lo = desc_kmajor_sw128(st + (a * 2 + 1) * S::A_TILE);
+            const uint32_t d = tmem + (uint32_t)(buf * S::BUF_COLS + a * BN);
 #pragma unroll
-          for (int kk = 0; kk < kBK / 8; ++kk) {
-            // 8 tf32 = 32 bytes per MMA: advance the start address by 2 (16-byte units)
-            mma_tf32(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
-            if (NSPLIT == 3) {
-              mma_tf32(d, da_hi + 2 * kk, db_lo + 2 * kk, idesc, 1u);
-              mma_tf32(d, da_lo + 2 * kk, db_hi + 2 * kk, idesc, 1u);
+            for (int kk = 0; kk < kBK / 8; ++kk) {
+              // 8 tf32 = 32 bytes per MMA: advance the start address by 2 (16-byte units)
+              mma_tf32(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
+              if (NSPLIT == 3) {
+                mma_tf32(d, da_hi + 2 * kk, db_lo + 2 * kk, idesc, 1u);
+                mma_tf32(d, da_lo + 2 * kk, db_hi + 2 * kk, idesc, 1u);
+              }
             }
           }
+          mma_commit(&empty[s]);
+          if (last) {
+            mma_commit(&cfull[buf]);
+            ++c;
+          }
         }
-        mma_commit(&empty[s]);
-        if ((kb % kChunkKB) == kChunkKB - 1 || kb == nk - 1) mma_commit(&cfull[buf]);
       }
     }
     __syncwarp();
   } else {
-    // drain every chunk into FP32 registers (round-to-nearest), then the epilogue
-    float v[NA * BN];
-#pragma unroll
-    for (int i = 0; i < NA * BN; ++i) v[i] = 0.0f;
+    // drain every chunk into FP32 registers (round-to-nearest), then the epilogue; warp w
+    // reads TMEM lane quarter w % 4 and column group w / 4
+    const int quarter = warp & 3, group = warp >> 2;
+    uint32_t c = 0;  // chunks so far (all tiles)
     bool ok = true;
-    for (int c = 0; c < nchunks; ++c) {
-      const int buf = c & 1;
-      if (ok && !mbar_wait(&cfull[buf], (c >> 1) & 1, abort_flag, status)) ok = false;
-      // tcgen05.ld is warp-collective: decide per warp
-      ok = __all_sync(0xffffffffu, ok) != 0;
-      if (!ok) break;
-      tc_fence_after();
+    for (int l = blockIdx.x; l < ntiles; l += gridDim.x) {
+      int z, mt, nt;
+      order.decode(l, z, mt, nt);
+      float v[R::kGroupCols];
 #pragma unroll
-      for (int q = 0; q < NA * BN / 32; ++q) {
-        float t[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * S::BUF_COLS + q * 32), t);
+      for (int i = 0; i < R::kGroupCols; ++i) v[i] = 0.0f;
+      for (int ch = 0; ch < nchunks && ok; ++ch, ++c) {
+        const uint32_t buf = c & 1;
+        if (!mbar_wait(&cfull[buf], (c >> 1) & 1, abort_flag, status)) ok = false;
+        // tcgen05.ld is warp-collective: decide per warp
+        ok = __all_sync(0xffffffffu, ok) != 0;
+        if (!ok) break;
+        tc_fence_after();
 #pragma unroll
-        for (int i = 0; i < 32; ++i) v[q * 32 + i] += t[i];
+        for (int q = 0; q < R::kGroupCols / 32; ++q) {
+          float t[32];
+          tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) +
+                        (uint32_t)(buf * S::BUF_COLS + group * R::kGroupCols + q * 32),
+                    t);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v[q * 32 + i] += t[i];
+        }
+        tc_fence_before();
+        mbar_arrive_cta(&cempty[buf]);
       }
-      tc_fence_before();
-      mbar_arrive_cta(&cempty[buf]);
+      // every epilogue thread takes this vote once per tile, so all of them leave together;
+      // a column group hands its columns to the epilogue as a tile starting at its own offset
+      if (!epi_all(ok && !*abort_flag, R::kEpiThreads)) break;
+      epi(z, mt * kBM + quarter * 32 + lane, nt * BN + group * (R::kGroupCols / NA), v, epi_smem);
     }
-    // epilogues may synchronise the 128 epilogue threads: decide for all four warps together
-    if (epi_all(ok && !*abort_flag)) epi(z, m0 + warp * 32 + lane, n0, v, smem);
   }
   tc_fence_before();
   __syncthreads();

@@ -74,10 +74,11 @@ def test_mixed_vhs_3pass():
 
 
 @pytest.mark.parametrize("M,N,W", [(64, 8, 6), (200, 32, 6), (108, 15, 6), (128, 16, 5), (64, 4, 300),
-                                   (260, 4, 3)])
+                                   (200, 13, 5), (256, 24, 4), (260, 4, 3)])
 def test_mixed_orbital_update_3pass(M, N, W):
-    """One-launch chain (M <= 256; W = 300 > SM count exercises the persistent walker loop) and the
-    per-term launches (M = 260) against the oracle's one-body, Taylor-6, one-body."""
+    """One-launch chain (M <= 256: one or two 128-row tiles, orbital groups partly or wholly past N;
+    W = 300 > SM count exercises the persistent walker loop) and the per-term launches (M = 260)
+    against the oracle's one-body, Taylor-6, one-body."""
     from ipie_b200 import synthetic
     from ipie_b200._lib import call, ptr, stream
 
