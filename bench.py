@@ -437,10 +437,15 @@ def run_ours(args):
     phases = r["phases"]
     dom = max((k for k in phases if k in fl), key=lambda k: phases[k][1])
     n_launch, tot_ms = phases[dom]
+    # tensor pipe of each mixed-form phase: every product is a 3-pass hi/lo product, FP16 operands
+    # (kind::f16, same tensor rate as bf16) for the force bias and VHS, TF32 for the orbital chain
+    mixed_pipe = {"force_bias": "f16", "vhs": "f16", "orbitals": "tf32"}
+    pipe_peak = {"f16": (peaks["bf16_tflops"], "f16 (3 passes)",
+                         f"{peaks['source']} cuBLAS bf16 8192^3 on B200 (MEASURED_PEAKS.json; fp16 runs at the bf16 rate)"),
+                 "tf32": (peaks["tf32_tflops"], "tf32 (3 passes)", "measured cuBLAS TF32 8192^3 on B200 (tcgen05)")}
     if head == "mixed":
-        # every mixed-form product is a 3-pass TF32 product (hi/lo split); peak = measured TF32
         achieved = 3 * fl[dom] * W * n_launch / (tot_ms / 1e3) / 1e12
-        peak, pipe, src = peaks["tf32_tflops"], "tf32 (3 passes)", "measured cuBLAS TF32 8192^3 on B200 (tcgen05)"
+        peak, pipe, src = pipe_peak[mixed_pipe.get(dom, "tf32")]
     else:
         achieved = fl[dom] * W * n_launch / (tot_ms / 1e3) / 1e12
         peak, pipe, src = peaks["fp64_tflops"], "fp64 (DMMA)", "measured cuBLAS DGEMM 8192^3 on B200"
@@ -450,9 +455,12 @@ def run_ours(args):
         "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled by walkers)",
         "peak_source": src,
         "phase_ms_per_step": {k: round(v[1] / r["phase_steps"], 4) for k, v in sorted(phases.items())},
-        # every tensor-core phase against the same peak (executed FLOPs: 3 passes in the mixed form)
-        "phase_frac_of_peak": {k: round((3 if head == "mixed" else 1) * fl[k] * W * v[0] / (v[1] / 1e3) / 1e12 / peak, 4)
+        # every tensor-core phase against its pipe's peak (executed FLOPs: 3 passes in the mixed form)
+        "phase_frac_of_peak": {k: round((3 if head == "mixed" else 1) * fl[k] * W * v[0] / (v[1] / 1e3) / 1e12
+                                        / (pipe_peak[mixed_pipe.get(k, "tf32")][0] if head == "mixed" else peak), 4)
                                for k, v in sorted(phases.items()) if k in fl and k != "greens_function" and v[1] > 0},
+        "phase_pipe": ({k: mixed_pipe.get(k, "tf32") for k in phases if k in fl and k != "greens_function"}
+                       if head == "mixed" else None),
         "phase_timing": f"{r['phase_steps']} steps launched kernel by kernel with CUDA events between phases",
     }
     step_flops = (sum(v for k, v in fl.items() if k != "orbitals") * W + fl_energy * W / 25.0)
@@ -526,7 +534,7 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "tf32+f64" if head == "mixed" else "f64",
+            "dtype": "f16+tf32+f64" if head == "mixed" else "f64",
             "data": "synthetic",
             "config": line_config(wl, W, world, head),
             "forms": forms_out,

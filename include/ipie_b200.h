@@ -221,33 +221,39 @@ int ipie_b200_normal_fill(double* out, long long n, unsigned long long seed, uns
 int ipie_b200_normal_fill_dev(double* out, long long n, unsigned long long seed, unsigned long long* counter,
                               void* stream);
 
-/* ---- mixed-precision form: TF32 tensor cores (tcgen05), FP32 accumulation ----
- * FP64 stays in the overlap LU/determinant, the Green's function solve,
- * Gram-Schmidt, the weights/phases and the orbital accumulation. */
+/* ---- mixed-precision form: tcgen05 tensor cores, FP32 accumulation ----
+ * 3-pass products of operands split into head and remainder: FP16 (binary16,
+ * scaled by powers of two) for the force bias, VHS and exchange, TF32 for the
+ * orbital update.  FP64 stays in the overlap LU/determinant, the Green's
+ * function solve, Gram-Schmidt, the weights/phases and the orbital accumulation. */
 
-/* Force bias as a 3-pass TF32 product (FP32 accumulation, FP64 output), from the
- * padded half-rotated Cholesky split (ipie_b200_rchol_pad_split).  Same contract
- * and spin-alias convention as ipie_b200_construct_force_bias_batch_single_det;
- * gwork: 2*W*2*32*M floats; M % 4 == 0. */
-int ipie_b200_construct_force_bias_mixed(const float* ra_hi, const float* ra_lo, const float* rb_hi,
-                                         const float* rb_lo, const void* ghalfa, const void* ghalfb, float* gwork,
-                                         int W, int X, int M, int na, int nb, void* vbias, unsigned int* status,
-                                         void* stream);
+/* Force bias as a 3-pass FP16 product (FP32 accumulation, FP64 output), from the
+ * padded half-rotated Cholesky split (ipie_b200_rchol_pad_split, its scale
+ * r*_scale); the Green's function is split per walker with its own scale inside
+ * gwork.  Same contract and spin-alias convention as
+ * ipie_b200_construct_force_bias_batch_single_det; gwork: 2*W*2*32*M floats. */
+int ipie_b200_construct_force_bias_mixed(const void* ra_hi, const void* ra_lo, double ra_scale, const void* rb_hi,
+                                         const void* rb_lo, double rb_scale, const void* ghalfa, const void* ghalfb,
+                                         float* gwork, int W, int X, int M, int na, int nb, void* vbias,
+                                         unsigned int* status, void* stream);
 
 /* ipie_b200_field_shift that also (or only: xshifted may be NULL) writes the
- * shifted fields as planar (W, 2, X) fp32 TF32 head/remainder pairs. */
+ * shifted fields x 64 as planar (W, 2, Xp) binary16 head/remainder pairs,
+ * Xp = X rounded up to a multiple of 8 (the pad columns are not written). */
 int ipie_b200_field_shift_mixed(const void* vbias, const double* xi, const void* mf_shift, int W, int X,
-                                double sqrt_dt, double bound, void* xshifted, float* xs_hi, float* xs_lo, void* cmf,
+                                double sqrt_dt, double bound, void* xshifted, void* xs_hi, void* xs_lo, void* cmf,
                                 void* cfb, void* stream);
 
-/* VHS = i sqrt(dt) L . xshifted as a 3-pass TF32 product (~2^-22 relative),
- * written as four planar (W, M, M) fp32 arrays: Re/Im x TF32 head/remainder.
- * cp_hi/cp_lo: packed Cholesky (P, X) split; xs_hi/xs_lo from
- * ipie_b200_field_shift_mixed; X % 4 == 0.  replaces (mixed form):
- * propagation/phaseless_generic.py:66-97. */
-int ipie_b200_construct_vhs_mixed(const float* cp_hi, const float* cp_lo, const int* idx_i, const int* idx_j, int M,
-                                  int X, const float* xs_hi, const float* xs_lo, int W, double sqrt_dt, float* v_re_hi,
-                                  float* v_re_lo, float* v_im_hi, float* v_im_lo, unsigned int* status, void* stream);
+/* VHS = i sqrt(dt) L . xshifted as a 3-pass FP16 tensor-core product (FP32
+ * accumulation, ~2^-22 relative), written as four planar (W, M, M) fp32 arrays:
+ * Re/Im x TF32 head/remainder.  cp_hi/cp_lo: packed Cholesky (P, Xp) x cp_scale
+ * (a power of two putting its largest entry near 2^14) split into binary16
+ * (ipie_b200_split_f16); xs_hi/xs_lo from ipie_b200_field_shift_mixed.  replaces
+ * (mixed form): propagation/phaseless_generic.py:66-97. */
+int ipie_b200_construct_vhs_mixed(const void* cp_hi, const void* cp_lo, const int* idx_i, const int* idx_j, int M,
+                                  int X, const void* xs_hi, const void* xs_lo, int W, double sqrt_dt, double cp_scale,
+                                  float* v_re_hi, float* v_re_lo, float* v_im_hi, float* v_im_lo, unsigned int* status,
+                                  void* stream);
 
 /* phi_out = E exp(V) E phi_in per walker with every product a 3-pass TF32
  * tensor-core GEMM (E = expH1 hi/lo (M, lde) fp32, lde % 4 == 0; V planar from
@@ -259,37 +265,42 @@ int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float* e_lo, int
                                        const void* phi_in, void* phi_out, float* work, int W, int M, int N, int nmax,
                                        unsigned int* status, void* stream);
 
-/* Half-rotated Cholesky rows (x, i) padded to NP = 8/16/32 >= N, as fp32
- * TF32 head/remainder (X*NP, M) arrays: the left operand of the mixed energy. */
-int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, float* hi, float* lo, void* stream);
+/* Half-rotated Cholesky rows (x, i) padded to NP = 8/16/32 >= N and columns padded
+ * to Mp = M rounded up to a multiple of 8, times `scale` (a power of two; the
+ * largest entry near 2^14), as binary16 head/remainder (X*NP, Mp) arrays (zeros
+ * in the pads): the left operand of the mixed force bias and exchange. */
+int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, double scale, void* hi, void* lo,
+                              void* stream);
 
 /* Exchange of one spin block in the mixed form: exx[w] (complex) = sum_x sum_ij T_ij T_ji,
- * T = rchol_x (N x M) . Ghalf_w^T, as 3-pass TF32 tensor-core products with FP64 bilinear
- * sums.  r_hi/r_lo: the padded split rows of ipie_b200_rchol_pad_split (the first X
- * Cholesky vectors of a larger array may be passed with a smaller X); gwork: 2*W*2*32*M
+ * T = rchol_x (N x M) . Ghalf_w^T, as 3-pass FP16 tensor-core products with FP64 bilinear
+ * sums.  r_hi/r_lo: the padded split rows of ipie_b200_rchol_pad_split with its scale
+ * r_scale (the first X Cholesky vectors of a larger array may be passed with a smaller
+ * X); gwork: 2*W*2*32*M
  * floats; part: (ceil(X*NP/128) + 1) * W complex.  With the trial reference (ghalf_trial,
  * kmat, raw_trial[1]; see ipie_b200_local_energy_mixed) only G - G_T passes through the
  * tensor cores; ghalf_trial NULL disables it.
  * replaces (mixed form): estimators/local_energy_sd.py:263-303 (exx_kernel_batch_real_rchol). */
-int ipie_b200_exchange_mixed(const float* r_hi, const float* r_lo, const void* ghalf, const void* ghalf_trial,
-                             const void* kmat, const void* raw_trial, int W, int X, int M, int N, float* gwork,
-                             void* part, void* exx, unsigned int* status, void* stream);
+int ipie_b200_exchange_mixed(const void* r_hi, const void* r_lo, double r_scale, const void* ghalf,
+                             const void* ghalf_trial, const void* kmat, const void* raw_trial, int W, int X, int M,
+                             int N, float* gwork, void* part, void* exx, unsigned int* status, void* stream);
 
-/* Local energy of the mixed form: the exchange as 3-pass TF32 tensor-core
+/* Local energy of the mixed form: the exchange as 3-pass FP16 tensor-core
  * products (T never stored, bilinear sums in FP64); Coulomb vector and e1b in
  * FP64.  Same contract and spin-alias convention as
- * ipie_b200_local_energy_single_det_batch; rchola/rcholb FP64, r*_hi/lo from
- * ipie_b200_rchol_pad_split; gwork: 2*W*2*32*M floats; work: W*X + rows*W
- * complex with rows = sum over spin blocks of ceil(X*NP/128) (+1 per spin
- * block with the trial reference); M % 4 == 0.
+ * ipie_b200_local_energy_single_det_batch; rchola/rcholb FP64, r*_hi/lo and
+ * r*_scale from ipie_b200_rchol_pad_split; gwork: 2*W*2*32*M floats; work:
+ * W*X + rows*W complex with rows = sum over spin blocks of ceil(X*NP/128)
+ * (+1 per spin block with the trial reference).
  * Trial reference (optional; ghalf_trial_a NULL disables it): the trial's
  * Ghalf_s (N_s, M), the exchange gradient there K_s (N_s, M) and raw_trial[s]
  * = sum_x tr(T_s T_s) at the trial (complex); the tensor cores then only see
  * G - G_T and raw(G_T) + K.(G - G_T) is added in FP64, so the exchange error
  * scales with the walker's distance from the trial.
  * replaces (mixed form): estimators/local_energy_sd.py:987-1080. */
-int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const float* ra_hi,
-                                 const float* ra_lo, const float* rb_hi, const float* rb_lo, const void* rH1a,
+int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const void* ra_hi,
+                                 const void* ra_lo, double ra_scale, const void* rb_hi, const void* rb_lo,
+                                 double rb_scale, const void* rH1a,
                                  const void* rH1b, double ecore, const void* ghalfa, const void* ghalfb,
                                  const void* ghalf_trial_a, const void* ghalf_trial_b, const void* kmat_a,
                                  const void* kmat_b, const void* raw_trial, int W, int X, int M, int na, int nb,
@@ -352,6 +363,18 @@ int ipie_b200_split_tf32(const double* x, float* hi, float* lo, long long n, voi
 int ipie_b200_umma_gemm_test(const float* a0_hi, const float* a0_lo, const float* a1_hi, const float* a1_lo,
                              const float* b_hi, const float* b_lo, float* c, int M, int N, int K, int na, int nsplit,
                              unsigned int* status, void* stream);
+
+/* Split FP64 values, scaled by a power of two, into FP16 head and remainder:
+ * x * scale ~= hi + lo (IEEE binary16 arrays; lo may be NULL).  ~2^-22 relative
+ * while |x * scale| lies in [2^-3, 65504].  No counterpart in ipie. */
+int ipie_b200_split_f16(const double* x, void* hi, void* lo, long long n, double scale, void* stream);
+
+/* Validation entry of the tcgen05 GEMM core on FP16 operands (kind::f16, FP32
+ * accumulation): c[row][col] = sum_k A[row][k] B[col][k], A (M,K) and B (N,K)
+ * row-major binary16 with K % 8 == 0; nsplit = 1 or 3 (hi/lo, the *_lo operands
+ * used).  No counterpart in ipie. */
+int ipie_b200_umma_gemm_f16_test(const void* a_hi, const void* a_lo, const void* b_hi, const void* b_lo, float* c,
+                                 int M, int N, int K, int nsplit, unsigned int* status, void* stream);
 
 #ifdef __cplusplus
 }

@@ -39,13 +39,14 @@ SIGNATURES = {
     "ipie_b200_exchange_noalloc": [P, P, I, I, I, I, P, P],
     "ipie_b200_local_energy_single_det_batch": [I, P, P, P, P, D, P, P, I, I, I, I, I, P, P, P, P],
     "ipie_b200_walker_sums": [I, P, P, P, P, P, I, P],
-    "ipie_b200_construct_force_bias_mixed": [P, P, P, P, P, P, P, I, I, I, I, I, P, P, P],
+    "ipie_b200_construct_force_bias_mixed": [P, P, D, P, P, D, P, P, P, I, I, I, I, I, P, P, P],
     "ipie_b200_field_shift_mixed": [P, P, P, I, I, D, D, P, P, P, P, P, P],
-    "ipie_b200_construct_vhs_mixed": [P, P, P, P, I, I, P, P, I, D, P, P, P, P, P, P],
+    "ipie_b200_construct_vhs_mixed": [P, P, P, P, I, I, P, P, I, D, D, P, P, P, P, P, P],
     "ipie_b200_propagate_orbitals_mixed": [P, P, I, P, P, P, P, P, P, P, I, I, I, I, P, P],
-    "ipie_b200_rchol_pad_split": [P, I, I, I, P, P, P],
-    "ipie_b200_exchange_mixed": [P, P, P, P, P, P, I, I, I, I, P, P, P, P, P],
-    "ipie_b200_local_energy_mixed": [I, P, P, P, P, P, P, P, P, D, P, P, P, P, P, P, P, I, I, I, I, I, P, P, P, P, P],
+    "ipie_b200_rchol_pad_split": [P, I, I, I, D, P, P, P],
+    "ipie_b200_exchange_mixed": [P, P, D, P, P, P, P, I, I, I, I, P, P, P, P, P],
+    "ipie_b200_local_energy_mixed": [I, P, P, P, P, D, P, P, D, P, P, D, P, P, P, P, P, P, P, I, I, I, I, I, P, P, P,
+                                     P, P],
     "ipie_b200_energy_combine": [I, I, I, I, I, P, P, P, P, D, P, P, I, D, D, D, P, P, P],
     "ipie_b200_mlp_forward": [P, I, I, I, P, P, P, P, P],
     "ipie_b200_mlp_backward": [P, P, I, I, I, P, P, P, P, P, P, P],
@@ -58,6 +59,8 @@ SIGNATURES = {
     "ipie_b200_rotate_onebody": [P, P, I, I, P, P],
     "ipie_b200_split_tf32": [P, P, P, ctypes.c_longlong, P],
     "ipie_b200_umma_gemm_test": [P, P, P, P, P, P, P, I, I, I, I, I, P, P],
+    "ipie_b200_split_f16": [P, P, P, ctypes.c_longlong, D, P],
+    "ipie_b200_umma_gemm_f16_test": [P, P, P, P, P, I, I, I, I, P, P],
     "ipie_b200_normal_fill": [P, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_ulonglong, P],
     "ipie_b200_normal_fill_dev": [P, ctypes.c_longlong, ctypes.c_ulonglong, P, P],
 }

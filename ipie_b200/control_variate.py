@@ -233,14 +233,14 @@ class EnergyParts:
             else:
                 sub = gh
             if self.precision == "mixed":
-                hi, lo = ops[s_]
+                hi, lo, rs = ops[s_]
                 NP = 8 if n <= 8 else 16 if n <= 16 else 32
                 rows = (X * NP + 127) // 128 + 1
                 part = torch.empty(rows * S, dtype=C128, device=walkers.device)
                 gwork = torch.empty(2 * S * 2 * 32 * M, dtype=F32, device=walkers.device)
                 exx = torch.empty(S, dtype=C128, device=walkers.device)
                 ref = nchol is None  # the trial reference belongs to the full Cholesky sum
-                call("ipie_b200_exchange_mixed", ptr(hi), ptr(lo), ptr(sub),
+                call("ipie_b200_exchange_mixed", ptr(hi), ptr(lo), rs, ptr(sub),
                      ptr(self.ghalf_trial[s_]) if ref else None, ptr(self.kmat[s_]) if ref else None,
                      ptr(self.raw_trial[s_:s_ + 1]) if ref else None, S, X, M, n, ptr(gwork), ptr(part), ptr(exx),
                      ptr(walkers.status), stream())

@@ -15,9 +15,14 @@ cudaError_t launch_gf_lu32(const double2* phia, const double2* phib, int W, int 
 cudaError_t launch_gf_overlap(const double2* phia, const double2* phib, int W, int M, int na, int nb,
                               const double2* psia_c, const double2* psib_c, const double* log_shift, double2* ghalfa,
                               double2* ghalfb, double2* ovlp, double2* logdet, unsigned* status, cudaStream_t st);
+// Fixed power-of-two scale of the FP16 field operand of the mixed VHS product (|xs| < 1023 fits).
+constexpr double kFieldScaleF16 = 64.0;
+// FP16 operand rows are padded to a multiple of 8 halves (16-byte TMA strides).
+__host__ __device__ inline int f16_ld(int k) { return (k + 7) & ~7; }
+// xs_hi/xs_lo (binary16, optional): the shifted fields x kFieldScaleF16, planar (W, 2, f16_ld(X)).
 cudaError_t launch_field_shift(const double2* vbias, const double* xi, const double2* mf, int W, int X, double sqrt_dt,
                                double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st,
-                               float* xs_hi = nullptr, float* xs_lo = nullptr);
+                               void* xs_hi = nullptr, void* xs_lo = nullptr);
 cudaError_t launch_update_weight(int W, const double2* ovlp_new, const double2* cfb, const double2* cmf,
                                  const double* eshift, double dt, double ebound, const double* wbound, double2* ovlp,
                                  double2* ehyb, double* weight, unsigned* status, cudaStream_t st);

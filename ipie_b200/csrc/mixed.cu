@@ -59,6 +59,42 @@ cudaError_t make_map(CUtensorMap* m, const float* base, long long rows, long lon
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// 2-D K-major FP16 operand: `rows` rows of `k` halves, row stride `ld` halves (ld % 8 == 0),
+// tiles of box_rows x 64 loaded 128B-swizzled; out-of-range elements read as 0.
+cudaError_t make_map_f16(CUtensorMap* m, const void* base, long long rows, long long k, long long ld, int box_rows) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 8) || rows <= 0 || k <= 0) return cudaErrorInvalidValue;
+  cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// hi = FP16(x * scale), lo = FP16(x * scale - hi): the split of the FP16 3-pass product.
+__global__ void split_f16_kernel(const double* __restrict__ x, __half* __restrict__ hi, __half* __restrict__ lo,
+                                 long long n, double scale) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    __half h, l;
+    split_f16(x[i], scale, h, l);
+    hi[i] = h;
+    if (lo) lo[i] = l;
+  }
+}
+
+cudaError_t launch_split_f16(const double* x, __half* hi, __half* lo, long long n, double scale, cudaStream_t st) {
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  split_f16_kernel<<<(unsigned)blocks, 256, 0, st>>>(x, hi, lo, n, scale);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // hi = TF32(x), lo = TF32(x - hi) (both rounded to nearest): the split of the 3-pass product.
 __global__ void split_tf32_kernel(const double* __restrict__ x, float* __restrict__ hi, float* __restrict__ lo,
                                   long long n) {
@@ -99,17 +135,19 @@ struct EpiStoreF32 {
 // tiles: (column tiles, row tiles, batches) of the output; m_fast orders the tile list with the
 // row-tile index fastest (see TileOrder).  persistent: one CTA per SM walks the tile list;
 // otherwise one CTA per tile.
-template <int BN, int NA, int NSPLIT, int STAGES, class Epi>
+template <int BN, int NA, int NSPLIT, int STAGES, class Epi, int KIND = KIND_TF32>
 cudaError_t launch_umma(const GemmMaps& maps, int K, int a_rows_per_batch, int b_rows_per_batch, dim3 tiles, Epi epi,
-                        unsigned* status, cudaStream_t st, bool m_fast = false, bool persistent = true) {
+                        unsigned* status, cudaStream_t st, bool m_fast = false, bool persistent = true,
+                        int m_group = 0) {
   using S = GemmShape<BN, NA, NSPLIT, STAGES, EpiSmem<Epi>::value>;
-  auto kern = umma_gemm_kernel<BN, NA, NSPLIT, STAGES, Epi>;
+  auto kern = umma_gemm_kernel<BN, NA, NSPLIT, STAGES, Epi, KIND>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_BYTES);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 0;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-  const TileOrder order{(int)tiles.y, (int)tiles.x, (int)tiles.z, m_fast ? 1 : 0};
+  const TileOrder order{(int)tiles.y, (int)tiles.x, (int)tiles.z, m_fast ? 1 : 0,
+                        m_group > 0 ? m_group : (int)tiles.y};
   const long long ntiles = (long long)tiles.x * tiles.y * tiles.z;
   if (ntiles <= 0 || ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
   const int grid = (int)(persistent && ntiles > sms ? sms : ntiles);
@@ -136,10 +174,41 @@ static cudaError_t gemm_test(const float* const* a_hi, const float* const* a_lo,
   return launch_umma<BN, NA, NSPLIT, STAGES>(maps, K, 0, 0, grid, EpiStoreF32<BN, NA>{c, M, N}, status, st);
 }
 
+static cudaError_t gemm_test_f16(const void* a_hi, const void* a_lo, const void* b_hi, const void* b_lo, float* c,
+                                 int M, int N, int K, int nsplit, unsigned* status, cudaStream_t st) {
+  constexpr int BN = 128;
+  GemmMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  cudaError_t e;
+  if ((e = make_map_f16(&maps.a_hi[0], a_hi, M, K, K, kBM)) != cudaSuccess) return e;
+  if (nsplit == 3 && (e = make_map_f16(&maps.a_lo[0], a_lo, M, K, K, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_hi, b_hi, N, K, K, BN)) != cudaSuccess) return e;
+  if (nsplit == 3 && (e = make_map_f16(&maps.b_lo, b_lo, N, K, K, BN)) != cudaSuccess) return e;
+  dim3 grid((N + BN - 1) / BN, (M + kBM - 1) / kBM, 1);
+  if (nsplit == 3)
+    return launch_umma<BN, 1, 3, 3, EpiStoreF32<BN, 1>, KIND_F16>(maps, K, 0, 0, grid, EpiStoreF32<BN, 1>{c, M, N},
+                                                                  status, st);
+  return launch_umma<BN, 1, 1, 4, EpiStoreF32<BN, 1>, KIND_F16>(maps, K, 0, 0, grid, EpiStoreF32<BN, 1>{c, M, N},
+                                                                status, st);
+}
+
 }  // namespace umma
 }  // namespace ipie_b200
 
 using namespace ipie_b200;
+
+extern "C" int ipie_b200_split_f16(const double* x, void* hi, void* lo, long long n, double scale, void* stream) {
+  return (int)umma::launch_split_f16(x, reinterpret_cast<__half*>(hi), reinterpret_cast<__half*>(lo), n, scale,
+                                     reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ipie_b200_umma_gemm_f16_test(const void* a_hi, const void* a_lo, const void* b_hi, const void* b_lo,
+                                            float* c, int M, int N, int K, int nsplit, unsigned int* status,
+                                            void* stream) {
+  if (K % 8 || M <= 0 || N <= 0 || K <= 0 || (nsplit != 1 && nsplit != 3)) return (int)cudaErrorInvalidValue;
+  return (int)umma::gemm_test_f16(a_hi, a_lo, b_hi, b_lo, c, M, N, K, nsplit, status,
+                                  reinterpret_cast<cudaStream_t>(stream));
+}
 
 extern "C" int ipie_b200_split_tf32(const double* x, float* hi, float* lo, long long n, void* stream) {
   return (int)umma::launch_split_tf32(x, hi, lo, n, reinterpret_cast<cudaStream_t>(stream));
@@ -178,7 +247,8 @@ template <int BN>
 struct EpiVbiasF {
   double2* vbias;
   int X, W;
-  double scale;
+  double scale;               // overall factor, divided by the operands' power-of-two scales below
+  const double* walker_scale;  // per-walker scale of the Green's-function operand (NULL: 1)
   int accumulate;
   __device__ __forceinline__ void operator()(int, int x, int n0, const float* v, uint8_t*) const {
     if (x >= X) return;
@@ -187,7 +257,8 @@ struct EpiVbiasF {
       const int w = (n0 >> 1) + q;
       if (w < W) {
         const size_t i = (size_t)w * X + x;
-        double2 r = make_double2(scale * (double)v[2 * q], scale * (double)v[2 * q + 1]);
+        const double f = walker_scale != nullptr ? scale / walker_scale[w] : scale;
+        double2 r = make_double2(f * (double)v[2 * q], f * (double)v[2 * q + 1]);
         if (accumulate) r = cadd(r, vbias[i]);
         vbias[i] = r;
       }
@@ -336,6 +407,8 @@ struct EpiExchange {
   static_assert(32 % NP == 0, "an x block must not straddle warps");
   double2* part;
   int X, W, N;
+  double inv_rscale2;          // 1 / (Cholesky operand scale)^2
+  const double* walker_scale;  // per-walker scale of the Green's-function operand
   __device__ __forceinline__ void operator()(int, int row, int n0, const float* v, uint8_t* smem) const {
     const int mt = row / kBM;  // row tile
     float* sC = reinterpret_cast<float*>(smem);
@@ -364,7 +437,13 @@ struct EpiExchange {
         sr += __shfl_xor_sync(0xffffffffu, sr, o);
         si += __shfl_xor_sync(0xffffffffu, si, o);
       }
-      if (j == 0) wpart[xl * WB + wl] = make_double2(sr, si);
+      if (j == 0) {
+        // undo the operand scales: T = acc / (s_r s_w), the sum is quadratic in T
+        const int w = (n0 / (2 * NP)) + wl;
+        const double iw = w < W ? 1.0 / walker_scale[w] : 0.0;
+        const double f = inv_rscale2 * iw * iw;
+        wpart[xl * WB + wl] = make_double2(f * sr, f * si);
+      }
     }
     epi_sync();
     if (tid < WB) {
@@ -379,38 +458,63 @@ struct EpiExchange {
   }
 };
 
-// rchol (X, N*M) double -> rows (x, i) padded to NP: (X*NP, M) fp32 hi/lo, zero rows for i >= N.
-__global__ void rchol_pad_split_kernel(const double* __restrict__ r, int X, int N, int M, int NP, float* __restrict__ hi,
-                                       float* __restrict__ lo) {
-  const long long total = (long long)X * NP * M;
+// rchol (X, N*M) double -> rows (x, i) padded to NP, columns padded to Mp = f16_ld(M):
+// (X*NP, Mp) binary16 hi/lo of rchol x scale, zeros for i >= N and m >= M.
+__global__ void rchol_pad_f16_kernel(const double* __restrict__ r, int X, int N, int M, int NP, int Mp, double scale,
+                                     __half* __restrict__ hi, __half* __restrict__ lo) {
+  const long long total = (long long)X * NP * Mp;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    const int m = (int)(e % M);
-    const long long t = e / M;
+    const int m = (int)(e % Mp);
+    const long long t = e / Mp;
     const int i = (int)(t % NP);
     const long long x = t / NP;
-    const double val = i < N ? r[(x * N + i) * M + m] : 0.0;
-    float h, l;
-    split_tf32(val, h, l);
+    const double val = (i < N && m < M) ? r[(x * N + i) * M + m] : 0.0;
+    __half h, l;
+    split_f16(val, scale, h, l);
     hi[e] = h;
     lo[e] = l;
   }
 }
 
-// Ghalf (W, N, M) complex double -> planar padded (W, 2, NP, M) fp32 hi/lo, zero rows j >= N.
-// With gref (N, M) given, the split operand is Ghalf - gref (the deviation from the trial).
-__global__ void ghalf_pad_split_kernel(const double2* __restrict__ g, const double2* __restrict__ gref, int W, int N,
-                                       int M, int NP, float* __restrict__ hi, float* __restrict__ lo) {
-  const long long total = (long long)W * 2 * NP * M;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    const int m = (int)(e % M);
-    long long t = e / M;
-    const int j = (int)(t % NP);
-    t /= NP;
-    const int c = (int)(t % 2);
-    const long long w = t / 2;
+// Ghalf (W, N, M) complex double -> planar padded (W, 2, NP, Mp) binary16 hi/lo of Ghalf x s_w,
+// zeros for j >= N and m >= M; s_w = 2^(14 - e) with max_w |Re, Im| = f 2^e, f in [0.5, 1), so
+// the walker's largest entry lands in [2^13, 2^14).  With gref (N, M) given, the operand is
+// Ghalf - gref (the deviation from the trial).  One CTA per walker: a max pass, then the split
+// (the second read of the walker's block comes from cache).  scale[w] = s_w.
+__global__ void __launch_bounds__(256) ghalf_pad_f16_kernel(const double2* __restrict__ g,
+                                                            const double2* __restrict__ gref, int N, int M, int NP,
+                                                            int Mp, __half* __restrict__ hi, __half* __restrict__ lo,
+                                                            double* __restrict__ scale) {
+  __shared__ double red[8];
+  const int w = blockIdx.x, tid = threadIdx.x;
+  const double2* gw = g + (size_t)w * N * M;
+  double mx = 0.0;
+  for (int e = tid; e < N * M; e += 256) {
+    double2 z = gw[e];
+    if (gref != nullptr) {
+      const double2 r = gref[e];
+      z.x -= r.x;
+      z.y -= r.y;
+    }
+    mx = fmax(mx, fmax(fabs(z.x), fabs(z.y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((tid & 31) == 0) red[tid >> 5] = mx;
+  __syncthreads();
+  mx = red[0];
+#pragma unroll
+  for (int k = 1; k < 8; ++k) mx = fmax(mx, red[k]);
+  int ex = 0;
+  if (mx > 0.0 && isfinite(mx)) frexp(mx, &ex);
+  const double sw = ldexp(1.0, 14 - ex);
+  if (tid == 0) scale[w] = sw;
+  const long long base = (long long)w * 2 * NP * Mp;
+  for (int e = tid; e < 2 * NP * Mp; e += 256) {
+    const int m = e % Mp, t = e / Mp, j = t % NP, c = t / NP;
     double val = 0.0;
-    if (j < N) {
-      double2 z = g[(w * N + j) * M + m];
+    if (j < N && m < M) {
+      double2 z = gw[(size_t)j * M + m];
       if (gref != nullptr) {
         const double2 r = gref[(size_t)j * M + m];
         z.x -= r.x;
@@ -418,27 +522,45 @@ __global__ void ghalf_pad_split_kernel(const double2* __restrict__ g, const doub
       }
       val = c ? z.y : z.x;
     }
-    float h, l;
-    split_tf32(val, h, l);
-    hi[e] = h;
-    lo[e] = l;
+    __half h, l;
+    split_f16(val, sw, h, l);
+    hi[base + e] = h;
+    lo[base + e] = l;
   }
 }
 
 int exchange_np(int N) { return N <= 8 ? 8 : N <= 16 ? 16 : N <= 32 ? 32 : -1; }
 
-cudaError_t mixed_rchol_pad(const double* rchol, int X, int N, int M, float* hi, float* lo, cudaStream_t st) {
+cudaError_t mixed_rchol_pad(const double* rchol, int X, int N, int M, double scale, __half* hi, __half* lo,
+                            cudaStream_t st) {
   const int NP = exchange_np(N);
   if (NP < 0) return cudaErrorInvalidValue;
-  rchol_pad_split_kernel<<<grid_for((long long)X * NP * M), 256, 0, st>>>(rchol, X, N, M, NP, hi, lo);
+  const int Mp = f16_ld(M);
+  rchol_pad_f16_kernel<<<grid_for((long long)X * NP * Mp), 256, 0, st>>>(rchol, X, N, M, NP, Mp, scale, hi, lo);
   note_launch();
   return cudaGetLastError();
 }
 
-// Padded planar Green's function (TF32 head/remainder) of one spin block.
-static cudaError_t pad_ghalf(const double2* ghalf, int W, int M, int N, int NP, float* g_hi, float* g_lo,
-                             cudaStream_t st, const double2* gref = nullptr) {
-  ghalf_pad_split_kernel<<<grid_for((long long)W * 2 * NP * M), 256, 0, st>>>(ghalf, gref, W, N, M, NP, g_hi, g_lo);
+// The Green's-function operand of the FP16 products, carved from the caller's fp32 work array
+// (2 W 2 32 M floats, more than the binary16 hi/lo of (W, 2, NP, Mp) plus W scales need).
+struct GPad {
+  __half* hi;
+  __half* lo;
+  double* scale;
+};
+static GPad carve_gpad(float* gwork, int W, int NP, int M) {
+  const size_t n = (size_t)W * 2 * NP * f16_ld(M);
+  GPad g;
+  g.hi = reinterpret_cast<__half*>(gwork);
+  g.lo = g.hi + n;
+  g.scale = reinterpret_cast<double*>(reinterpret_cast<uintptr_t>(g.lo + n + 7) & ~uintptr_t(7));
+  return g;
+}
+
+// Padded planar Green's function (FP16 head/remainder, per-walker scale) of one spin block.
+static cudaError_t pad_ghalf(const double2* ghalf, int W, int M, int N, int NP, const GPad& gp, cudaStream_t st,
+                             const double2* gref = nullptr) {
+  ghalf_pad_f16_kernel<<<W, 256, 0, st>>>(ghalf, gref, N, M, NP, f16_ld(M), gp.hi, gp.lo, gp.scale);
   note_launch();
   return cudaGetLastError();
 }
@@ -470,73 +592,80 @@ static cudaError_t exchange_ref_row(const double2* g, const double2* gref, const
   return cudaGetLastError();
 }
 
-// X[w][x] (scale, accumulate as the force bias) = sum_k rchol[x][k] Ghalf[w][k] as a 3-pass TF32
-// product of the padded operands (rows (x) of (X, NP*M), rows (w, c) of (2W, NP*M)).
-static cudaError_t coulomb3(const float* r_hi, const float* r_lo, const float* g_hi, const float* g_lo, int W, int X,
-                            int M, int NP, double2* xv, int accumulate, double scale, unsigned* status,
-                            cudaStream_t st) {
+// X[w][x] (scale, accumulate as the force bias) = sum_k rchol[x][k] Ghalf[w][k] as a 3-pass FP16
+// product of the padded operands: rows (x) of (X, NP*Mp) x rscale, rows (w, c) of (2W, NP*Mp)
+// with per-walker scales (the pads are zero in both, so K runs over them).
+static cudaError_t coulomb3(const void* r_hi, const void* r_lo, double rscale, const GPad& gp, int W, int X, int M,
+                            int NP, double2* xv, int accumulate, double scale, unsigned* status, cudaStream_t st) {
   constexpr int BN = 128;
-  const long long K = (long long)NP * M;
-  if (K % 4) return cudaErrorInvalidValue;
+  const long long K = (long long)NP * f16_ld(M);
   GemmMaps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = make_map(&maps.a_hi[0], r_hi, X, K, K, kBM)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.a_lo[0], r_lo, X, K, K, kBM)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.b_hi, g_hi, 2LL * W, K, K, BN)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.b_lo, g_lo, 2LL * W, K, K, BN)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_hi[0], r_hi, X, K, K, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_lo[0], r_lo, X, K, K, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_hi, gp.hi, 2LL * W, K, K, BN)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_lo, gp.lo, 2LL * W, K, K, BN)) != cudaSuccess) return e;
   dim3 grid((2 * W + BN - 1) / BN, (X + kBM - 1) / kBM, 1);
   // row tiles fastest: the Cholesky operand (X rows) stays in L2 while the Green's function streams
-  return launch_umma<BN, 1, 3, 3>(maps, (int)K, 0, 0, grid, EpiVbiasF<BN>{xv, X, W, scale, accumulate}, status, st,
-                                  true);
+  const EpiVbiasF<BN> epi{xv, X, W, scale / rscale, gp.scale, accumulate};
+  return launch_umma<BN, 1, 3, 3, EpiVbiasF<BN>, KIND_F16>(maps, (int)K, 0, 0, grid, epi, status, st, true);
 }
 
-// Exchange partials of one spin block as a 3-pass TF32 product: (X*NP, M) x (W*2*NP, M)^T.
+// Exchange partials of one spin block as a 3-pass FP16 product: (X*NP, M) x (W*2*NP, M)^T, rows
+// of both operands padded to Mp halves (TMA reads the pads as zeros).
 template <int NP>
-static cudaError_t exchange3_np(const float* r_hi, const float* r_lo, const float* g_hi, const float* g_lo, int W,
-                                int X, int M, int N, double2* part, unsigned* status, cudaStream_t st) {
+static cudaError_t exchange3_np(const void* r_hi, const void* r_lo, double rscale, const GPad& gp, int W, int X, int M,
+                                int N, double2* part, unsigned* status, cudaStream_t st) {
   constexpr int BN = 128;
+  const int Mp = f16_ld(M);
   GemmMaps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = make_map(&maps.a_hi[0], r_hi, (long long)X * NP, M, M, kBM)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.a_lo[0], r_lo, (long long)X * NP, M, M, kBM)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.b_hi, g_hi, (long long)W * 2 * NP, M, M, BN)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.b_lo, g_lo, (long long)W * 2 * NP, M, M, BN)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_hi[0], r_hi, (long long)X * NP, M, Mp, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_lo[0], r_lo, (long long)X * NP, M, Mp, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_hi, gp.hi, (long long)W * 2 * NP, M, Mp, BN)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_lo, gp.lo, (long long)W * 2 * NP, M, Mp, BN)) != cudaSuccess) return e;
   dim3 grid((W * 2 * NP + BN - 1) / BN, (X * NP + kBM - 1) / kBM, 1);
-  // row tiles fastest: the consecutive tiles of the resident CTAs sweep the padded Cholesky
-  // operand (the smaller one, kept in L2) against one Green's-function tile
-  return launch_umma<BN, 1, 3, 2>(maps, M, 0, 0, grid, EpiExchange<NP, BN>{part, X, W, N}, status, st, true);
+  // row tiles fastest, in groups of 148 (~15 MB of the padded Cholesky operand at M = 200):
+  // one wave of CTAs multiplies a group against one Green's-function tile, the group stays in
+  // L2 for the whole sweep over the walkers and the Green's function streams once per group
+  const EpiExchange<NP, BN> epi{part, X, W, N, 1.0 / (rscale * rscale), gp.scale};
+  return launch_umma<BN, 1, 3, 2, EpiExchange<NP, BN>, KIND_F16>(maps, M, 0, 0, grid, epi, status, st, true, true,
+                                                                 148);
 }
 
-static cudaError_t exchange3(const float* r_hi, const float* r_lo, const float* g_hi, const float* g_lo, int W, int X,
-                             int M, int N, double2* part, unsigned* status, cudaStream_t st) {
+static cudaError_t exchange3(const void* r_hi, const void* r_lo, double rscale, const GPad& gp, int W, int X, int M,
+                             int N, double2* part, unsigned* status, cudaStream_t st) {
   switch (exchange_np(N)) {
-    case 8: return exchange3_np<8>(r_hi, r_lo, g_hi, g_lo, W, X, M, N, part, status, st);
-    case 16: return exchange3_np<16>(r_hi, r_lo, g_hi, g_lo, W, X, M, N, part, status, st);
-    case 32: return exchange3_np<32>(r_hi, r_lo, g_hi, g_lo, W, X, M, N, part, status, st);
+    case 8: return exchange3_np<8>(r_hi, r_lo, rscale, gp, W, X, M, N, part, status, st);
+    case 16: return exchange3_np<16>(r_hi, r_lo, rscale, gp, W, X, M, N, part, status, st);
+    case 32: return exchange3_np<32>(r_hi, r_lo, rscale, gp, W, X, M, N, part, status, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
 int exchange3_rows(int X, int N) { return (X * exchange_np(N) + kBM - 1) / kBM; }
 
-cudaError_t mixed_vhs(const float* cp_hi, const float* cp_lo, const int* ii, const int* jj, int P, int X, int M,
-                      const float* xs_hi, const float* xs_lo, int W, double sqrt_dt, float* re_hi, float* re_lo,
-                      float* im_hi, float* im_lo, unsigned* status, cudaStream_t st) {
-  // 128 x 256 tiles (two column groups of 128): half the re-reads of the packed Cholesky.
-  // One CTA per tile: measured faster here than persistent CTAs (2.2 vs 2.5 ms at 2048 walkers)
+cudaError_t mixed_vhs(const void* cp_hi, const void* cp_lo, const int* ii, const int* jj, int P, int X, int M,
+                      const void* xs_hi, const void* xs_lo, int W, double sqrt_dt, double cp_scale, float* re_hi,
+                      float* re_lo, float* im_hi, float* im_lo, unsigned* status, cudaStream_t st) {
+  // FP16 operands (packed Cholesky x cp_scale, fields x kFieldScaleF16) on 128 x 256 tiles
+  // (two column groups of 128: half the re-reads of the packed Cholesky).  One CTA per tile:
+  // measured faster here than persistent CTAs.
   constexpr int BN = 256;
+  const int ldx = f16_ld(X);
   GemmMaps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = make_map(&maps.a_hi[0], cp_hi, P, X, X, kBM)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.a_lo[0], cp_lo, P, X, X, kBM)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.b_hi, xs_hi, 2LL * W, X, X, BN)) != cudaSuccess) return e;
-  if ((e = make_map(&maps.b_lo, xs_lo, 2LL * W, X, X, BN)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_hi[0], cp_hi, P, X, ldx, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_lo[0], cp_lo, P, X, ldx, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_hi, xs_hi, 2LL * W, X, ldx, BN)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_lo, xs_lo, 2LL * W, X, ldx, BN)) != cudaSuccess) return e;
   dim3 grid((2 * W + BN - 1) / BN, (P + kBM - 1) / kBM, 1);
-  EpiVHSSplit<128> epi{re_hi, re_lo, im_hi, im_lo, ii, jj, P, M, W, (float)sqrt_dt};
-  return launch_umma<BN, 1, 3, 2>(maps, X, 0, 0, grid, epi, status, st, false, false);
+  const double unscale = sqrt_dt / (cp_scale * kFieldScaleF16);  // powers of two: exact
+  EpiVHSSplit<128> epi{re_hi, re_lo, im_hi, im_lo, ii, jj, P, M, W, (float)unscale};
+  return launch_umma<BN, 1, 3, 2, EpiVHSSplit<128>, KIND_F16>(maps, X, 0, 0, grid, epi, status, st, false, false);
 }
 
 // Orbital update of one spin block: phi_out = E exp(V) E phi_in (Taylor order nmax),
@@ -592,27 +721,28 @@ cudaError_t mixed_orbitals(const float* e_hi, const float* e_lo, int Mp, const f
 }  // namespace umma
 }  // namespace ipie_b200
 
-extern "C" int ipie_b200_construct_force_bias_mixed(const float* ra_hi, const float* ra_lo, const float* rb_hi,
-                                                    const float* rb_lo, const void* ghalfa, const void* ghalfb,
-                                                    float* gwork, int W, int X, int M, int na, int nb, void* vbias,
-                                                    unsigned int* status, void* stream) {
+extern "C" int ipie_b200_construct_force_bias_mixed(const void* ra_hi, const void* ra_lo, double ra_scale,
+                                                    const void* rb_hi, const void* rb_lo, double rb_scale,
+                                                    const void* ghalfa, const void* ghalfb, float* gwork, int W, int X,
+                                                    int M, int na, int nb, void* vbias, unsigned int* status,
+                                                    void* stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const bool alias = nb == na && nb > 0 && rb_hi == ra_hi && ghalfb == ghalfa;
   const int NPa = umma::exchange_np(na), NPb = nb > 0 ? umma::exchange_np(nb) : 8;
-  if (NPa < 0 || NPb < 0 || M % 4) return (int)cudaErrorInvalidValue;
-  float* g_hi = gwork;
-  float* g_lo = gwork + (size_t)W * 2 * 32 * M;
+  if (NPa < 0 || NPb < 0 || M < 4 || !(ra_scale > 0.0) || (nb > 0 && !(rb_scale > 0.0))) return (int)cudaErrorInvalidValue;
+  const umma::GPad gp = umma::carve_gpad(gwork, W, 32, M);
   double2* v = reinterpret_cast<double2*>(vbias);
-  cudaError_t e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfa), W, M, na, NPa, g_hi, g_lo, st);
-  if (e == cudaSuccess) e = umma::coulomb3(ra_hi, ra_lo, g_hi, g_lo, W, X, M, NPa, v, 0, alias ? 2.0 : 1.0, status, st);
+  cudaError_t e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfa), W, M, na, NPa, gp, st);
+  if (e == cudaSuccess)
+    e = umma::coulomb3(ra_hi, ra_lo, ra_scale, gp, W, X, M, NPa, v, 0, alias ? 2.0 : 1.0, status, st);
   if (e != cudaSuccess || nb == 0 || alias) return (int)e;
-  e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfb), W, M, nb, NPb, g_hi, g_lo, st);
-  if (e == cudaSuccess) e = umma::coulomb3(rb_hi, rb_lo, g_hi, g_lo, W, X, M, NPb, v, 1, 1.0, status, st);
+  e = umma::pad_ghalf(reinterpret_cast<const double2*>(ghalfb), W, M, nb, NPb, gp, st);
+  if (e == cudaSuccess) e = umma::coulomb3(rb_hi, rb_lo, rb_scale, gp, W, X, M, NPb, v, 1, 1.0, status, st);
   return (int)e;
 }
 
 extern "C" int ipie_b200_field_shift_mixed(const void* vbias, const double* xi, const void* mf_shift, int W, int X,
-                                           double sqrt_dt, double bound, void* xshifted, float* xs_hi, float* xs_lo,
+                                           double sqrt_dt, double bound, void* xshifted, void* xs_hi, void* xs_lo,
                                            void* cmf, void* cfb, void* stream) {
   return (int)launch_field_shift(reinterpret_cast<const double2*>(vbias), xi, reinterpret_cast<const double2*>(mf_shift),
                                  W, X, sqrt_dt, bound, reinterpret_cast<double2*>(xshifted),
@@ -620,13 +750,13 @@ extern "C" int ipie_b200_field_shift_mixed(const void* vbias, const double* xi, 
                                  reinterpret_cast<cudaStream_t>(stream), xs_hi, xs_lo);
 }
 
-extern "C" int ipie_b200_construct_vhs_mixed(const float* cp_hi, const float* cp_lo, const int* idx_i,
-                                             const int* idx_j, int M, int X, const float* xs_hi, const float* xs_lo,
-                                             int W, double sqrt_dt, float* v_re_hi, float* v_re_lo, float* v_im_hi,
-                                             float* v_im_lo, unsigned int* status, void* stream) {
-  if (X % 4) return (int)cudaErrorInvalidValue;
-  return (int)umma::mixed_vhs(cp_hi, cp_lo, idx_i, idx_j, M * (M + 1) / 2, X, M, xs_hi, xs_lo, W, sqrt_dt, v_re_hi,
-                              v_re_lo, v_im_hi, v_im_lo, status, reinterpret_cast<cudaStream_t>(stream));
+extern "C" int ipie_b200_construct_vhs_mixed(const void* cp_hi, const void* cp_lo, const int* idx_i,
+                                             const int* idx_j, int M, int X, const void* xs_hi, const void* xs_lo,
+                                             int W, double sqrt_dt, double cp_scale, float* v_re_hi, float* v_re_lo,
+                                             float* v_im_hi, float* v_im_lo, unsigned int* status, void* stream) {
+  if (!(cp_scale > 0.0)) return (int)cudaErrorInvalidValue;
+  return (int)umma::mixed_vhs(cp_hi, cp_lo, idx_i, idx_j, M * (M + 1) / 2, X, M, xs_hi, xs_lo, W, sqrt_dt, cp_scale,
+                              v_re_hi, v_re_lo, v_im_hi, v_im_lo, status, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float* e_lo, int lde, const float* v_re_hi,
@@ -645,8 +775,11 @@ extern "C" int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float
                                    reinterpret_cast<cudaStream_t>(stream));
 }
 
-extern "C" int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, float* hi, float* lo, void* stream) {
-  return (int)umma::mixed_rchol_pad(rchol, X, N, M, hi, lo, reinterpret_cast<cudaStream_t>(stream));
+extern "C" int ipie_b200_rchol_pad_split(const double* rchol, int X, int N, int M, double scale, void* hi, void* lo,
+                                         void* stream) {
+  if (!(scale > 0.0)) return (int)cudaErrorInvalidValue;
+  return (int)umma::mixed_rchol_pad(rchol, X, N, M, scale, reinterpret_cast<__half*>(hi), reinterpret_cast<__half*>(lo),
+                                    reinterpret_cast<cudaStream_t>(stream));
 }
 
 // Per-walker sum of the exchange partial rows: out[w] = sum_t part[t * W + w].
@@ -658,21 +791,20 @@ __global__ void row_sum_kernel(const double2* __restrict__ part, int rows, int W
   out[w] = acc;
 }
 
-extern "C" int ipie_b200_exchange_mixed(const float* r_hi, const float* r_lo, const void* ghalf,
+extern "C" int ipie_b200_exchange_mixed(const void* r_hi, const void* r_lo, double r_scale, const void* ghalf,
                                         const void* ghalf_trial, const void* kmat, const void* raw_trial, int W, int X,
                                         int M, int N, float* gwork, void* part, void* exx, unsigned int* status,
                                         void* stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   using CC = const double2*;
   const int NP = umma::exchange_np(N);
-  if (NP < 0 || M % 4 || W <= 0 || X <= 0) return (int)cudaErrorInvalidValue;
+  if (NP < 0 || M < 4 || W <= 0 || X <= 0 || !(r_scale > 0.0)) return (int)cudaErrorInvalidValue;
   const bool delta = ghalf_trial != nullptr;
   if (delta && (kmat == nullptr || raw_trial == nullptr)) return (int)cudaErrorInvalidValue;
-  float* g_hi = gwork;
-  float* g_lo = gwork + (size_t)W * 2 * 32 * M;
+  const umma::GPad gp = umma::carve_gpad(gwork, W, 32, M);
   double2* p = reinterpret_cast<double2*>(part);
-  cudaError_t e = umma::pad_ghalf((CC)ghalf, W, M, N, NP, g_hi, g_lo, st, delta ? (CC)ghalf_trial : nullptr);
-  if (e == cudaSuccess) e = umma::exchange3(r_hi, r_lo, g_hi, g_lo, W, X, M, N, p, status, st);
+  cudaError_t e = umma::pad_ghalf((CC)ghalf, W, M, N, NP, gp, st, delta ? (CC)ghalf_trial : nullptr);
+  if (e == cudaSuccess) e = umma::exchange3(r_hi, r_lo, r_scale, gp, W, X, M, N, p, status, st);
   if (e != cudaSuccess) return (int)e;
   int rows = umma::exchange3_rows(X, N);
   if (delta) {
@@ -685,9 +817,9 @@ extern "C" int ipie_b200_exchange_mixed(const float* r_hi, const float* r_lo, co
   return (int)cudaGetLastError();
 }
 
-extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const float* ra_hi,
-                                            const float* ra_lo, const float* rb_hi, const float* rb_lo,
-                                            const void* rH1a, const void* rH1b, double ecore, const void* ghalfa,
+extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const void* ra_hi,
+                                            const void* ra_lo, double ra_scale, const void* rb_hi, const void* rb_lo,
+                                            double rb_scale, const void* rH1a, const void* rH1b, double ecore, const void* ghalfa,
                                             const void* ghalfb, const void* ghalf_trial_a,
                                             const void* ghalf_trial_b, const void* kmat_a, const void* kmat_b,
                                             const void* raw_trial, int W, int X, int M, int na, int nb, float* gwork,
@@ -702,24 +834,24 @@ extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const
   double2* xv = reinterpret_cast<double2*>(work);
   double2* part = xv + (size_t)W * X;
   const int NPa = umma::exchange_np(na), NPb = nb > 0 ? umma::exchange_np(nb) : 8;
-  if (NPa < 0 || NPb < 0 || M % 4) return (int)cudaErrorInvalidValue;
-  float* g_hi = gwork;
-  float* g_lo = gwork + (size_t)W * 2 * 32 * M;
+  if (NPa < 0 || NPb < 0 || M < 4 || !(ra_scale > 0.0) || (use_b && !(rb_scale > 0.0))) return (int)cudaErrorInvalidValue;
+  const umma::GPad gp = umma::carve_gpad(gwork, W, 32, M);
   // Coulomb vector in FP64 (DMMA): the Coulomb energy is the large, cancellation-free term
   cudaError_t e = launch_force_bias(rchola, reinterpret_cast<const double2*>(ghalfa), W, X, na * M, xv, 0, st,
                                     alias ? 2.0 : 1.0);
   if (e == cudaSuccess && use_b)
     e = launch_force_bias(rcholb, reinterpret_cast<const double2*>(ghalfb), W, X, nb * M, xv, 1, st);
   if (e != cudaSuccess) return (int)e;
-  // exchange: 3-pass TF32 tensor-core products (of G - G_T when the trial reference is given),
+  // exchange: 3-pass FP16 tensor-core products (of G - G_T when the trial reference is given),
   // bilinear sums in FP64; the reference row adds raw(G_T) + K.(G - G_T) in FP64
-  e = umma::pad_ghalf((CC)ghalfa, W, M, na, NPa, g_hi, g_lo, st, delta ? (CC)ghalf_trial_a : nullptr);
-  if (e == cudaSuccess) e = umma::exchange3(ra_hi, ra_lo, g_hi, g_lo, W, X, M, na, part, status, st);
+  e = umma::pad_ghalf((CC)ghalfa, W, M, na, NPa, gp, st, delta ? (CC)ghalf_trial_a : nullptr);
+  if (e == cudaSuccess) e = umma::exchange3(ra_hi, ra_lo, ra_scale, gp, W, X, M, na, part, status, st);
   if (e != cudaSuccess) return (int)e;
   int rows = umma::exchange3_rows(X, na);
   if (use_b) {
-    e = umma::pad_ghalf((CC)ghalfb, W, M, nb, NPb, g_hi, g_lo, st, delta ? (CC)ghalf_trial_b : nullptr);
-    if (e == cudaSuccess) e = umma::exchange3(rb_hi, rb_lo, g_hi, g_lo, W, X, M, nb, part + (size_t)rows * W, status, st);
+    e = umma::pad_ghalf((CC)ghalfb, W, M, nb, NPb, gp, st, delta ? (CC)ghalf_trial_b : nullptr);
+    if (e == cudaSuccess)
+      e = umma::exchange3(rb_hi, rb_lo, rb_scale, gp, W, X, M, nb, part + (size_t)rows * W, status, st);
     if (e != cudaSuccess) return (int)e;
     rows += umma::exchange3_rows(X, nb);
   }

@@ -9,6 +9,7 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 
 #include "common.cuh"
@@ -164,6 +165,23 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool neg_a = fal
          | ((uint32_t)(M >> 4) << 24);   // M / 16
 }
 
+// Instruction descriptor: kind::f16 with FP16 A and B (format 0), D fp32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
+  return (1u << 4)                       // D format f32
+         | ((uint32_t)(N >> 3) << 17)    // N / 8
+         | ((uint32_t)(M >> 4) << 24);   // M / 16
+}
+
+// 128 x N x 16 FP16 product accumulated in FP32 (one 32-byte K step of a 128-byte row, like kind::tf32)
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\ntcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate) {
   asm volatile(
@@ -198,6 +216,21 @@ __device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
 __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
   hi = round_tf32((float)x);
   lo = round_tf32((float)(x - (double)hi));
+}
+
+// Split of a scaled value into FP16 head and remainder: x * scale ~= hi + lo to ~2^-22 relative
+// while |x * scale| stays in [2^-3, 65504] (below that lo is subnormal and the split carries an
+// absolute ~2^-25 instead).  scale is a power of two chosen by the caller, so the unscaling of
+// the product is exact.
+__device__ __forceinline__ void split_f16(double x, double scale, __half& hi, __half& lo) {
+  const double y = x * scale;
+  hi = __double2half(y);
+  lo = __double2half(y - (double)__half2float(hi));
+}
+__device__ __forceinline__ void split_f16(float x, float scale, __half& hi, __half& lo) {
+  const float y = x * scale;
+  hi = __float2half_rn(y);
+  lo = __float2half_rn(y - __half2float(hi));
 }
 
 }  // namespace umma

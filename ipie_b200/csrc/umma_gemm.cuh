@@ -2,11 +2,13 @@
 //
 // One CTA computes a 128 x BN tile of
 //     D_a = sum_k A_a[m, k] B[n, k]          a = 0 .. NA-1   (NA left operands share B)
-// with A_a and B K-major fp32 in global memory, read through TMA into
-// 128B-swizzled shared memory and multiplied as TF32 on the 5th-gen tensor
-// cores.  NSPLIT = 3 adds the hi/lo correction products A_hi B_lo + A_lo B_hi
-// (each operand pre-split into a TF32 head and remainder, ~2^-22 relative);
-// NSPLIT = 1 is plain TF32.
+// with A_a and B K-major in global memory, read through TMA into 128B-swizzled
+// shared memory and multiplied on the 5th-gen tensor cores, either as TF32
+// (fp32 words, KIND_TF32) or as FP16 (KIND_F16: half the bytes per K and twice
+// the tensor rate; operands carry a power-of-two scale that the epilogue
+// removes).  NSPLIT = 3 adds the hi/lo correction products A_hi B_lo + A_lo B_hi
+// (each operand pre-split into a head and remainder, ~2^-22 relative for TF32
+// and for in-range FP16); NSPLIT = 1 is a single product.
 //
 // Accumulation in chunks: the tensor core's FP32 accumulator loses about half
 // an ulp per accumulation step, always toward zero, so a long K sum in TMEM
@@ -47,6 +49,11 @@ struct GemmMaps {
 constexpr int kBM = 128;
 constexpr int kBK = 32;  // fp32 per 128-byte row
 
+// Operand kinds: a stage holds 128-byte K rows of either
+constexpr int KIND_TF32 = 0;  // fp32 words read as TF32 (32 per row, kind::tf32)
+constexpr int KIND_F16 = 1;   // FP16 (64 per row, kind::f16)
+__host__ __device__ constexpr int kblock_elems(int kind) { return kind == KIND_F16 ? 64 : 32; }
+
 __host__ __device__ constexpr int tmem_cols_for(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : n <= 256 ? 256 : 512; }
 
 constexpr int kChunkKB = 2;  // k-blocks (of 32) accumulated in TMEM before a drain
@@ -79,21 +86,29 @@ __device__ __forceinline__ void mbar_arrive_cta(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Order of the output tiles: tile l (of nm x nn x nz) has batch z = l / (nm * nn) and, inside the
-// batch, the row-tile index fastest (m_fast) or the column-tile index fastest.  The CTAs resident
-// at one time take consecutive tiles, so the operand that is swept along the fast index should
-// be the one that fits in L2.
+// Order of the output tiles: tile l (of nm x nn x nz) has batch z = l / (nm * nn); inside the
+// batch either the column-tile index runs fastest, or (m_fast) the row tiles are taken in
+// groups of m_group: within a group the row-tile index runs fastest over the group's row
+// tiles for every column tile in turn.  The CTAs resident at one time take consecutive tiles,
+// so the operand swept along the fast index should fit in L2: a whole row-tile group of A
+// stays there while the column tiles of B stream past it once per group.
 struct TileOrder {
   int nm, nn, nz;
   int m_fast;
+  int m_group;  // row tiles per group (m_fast); nm or more: one group
   __host__ __device__ int count() const { return nm * nn * nz; }
   __device__ void decode(int l, int& z, int& mt, int& nt) const {
     const int per = nm * nn;
     z = l / per;
     const int r = l - z * per;
     if (m_fast) {
-      mt = r % nm;
-      nt = r / nm;
+      const int span = m_group * nn;  // tiles of one full group
+      const int g = r / span;
+      const int m0 = g * m_group;
+      const int gm = min(m_group, nm - m0);  // the last group may be shorter
+      const int rem = r - g * span;          // < gm * nn
+      mt = m0 + rem % gm;
+      nt = rem / gm;
     } else {
       nt = r % nn;
       mt = r / nn;
@@ -133,7 +148,7 @@ struct GemmShape {
 // Persistent CTAs: CTA b computes tiles b, b + gridDim.x, ...; the stage ring, the chunk counter
 // and the two TMEM buffers run on across tiles, so one tile's epilogue overlaps the next tile's
 // loads and first MMAs.
-template <int BN, int NA, int NSPLIT, int STAGES, class Epi>
+template <int BN, int NA, int NSPLIT, int STAGES, class Epi, int KIND = KIND_TF32>
 __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
     umma_gemm_kernel(const __grid_constant__ GemmMaps maps, int K, int a_rows_per_batch, int b_rows_per_batch,
                      TileOrder order, Epi epi, unsigned* status) {
@@ -168,7 +183,8 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  const int nk = (K + kBK - 1) / kBK;
+  constexpr int KB = kblock_elems(KIND);  // K elements per k-block (one 128-byte row)
+  const int nk = (K + KB - 1) / KB;
   const int nchunks = (nk + kChunkKB - 1) / kChunkKB;
   const int ntiles = order.count();
 
@@ -195,7 +211,7 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
           }
           mbar_expect_tx(&full[s], S::STAGE_BYTES);
           uint8_t* st = smem + s * S::STAGE_BYTES;
-          const int k = kb * kBK;
+          const int k = kb * KB;
 #pragma unroll
           for (int a = 0; a < NA; ++a) {
             tma_load_2d(st + (a * (S::NAT / NA)) * S::A_TILE, &maps.a_hi[a], k, arow, &full[s]);
@@ -209,7 +225,7 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
     __syncwarp();
   } else if (warp == R::kMmaWarp) {
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_tf32(kBM, BN);
+      constexpr uint32_t idesc = KIND == KIND_F16 ? idesc_f16(kBM, BN) : idesc_tf32(kBM, BN);
       uint32_t g = 0, c = 0;  // stage uses and chunks so far (all tiles)
       bool ok = true;
       for (int l = blockIdx.x; l < ntiles && ok; l += gridDim.x) {
@@ -236,12 +252,20 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
             const uint64_t da_lo = desc_kmajor_sw128(st + (a * 2 + 1) * S::A_TILE);
             const uint32_t d = tmem + (uint32_t)(buf * S::BUF_COLS + a * BN);
 #pragma unroll
-            for (int kk = 0; kk < kBK / 8; ++kk) {
-              // 8 tf32 = 32 bytes per MMA: advance the start address by 2 (16-byte units)
-              mma_tf32(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
-              if (NSPLIT == 3) {
-                mma_tf32(d, da_hi + 2 * kk, db_lo + 2 * kk, idesc, 1u);
-                mma_tf32(d, da_lo + 2 * kk, db_hi + 2 * kk, idesc, 1u);
+            for (int kk = 0; kk < 4; ++kk) {
+              // 32 bytes of K per MMA (8 tf32 or 16 fp16): advance the start address by 2 (16-byte units)
+              if constexpr (KIND == KIND_F16) {
+                mma_f16(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
+                if (NSPLIT == 3) {
+                  mma_f16(d, da_hi + 2 * kk, db_lo + 2 * kk, idesc, 1u);
+                  mma_f16(d, da_lo + 2 * kk, db_hi + 2 * kk, idesc, 1u);
+                }
+              } else {
+                mma_tf32(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
+                if (NSPLIT == 3) {
+                  mma_tf32(d, da_hi + 2 * kk, db_lo + 2 * kk, idesc, 1u);
+                  mma_tf32(d, da_lo + 2 * kk, db_hi + 2 * kk, idesc, 1u);
+                }
               }
             }
           }

@@ -4,6 +4,8 @@
 //
 // One CTA owns one walker (both spin blocks) for the kernels that need the
 // walker's whole Slater matrix; its M x N orbitals live in shared memory.
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -239,26 +241,23 @@ cudaError_t launch_gf_overlap(const double2* phia, const double2* phib, int W, i
 //   xs = xi - xbar;  cmf = -sqrt(dt) sum_x xs mf;  cfb = sum_x xi xbar - xbar^2/2
 // One CTA per 32 walkers; the (X, W) transposed store goes through smem.
 // ---------------------------------------------------------------------------
-// TF32 head and TF32 remainder of x, both rounded to nearest (the 3-pass operand split)
-__device__ __forceinline__ float round_to_tf32(float x) {
-  uint32_t h;
-  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(x));
-  return __uint_as_float(h);
-}
-__device__ __forceinline__ void split_store_tf32(float* hi, float* lo, size_t i, double x) {
-  const float hf = round_to_tf32((float)x);
-  hi[i] = hf;
-  lo[i] = round_to_tf32((float)(x - (double)hf));
+// FP16 head and remainder of the scaled x, both rounded to nearest (the 3-pass operand split)
+__device__ __forceinline__ void split_store_f16(__half* hi, __half* lo, size_t i, double x) {
+  const double y = x * kFieldScaleF16;
+  const __half h = __double2half(y);
+  hi[i] = h;
+  lo[i] = __double2half(y - (double)__half2float(h));
 }
 
-// xs_hi/xs_lo (optional): the shifted fields as planar (W, 2, X) fp32 TF32 head/remainder,
-// the right operand of the mixed-precision VHS product.
+// xs_hi/xs_lo (optional): the shifted fields x kFieldScaleF16 as planar (W, 2, ldx) FP16
+// head/remainder, the right operand of the mixed-precision VHS product.
 __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restrict__ vbias, const double* __restrict__ xi,
                                                           const double2* __restrict__ mf, int W, int X, double sqrt_dt,
                                                           double bound, double2* __restrict__ xshifted,
                                                           double2* __restrict__ cmf, double2* __restrict__ cfb,
-                                                          float* __restrict__ xs_hi, float* __restrict__ xs_lo) {
+                                                          __half* __restrict__ xs_hi, __half* __restrict__ xs_lo) {
   __shared__ double2 tile[32][33];
+  const int ldx = f16_ld(X);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int w0 = blockIdx.x * 32;
   double2 acc_mf[4], acc_fb[4];
@@ -279,8 +278,8 @@ __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restr
         const double r = xi[(size_t)w * X + x];
         xs = make_double2(r - xb.x, -xb.y);
         if (xs_hi != nullptr) {
-          split_store_tf32(xs_hi, xs_lo, ((size_t)w * 2) * X + x, xs.x);
-          split_store_tf32(xs_hi, xs_lo, ((size_t)w * 2 + 1) * X + x, xs.y);
+          split_store_f16(xs_hi, xs_lo, ((size_t)w * 2) * ldx + x, xs.x);
+          split_store_f16(xs_hi, xs_lo, ((size_t)w * 2 + 1) * ldx + x, xs.y);
         }
         acc_mf[q] = cadd(acc_mf[q], cmul(xs, m));
         double2 xb2 = cmul(xb, xb);
@@ -310,9 +309,9 @@ __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restr
 
 cudaError_t launch_field_shift(const double2* vbias, const double* xi, const double2* mf, int W, int X, double sqrt_dt,
                                double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st,
-                               float* xs_hi, float* xs_lo) {
-  field_shift_kernel<<<(W + 31) / 32, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, xshifted, cmf, cfb, xs_hi,
-                                                    xs_lo);
+                               void* xs_hi, void* xs_lo) {
+  field_shift_kernel<<<(W + 31) / 32, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, xshifted, cmf, cfb,
+                                                    static_cast<__half*>(xs_hi), static_cast<__half*>(xs_lo));
   note_launch();
   return cudaGetLastError();
 }

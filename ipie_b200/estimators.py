@@ -43,21 +43,26 @@ def _local_energy(hamiltonian, walkers, trial, rhf):
 
 
 def _mixed_energy_operands(trial, hamiltonian):
-    """Padded TF32 head/remainder copies of the half-rotated Cholesky (built once per trial)."""
+    """Padded FP16 head/remainder copies of the half-rotated Cholesky with their power-of-two
+    scale, (hi, lo, scale) per spin (built once per trial)."""
     if getattr(trial, "_rpad", None) is not None:
         return trial._rpad
     X, M = hamiltonian.nchol, hamiltonian.nbasis
+    Mp = (M + 7) // 8 * 8
     out = []
     for r, n in ((trial._rchola, trial.nalpha), (trial._rcholb, trial.nbeta)):
         if out and r is trial._rchola:
             out.append(out[0])
             continue
         NP = 8 if n <= 8 else 16 if n <= 16 else 32
-        hi = torch.empty(X * NP * M, dtype=torch.float32, device=trial.device)
+        hi = torch.empty(X * NP * Mp, dtype=torch.float16, device=trial.device)
         lo = torch.empty_like(hi)
+        scale = 1.0
         if n > 0:
-            call("ipie_b200_rchol_pad_split", ptr(r), X, n, M, ptr(hi), ptr(lo), stream())
-        out.append((hi, lo))
+            rmax = float(r.abs().max().item()) or 1.0
+            scale = 2.0 ** (14 - int(np.ceil(np.log2(rmax))))
+            call("ipie_b200_rchol_pad_split", ptr(r), X, n, M, scale, ptr(hi), ptr(lo), stream())
+        out.append((hi, lo, scale))
     trial._rpad = out
     return out
 
@@ -103,7 +108,7 @@ def local_energy_mixed(system, hamiltonian, walkers, trial, rhf=False, reference
     """Mixed-precision local energy: the exchange as 3-pass TF32 tensor-core products
     (around the trial when ``reference``), Coulomb and one-body in FP64."""
     W, X, M = walkers.nwalkers, hamiltonian.nchol, hamiltonian.nbasis
-    (ra_hi, ra_lo), (rb_hi, rb_lo) = _mixed_energy_operands(trial, hamiltonian)
+    (ra_hi, ra_lo, ra_s), (rb_hi, rb_lo, rb_s) = _mixed_energy_operands(trial, hamiltonian)
     rows = 2
     for n in (walkers.nup, walkers.ndown):
         NP = 8 if n <= 8 else 16 if n <= 16 else 32
@@ -117,7 +122,7 @@ def local_energy_mixed(system, hamiltonian, walkers, trial, rhf=False, reference
     energy = torch.empty(W, 3, dtype=C128, device=walkers.device)
     gts, ks, raw = exchange_reference(trial, hamiltonian) if reference else ((None, None), (None, None), None)
     call("ipie_b200_local_energy_mixed", int(rhf), ptr(trial._rchola), ptr(trial._rcholb), ptr(ra_hi), ptr(ra_lo),
-         ptr(rb_hi), ptr(rb_lo), ptr(trial._rH1a),
+         ra_s, ptr(rb_hi), ptr(rb_lo), rb_s, ptr(trial._rH1a),
          ptr(trial._rH1b), hamiltonian.ecore, ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), ptr(gts[0]), ptr(gts[1]),
          ptr(ks[0]), ptr(ks[1]), ptr(raw), W, X, M, walkers.nup,
          walkers.ndown, ptr(walkers._energy_gwork), ptr(buf), ptr(energy), ptr(walkers.status), stream())

@@ -102,8 +102,9 @@ class Workspace:
         W, M, X, N = self.W, self.M, self.X, max(self.na, self.nb)
         f32, dev = torch.float32, self.dev
         self.gwork = torch.empty(2 * W * 2 * 32 * M, dtype=f32, device=dev)
-        self.xs_hi = torch.empty(W, 2, X, dtype=f32, device=dev)
-        self.xs_lo = torch.empty(W, 2, X, dtype=f32, device=dev)
+        Xp = (X + 7) // 8 * 8  # binary16 rows padded to 16 bytes
+        self.xs_hi = torch.empty(W, 2, Xp, dtype=torch.float16, device=dev)
+        self.xs_lo = torch.empty(W, 2, Xp, dtype=torch.float16, device=dev)
         self.v_planar = [torch.empty(W, M, M, dtype=f32, device=dev) for _ in range(4)]  # re_hi, re_lo, im_hi, im_lo
         self.orb_work = torch.empty(4 * W * 2 * N * M, dtype=f32, device=dev)
 
@@ -173,12 +174,22 @@ class PhaselessGeneric:
         dev = self.device
         P = hamiltonian.npacked
         f32 = torch.float32
-        self.cp_hi = torch.empty(P, X, dtype=f32, device=dev)
-        self.cp_lo = torch.empty(P, X, dtype=f32, device=dev)
-        call("ipie_b200_split_tf32", ptr(hamiltonian.chol_packed), ptr(self.cp_hi), ptr(self.cp_lo), P * X, stream())
+        # packed Cholesky as the FP16 operand of the VHS product, scaled by a power of two that
+        # puts its largest entry near 2^14; rows padded to a multiple of 8 halves
+        Xp = (X + 7) // 8 * 8
+        cmax = float(hamiltonian.chol_packed.abs().max().item()) or 1.0
+        self.cp_scale = 2.0 ** (14 - int(np.ceil(np.log2(cmax))))
+        cp = hamiltonian.chol_packed
+        if Xp != X:
+            cp = torch.zeros(P, Xp, dtype=cp.dtype, device=dev)
+            cp[:, :X] = hamiltonian.chol_packed
+        self.cp_hi = torch.empty(P, Xp, dtype=torch.float16, device=dev)
+        self.cp_lo = torch.empty(P, Xp, dtype=torch.float16, device=dev)
+        call("ipie_b200_split_f16", ptr(cp), ptr(self.cp_hi), ptr(self.cp_lo), P * Xp, self.cp_scale, stream())
+        del cp
         from .estimators import _mixed_energy_operands
 
-        # padded half-rotated Cholesky TF32 head/remainder: force bias and energy share it
+        # padded half-rotated Cholesky FP16 head/remainder: force bias and energy share it
         self.rpad = _mixed_energy_operands(trial, hamiltonian)
         self.lde = M
         # the one-body factor enters the mixed orbital update as E - I (the identity is added in FP64)
@@ -338,8 +349,8 @@ class PhaselessGeneric:
         ws = self.ws
         W, X, M = walkers.nwalkers, hamiltonian.nchol, walkers.nbasis
         self.timer.start("force_bias")
-        (ra_hi, ra_lo), (rb_hi, rb_lo) = self.rpad
-        call("ipie_b200_construct_force_bias_mixed", ptr(ra_hi), ptr(ra_lo), ptr(rb_hi), ptr(rb_lo),
+        (ra_hi, ra_lo, ra_s), (rb_hi, rb_lo, rb_s) = self.rpad
+        call("ipie_b200_construct_force_bias_mixed", ptr(ra_hi), ptr(ra_lo), ra_s, ptr(rb_hi), ptr(rb_lo), rb_s,
              ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), ptr(ws.gwork), W, X, M, walkers.nup, walkers.ndown,
              ptr(ws.vbias), ptr(walkers.status), stream())
         self.timer.stop("force_bias")
@@ -354,8 +365,8 @@ class PhaselessGeneric:
         self.timer.start("vhs")
         v = ws.v_planar
         call("ipie_b200_construct_vhs_mixed", ptr(self.cp_hi), ptr(self.cp_lo), ptr(hamiltonian.sym_idx_i),
-             ptr(hamiltonian.sym_idx_j), M, X, ptr(ws.xs_hi), ptr(ws.xs_lo), W, self.sqrt_dt, ptr(v[0]), ptr(v[1]),
-             ptr(v[2]), ptr(v[3]), ptr(walkers.status), stream())
+             ptr(hamiltonian.sym_idx_j), M, X, ptr(ws.xs_hi), ptr(ws.xs_lo), W, self.sqrt_dt, self.cp_scale,
+             ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]), ptr(walkers.status), stream())
         self.timer.stop("vhs")
         self.timer.start("orbitals")
         for s_, (phi_name, tmp_name, n) in enumerate((("phia", "phia_tmp", walkers.nup),

@@ -42,10 +42,10 @@ def test_mixed_force_bias_3pass():
 
     ws = pm._workspace(walkers, ham)
     out = torch.empty_like(ref)
-    (ra_hi, ra_lo), (rb_hi, rb_lo) = pm.rpad
-    call("ipie_b200_construct_force_bias_mixed", ptr(ra_hi), ptr(ra_lo), ptr(rb_hi), ptr(rb_lo), ptr(walkers.Ghalfa),
-         ptr(walkers.Ghalfb), ptr(ws.gwork), 40, s.nchol, s.nbasis, s.nup, s.ndown, ptr(out), ptr(walkers.status),
-         stream())
+    (ra_hi, ra_lo, ra_s), (rb_hi, rb_lo, rb_s) = pm.rpad
+    call("ipie_b200_construct_force_bias_mixed", ptr(ra_hi), ptr(ra_lo), ra_s, ptr(rb_hi), ptr(rb_lo), rb_s,
+         ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), ptr(ws.gwork), 40, s.nchol, s.nbasis, s.nup, s.ndown, ptr(out),
+         ptr(walkers.status), stream())
     assert rel(out, ref) < 1e-5
     walkers.check_status()
 
@@ -66,8 +66,8 @@ def test_mixed_vhs_3pass():
     ref = prop.construct_VHS(ham, xs)
     v = ws.v_planar
     call("ipie_b200_construct_vhs_mixed", ptr(pm.cp_hi), ptr(pm.cp_lo), ptr(ham.sym_idx_i), ptr(ham.sym_idx_j),
-         s.nbasis, s.nchol, ptr(ws.xs_hi), ptr(ws.xs_lo), W, pm.sqrt_dt, ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]),
-         ptr(walkers.status), stream())
+         s.nbasis, s.nchol, ptr(ws.xs_hi), ptr(ws.xs_lo), W, pm.sqrt_dt, pm.cp_scale, ptr(v[0]), ptr(v[1]), ptr(v[2]),
+         ptr(v[3]), ptr(walkers.status), stream())
     got = (v[0].double() + v[1].double()) + 1j * (v[2].double() + v[3].double())
     assert rel(got, ref) < 1e-5
     walkers.check_status()
