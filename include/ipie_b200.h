@@ -245,15 +245,34 @@ int ipie_b200_field_shift_mixed(const void* vbias, const double* xi, const void*
                                 void* cfb, void* stream);
 
 /* VHS = i sqrt(dt) L . xshifted as a 3-pass FP16 tensor-core product (FP32
- * accumulation, ~2^-22 relative), written as four planar (W, M, M) fp32 arrays:
- * Re/Im x TF32 head/remainder.  cp_hi/cp_lo: packed Cholesky (P, Xp) x cp_scale
- * (a power of two putting its largest entry near 2^14) split into binary16
- * (ipie_b200_split_f16); xs_hi/xs_lo from ipie_b200_field_shift_mixed.  replaces
- * (mixed form): propagation/phaseless_generic.py:66-97. */
+ * accumulation, ~2^-22 relative), written as four planar arrays Re/Im x head/
+ * remainder: f16_planes = 0: fp32 TF32 head/remainder (W, M, M) (the operands of
+ * ipie_b200_propagate_orbitals_mixed); f16_planes = 1: binary16 head/remainder
+ * of V x v_scale (a power of two, > 0), (W, M, Mp) with Mp = M rounded up to a
+ * multiple of 8 (the operands of ipie_b200_propagate_orbitals_mixed16).
+ * cp_hi/cp_lo: packed Cholesky (P, Xp) x cp_scale (a power of two putting its
+ * largest entry near 2^14) split into binary16 (ipie_b200_split_f16); xs_hi/xs_lo
+ * from ipie_b200_field_shift_mixed.  replaces (mixed form):
+ * propagation/phaseless_generic.py:66-97. */
 int ipie_b200_construct_vhs_mixed(const void* cp_hi, const void* cp_lo, const int* idx_i, const int* idx_j, int M,
                                   int X, const void* xs_hi, const void* xs_lo, int W, double sqrt_dt, double cp_scale,
-                                  float* v_re_hi, float* v_re_lo, float* v_im_hi, float* v_im_lo, unsigned int* status,
-                                  void* stream);
+                                  int f16_planes, double v_scale, void* v_re_hi, void* v_re_lo, void* v_im_hi,
+                                  void* v_im_lo, unsigned int* status, void* stream);
+
+/* 1 when ipie_b200_propagate_orbitals_mixed16 takes this spin block (M <= 256, 1 <= N <= 32). */
+int ipie_b200_orbital_chain16_fits(int M, int N);
+
+/* phi_out = E exp(V) E phi_in per walker (Taylor order nmax) in one launch, every
+ * product a 3-pass FP16 tensor-core product (FP32 accumulation); the walker's
+ * Taylor terms stay on chip, each with its own exact power-of-two scale, and phi
+ * accumulates as head/tail float pairs (~2^-47) between FP64 input and output.
+ * e_hi/e_lo: (E - I) x e_scale (M, Mp) binary16 head/remainder (E real); v_*:
+ * the f16_planes output of ipie_b200_construct_vhs_mixed with its v_scale.
+ * replaces (mixed form): propagation/phaseless_base.py:321-327. */
+int ipie_b200_propagate_orbitals_mixed16(const void* e_hi, const void* e_lo, double e_scale, const void* v_re_hi,
+                                         const void* v_re_lo, const void* v_im_hi, const void* v_im_lo,
+                                         double v_scale, const void* phi_in, void* phi_out, int W, int M, int N,
+                                         int nmax, unsigned int* status, void* stream);
 
 /* phi_out = E exp(V) E phi_in per walker with every product a 3-pass TF32
  * tensor-core GEMM (E = expH1 hi/lo (M, lde) fp32, lde % 4 == 0; V planar from

@@ -41,7 +41,9 @@ SIGNATURES = {
     "ipie_b200_walker_sums": [I, P, P, P, P, P, I, P],
     "ipie_b200_construct_force_bias_mixed": [P, P, D, P, P, D, P, P, P, I, I, I, I, I, P, P, P],
     "ipie_b200_field_shift_mixed": [P, P, P, I, I, D, D, P, P, P, P, P, P],
-    "ipie_b200_construct_vhs_mixed": [P, P, P, P, I, I, P, P, I, D, D, P, P, P, P, P, P],
+    "ipie_b200_construct_vhs_mixed": [P, P, P, P, I, I, P, P, I, D, D, I, D, P, P, P, P, P, P],
+    "ipie_b200_orbital_chain16_fits": [I, I],
+    "ipie_b200_propagate_orbitals_mixed16": [P, P, D, P, P, P, P, D, P, P, I, I, I, I, P, P],
     "ipie_b200_propagate_orbitals_mixed": [P, P, I, P, P, P, P, P, P, P, I, I, I, I, P, P],
     "ipie_b200_rchol_pad_split": [P, I, I, I, D, P, P, P],
     "ipie_b200_exchange_mixed": [P, P, D, P, P, P, P, I, I, I, I, P, P, P, P, P],

@@ -71,9 +71,11 @@ cudaError_t mixed_orbital_chain(const float* e_hi, const float* e_lo, int lde, c
                                 const float* v_re_lo, const float* v_im_hi, const float* v_im_lo,
                                 const double2* phi_in, double2* phi_out, int W, int M, int N, int nmax,
                                 unsigned* status, cudaStream_t st);
-cudaError_t mixed_vhs(const float* cp_hi, const float* cp_lo, const int* ii, const int* jj, int P, int X, int M,
-                      const float* xs_hi, const float* xs_lo, int W, double sqrt_dt, float* re_hi, float* re_lo,
-                      float* im_hi, float* im_lo, unsigned* status, cudaStream_t st);
+bool orbital_chain16_fits(int M, int N);
+cudaError_t mixed_orbital_chain16(const void* e_hi, const void* e_lo, float e_scale, const void* v_re_hi,
+                                  const void* v_re_lo, const void* v_im_hi, const void* v_im_lo, float v_scale,
+                                  const double2* phi_in, double2* phi_out, int W, int M, int N, int nmax,
+                                  unsigned* status, cudaStream_t st);
 cudaError_t mixed_orbitals(const float* e_hi, const float* e_lo, int Mp, const float* v_re_hi, const float* v_re_lo,
                            const float* v_im_hi, const float* v_im_lo, const double2* phi_in, double2* phi_out,
                            float* b0_hi, float* b0_lo, float* b1_hi, float* b1_lo, int W, int M, int N, int nmax,

@@ -75,6 +75,25 @@ cudaError_t make_map_f16(CUtensorMap* m, const void* base, long long rows, long 
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// 3-D batched K-major FP16 operand: `batch` matrices of `rows` x `k` halves (row stride ld
+// halves, ld % 8 == 0; matrix stride rows * ld), tiles of box_rows x 64 of one matrix; rows past
+// `rows` and columns past `k` read as 0 (no traffic).
+cudaError_t make_map_f16_batched(CUtensorMap* m, const void* base, long long batch, long long rows, long long k,
+                                 long long ld, int box_rows) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 8) || rows <= 0 || k <= 0 || batch <= 0 || ld < k)
+    return cudaErrorInvalidValue;
+  cuuint64_t dims[3] = {(cuuint64_t)k, (cuuint64_t)rows, (cuuint64_t)batch};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)rows * ld * 2};
+  cuuint32_t box[3] = {64, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 // hi = FP16(x * scale), lo = FP16(x * scale - hi): the split of the FP16 3-pass product.
 __global__ void split_f16_kernel(const double* __restrict__ x, __half* __restrict__ hi, __half* __restrict__ lo,
                                  long long n, double scale) {
@@ -291,6 +310,41 @@ struct EpiVHSSplit {
         if (i != j) {
           store_split(re_hi, re_lo, b, vre);
           store_split(im_hi, im_lo, b, vim);
+        }
+      }
+    }
+  }
+};
+
+// VHS for the FP16 orbital chain: V x v_scale written to both triangles of four planar
+// (W, M, ld) binary16 arrays (re/im x head/remainder; ld = M rounded up to 8, the pad columns
+// are not written).
+template <int BN>
+struct EpiVHSF16 {
+  __half *re_hi, *re_lo, *im_hi, *im_lo;
+  const int* ii;
+  const int* jj;
+  int P, M, ld, W;
+  float f;  // sqrt(dt) v_scale / (operand scales)
+  __device__ __forceinline__ static void put(__half* hi, __half* lo, size_t i, float x) {
+    const __half h = __float2half_rn(x);
+    hi[i] = h;
+    lo[i] = __float2half_rn(x - __half2float(h));
+  }
+  __device__ __forceinline__ void operator()(int, int p, int n0, const float* v, uint8_t*) const {
+    if (p >= P) return;
+    const int i = ii[p], j = jj[p];
+#pragma unroll
+    for (int q = 0; q < BN / 2; ++q) {
+      const int w = (n0 >> 1) + q;
+      if (w < W) {
+        const float vre = -f * v[2 * q + 1], vim = f * v[2 * q];
+        const size_t a = ((size_t)w * M + i) * ld + j, b = ((size_t)w * M + j) * ld + i;
+        put(re_hi, re_lo, a, vre);
+        put(im_hi, im_lo, a, vim);
+        if (i != j) {
+          put(re_hi, re_lo, b, vre);
+          put(im_hi, im_lo, b, vim);
         }
       }
     }
@@ -648,8 +702,9 @@ static cudaError_t exchange3(const void* r_hi, const void* r_lo, double rscale, 
 int exchange3_rows(int X, int N) { return (X * exchange_np(N) + kBM - 1) / kBM; }
 
 cudaError_t mixed_vhs(const void* cp_hi, const void* cp_lo, const int* ii, const int* jj, int P, int X, int M,
-                      const void* xs_hi, const void* xs_lo, int W, double sqrt_dt, double cp_scale, float* re_hi,
-                      float* re_lo, float* im_hi, float* im_lo, unsigned* status, cudaStream_t st) {
+                      const void* xs_hi, const void* xs_lo, int W, double sqrt_dt, double cp_scale, int f16_planes,
+                      double v_scale, void* re_hi, void* re_lo, void* im_hi, void* im_lo, unsigned* status,
+                      cudaStream_t st) {
   // FP16 operands (packed Cholesky x cp_scale, fields x kFieldScaleF16) on 128 x 256 tiles
   // (two column groups of 128: half the re-reads of the packed Cholesky).  One CTA per tile:
   // measured faster here than persistent CTAs.
@@ -664,7 +719,13 @@ cudaError_t mixed_vhs(const void* cp_hi, const void* cp_lo, const int* ii, const
   if ((e = make_map_f16(&maps.b_lo, xs_lo, 2LL * W, X, ldx, BN)) != cudaSuccess) return e;
   dim3 grid((2 * W + BN - 1) / BN, (P + kBM - 1) / kBM, 1);
   const double unscale = sqrt_dt / (cp_scale * kFieldScaleF16);  // powers of two: exact
-  EpiVHSSplit<128> epi{re_hi, re_lo, im_hi, im_lo, ii, jj, P, M, W, (float)unscale};
+  if (f16_planes) {
+    using H = __half*;
+    EpiVHSF16<128> epi{H(re_hi), H(re_lo), H(im_hi), H(im_lo), ii, jj, P, M, f16_ld(M), W, (float)(unscale * v_scale)};
+    return launch_umma<BN, 1, 3, 2, EpiVHSF16<128>, KIND_F16>(maps, X, 0, 0, grid, epi, status, st, false, false);
+  }
+  using F = float*;
+  EpiVHSSplit<128> epi{F(re_hi), F(re_lo), F(im_hi), F(im_lo), ii, jj, P, M, W, (float)unscale};
   return launch_umma<BN, 1, 3, 2, EpiVHSSplit<128>, KIND_F16>(maps, X, 0, 0, grid, epi, status, st, false, false);
 }
 
@@ -752,11 +813,26 @@ extern "C" int ipie_b200_field_shift_mixed(const void* vbias, const double* xi, 
 
 extern "C" int ipie_b200_construct_vhs_mixed(const void* cp_hi, const void* cp_lo, const int* idx_i,
                                              const int* idx_j, int M, int X, const void* xs_hi, const void* xs_lo,
-                                             int W, double sqrt_dt, double cp_scale, float* v_re_hi, float* v_re_lo,
-                                             float* v_im_hi, float* v_im_lo, unsigned int* status, void* stream) {
-  if (!(cp_scale > 0.0)) return (int)cudaErrorInvalidValue;
+                                             int W, double sqrt_dt, double cp_scale, int f16_planes, double v_scale,
+                                             void* v_re_hi, void* v_re_lo, void* v_im_hi, void* v_im_lo,
+                                             unsigned int* status, void* stream) {
+  if (!(cp_scale > 0.0) || (f16_planes && !(v_scale > 0.0))) return (int)cudaErrorInvalidValue;
   return (int)umma::mixed_vhs(cp_hi, cp_lo, idx_i, idx_j, M * (M + 1) / 2, X, M, xs_hi, xs_lo, W, sqrt_dt, cp_scale,
-                              v_re_hi, v_re_lo, v_im_hi, v_im_lo, status, reinterpret_cast<cudaStream_t>(stream));
+                              f16_planes, v_scale, v_re_hi, v_re_lo, v_im_hi, v_im_lo, status,
+                              reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ipie_b200_orbital_chain16_fits(int M, int N) { return umma::orbital_chain16_fits(M, N) ? 1 : 0; }
+
+extern "C" int ipie_b200_propagate_orbitals_mixed16(const void* e_hi, const void* e_lo, double e_scale,
+                                                    const void* v_re_hi, const void* v_re_lo, const void* v_im_hi,
+                                                    const void* v_im_lo, double v_scale, const void* phi_in,
+                                                    void* phi_out, int W, int M, int N, int nmax,
+                                                    unsigned int* status, void* stream) {
+  return (int)umma::mixed_orbital_chain16(e_hi, e_lo, (float)e_scale, v_re_hi, v_re_lo, v_im_hi, v_im_lo,
+                                          (float)v_scale, reinterpret_cast<const double2*>(phi_in),
+                                          reinterpret_cast<double2*>(phi_out), W, M, N, nmax, status,
+                                          reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int ipie_b200_propagate_orbitals_mixed(const float* e_hi, const float* e_lo, int lde, const float* v_re_hi,

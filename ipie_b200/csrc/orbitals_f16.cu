@@ -1,0 +1,486 @@
+// Fused mixed-precision orbital update of one spin block on FP16 operands, one
+// walker per CTA at a time (persistent CTAs):
+//
+//     phi <- phi + (E - I) phi                  (one-body, FP64 add of the product)
+//     T_0 = phi;  T_k = V T_{k-1} / k;  phi += T_k   (k = 1 .. nmax, Taylor series of exp(V))
+//     phi <- phi + (E - I) phi                  (one-body)
+//
+// Every product is a 3-pass FP16 tcgen05 GEMM (A_hi B_hi + A_hi B_lo + A_lo B_hi,
+// kind::f16, FP32 accumulators in TMEM) of operands split into binary16 head and
+// remainder after a power-of-two scale: E - I by e_scale and V by v_scale (fixed
+// per call, chosen by the caller), and the right operand B (the walker's current
+// T_k or phi) by its own exact scale, 2^(14 - e) for max|B| = f 2^e, f in [0.5, 1),
+// found with a CTA-wide max before B is written.  The split carries ~2^-22
+// relative accuracy of every entry within ~2^16 of the largest, like the TF32
+// split.  phi accumulates in TMEM as head/tail float pairs (~2^-47 relative)
+// between the first one-body factor, read from FP64 global memory, and the
+// last, written to it in FP64.
+//
+// What stays on chip: B (planar rows -- Re of orbital n at row n, Im at row
+// BN/2 + n -- FP16 head and remainder) lives in shared memory for the whole
+// chain; each term's epilogue writes the next term's operand straight into the
+// 128B-swizzled K-major layout the MMA reads, so T_k never goes to global
+// memory.  Only the left operands stream through TMA: the walker's VHS planes
+// (re/im, hi/lo; 3-D tensor map, rows and columns past M zero-filled without
+// traffic; the same ~0.3 MB for every term, so after the first term they come
+// from L2) and the shared E - I.
+//
+// Roles (BN = 64: 576 threads): warps 0..4G-1 epilogue (warp w: TMEM lane quarter
+// w % 4, i.e. one output row per thread, and orbital group w / 4 of G = BN / 16
+// groups of 8), then one warp whose lane 0 is the TMA producer and one whose lane
+// 0 issues the MMAs.  Barriers: full/empty per stage (TMA <-> MMA), accb[mt]
+// (MMA -> epilogue, once per 128-row tile and term), bready (epilogue -> MMA, one
+// arrival per epilogue thread per term: B written and TMEM read), and the named
+// barrier 1 of the epilogue threads around the CTA-wide max of each new B.
+// Every mbarrier wait is bounded (umma.cuh); a timeout raises the status bit and
+// all roles leave their loops (the epilogue threads still meet at their named
+// barrier in the same order), then TMEM is released.
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include "../../include/ipie_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+#include "umma.cuh"
+
+namespace ipie_b200 {
+namespace umma {
+
+cudaError_t make_map_f16(CUtensorMap* m, const void* base, long long rows, long long k, long long ld, int box_rows);
+cudaError_t make_map_f16_batched(CUtensorMap* m, const void* base, long long batch, long long rows, long long k,
+                                 long long ld, int box_rows);
+
+namespace {
+
+struct Chain16Maps {
+  CUtensorMap e_hi, e_lo;  // E - I (M x Mp halves), box 128 x 64
+  CUtensorMap v[4];        // VHS planes re_hi, im_hi, re_lo, im_lo (W, M, Mp halves), box 1 x 128 x 64
+};
+
+constexpr int kATile = 128 * 128;        // bytes: 128 rows x 64 halves
+constexpr int kStages = 4;
+constexpr int kStageBytes = 2 * kATile;  // re and im planes of one part (hi or lo)
+constexpr int kMaxM = 256;
+constexpr int kKB = kMaxM / 64;          // k-blocks of 64 reserved for B (M <= 256)
+
+template <int BN>
+struct Chain16Roles {
+  static constexpr int kGroups = BN / 16;
+  static constexpr int kEpiWarps = 4 * kGroups;
+  static constexpr int kEpiThreads = 32 * kEpiWarps;
+  static constexpr int kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
+  static constexpr int kThreads = kEpiThreads + 64;
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+// byte offset of B element (row n, k) inside one B region (hi or lo): k-block tiles of BN rows x
+// 128 bytes (64 halves), 16-byte chunks (8 halves) XOR-swizzled with the row (TMA's 128B pattern)
+template <int BN>
+__device__ __forceinline__ uint32_t b16_offset(int n, int k) {
+  const int kb = k >> 6, kc = k & 63;
+  return (uint32_t)(kb * BN * 128 + n * 128 + ((((kc >> 3) ^ (n & 7)) << 4) | ((kc & 7) << 1)));
+}
+
+// B element = binary16 head and remainder of x * s (s a power of two)
+template <int BN>
+__device__ __forceinline__ void put_b16(uint8_t* bhi, uint8_t* blo, int n, int k, float x, float s) {
+  const uint32_t o = b16_offset<BN>(n, k);
+  const float y = x * s;
+  const __half h = __float2half_rn(y);
+  *reinterpret_cast<__half*>(bhi + o) = h;
+  *reinterpret_cast<__half*>(blo + o) = __float2half_rn(y - __half2float(h));
+}
+
+// (a, b) += x for a head/tail float pair a + b (|b| <= ulp(a)/2): Knuth's two-sum of a and x,
+// then the tail folded back; ~2^-47 relative, enough to accumulate the FP32 Taylor terms
+// of phi without a round trip through FP64 global memory.
+__device__ __forceinline__ void ff_add(float& a, float& b, float x) {
+  const float s = a + x;
+  const float v = s - a;
+  const float e = (a - (s - v)) + (x - v);
+  const float t = b + e;
+  a = s + t;
+  b = t - (a - s);
+}
+
+// scale of a new B from its largest magnitude: 2^(14 - e) for max = f 2^e, f in [0.5, 1); capped
+// at 2^64 (a term below 2^-51 of unit orbitals stays smaller than the ideal range, and the
+// unscaling factor 1 / (k v_scale s) stays a normal float)
+__device__ __forceinline__ float b_scale_for(float mx) {
+  if (!(mx > 0.0f) || !isfinite(mx)) return 1.0f;
+  int e;
+  frexpf(mx, &e);
+  return ldexpf(1.0f, 14 - max(e, -50));
+}
+
+// CTA-wide max of |v| and AND of ok over the nthreads epilogue threads, in one barrier (named
+// barrier 1, which also orders the shared-memory atomics before the read).  Slot u % 3 of smax
+// takes this max; slot (u + 2) % 3 is cleared for the one after next (its last reader passed
+// the barrier before this one).  Every epilogue thread takes part every time, so a failed wait
+// anywhere makes all of them leave at the same point.
+__device__ __forceinline__ bool epi_max_vote(float v, bool ok, unsigned* smax, uint32_t& u, int nthreads,
+                                             float& mx) {
+  const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v)));
+  if ((threadIdx.x & 31) == 0) atomicMax(&smax[u % 3], bits);
+  uint32_t r;
+  asm volatile(
+      "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.and.pred q, 1, %2, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)ok), "r"(nthreads)
+      : "memory");
+  mx = __uint_as_float(*reinterpret_cast<volatile unsigned*>(&smax[u % 3]));
+  if (threadIdx.x == 0) smax[(u + 2) % 3] = 0u;
+  ++u;
+  return r != 0;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
+    orbital_chain16_kernel(const __grid_constant__ Chain16Maps maps, float e_scale, float v_scale,
+                           const double2* __restrict__ phi_in, double2* __restrict__ phi_out, int W, int M, int N,
+                           int nmax, unsigned* status) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int KB = (M + 63) / 64, MT = (M + 127) / 128;
+  constexpr int kBTile = BN * 128;
+  constexpr int kH = BN / 2;  // Im rows start here
+  using R = Chain16Roles<BN>;
+  constexpr int kEpiThreads = R::kEpiThreads, kThreads = R::kThreads;
+  constexpr int kProducerWarp = R::kProducerWarp, kMmaWarp = R::kMmaWarp;
+  uint8_t* b_hi = smem;
+  uint8_t* b_lo = smem + kKB * kBTile;
+  uint8_t* stg = smem + 2 * kKB * kBTile;
+  uint64_t* full = reinterpret_cast<uint64_t*>(stg + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* accb = empty + kStages;  // one per 128-row tile (M <= 256)
+  uint64_t* bready = accb + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bready + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  unsigned* smax = reinterpret_cast<unsigned*>(tmem_slot + 2);  // [3]
+  // TMEM columns: accumulators 2 m-tiles x 2 left operands x BN, then phi as head/tail float
+  // pairs (2 m-tiles x [head BN | tail BN])
+  constexpr uint32_t kTmemCols = 8 * BN;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&accb[0], 1);
+    mbar_init(&accb[1], 1);
+    mbar_init(bready, kEpiThreads);
+    *abort_flag = 0;
+    smax[0] = smax[1] = smax[2] = 0u;
+    mbar_fence_init();
+  }
+  // rows n >= N (and kH + n >= kH + N) and k >= M of B stay zero for the whole kernel
+  for (int i = threadIdx.x; i < 2 * kKB * kBTile / 16; i += kThreads)
+    reinterpret_cast<int4*>(smem)[i] = make_int4(0, 0, 0, 0);
+  fence_proxy_async_smem();
+  if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int nterms = nmax + 2;
+
+  if (warp == kProducerWarp) {
+    // ------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      tma_prefetch_desc(&maps.e_hi);
+      tma_prefetch_desc(&maps.e_lo);
+      for (int i = 0; i < 4; ++i) tma_prefetch_desc(&maps.v[i]);
+      uint32_t g = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < W && ok; w += gridDim.x)
+        for (int t = 0; t < nterms && ok; ++t) {
+          const bool onebody = (t == 0 || t == nterms - 1);
+          for (int mt = 0; mt < MT && ok; ++mt)
+            for (int kb = 0; kb < KB && ok; ++kb)
+              for (int part = 0; part < 2; ++part, ++g) {
+                const uint32_t s = g % kStages, r = g / kStages;
+                if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) {
+                  ok = false;
+                  break;
+                }
+                uint8_t* st = stg + s * kStageBytes;
+                if (onebody) {
+                  mbar_expect_tx(&full[s], kATile);
+                  tma_load_2d(st, part ? &maps.e_lo : &maps.e_hi, kb * 64, mt * 128, &full[s]);
+                } else {
+                  // rows and columns past M of the walker's matrix are zero-filled by TMA (no traffic)
+                  mbar_expect_tx(&full[s], 2 * kATile);
+                  tma_load_3d(st, &maps.v[2 * part], kb * 64, mt * 128, w, &full[s]);
+                  tma_load_3d(st + kATile, &maps.v[2 * part + 1], kb * 64, mt * 128, w, &full[s]);
+                }
+              }
+        }
+    }
+    __syncwarp();
+  } else if (warp == kMmaWarp) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_f16(128, BN);
+      uint32_t g = 0, term = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < W && ok; w += gridDim.x)
+        for (int t = 0; t < nterms && ok; ++t, ++term) {
+          const bool onebody = (t == 0 || t == nterms - 1);
+          if (!mbar_wait(bready, term & 1, abort_flag, status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          for (int mt = 0; mt < MT && ok; ++mt)
+            for (int kb = 0; kb < KB && ok; ++kb)
+              for (int part = 0; part < 2; ++part, ++g) {
+                const uint32_t s = g % kStages, r = g / kStages;
+                if (!mbar_wait(&full[s], r & 1, abort_flag, status)) {
+                  ok = false;
+                  break;
+                }
+                tc_fence_after();
+                uint8_t* st = stg + s * kStageBytes;
+                const uint64_t a0 = desc_kmajor_sw128(st), a1 = desc_kmajor_sw128(st + kATile);
+                const uint64_t bh = desc_kmajor_sw128(b_hi + kb * kBTile), bl = desc_kmajor_sw128(b_lo + kb * kBTile);
+                const uint32_t d0 = tmem + (uint32_t)((mt * 2 + 0) * BN), d1 = tmem + (uint32_t)((mt * 2 + 1) * BN);
+                // K steps of 16 past M are all zero: skip them
+                const int kk_end = min(4, (M - kb * 64 + 15) / 16);
+                for (int kk = 0; kk < kk_end; ++kk) {
+                  const uint32_t acc = (kb > 0 || kk > 0 || part > 0) ? 1u : 0u;
+                  if (part == 0) {
+                    mma_f16(d0, a0 + 2 * kk, bh + 2 * kk, idesc, acc);
+                    mma_f16(d0, a0 + 2 * kk, bl + 2 * kk, idesc, 1u);
+                    if (!onebody) {
+                      mma_f16(d1, a1 + 2 * kk, bh + 2 * kk, idesc, acc);
+                      mma_f16(d1, a1 + 2 * kk, bl + 2 * kk, idesc, 1u);
+                    }
+                  } else {
+                    mma_f16(d0, a0 + 2 * kk, bh + 2 * kk, idesc, 1u);
+                    if (!onebody) mma_f16(d1, a1 + 2 * kk, bh + 2 * kk, idesc, 1u);
+                  }
+                }
+                mma_commit(&empty[s]);
+                if (kb == KB - 1 && part == 1) mma_commit(&accb[mt]);
+              }
+        }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue warps
+    constexpr int kHalf = kH / R::kGroups;
+    static_assert(kHalf == 8, "one group of 8 orbitals per epilogue warp");
+    const int quarter = warp & 3, half = warp >> 2;  // lane quarter, orbital group
+    const int c0 = half * kHalf;                     // this warp's first orbital
+    const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+    uint32_t term = 0, u = 0;
+    bool ok = true, voted_out = false;
+    // the walker loop ends only through the votes, which every epilogue thread takes together
+    for (int w = blockIdx.x; w < W; w += gridDim.x) {
+      const double2* pin = phi_in + (size_t)w * M * N;
+      double2* pout = phi_out + (size_t)w * M * N;
+      // prologue: B = planar split of the walker's starting orbitals x their exact scale, read
+      // coalesced (consecutive threads take consecutive elements of the row-major M x N block);
+      // the second read comes from cache
+      float pmax = 0.0f;
+      for (int i = threadIdx.x; i < M * N; i += kEpiThreads) {
+        const double2 z = pin[i];
+        pmax = fmaxf(pmax, fmaxf(fabsf((float)z.x), fabsf((float)z.y)));
+      }
+      float mx;
+      if (!epi_max_vote(pmax, ok && !*abort_flag, smax, u, kEpiThreads, mx)) break;
+      float sb = b_scale_for(mx);  // scale of the current B
+      for (int i = threadIdx.x; i < M * N; i += kEpiThreads) {
+        const int m = i / N, n = i - m * N;
+        const double2 z = pin[i];
+        put_b16<BN>(b_hi, b_lo, n, m, (float)z.x, sb);
+        put_b16<BN>(b_hi, b_lo, kH + n, m, (float)z.y, sb);
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(bready);
+      for (int t = 0; t < nterms; ++t, ++term) {
+        const bool onebody = (t == 0 || t == nterms - 1);
+        const bool last = t == nterms - 1;
+        // the accumulator holds the product of the scaled operands
+        const float unscale = onebody ? 1.0f / (e_scale * sb) : 1.0f / ((float)t * v_scale * sb);
+        // the next B's values (unscaled) wait in this warp's own, already read accumulator
+        // columns until the CTA-wide max gives their scale
+        float lmax = 0.0f;
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+          if (mt >= MT) break;
+          // each 128-row tile has its own accumulator barrier, so the first tile's epilogue
+          // overlaps the second tile's MMAs; a failed wait skips the work, not the vote below
+          if (ok && !mbar_wait(&accb[mt], term & 1, abort_flag, status)) ok = false;
+          ok = __all_sync(0xffffffffu, ok) != 0;
+          if (!ok) continue;
+          tc_fence_after();
+          // a warp whose 32 rows all lie past M, or whose orbitals all lie past N, has nothing to do
+          if (mt * 128 + quarter * 32 >= M || c0 >= N) continue;
+          const int m = mt * 128 + quarter * 32 + lane;
+          const bool row_ok = m < M;
+          const uint32_t dc0 = lane_base + (uint32_t)((mt * 2 + 0) * BN);
+          const uint32_t dc1 = lane_base + (uint32_t)((mt * 2 + 1) * BN);
+          const uint32_t ac = lane_base + (uint32_t)(4 * BN + mt * 2 * BN);  // acc: head [0, BN), tail [BN, 2BN)
+          // real parts, then imaginary parts; TMEM reads/writes are warp-collective, so every
+          // lane takes part and rows past M only skip their global writes
+#pragma unroll
+          for (int p = 0; p < 2; ++p) {
+            // p = 0: Re = D0[n] - D1[kH + n]; p = 1: Im = D0[kH + n] + D1[n]
+            // (one-body: D0[n] and D0[kH + n] with the real left operand E - I)
+            const int cx = (p ? kH : 0) + c0, cy = (p ? 0 : kH) + c0;
+            uint32_t x[8], y[8], ha[8], ta[8], nbits[8];
+            tmem_ld8(tmem + dc0 + cx, x);
+            if (!onebody) tmem_ld8(tmem + dc1 + cy, y);
+            if (t > 0) {
+              tmem_ld8(tmem + ac + cx, ha);
+              tmem_ld8(tmem + ac + BN + cx, ta);
+            }
+            tmem_wait_ld();
+            reg_after_wait(x);
+            if (!onebody) reg_after_wait(y);
+            if (t > 0) {
+              reg_after_wait(ha);
+              reg_after_wait(ta);
+            }
+            double base[8];
+            if (t == 0) {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                const double* src = reinterpret_cast<const double*>(pin + (size_t)m * N + c0 + q) + p;
+                base[q] = (row_ok && c0 + q < N) ? *src : 0.0;
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const int n = c0 + q;
+              float uq = __uint_as_float(x[q]);
+              if (!onebody) uq = p ? uq + __uint_as_float(y[q]) : uq - __uint_as_float(y[q]);
+              const float vq = uq * unscale;  // (E - I) phi, or T_t
+              const bool live = row_ok && n < N;
+              float nb = 0.0f;  // the next B value
+              if (t == 0) {
+                // phi after the first one-body factor, kept as a head/tail float pair
+                const double o = base[q] + (double)vq;
+                const float hh = (float)o;
+                ha[q] = __float_as_uint(hh);
+                ta[q] = __float_as_uint((float)(o - (double)hh));
+                nb = hh;
+              } else if (last) {
+                const double o = (double)__uint_as_float(ha[q]) + (double)__uint_as_float(ta[q]) + (double)vq;
+                if (live) reinterpret_cast<double*>(pout + (size_t)m * N + n)[p] = o;
+              } else {
+                float a = __uint_as_float(ha[q]), b = __uint_as_float(ta[q]);
+                ff_add(a, b, vq);
+                ha[q] = __float_as_uint(a);
+                ta[q] = __float_as_uint(b);
+                nb = t < nmax ? vq : a + b;
+              }
+              if (!live) nb = 0.0f;
+              nbits[q] = __float_as_uint(nb);
+              lmax = fmaxf(lmax, fabsf(nb));
+            }
+            if (!last) {
+              tmem_st8(tmem + ac + cx, ha);
+              tmem_st8(tmem + ac + BN + cx, ta);
+              tmem_st8(tmem + dc0 + cx, nbits);
+            }
+          }
+        }
+        tmem_wait_st();
+        if (!last) {
+          // B of the next term, scaled by its own exact power of two
+          if (!epi_max_vote(lmax, ok && !*abort_flag, smax, u, kEpiThreads, mx)) {
+            voted_out = true;
+            break;
+          }
+          sb = b_scale_for(mx);
+          if (c0 < N) {
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+              if (mt >= MT || mt * 128 + quarter * 32 >= M) continue;  // warp-uniform: the loads are collective
+              const int m = mt * 128 + quarter * 32 + lane;
+              const uint32_t dc0 = lane_base + (uint32_t)((mt * 2 + 0) * BN);
+#pragma unroll
+              for (int p = 0; p < 2; ++p) {
+                uint32_t hb[8];
+                tmem_ld8(tmem + dc0 + (p ? kH : 0) + c0, hb);
+                tmem_wait_ld();
+                reg_after_wait(hb);
+                if (m < M)
+#pragma unroll
+                  for (int q = 0; q < 8; ++q)
+                    if (c0 + q < N) put_b16<BN>(b_hi, b_lo, (p ? kH : 0) + c0 + q, m, __uint_as_float(hb[q]), sb);
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        if (!last) {
+          fence_proxy_async_smem();
+          mbar_arrive(bready);
+        }
+      }
+      // a failed vote stops all epilogue threads together; a failed wait in the last term is
+      // carried into the next walker's first vote
+      if (voted_out) break;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+}
+
+template <int BN>
+cudaError_t launch_chain16(const Chain16Maps& maps, float e_scale, float v_scale, const double2* phi_in,
+                           double2* phi_out, int W, int M, int N, int nmax, unsigned* status, cudaStream_t st) {
+  const size_t smem = 1024 + 2 * (size_t)kKB * BN * 128 + kStages * kStageBytes + 256;
+  auto kern = orbital_chain16_kernel<BN>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  const int grid = W < sms ? W : sms;
+  kern<<<grid, Chain16Roles<BN>::kThreads, smem, st>>>(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status);
+  note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+bool orbital_chain16_fits(int M, int N) { return M >= 1 && M <= kMaxM && N >= 1 && N <= 32; }
+
+// One launch for the whole mixed orbital update of one spin block (see the file comment).
+// e_hi/e_lo: (E - I) x e_scale (M, f16_ld(M)) binary16; v_*: VHS planes x v_scale (W, M, f16_ld(M)).
+cudaError_t mixed_orbital_chain16(const void* e_hi, const void* e_lo, float e_scale, const void* v_re_hi,
+                                  const void* v_re_lo, const void* v_im_hi, const void* v_im_lo, float v_scale,
+                                  const double2* phi_in, double2* phi_out, int W, int M, int N, int nmax,
+                                  unsigned* status, cudaStream_t st) {
+  if (!orbital_chain16_fits(M, N) || nmax < 1 || phi_in == phi_out || W <= 0 || !(e_scale > 0.0f) ||
+      !(v_scale > 0.0f))
+    return cudaErrorInvalidValue;
+  const int ld = f16_ld(M);
+  Chain16Maps maps;
+  memset(&maps, 0, sizeof(maps));
+  cudaError_t e;
+  if ((e = make_map_f16(&maps.e_hi, e_hi, M, M, ld, 128)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.e_lo, e_lo, M, M, ld, 128)) != cudaSuccess) return e;
+  const void* planes[4] = {v_re_hi, v_im_hi, v_re_lo, v_im_lo};
+  for (int i = 0; i < 4; ++i)
+    if ((e = make_map_f16_batched(&maps.v[i], planes[i], W, M, M, ld, 128)) != cudaSuccess) return e;
+  if (2 * N <= 32) return launch_chain16<32>(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
+  return launch_chain16<64>(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
+}
+
+}  // namespace umma
+}  // namespace ipie_b200

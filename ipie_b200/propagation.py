@@ -21,7 +21,7 @@ import numpy as np
 import scipy.linalg
 import torch
 
-from ._lib import call, ptr, stream
+from ._lib import call, lib, ptr, stream
 from .trial import force_bias_into, greens_function_into, overlap_into
 
 C128 = torch.complex128
@@ -97,16 +97,22 @@ class Workspace:
         self.xi_copied = torch.cuda.Event() if torch.cuda.is_available() else None
         self.dev = dev
 
-    def add_mixed(self):
-        """fp32 buffers of the mixed form."""
+    def add_mixed(self, chain16):
+        """Buffers of the mixed form; ``chain16``: the orbital update runs as the FP16 chain
+        (binary16 VHS planes), otherwise as TF32 products (fp32 planes and work)."""
         W, M, X, N = self.W, self.M, self.X, max(self.na, self.nb)
-        f32, dev = torch.float32, self.dev
+        f32, f16, dev = torch.float32, torch.float16, self.dev
         self.gwork = torch.empty(2 * W * 2 * 32 * M, dtype=f32, device=dev)
         Xp = (X + 7) // 8 * 8  # binary16 rows padded to 16 bytes
-        self.xs_hi = torch.empty(W, 2, Xp, dtype=torch.float16, device=dev)
-        self.xs_lo = torch.empty(W, 2, Xp, dtype=torch.float16, device=dev)
-        self.v_planar = [torch.empty(W, M, M, dtype=f32, device=dev) for _ in range(4)]  # re_hi, re_lo, im_hi, im_lo
-        self.orb_work = torch.empty(4 * W * 2 * N * M, dtype=f32, device=dev)
+        self.xs_hi = torch.empty(W, 2, Xp, dtype=f16, device=dev)
+        self.xs_lo = torch.empty(W, 2, Xp, dtype=f16, device=dev)
+        if chain16:
+            Mp = (M + 7) // 8 * 8
+            self.v_planar = [torch.empty(W, M, Mp, dtype=f16, device=dev) for _ in range(4)]  # re_hi, re_lo, im_hi, im_lo
+            self.orb_work = torch.empty(0, dtype=f32, device=dev)
+        else:
+            self.v_planar = [torch.empty(W, M, M, dtype=f32, device=dev) for _ in range(4)]
+            self.orb_work = torch.empty(4 * W * 2 * N * M, dtype=f32, device=dev)
 
 
 class PhaselessGeneric:
@@ -162,12 +168,13 @@ class PhaselessGeneric:
         if ws is None or (ws.W, ws.M, ws.na, ws.nb, ws.X) != (W, M, walkers.nup, walkers.ndown, X):
             self.ws = Workspace(W, M, walkers.nup, walkers.ndown, X, walkers.device)
             if self.precision == "mixed":
-                self.ws.add_mixed()
+                self.ws.add_mixed(self.chain16)
         return self.ws
 
     def _mixed_setup(self, hamiltonian, trial):
-        """TF32 operands of the mixed form, prepared once: packed Cholesky hi/lo,
-        half-rotated Cholesky hi/lo (padded), expH1 - I hi/lo."""
+        """Operands of the mixed form, prepared once: packed Cholesky FP16 hi/lo, half-rotated
+        Cholesky FP16 hi/lo (padded), expH1 - I as FP16 hi/lo (the FP16 orbital chain, which
+        takes blocks of M <= 256 and N <= 32) and as TF32 hi/lo (the per-term products)."""
         M, X = hamiltonian.nbasis, hamiltonian.nchol
         if M % 4 or X % 4 or self.expH1_complex:
             raise NotImplementedError("the mixed form needs nbasis and nchol multiples of 4 and a real expH1")
@@ -194,6 +201,24 @@ class PhaselessGeneric:
         self.lde = M
         # the one-body factor enters the mixed orbital update as E - I (the identity is added in FP64)
         e = torch.from_numpy(np.ascontiguousarray(self.expH1.real - np.eye(M)[None])).to(dev)
+        self.chain16 = all(lib().ipie_b200_orbital_chain16_fits(M, n) == 1
+                           for n in (trial.nalpha, trial.nbeta) if n > 0)
+        if self.chain16:
+            # binary16 operands of the orbital chain, rows padded to 8 halves: E - I with one
+            # power-of-two scale, and the scale of the VHS planes from a bound on their entries,
+            # |V| <= sqrt(dt) max_p sum_x |L_px| max|x_shifted| with |x_shifted| < 9 + the force-
+            # bias cap (the normal draws stay below 9), so the planes never reach 2^15
+            Mp = (M + 7) // 8 * 8
+            ep = torch.zeros(2, M, Mp, dtype=torch.float64, device=dev)
+            ep[:, :, :M] = e
+            emax = float(e.abs().max().item())
+            self.e_scale = 2.0 ** (14 - math.frexp(emax)[1]) if emax > 0 else 1.0
+            self.e16_hi = torch.empty(2, M, Mp, dtype=torch.float16, device=dev)
+            self.e16_lo = torch.empty(2, M, Mp, dtype=torch.float16, device=dev)
+            call("ipie_b200_split_f16", ptr(ep), ptr(self.e16_hi), ptr(self.e16_lo), ep.numel(), self.e_scale, stream())
+            l1 = float(hamiltonian.chol_packed.abs().sum(1).max().item())
+            vbound = self.sqrt_dt * l1 * (9.0 + float(self.fbbound))
+            self.v_scale = 2.0 ** (14 - math.frexp(vbound)[1]) if vbound > 0 else 1.0
         self.e_hi = torch.empty(2, M, M, dtype=f32, device=dev)
         self.e_lo = torch.empty(2, M, M, dtype=f32, device=dev)
         call("ipie_b200_split_tf32", ptr(e), ptr(self.e_hi), ptr(self.e_lo), e.numel(), stream())
@@ -366,7 +391,8 @@ class PhaselessGeneric:
         v = ws.v_planar
         call("ipie_b200_construct_vhs_mixed", ptr(self.cp_hi), ptr(self.cp_lo), ptr(hamiltonian.sym_idx_i),
              ptr(hamiltonian.sym_idx_j), M, X, ptr(ws.xs_hi), ptr(ws.xs_lo), W, self.sqrt_dt, self.cp_scale,
-             ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]), ptr(walkers.status), stream())
+             int(self.chain16), self.v_scale if self.chain16 else 0.0, ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]),
+             ptr(walkers.status), stream())
         self.timer.stop("vhs")
         self.timer.start("orbitals")
         for s_, (phi_name, tmp_name, n) in enumerate((("phia", "phia_tmp", walkers.nup),
@@ -374,9 +400,14 @@ class PhaselessGeneric:
             if n == 0 or (s_ == 1 and walkers.spin_alias):
                 continue
             phi, tmp = getattr(walkers, phi_name), getattr(ws, tmp_name)
-            call("ipie_b200_propagate_orbitals_mixed", ptr(self.e_hi[s_]), ptr(self.e_lo[s_]), self.lde, ptr(v[0]),
-                 ptr(v[1]), ptr(v[2]), ptr(v[3]), ptr(phi), ptr(tmp), ptr(ws.orb_work), W, M, n, self.exp_nmax,
-                 ptr(walkers.status), stream())
+            if self.chain16:
+                call("ipie_b200_propagate_orbitals_mixed16", ptr(self.e16_hi[s_]), ptr(self.e16_lo[s_]), self.e_scale,
+                     ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]), self.v_scale, ptr(phi), ptr(tmp), W, M, n,
+                     self.exp_nmax, ptr(walkers.status), stream())
+            else:
+                call("ipie_b200_propagate_orbitals_mixed", ptr(self.e_hi[s_]), ptr(self.e_lo[s_]), self.lde,
+                     ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]), ptr(phi), ptr(tmp), ptr(ws.orb_work), W, M, n,
+                     self.exp_nmax, ptr(walkers.status), stream())
             setattr(walkers, phi_name, tmp)
             setattr(ws, tmp_name, phi)
         walkers.sync_alias()

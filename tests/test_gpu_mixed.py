@@ -1,7 +1,7 @@
-"""The mixed-precision form (TF32 tensor cores) against the FP64 form.
+"""The mixed-precision form (FP16 and TF32 tensor cores) against the FP64 form.
 
 Tolerances follow the arithmetic: the force bias, VHS, orbital and exchange
-products are 3-pass TF32 (~2^-22 relative per product); walker weights and
+products are 3-pass FP16 or TF32 (~2^-22 relative per product); walker weights and
 overlaps after a few steps stay within 1e-5 of the FP64 path; the local energy,
 expanded around the trial, within 1e-6 (exact at the trial itself).
 """
@@ -64,11 +64,20 @@ def test_mixed_vhs_3pass():
     call("ipie_b200_field_shift_mixed", ptr(vb), ptr(xi), ptr(pm.mf_shift_dev), W, s.nchol, pm.sqrt_dt, 1.0, ptr(xs),
          ptr(ws.xs_hi), ptr(ws.xs_lo), ptr(ws.cmf), ptr(ws.cfb), stream())
     ref = prop.construct_VHS(ham, xs)
+    M = s.nbasis
+    # binary16 planes x v_scale (the FP16 orbital chain's operands), then fp32 TF32 planes
+    assert pm.chain16
     v = ws.v_planar
     call("ipie_b200_construct_vhs_mixed", ptr(pm.cp_hi), ptr(pm.cp_lo), ptr(ham.sym_idx_i), ptr(ham.sym_idx_j),
-         s.nbasis, s.nchol, ptr(ws.xs_hi), ptr(ws.xs_lo), W, pm.sqrt_dt, pm.cp_scale, ptr(v[0]), ptr(v[1]), ptr(v[2]),
-         ptr(v[3]), ptr(walkers.status), stream())
-    got = (v[0].double() + v[1].double()) + 1j * (v[2].double() + v[3].double())
+         M, s.nchol, ptr(ws.xs_hi), ptr(ws.xs_lo), W, pm.sqrt_dt, pm.cp_scale, 1, pm.v_scale, ptr(v[0]), ptr(v[1]),
+         ptr(v[2]), ptr(v[3]), ptr(walkers.status), stream())
+    got = ((v[0].double() + v[1].double()) + 1j * (v[2].double() + v[3].double()))[:, :, :M] / pm.v_scale
+    assert rel(got, ref) < 1e-5
+    v32 = [torch.empty(W, M, M, dtype=torch.float32, device="cuda") for _ in range(4)]
+    call("ipie_b200_construct_vhs_mixed", ptr(pm.cp_hi), ptr(pm.cp_lo), ptr(ham.sym_idx_i), ptr(ham.sym_idx_j),
+         M, s.nchol, ptr(ws.xs_hi), ptr(ws.xs_lo), W, pm.sqrt_dt, pm.cp_scale, 0, 0.0, ptr(v32[0]), ptr(v32[1]),
+         ptr(v32[2]), ptr(v32[3]), ptr(walkers.status), stream())
+    got = (v32[0].double() + v32[1].double()) + 1j * (v32[2].double() + v32[3].double())
     assert rel(got, ref) < 1e-5
     walkers.check_status()
 
@@ -101,6 +110,54 @@ def test_mixed_orbital_update_3pass(M, N, W):
     work = torch.empty(4 * W * 2 * N * M, dtype=torch.float32, device="cuda")
     call("ipie_b200_propagate_orbitals_mixed", ptr(pm.e_hi[0]), ptr(pm.e_lo[0]), pm.lde, ptr(planes[0]), ptr(planes[1]),
          ptr(planes[2]), ptr(planes[3]), ptr(pa_d), ptr(out), ptr(work), W, M, N, 6, ptr(walkers.status), stream())
+    assert rel(out, ref) < 1e-5
+    walkers.check_status()
+
+
+def _split16_padded(x, scale):
+    """(W, M, M) real -> binary16 head/remainder (W, M, Mp) of x * scale, Mp = M rounded up to 8."""
+    from ipie_b200._lib import call, ptr, stream
+
+    W, M, _ = x.shape
+    Mp = (M + 7) // 8 * 8
+    xp = torch.zeros(W, M, Mp, dtype=torch.float64, device="cuda")
+    xp[:, :, :M] = x
+    hi = torch.empty(W, M, Mp, dtype=torch.float16, device="cuda")
+    lo = torch.empty_like(hi)
+    call("ipie_b200_split_f16", ptr(xp), ptr(hi), ptr(lo), xp.numel(), scale, stream())
+    return hi, lo
+
+
+@pytest.mark.parametrize("M,N,W,vmag", [(64, 8, 6, 1.0), (200, 32, 6, 1.0), (108, 15, 6, 1.0), (128, 16, 5, 1.0),
+                                        (64, 4, 300, 1.0), (200, 13, 5, 1.0), (256, 24, 4, 1.0), (76, 10, 4, 1.0),
+                                        (200, 32, 4, 1e-3), (200, 32, 4, 30.0)])
+def test_mixed_orbital_chain16(M, N, W, vmag):
+    """The FP16 orbital chain (one or two 128-row tiles, orbital groups partly or wholly past N,
+    M not a multiple of 8, W = 300 > SM count for the persistent walker loop) against the oracle's
+    one-body, Taylor-6, one-body; vmag scales the VHS by 1e-3 and 30 so that the Taylor terms
+    span many binades (each term's B carries its own scale)."""
+    import math
+
+    from ipie_b200 import synthetic
+    from ipie_b200._lib import call, ptr, stream
+
+    s = synthetic.generate(M, (N, N), 2 * M, decay=30.0, seed=9, uhf=True, chol_scale="stable")
+    ham, trial, walkers, prop, pm = _mixed_objects(s, W)
+    assert pm.chain16
+    pa, _ = _walker_pert(s, W, 4)
+    rng = np.random.default_rng(2)
+    xs = dev(rng.normal(size=(s.nchol, W)) + 0.2j * rng.normal(size=(s.nchol, W)))
+    vhs = prop.construct_VHS(ham, xs) * vmag
+    pa_d = dev(pa)
+    E = prop.expH1[0].real
+    ref = np.einsum("pq,wqn->wpn", E, O.apply_exponential(np.einsum("pq,wqn->wpn", E, pa), vhs.cpu().numpy(), 6))
+    vmax = max(vhs.real.abs().max().item(), vhs.imag.abs().max().item())
+    vs = 2.0 ** (14 - math.frexp(vmax)[1])
+    vr = _split16_padded(vhs.real.contiguous(), vs)
+    vi = _split16_padded(vhs.imag.contiguous(), vs)
+    out = torch.empty_like(pa_d)
+    call("ipie_b200_propagate_orbitals_mixed16", ptr(pm.e16_hi[0]), ptr(pm.e16_lo[0]), pm.e_scale, ptr(vr[0]),
+         ptr(vr[1]), ptr(vi[0]), ptr(vi[1]), vs, ptr(pa_d), ptr(out), W, M, N, 6, ptr(walkers.status), stream())
     assert rel(out, ref) < 1e-5
     walkers.check_status()
 
