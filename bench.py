@@ -437,9 +437,9 @@ def run_ours(args):
     phases = r["phases"]
     dom = max((k for k in phases if k in fl), key=lambda k: phases[k][1])
     n_launch, tot_ms = phases[dom]
-    # tensor pipe of each mixed-form phase: every product is a 3-pass hi/lo product, FP16 operands
-    # (kind::f16, same tensor rate as bf16) for the force bias and VHS, TF32 for the orbital chain
-    mixed_pipe = {"force_bias": "f16", "vhs": "f16", "orbitals": "tf32"}
+    # tensor pipe of each mixed-form phase: every product is a 3-pass hi/lo product on FP16
+    # operands (kind::f16, same tensor rate as bf16) -- the force bias, VHS and the orbital chain
+    mixed_pipe = {"force_bias": "f16", "vhs": "f16", "orbitals": "f16"}
     pipe_peak = {"f16": (peaks["bf16_tflops"], "f16 (3 passes)",
                          f"{peaks['source']} cuBLAS bf16 8192^3 on B200 (MEASURED_PEAKS.json; fp16 runs at the bf16 rate)"),
                  "tf32": (peaks["tf32_tflops"], "tf32 (3 passes)", "measured cuBLAS TF32 8192^3 on B200 (tcgen05)")}
@@ -534,7 +534,7 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f16+tf32+f64" if head == "mixed" else "f64",
+            "dtype": "f16+f64" if head == "mixed" else "f64",
             "data": "synthetic",
             "config": line_config(wl, W, world, head),
             "forms": forms_out,

@@ -1,15 +1,18 @@
 // Green's function and overlap for spin blocks of N <= 32 electrons, one
-// 128-thread CTA per walker with a small shared-memory footprint (~34 KB) so
-// that several walkers share an SM:
+// 128-thread CTA per walker (~47 KB of shared memory, three walkers per SM):
 //
 //   O = phi^T psi*  (N x N): phi and psi* stream through shared memory in
 //       16-row chunks; each thread accumulates a 2 x 4 block of O in registers;
-//   P O = L U: partial pivoting on |.| in shared memory (warp 0 picks the
-//       pivot, all threads update);  log|det O| = sum log|U_kk|,
-//       phase = (-1)^swaps prod U_kk / |U_kk|;
-//   Ghalf[:, m] = O^{-1} phi[m, :]^T: thread m loads its row of phi in pivot
-//       order straight into registers and runs both triangular solves there
-//       (L and U are read as shared-memory broadcasts), then stores column m.
+//   X = (P O)^-1 by Gauss-Jordan elimination in place in shared memory with
+//       partial pivoting on |.| (warp 0 picks the pivot, all threads update) --
+//       the pivots are those of the LU factorisation, so
+//       log|det O| = sum log|pivot_k|, phase = (-1)^swaps prod pivot_k / |pivot_k|
+//       (one pivot per lane of warp 0, reduced with shuffles);
+//   Ghalf[i, m] = sum_r X[i, r] phi[m, perm(r)] (= (O^-1 phi^T)[i, m]): a
+//       register-tiled product -- warp w takes rows 8w..8w+7, lane l the
+//       columns l + 32q (q < 3, so 96 columns per pass), phi staged in shared
+//       memory 4 permuted columns at a time, transposed -- instead of one
+//       latency-bound pair of triangular solves per column.
 // ovlp_w = prod_s phase_s * exp(sum_s log|det O_s| - log_shift_w).
 // Same contract as gf_overlap_kernel (walkers.cu), which keeps N > 32.
 #include "common.cuh"
@@ -20,18 +23,23 @@ namespace ipie_b200 {
 namespace {
 
 constexpr int kThreads = 128;
-constexpr int kChunk = 16;  // rows of phi / psi* per shared-memory chunk
+constexpr int kChunk = 16;  // rows of phi / psi* per shared-memory chunk of the O product
 constexpr int kNP = 33;     // row stride of O in shared memory
+constexpr int kRC = 4;      // permuted columns of phi per staged chunk of the Ghalf product
+constexpr int kMQ = 3;      // columns of Ghalf per lane and pass (96 per pass)
+constexpr int kMS = 32 * kMQ + 1;  // row stride of the staged phi^T chunk (odd in 16-byte units)
+static_assert(kRC * kMS <= 2 * kChunk * 32, "the staged phi^T chunk reuses the O product's staging buffers");
 
-struct SpinLU32 {
+struct SpinDet32 {
   double logabs;
   double2 phase;
 };
 
-// Factor one spin block; leaves L\U (unit L) in sO, the row order in sPerm, 1/U_kk in sInv.
-__device__ SpinLU32 factor_block(const double2* __restrict__ phi, const double2* __restrict__ psic, int M, int N,
-                                 double2 (*sO)[kNP], double2 (*sPhi)[32], double2 (*sPsi)[32], int* sPerm,
-                                 double2* sInv, double2* red, unsigned* status) {
+// O = phi^T psi* for one spin block into sO; then its inverse (of the row-permuted O) in place,
+// the row order in sPerm and log|det|, phase from the pivots.
+__device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2* __restrict__ psic, int M, int N,
+                                  double2 (*sO)[kNP], double2 (*sPhi)[32], double2 (*sPsi)[32], int* sPerm,
+                                  double2* sPiv, double2* red, unsigned* status) {
   const int tid = threadIdx.x;
   // ---- O = phi^T psi*: thread (ti, tj) owns rows {ti, ti+16} x columns {tj + 8q}
   const int ti = tid >> 3, tj = tid & 7;
@@ -69,7 +77,8 @@ __device__ SpinLU32 factor_block(const double2* __restrict__ phi, const double2*
     for (int q = 0; q < 4; ++q) sO[ti + 16 * a][tj + 8 * q] = acc[a][q];
   if (tid < 32) sPerm[tid] = tid;
   __syncthreads();
-  // ---- LU with partial pivoting
+  // ---- Gauss-Jordan with partial pivoting, in place: after step k row k holds the k-th row of
+  // the reduced inverse and column k the multipliers
   int swaps = 0;
   for (int k = 0; k < N; ++k) {
     if (tid < 32) {
@@ -99,100 +108,131 @@ __device__ SpinLU32 factor_block(const double2* __restrict__ phi, const double2*
         sPerm[k] = sPerm[bi];
         sPerm[bi] = t;
       }
-      if (tid == 0) red[4] = make_double2((double)bi, 0.0);
+      if (bi != k) ++swaps;  // warp-uniform: every lane of warp 0 counts
       __syncwarp();
       if (tid == 0) {
         const double2 pv = sO[k][k];
         if (pv.x == 0.0 && pv.y == 0.0) flag(status, STATUS_SINGULAR);
-        sInv[k] = cdiv(make_double2(1.0, 0.0), pv);
+        sPiv[k] = pv;
+        red[5] = cdiv(make_double2(1.0, 0.0), pv);
       }
     }
     __syncthreads();
-    if ((int)red[4].x != k) ++swaps;
-    const double2 ip = sInv[k];
-    const int rem = N - k - 1;
-    // column k of L, then the trailing update (each thread recomputes its multiplier)
-    for (int e = tid; e < rem * rem; e += kThreads) {
-      const int r = k + 1 + e / rem, c = k + 1 + e % rem;
-      const double2 l = cmul(sO[r][k], ip);
-      sO[r][c] = csub(sO[r][c], cmul(l, sO[k][c]));
+    const double2 inv = red[5];
+    // a_ij -= a_ik a_kj / a_kk for i, j != k (row k and column k are only read here)
+    for (int e = tid; e < N * N; e += kThreads) {
+      const int i = e / N, j = e - (e / N) * N;
+      if (i != k && j != k) sO[i][j] = csub(sO[i][j], cmul(cmul(sO[i][k], inv), sO[k][j]));
     }
     __syncthreads();
-    for (int r = k + 1 + tid; r < N; r += kThreads) sO[r][k] = cmul(sO[r][k], ip);
+    // row k scaled by 1/a_kk, column k by -1/a_kk, a_kk <- 1/a_kk
+    for (int e = tid; e < 2 * N; e += kThreads) {
+      const int idx = e >> 1;
+      if (idx == k) {
+        if (e & 1) sO[k][k] = inv;
+      } else if (e & 1) {
+        sO[k][idx] = cmul(sO[k][idx], inv);
+      } else {
+        const double2 v = cmul(sO[idx][k], inv);
+        sO[idx][k] = make_double2(-v.x, -v.y);
+      }
+    }
     __syncthreads();
   }
-  SpinLU32 out;
-  if (tid == 0) {
+  // ---- log|det| and phase from the pivots, one per lane of warp 0
+  if (tid < 32) {
     double la = 0.0;
-    double2 ph = make_double2((swaps & 1) ? -1.0 : 1.0, 0.0);
-    for (int k = 0; k < N; ++k) {
-      const double2 u = sO[k][k];
+    double2 ph = make_double2(1.0, 0.0);
+    if (tid < N) {
+      const double2 u = sPiv[tid];
       const double a = cabs_(u);
-      la += log(a);
-      ph = cmul(ph, make_double2(u.x / a, u.y / a));
+      la = log(a);
+      ph = make_double2(u.x / a, u.y / a);
     }
-    red[0] = make_double2(la, 0.0);
-    red[1] = ph;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      la += __shfl_xor_sync(0xffffffffu, la, o);
+      const double2 q = make_double2(__shfl_xor_sync(0xffffffffu, ph.x, o), __shfl_xor_sync(0xffffffffu, ph.y, o));
+      ph = cmul(ph, q);
+    }
+    if (tid == 0) {
+      red[0] = make_double2(la, 0.0);
+      red[1] = (swaps & 1) ? make_double2(-ph.x, -ph.y) : ph;
+    }
   }
   __syncthreads();
+  SpinDet32 out;
   out.logabs = red[0].x;
   out.phase = red[1];
   return out;
 }
 
-// Ghalf (N, M) of one spin block from the factors in shared memory.
-__device__ void solve_block(const double2* __restrict__ phi, int M, int N, double2 (*sO)[kNP], const int* sPerm,
-                            const double2* sInv, double2* __restrict__ ghalf, double2* __restrict__ ghalf2) {
-  for (int m = threadIdx.x; m < M; m += kThreads) {
-    double2 y[32];
-    const double2* row = phi + (size_t)m * N;
+// Ghalf (N, M) of one spin block from X = (P O)^-1 in sO: Ghalf[i, m] = sum_r X[i, r] phi[m, perm(r)].
+__device__ void ghalf_block(const double2* __restrict__ phi, int M, int N, double2 (*sO)[kNP], const int* sPerm,
+                            double2* sPT, double2* __restrict__ ghalf, double2* __restrict__ ghalf2) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int i0 = warp * 8;  // this warp's rows
+  for (int m0 = 0; m0 < M; m0 += 32 * kMQ) {
+    double2 acc[8][kMQ];
 #pragma unroll
-    for (int i = 0; i < 32; ++i) y[i] = i < N ? row[sPerm[i]] : make_double2(0.0, 0.0);
-    // L y = P b (unit lower); square loops with compile-time bounds keep y in registers
+    for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int i = 1; i < 32; ++i) {
-      if (i < N) {
-        double2 s = y[i];
+      for (int q = 0; q < kMQ; ++q) acc[a][q] = make_double2(0.0, 0.0);
+    for (int r0 = 0; r0 < N; r0 += kRC) {
+      __syncthreads();
+      // stage phi[m0 + ml][perm(r0 + rr)] as sPT[rr][ml]: consecutive threads take consecutive rr
+      for (int e = tid; e < kRC * 32 * kMQ; e += kThreads) {
+        const int rr = e % kRC, ml = e / kRC;
+        const int r = r0 + rr, m = m0 + ml;
+        sPT[rr * kMS + ml] = (r < N && m < M) ? phi[(size_t)m * N + sPerm[r]] : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-          if (j < i) s = csub(s, cmul(sO[i][j], y[j]));
-        y[i] = s;
+      for (int rr = 0; rr < kRC; ++rr) {
+        double2 x[8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) x[a] = sO[i0 + a][min(r0 + rr, 31)];
+        if (r0 + rr >= N) continue;  // uniform
+#pragma unroll
+        for (int q = 0; q < kMQ; ++q) {
+          const double2 b = sPT[rr * kMS + lane + 32 * q];
+#pragma unroll
+          for (int a = 0; a < 8; ++a) {
+            acc[a][q].x += x[a].x * b.x - x[a].y * b.y;
+            acc[a][q].y += x[a].x * b.y + x[a].y * b.x;
+          }
+        }
       }
     }
-    // U x = y
 #pragma unroll
-    for (int ii = 0; ii < 32; ++ii) {
-      const int i = 31 - ii;
-      if (i < N) {
-        double2 s = y[i];
+    for (int a = 0; a < 8; ++a) {
+      const int i = i0 + a;
+      if (i >= N) break;
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-          if (j > i && j < N) s = csub(s, cmul(sO[i][j], y[j]));
-        y[i] = cmul(s, sInv[i]);
+      for (int q = 0; q < kMQ; ++q) {
+        const int m = m0 + lane + 32 * q;
+        if (m < M) {
+          ghalf[(size_t)i * M + m] = acc[a][q];
+          if (ghalf2 != nullptr) ghalf2[(size_t)i * M + m] = acc[a][q];
+        }
       }
     }
-#pragma unroll
-    for (int i = 0; i < 32; ++i)
-      if (i < N) {
-        ghalf[(size_t)i * M + m] = y[i];
-        if (ghalf2 != nullptr) ghalf2[(size_t)i * M + m] = y[i];
-      }
   }
 }
 
 template <bool WITH_GHALF>
-__global__ void __launch_bounds__(kThreads) gf_lu32_kernel(const double2* __restrict__ phia,
-                                                           const double2* __restrict__ phib, int M, int na, int nb,
-                                                           const double2* __restrict__ psia_c,
-                                                           const double2* __restrict__ psib_c,
-                                                           const double* __restrict__ log_shift,
-                                                           double2* __restrict__ ghalfa, double2* __restrict__ ghalfb,
-                                                           double2* __restrict__ ovlp, double2* __restrict__ logdet,
-                                                           unsigned* status) {
+__global__ void __launch_bounds__(kThreads, 3) gf_lu32_kernel(const double2* __restrict__ phia,
+                                                              const double2* __restrict__ phib, int M, int na,
+                                                              int nb, const double2* __restrict__ psia_c,
+                                                              const double2* __restrict__ psib_c,
+                                                              const double* __restrict__ log_shift,
+                                                              double2* __restrict__ ghalfa,
+                                                              double2* __restrict__ ghalfb,
+                                                              double2* __restrict__ ovlp, double2* __restrict__ logdet,
+                                                              unsigned* status) {
   __shared__ double2 sO[32][kNP];
-  __shared__ double2 sPhi[kChunk][32];
-  __shared__ double2 sPsi[kChunk][32];
-  __shared__ double2 sInv[32];
+  __shared__ double2 sStage[2 * kChunk * 32];  // phi / psi* chunks of O, then the staged phi^T chunks
+  __shared__ double2 sPiv[32];
   __shared__ double2 red[8];
   __shared__ int sPerm[32];
   const int w = blockIdx.x;
@@ -210,18 +250,20 @@ __global__ void __launch_bounds__(kThreads) gf_lu32_kernel(const double2* __rest
       continue;
     }
     const double2* phi = (s == 0 ? phia : phib) + (size_t)w * M * N;
-    const SpinLU32 lu = factor_block(phi, s == 0 ? psia_c : psib_c, M, N, sO, sPhi, sPsi, sPerm, sInv, red, status);
-    logsum += lu.logabs;
-    phase = cmul(phase, lu.phase);
+    auto sPhi = reinterpret_cast<double2(*)[32]>(sStage);
+    auto sPsi = reinterpret_cast<double2(*)[32]>(sStage + kChunk * 32);
+    const SpinDet32 d = invert_block(phi, s == 0 ? psia_c : psib_c, M, N, sO, sPhi, sPsi, sPerm, sPiv, red, status);
+    logsum += d.logabs;
+    phase = cmul(phase, d.phase);
     if (threadIdx.x == 0) {
-      red[2] = make_double2(lu.logabs, 0.0);
-      red[3] = lu.phase;
-      if (logdet != nullptr) logdet[(size_t)w * 2 + s] = make_double2(lu.logabs, atan2(lu.phase.y, lu.phase.x));
+      red[2] = make_double2(d.logabs, 0.0);
+      red[3] = d.phase;
+      if (logdet != nullptr) logdet[(size_t)w * 2 + s] = make_double2(d.logabs, atan2(d.phase.y, d.phase.x));
     }
     if (WITH_GHALF) {
       double2* g1 = (s == 0 ? ghalfa : ghalfb) + (size_t)w * N * M;
       double2* g2 = (s == 0 && alias && nb > 0 && ghalfb != ghalfa) ? ghalfb + (size_t)w * N * M : nullptr;
-      solve_block(phi, M, N, sO, sPerm, sInv, g1, g2);
+      ghalf_block(phi, M, N, sO, sPerm, sStage, g1, g2);
     }
     __syncthreads();
   }
