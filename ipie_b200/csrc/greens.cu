@@ -78,63 +78,72 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
   if (tid < 32) sPerm[tid] = tid;
   __syncthreads();
   // ---- Gauss-Jordan with partial pivoting, in place: after step k row k holds the k-th row of
-  // the reduced inverse and column k the multipliers
+  // the reduced inverse and column k the multipliers.  Two barriers per step: warp 0 finishes
+  // the previous step (row k-1 x 1/p, column k-1 x -1/p), picks and swaps the pivot row; then
+  // all threads update the rest (thread: column tid % 32, rows tid / 32 + 4r).
   int swaps = 0;
-  for (int k = 0; k < N; ++k) {
+  const int uj = tid & 31, ui = tid >> 5;
+  for (int k = 0; k <= N; ++k) {
     if (tid < 32) {
-      double best = -1.0;
-      int bi = k;
-      if (tid >= k && tid < N) {
-        best = cabs2(sO[tid][k]);
-        bi = tid;
+      if (k > 0) {
+        const int kp = k - 1;
+        const double2 pinv = red[5];
+        if (tid < N && tid != kp) {
+          sO[kp][tid] = cmul(sO[kp][tid], pinv);
+          const double2 v = cmul(sO[tid][kp], pinv);
+          sO[tid][kp] = make_double2(-v.x, -v.y);
+        }
+        __syncwarp();
+        if (tid == 0) sO[kp][kp] = pinv;
+        __syncwarp();
       }
+      if (k < N) {
+        double best = -1.0;
+        int bi = k;
+        if (tid >= k && tid < N) {
+          best = cabs2(sO[tid][k]);
+          bi = tid;
+        }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) {
+            best = ob;
+            bi = oi;
+          }
+        }
+        // swap rows k and bi (all N columns) and the row order
+        if (bi != k && tid < N) {
+          const double2 t = sO[k][tid];
+          sO[k][tid] = sO[bi][tid];
+          sO[bi][tid] = t;
+        }
+        if (bi != k && tid == 0) {
+          const int t = sPerm[k];
+          sPerm[k] = sPerm[bi];
+          sPerm[bi] = t;
+        }
+        if (bi != k) ++swaps;  // warp-uniform: every lane of warp 0 counts
+        __syncwarp();
+        if (tid == 0) {
+          const double2 pv = sO[k][k];
+          if (pv.x == 0.0 && pv.y == 0.0) flag(status, STATUS_SINGULAR);
+          sPiv[k] = pv;
+          red[5] = cdiv(make_double2(1.0, 0.0), pv);
         }
       }
-      // swap rows k and bi (all N columns) and the row order
-      if (bi != k && tid < N) {
-        const double2 t = sO[k][tid];
-        sO[k][tid] = sO[bi][tid];
-        sO[bi][tid] = t;
-      }
-      if (bi != k && tid == 0) {
-        const int t = sPerm[k];
-        sPerm[k] = sPerm[bi];
-        sPerm[bi] = t;
-      }
-      if (bi != k) ++swaps;  // warp-uniform: every lane of warp 0 counts
-      __syncwarp();
-      if (tid == 0) {
-        const double2 pv = sO[k][k];
-        if (pv.x == 0.0 && pv.y == 0.0) flag(status, STATUS_SINGULAR);
-        sPiv[k] = pv;
-        red[5] = cdiv(make_double2(1.0, 0.0), pv);
-      }
     }
     __syncthreads();
+    if (k == N) break;
+    // a_ij -= (a_ik / a_kk) a_kj for i, j != k (row k and column k are only read here)
     const double2 inv = red[5];
-    // a_ij -= a_ik a_kj / a_kk for i, j != k (row k and column k are only read here)
-    for (int e = tid; e < N * N; e += kThreads) {
-      const int i = e / N, j = e - (e / N) * N;
-      if (i != k && j != k) sO[i][j] = csub(sO[i][j], cmul(cmul(sO[i][k], inv), sO[k][j]));
-    }
-    __syncthreads();
-    // row k scaled by 1/a_kk, column k by -1/a_kk, a_kk <- 1/a_kk
-    for (int e = tid; e < 2 * N; e += kThreads) {
-      const int idx = e >> 1;
-      if (idx == k) {
-        if (e & 1) sO[k][k] = inv;
-      } else if (e & 1) {
-        sO[k][idx] = cmul(sO[k][idx], inv);
-      } else {
-        const double2 v = cmul(sO[idx][k], inv);
-        sO[idx][k] = make_double2(-v.x, -v.y);
+    if (uj < N && uj != k) {
+      const double2 akj = sO[k][uj];
+      for (int i = ui; i < N; i += 4) {
+        if (i == k) continue;
+        const double2 f = cmul(sO[i][k], inv);
+        sO[i][uj] = csub(sO[i][uj], cmul(f, akj));
       }
     }
     __syncthreads();

@@ -307,11 +307,53 @@ __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restr
   }
 }
 
+// The same shift without the (X, W) transposed copy: one warp per walker walks its row of
+// vbias / xi with coalesced loads, writes the binary16 split and reduces cmf, cfb with shuffles
+// (the mixed form, which needs no FP64 transposed fields; every SM gets walkers).
+__global__ void __launch_bounds__(256) field_shift_rows_kernel(const double2* __restrict__ vbias,
+                                                               const double* __restrict__ xi,
+                                                               const double2* __restrict__ mf, int W, int X,
+                                                               double sqrt_dt, double bound, double2* __restrict__ cmf,
+                                                               double2* __restrict__ cfb, __half* __restrict__ xs_hi,
+                                                               __half* __restrict__ xs_lo) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (w >= W) return;  // whole warps leave together
+  const int ldx = f16_ld(X);
+  double2 acc_mf = make_double2(0.0, 0.0), acc_fb = make_double2(0.0, 0.0);
+  for (int x = lane; x < X; x += 32) {
+    const double2 v = vbias[(size_t)w * X + x];
+    const double2 m = mf[x];
+    double2 xb = make_double2(-sqrt_dt * (-v.y - m.x), -sqrt_dt * (v.x - m.y));
+    const double a = cabs_(xb);
+    if (a > bound && a > 1e-13) xb = make_double2(xb.x / a, xb.y / a);
+    const double r = xi[(size_t)w * X + x];
+    const double2 xs = make_double2(r - xb.x, -xb.y);
+    if (xs_hi != nullptr) {
+      split_store_f16(xs_hi, xs_lo, ((size_t)w * 2) * ldx + x, xs.x);
+      split_store_f16(xs_hi, xs_lo, ((size_t)w * 2 + 1) * ldx + x, xs.y);
+    }
+    acc_mf = cadd(acc_mf, cmul(xs, m));
+    const double2 xb2 = cmul(xb, xb);
+    acc_fb = cadd(acc_fb, make_double2(r * xb.x - 0.5 * xb2.x, r * xb.y - 0.5 * xb2.y));
+  }
+  acc_mf = warp_sum2(acc_mf);
+  acc_fb = warp_sum2(acc_fb);
+  if (lane == 0) {
+    cmf[w] = cscale(acc_mf, -sqrt_dt);
+    cfb[w] = acc_fb;
+  }
+}
+
 cudaError_t launch_field_shift(const double2* vbias, const double* xi, const double2* mf, int W, int X, double sqrt_dt,
                                double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st,
                                void* xs_hi, void* xs_lo) {
-  field_shift_kernel<<<(W + 31) / 32, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, xshifted, cmf, cfb,
-                                                    static_cast<__half*>(xs_hi), static_cast<__half*>(xs_lo));
+  if (xshifted == nullptr)
+    field_shift_rows_kernel<<<(W + 7) / 8, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, cmf, cfb,
+                                                         static_cast<__half*>(xs_hi), static_cast<__half*>(xs_lo));
+  else
+    field_shift_kernel<<<(W + 31) / 32, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, xshifted, cmf, cfb,
+                                                      static_cast<__half*>(xs_hi), static_cast<__half*>(xs_lo));
   note_launch();
   return cudaGetLastError();
 }
