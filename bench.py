@@ -181,9 +181,9 @@ def barrier_max(value, world):
 # workload's walker count (the capture's traffic grows with the walkers it processes); the
 # capture and its command are summarised under profiles/.
 DRAM_TRAFFIC = {
-    # orbital chain at 512 walkers: 883.7 MB read + 114.5 MB written per launch
-    # (profiles/orbital_chain_gf_vhs_fb_c2_w512.md), x4 for 2048 walkers
-    ("c2_rhf_m200", "mixed", "orbitals"): 4 * (883.7e6 + 114.5e6),
+    # FP16 orbital chain at 512 walkers: 218.5 MB read + 35.4 MB written per launch
+    # (profiles/fp16_kernels_c2_w512.md), x4 for 2048 walkers (its traffic is per walker)
+    ("c2_rhf_m200", "mixed", "orbitals"): 4 * (218.5e6 + 35.4e6),
 }
 
 
