@@ -318,7 +318,12 @@ struct EpiVHSSplit {
 
 // VHS for the FP16 orbital chain: V x v_scale written to both triangles of four planar
 // (W, M, ld) binary16 arrays (re/im x head/remainder; ld = M rounded up to 8, the pad columns
-// are not written).
+// are not written).  A warp whose 32 pairs form a full 8 x 4 block strictly above the diagonal,
+// starting on a row and a column that are multiples of 4 (the packing puts such blocks first),
+// trades values by shuffles so that each lane writes one 8-byte
+// run per orientation and walker -- lane (r, c): plane c of row i0 + r, columns j0..j0+3, and
+// plane r % 4 of row j0 + c, columns i0 + 4 (r / 4) .. +3 -- instead of eight 2-byte stores;
+// other warps store pair by pair.
 template <int BN>
 struct EpiVHSF16 {
   __half *re_hi, *re_lo, *im_hi, *im_lo;
@@ -331,22 +336,65 @@ struct EpiVHSF16 {
     hi[i] = h;
     lo[i] = __float2half_rn(x - __half2float(h));
   }
+  __device__ __forceinline__ __half* plane(int k) const {
+    return k == 0 ? re_hi : k == 1 ? re_lo : k == 2 ? im_hi : im_lo;
+  }
+  // 16-bit plane k (0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo) out of the packed pairs a = (re_hi, re_lo), b = (im_hi, im_lo)
+  __device__ __forceinline__ static uint32_t pick(int k, uint32_t a, uint32_t b) {
+    const uint32_t x = k < 2 ? a : b;
+    return (k & 1) ? (x >> 16) : (x & 0xffffu);
+  }
   __device__ __forceinline__ void operator()(int, int p, int n0, const float* v, uint8_t*) const {
-    if (p >= P) return;
-    const int i = ii[p], j = jj[p];
+    const unsigned kFull = 0xffffffffu;
+    const int lane = threadIdx.x & 31, r = lane >> 2, c = lane & 3;
+    const bool live = p < P;
+    const int i = live ? ii[p] : 0, j = live ? jj[p] : 0;
+    const int i0 = __shfl_sync(kFull, i, 0), j0 = __shfl_sync(kFull, j, 0);
+    // the 8-byte runs need i0 and j0 on multiples of 4 (ld is a multiple of 8): blocks elsewhere
+    // (a diagonal tile's full rows can line up into one) take the pair-by-pair path
+    const bool block =
+        __all_sync(kFull, live && i == i0 + r && j == j0 + c && i0 + 7 < j0 && (i0 & 3) == 0 && (j0 & 3) == 0) != 0;
+    if (!block) {
+      if (!live) return;
+#pragma unroll
+      for (int q = 0; q < BN / 2; ++q) {
+        const int w = (n0 >> 1) + q;
+        if (w < W) {
+          const float vre = -f * v[2 * q + 1], vim = f * v[2 * q];
+          const size_t a = ((size_t)w * M + i) * ld + j, b = ((size_t)w * M + j) * ld + i;
+          put(re_hi, re_lo, a, vre);
+          put(im_hi, im_lo, a, vim);
+          if (i != j) {
+            put(re_hi, re_lo, b, vre);
+            put(im_hi, im_lo, b, vim);
+          }
+        }
+      }
+      return;
+    }
+    __half* dpl = plane(c);
+    __half* tpl = plane(r & 3);
+    const size_t doff = (size_t)(i0 + r) * ld + j0;                  // row i0 + r, columns j0 ..
+    const size_t toff = (size_t)(j0 + c) * ld + i0 + 4 * (r >> 2);  // row j0 + c, columns i0 + 4 (r / 4) ..
+    const size_t wstride = (size_t)M * ld;
+    const int dsrc = 4 * r, tsrc = 16 * (r >> 2) + c;
 #pragma unroll
     for (int q = 0; q < BN / 2; ++q) {
       const int w = (n0 >> 1) + q;
-      if (w < W) {
-        const float vre = -f * v[2 * q + 1], vim = f * v[2 * q];
-        const size_t a = ((size_t)w * M + i) * ld + j, b = ((size_t)w * M + j) * ld + i;
-        put(re_hi, re_lo, a, vre);
-        put(im_hi, im_lo, a, vim);
-        if (i != j) {
-          put(re_hi, re_lo, b, vre);
-          put(im_hi, im_lo, b, vim);
-        }
+      if (w >= W) break;  // the same for the whole warp
+      const float vre = -f * v[2 * q + 1], vim = f * v[2 * q];
+      const __half h0 = __float2half_rn(vre), h2 = __float2half_rn(vim);
+      const __half h1 = __float2half_rn(vre - __half2float(h0)), h3 = __float2half_rn(vim - __half2float(h2));
+      const uint32_t a = (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
+      const uint32_t b = (uint32_t)__half_as_ushort(h2) | ((uint32_t)__half_as_ushort(h3) << 16);
+      uint32_t d[4], e[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        d[t] = pick(c, __shfl_sync(kFull, a, dsrc + t), __shfl_sync(kFull, b, dsrc + t));
+        e[t] = pick(r & 3, __shfl_sync(kFull, a, tsrc + 4 * t), __shfl_sync(kFull, b, tsrc + 4 * t));
       }
+      *reinterpret_cast<uint2*>(dpl + w * wstride + doff) = make_uint2(d[0] | (d[1] << 16), d[2] | (d[3] << 16));
+      *reinterpret_cast<uint2*>(tpl + w * wstride + toff) = make_uint2(e[0] | (e[1] << 16), e[2] | (e[3] << 16));
     }
   }
 };
@@ -450,8 +498,8 @@ static unsigned grid_for(long long n) {
 // partial per (x tile, w).  The NP rows of one x lie in one warp (32 % NP == 0),
 // so each warp parks its own 32 rows in shared memory and walks its blocks
 // without a CTA barrier: lane (g, j), g = lane / NP, j = lane % NP, runs over the
-// rows i of x block g.  Products in FP32 (the operands carry TF32-product
-// errors already), sums in FP64.
+// rows i of x block g.  A lane's products and sum in FP32 (the operands carry the
+// split products' errors already), the sums across lanes and blocks in FP64.
 template <int NP, int BN>
 struct EpiExchange {
   static constexpr int LD = BN + 1;  // odd stride: row and column walks are both conflict-free
@@ -478,13 +526,18 @@ struct EpiExchange {
       const float* blk = sC + (xl * NP) * LD + wl * 2 * NP;
       double sr = 0.0, si = 0.0;
       if (xok && (n0 / (2 * NP)) + wl < W) {
+        // a lane's N products summed in FP32 (~2^-24 each, below the split products' own
+        // errors in the operands), then FP64 across lanes and blocks
+        float fr = 0.0f, fi = 0.0f;
 #pragma unroll 4
         for (int i = 0; i < N; ++i) {
           const float ar = blk[i * LD + j], ai = blk[i * LD + NP + j];
           const float br = blk[j * LD + i], bi = blk[j * LD + NP + i];
-          sr += (double)fmaf(ar, br, -ai * bi);
-          si += (double)fmaf(ar, bi, ai * br);
+          fr = fmaf(ar, br, fmaf(-ai, bi, fr));
+          fi = fmaf(ar, bi, fmaf(ai, br, fi));
         }
+        sr = fr;
+        si = fi;
       }
 #pragma unroll
       for (int o = NP / 2; o > 0; o >>= 1) {

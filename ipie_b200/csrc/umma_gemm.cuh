@@ -253,6 +253,8 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
             const uint32_t d = tmem + (uint32_t)(buf * S::BUF_COLS + a * BN);
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
+              // K steps wholly past K multiply TMA's zero fill: skip them
+              if (kk > 0 && kb * KB + kk * (KB / 4) >= K) break;
               // 32 bytes of K per MMA (8 tf32 or 16 fp16): advance the start address by 2 (16-byte units)
               if constexpr (KIND == KIND_F16) {
                 mma_f16(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
