@@ -599,7 +599,7 @@ def measure_peaks():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50, help="timed steps; multiples of 25 include whole energy blocks")
+    ap.add_argument("--steps", type=int, default=100, help="timed steps; multiples of 25 include whole energy blocks")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c2_rhf_m200", choices=sorted(WORKLOADS))
