@@ -109,6 +109,26 @@ def generate(
     )
 
 
+def generate_complex(nbasis: int, nocc, nchol: int, decay: float, seed: int = 7, uhf: bool = False,
+                     imag: float = 0.3, chol_scale="stable") -> SyntheticSystem:
+    """A complex-Cholesky system (ipie's ``GenericComplexChol`` input): the real system of
+    :func:`generate` with an imaginary part ``i * imag * K_x`` added to every Cholesky vector,
+    K_x a general (non-symmetric) N(0, 1) matrix under the same amplitude and decay, so that
+    both Hermitian parts A and B are non-zero; trial and initial walker as :func:`generate`."""
+    base = generate(nbasis, nocc, nchol, decay, seed=seed, uhf=uhf, chol_scale=chol_scale)
+    M, X = nbasis, nchol
+    if chol_scale == "literal":
+        chol_scale = 0.3
+    elif chol_scale == "stable":
+        chol_scale = 0.1 * np.sqrt(30.0 * 26.0 / (decay * nbasis))
+    rng = np.random.default_rng(seed + 1000)
+    g = np.arange(X, dtype=np.float64)
+    K = rng.normal(0.0, 1.0, size=(X, M, M)) * (imag * chol_scale * np.exp(-g / decay))[:, None, None]
+    chol = base.chol + 1.0j * np.ascontiguousarray(K.reshape(X, M * M).T)
+    return SyntheticSystem(nbasis=M, nup=base.nup, ndown=base.ndown, nchol=X, h1e=base.h1e,
+                           chol=np.ascontiguousarray(chol), ecore=base.ecore, psi=base.psi, init=base.init)
+
+
 # Named workloads: (nbasis, nocc, nchol, decay, walkers, steps, uhf)
 WORKLOADS = {
     "c0_rhf_m26": dict(nbasis=26, nocc=5, nchol=120, decay=30.0, walkers=64, steps=200, uhf=False),

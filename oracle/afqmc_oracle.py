@@ -151,6 +151,20 @@ class System:
     def nchol(self):
         return self.chol.shape[-1]
 
+    # the pieces that differ for a complex Cholesky Hamiltonian (oracle/complex_chol_oracle.py)
+    @property
+    def nfields(self):
+        return self.nchol
+
+    def vbias(self, w):
+        return force_bias(self, w)
+
+    def vhs(self, xshifted):
+        return construct_vhs(self, xshifted)
+
+    def local_energy(self, w):
+        return local_energy_single_det_uhf_batch(self, w)
+
 
 @dataclass
 class Walkers:
@@ -313,11 +327,11 @@ def propagate_walkers_two_body(sys_: System, w: Walkers, xi: np.ndarray | None =
     """Force bias, field draw, VHS, exponential; returns ``(cmf, cfb)``.
 
     ipie: ``propagation/phaseless_base.py:282-310`` and ``phaseless_generic.py:35-58``.
-    If ``xi`` (W, X) is not given it is drawn from numpy's global stream as ipie does.
+    If ``xi`` (W, nfields) is not given it is drawn from numpy's global stream as ipie does.
     """
-    W, X = w.nwalkers, sys_.nchol
+    W, X = w.nwalkers, sys_.nfields
     sqrt_dt = math.sqrt(sys_.dt)
-    vbias = force_bias(sys_, w)
+    vbias = sys_.vbias(w)
     xbar = -sqrt_dt * (1.0j * vbias - sys_.mf_shift)
     xbar = apply_bound_force_bias(xbar, 1.0)
     if xi is None:
@@ -326,7 +340,7 @@ def propagate_walkers_two_body(sys_: System, w: Walkers, xi: np.ndarray | None =
     cmf = -sqrt_dt * np.einsum("wx,x->w", xshifted, sys_.mf_shift)
     cfb = np.einsum("wx,wx->w", xi, xbar) - 0.5 * np.einsum("wx,wx->w", xbar, xbar)
     xshifted = xshifted.T.copy()
-    vhs = construct_vhs(sys_, xshifted)
+    vhs = sys_.vhs(xshifted)
     w.phia = apply_exponential(w.phia, vhs, sys_.exp_nmax)
     if sys_.ndown > 0:
         w.phib = apply_exponential(w.phib, vhs, sys_.exp_nmax)
@@ -692,7 +706,7 @@ class Accumulator:
 def energy_estimate(sys_: System, w: Walkers):
     """``EnergyEstimator.compute_estimator``: GF recomputed, weighted sums; ipie ``estimators/energy.py:156-165``."""
     greens_function(sys_, w)
-    e = local_energy_single_det_uhf_batch(sys_, w)
+    e = sys_.local_energy(w)
     return {
         "ENumer": np.sum(w.weight * e[:, 0].real),
         "EDenom": np.sum(w.weight),

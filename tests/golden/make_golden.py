@@ -2,7 +2,7 @@
 
 Run from the repository root with ipie's source tree available:
 
-    python tests/golden/make_golden.py /path/to/ipie-checkout [ad|pop]
+    python tests/golden/make_golden.py /path/to/ipie-checkout [ad|pop|complex]
 
 ipie needs ``plum`` and ``h5py``, which are absent here; the small stand-ins in
 ``_ref_shims/`` are put first on ``sys.path``.  mpi4py is absent, so ipie
@@ -283,7 +283,54 @@ def pop_control_fixture(name):
     print("wrote", name)
 
 
+def complex_fixture(name, sysw, nwalkers, seed, nsteps=3):
+    """ipie's complex-Cholesky path (``GenericComplexChol``): per-kernel outputs on perturbed
+    walkers, then ``nsteps`` of ``PhaselessGeneric.propagate_walkers`` with numpy's global
+    stream seeded (the fields are drawn as ipie draws them)."""
+    ham, trial, walkers, prop = build(sysw, nwalkers)
+    rng = np.random.default_rng(seed)
+    M, na, nb, X = sysw.nbasis, sysw.nup, sysw.ndown, sysw.nchol
+    W = nwalkers
+    pa = walkers.phia + 0.2 * (rng.normal(size=(W, M, na)) + 1j * rng.normal(size=(W, M, na)))
+    pb = walkers.phib + 0.2 * (rng.normal(size=(W, M, nb)) + 1j * rng.normal(size=(W, M, nb)))
+    walkers.phia = pa.copy()
+    walkers.phib = pb.copy()
+    out = dict(phia_in=pa, phib_in=pb)
+    out["ovlp"] = greens_function_single_det(walkers, trial)
+    out["Ghalfa"] = walkers.Ghalfa.copy()
+    out["Ghalfb"] = walkers.Ghalfb.copy()
+    out["vbias"] = trial.calc_force_bias(ham, walkers, MPIHandler())
+    xs = rng.normal(size=(2 * X, W)) + 0.3j * rng.normal(size=(2 * X, W))
+    out["xshifted"] = xs
+    out["VHS"] = prop.construct_VHS(ham, xs.copy())
+    system = Generic((sysw.nup, sysw.ndown))
+    out["energy_uhf"] = local_energy_single_det_uhf_batch(system, ham, walkers, trial)
+    out["mf_shift"] = prop.mf_shift
+    out["expH1"] = prop.expH1
+    out["h1e_mod"] = ham.h1e_mod
+    for k in ("rchola", "rcholb", "rcholbara", "rcholbarb", "rAa", "rAb", "rBa", "rBb", "rH1a", "rH1b"):
+        out[k] = getattr(trial, "_" + k)
+    # a short walk from the perturbed walkers with ipie's own draws
+    walkers.ovlp = out["ovlp"].copy()
+    np.random.seed(seed)
+    for step in range(nsteps):
+        prop.propagate_walkers(walkers, ham, trial, -7.0 if step else 0.0)
+    out["walk_weight"] = np.array(walkers.weight)
+    out["walk_ovlp"] = np.array(walkers.ovlp)
+    out["walk_phia"] = np.array(walkers.phia)
+    out["walk_phib"] = np.array(walkers.phib)
+    out["walk_hybrid_energy"] = np.array(walkers.hybrid_energy)
+    out["chol_checksum"] = checksum(sysw.chol)
+    out["psi_checksum"] = checksum(sysw.psi)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "complex":
+        cplx = synthetic.generate_complex(20, (4, 3), 60, decay=30.0, seed=3, uhf=True)
+        complex_fixture("complex_uhf_m20.npz", cplx, nwalkers=5, seed=21)
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[2] == "ad":
         ad_fixture("ad_onebody_m30.npz")
         sys.exit(0)
@@ -301,3 +348,5 @@ if __name__ == "__main__":
     known_answer_inputs("known_answers.npz")
     pop_control_fixture("pop_control.npz")
     ad_fixture("ad_onebody_m30.npz")
+    cplx = synthetic.generate_complex(20, (4, 3), 60, decay=30.0, seed=3, uhf=True)
+    complex_fixture("complex_uhf_m20.npz", cplx, nwalkers=5, seed=21)
