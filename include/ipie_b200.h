@@ -152,6 +152,39 @@ int ipie_b200_walker_gather(const int* src, int W, int M, int na, int nb, const 
                             void* ghalfa_out, void* ghalfb_out, void* hybrid_energy_out, void* ovlp_out,
                             void* phase_out, double* unscaled_weight_out, void* stream);
 
+/* ---- complex Cholesky Hamiltonians (ipie's GenericComplexChol: nfields = 2X, the first X
+ * fields coupling to A = (L + L^H)/2, the rest to B = i (L - L^H)/2) ---- */
+
+/* out[w][xoff + x] (accumulate: +=) sum_k (r_re + i r_im)[x][k] Ghalf[w][k]: one spin's term of
+ * the force bias [rA . G ; rB . G] or of the Coulomb vectors X1 = sum_s rchol_s . G_s and
+ * X2 = sum_s rcholbar_s . G_s; r_* (X, K) f64 with K = N*M, out rows of ld complex.
+ * replaces: propagation/force_bias.py:124-150 and estimators/local_energy_sd.py:205-262 (X1, X2). */
+int ipie_b200_force_bias_complex(const double* r_re, const double* r_im, const void* ghalf, int W, int X, int K,
+                                 void* out, int ld, int xoff, int accumulate, void* stream);
+
+/* VHS[w] = i sqrt(dt) (C . xshifted)[:, w] reshaped (M, M), C = [A | B] (M*M, F = 2X) complex
+ * as its parts c_re, c_im (M*M, F) f64; xshifted (F, W) complex.  Not symmetric: written whole.
+ * replaces: propagation/phaseless_generic.py:99-111. */
+int ipie_b200_construct_vhs_complex(const double* c_re, const double* c_im, int M, int F, const void* xshifted, int W,
+                                    double sqrt_dt, void* vhs, void* stream);
+
+/* exx[w] (accumulate: +=) 1/2 sum_x sum_ij T1_ij T2_ji with T1 = rchol_x . Ghalf_w^T and
+ * T2 = rcholbar_x . Ghalf_w^T for one spin block of a complex-Cholesky Hamiltonian, from the
+ * real exchange kernel by polarisation: pol (8, X, N*M) f64 holds rchol_a +- rcholbar_b for
+ * (a, b) = (re, re), (im, im), (re, im), (im, re) in that order, + before -; part: the
+ * workspace of ipie_b200_exchange (rows * W complex).
+ * replaces: estimators/local_energy_sd.py:307-355 (exx_kernel_batch_complex_rchol). */
+int ipie_b200_exchange_complex(const double* pol, const void* ghalf, int W, int X, int M, int N, void* part,
+                               void* exx, int accumulate, void* stream);
+
+/* energy[w] = (e1b + e2b, e1b, e2b) with e1b = sum_s Ghalf_s . rH1_s + ecore,
+ * e2b = 1/2 sum_x X1[w][x] X2[w][x] - exx[w] (X1, X2 (W, X) from ipie_b200_force_bias_complex;
+ * exx (W) the exchange, see the Python estimator).
+ * replaces: estimators/local_energy_sd.py:406-460. */
+int ipie_b200_energy_complex(const void* ghalfa, const void* ghalfb, int W, int NMa, int NMb, const void* rh1a,
+                             const void* rh1b, double ecore, const void* x1, const void* x2, int X, const void* exx,
+                             void* energy, void* stream);
+
 /* Exchange energy for callers that cannot allocate device memory (their device
  * memory is owned by their own pool allocator, or their loop cannot take the
  * implicit synchronisation of cudaMalloc/cudaFree).  No counterpart in ipie:

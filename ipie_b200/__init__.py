@@ -2,7 +2,7 @@
 
 The compute path is the in-tree CUDA library ``libipie_b200.so`` (sm_100a),
 reached through a thin ctypes layer (``ipie_b200._lib``).  Host classes mirror
-ipie's: ``Generic``/``GenericRealChol``, ``SingleDet``, ``UHFWalkers``,
+ipie's: ``Generic``/``GenericRealChol``/``GenericComplexChol``, ``SingleDet``, ``UHFWalkers``,
 ``PhaselessGeneric``, ``PopController``, the single-determinant local energies,
 ``EnergyEstimator`` and ``AFQMC``.
 """
@@ -11,6 +11,7 @@ __version__ = "0.1.0"
 _LAZY = {
     "Generic": "hamiltonian",
     "GenericRealChol": "hamiltonian",
+    "GenericComplexChol": "hamiltonian",
     "SingleDet": "trial",
     "UHFWalkers": "walkers",
     "PhaselessGeneric": "propagation",

@@ -62,6 +62,10 @@ SIGNATURES = {
     "ipie_b200_split_tf32": [P, P, P, ctypes.c_longlong, P],
     "ipie_b200_umma_gemm_test": [P, P, P, P, P, P, P, I, I, I, I, I, P, P],
     "ipie_b200_split_f16": [P, P, P, ctypes.c_longlong, D, P],
+    "ipie_b200_force_bias_complex": [P, P, P, I, I, I, P, I, I, I, P],
+    "ipie_b200_construct_vhs_complex": [P, P, I, I, P, I, D, P, P],
+    "ipie_b200_energy_complex": [P, P, I, I, I, P, P, D, P, P, I, P, P, P],
+    "ipie_b200_exchange_complex": [P, P, I, I, I, I, P, P, I, P],
     "ipie_b200_umma_gemm_f16_test": [P, P, P, P, P, I, I, I, I, P, P],
     "ipie_b200_normal_fill": [P, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_ulonglong, P],
     "ipie_b200_normal_fill_dev": [P, ctypes.c_longlong, ctypes.c_ulonglong, P, P],

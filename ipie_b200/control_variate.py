@@ -173,6 +173,8 @@ class EnergyParts:
         subsample expanded around the trial, as the mixed local energy does)."""
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision {precision!r}: 'fp64' or 'mixed'")
+        if getattr(hamiltonian, "complex_chol", False):
+            raise NotImplementedError("the energy control variate takes real Cholesky Hamiltonians")
         self.ham, self.trial = hamiltonian, trial
         self.precision = precision
         self.n_lead = max(1, hamiltonian.nchol // lead_fraction)

@@ -59,6 +59,31 @@ int ipie_b200_construct_vhs(const double* chol_packed, const int* idx_i, const i
   return (int)launch_vhs(chol_packed, idx_i, idx_j, P, X, M, CC2(xshifted), W, sqrt_dt, C2(vhs), ST(stream));
 }
 
+// ---- complex Cholesky (ipie's GenericComplexChol) ----
+int ipie_b200_force_bias_complex(const double* r_re, const double* r_im, const void* ghalf, int W, int X, int K,
+                                 void* out, int ld, int xoff, int accumulate, void* stream) {
+  if (W <= 0 || X <= 0 || K <= 0 || ld < xoff + X || xoff < 0) return (int)cudaErrorInvalidValue;
+  cudaError_t e = launch_force_bias_c(r_re, CC2(ghalf), W, X, K, C2(out), ld, xoff, accumulate, 1.0, 0.0, ST(stream));
+  if (e != cudaSuccess) return (int)e;
+  return (int)launch_force_bias_c(r_im, CC2(ghalf), W, X, K, C2(out), ld, xoff, 1, 0.0, 1.0, ST(stream));
+}
+
+int ipie_b200_construct_vhs_complex(const double* c_re, const double* c_im, int M, int F, const void* xshifted, int W,
+                                    double sqrt_dt, void* vhs, void* stream) {
+  if (M <= 0 || F <= 0 || W <= 0) return (int)cudaErrorInvalidValue;
+  cudaError_t e = launch_vhs_full(c_re, M, F, CC2(xshifted), W, sqrt_dt, C2(vhs), 0, ST(stream));
+  if (e != cudaSuccess) return (int)e;
+  return (int)launch_vhs_full(c_im, M, F, CC2(xshifted), W, sqrt_dt, C2(vhs), 1, ST(stream));
+}
+
+int ipie_b200_energy_complex(const void* ghalfa, const void* ghalfb, int W, int NMa, int NMb, const void* rh1a,
+                             const void* rh1b, double ecore, const void* x1, const void* x2, int X, const void* exx,
+                             void* energy, void* stream) {
+  if (W <= 0 || X <= 0 || NMa < 0 || NMb < 0) return (int)cudaErrorInvalidValue;
+  return (int)launch_energy_complex(CC2(ghalfa), CC2(ghalfb), W, NMa, NMb, CC2(rh1a), CC2(rh1b), ecore, CC2(x1),
+                                    CC2(x2), X, CC2(exx), C2(energy), ST(stream));
+}
+
 int ipie_b200_apply_exponential_batch(const void* vhs, const void* phi_in, void* phi_out, void* work, int W, int M,
                                       int N, int nmax, void* stream) {
   if (phi_in == phi_out) return (int)cudaErrorInvalidValue;
@@ -133,6 +158,31 @@ int ipie_b200_exchange(const double* rchol, const void* ghalf, int W, int X, int
   int rows = 0;
   if (part == nullptr) return (int)cudaErrorInvalidValue;
   return (int)launch_exchange(rchol, CC2(ghalf), W, X, M, N, C2(part), &rows, ST(stream));
+}
+
+// Exchange of one spin block of a complex-Cholesky Hamiltonian,
+//   exx_w = 1/2 sum_x sum_ij T1_ij T2_ji,  T1 = (R_re + i R_im)_x G^T,  T2 = (S_re + i S_im)_x G^T
+// (R = rchol, S = rcholbar), from the real exchange kernel by polarisation: with
+// E(P) = sum_x sum_ij [P_x G^T]_ij [P_x G^T]_ji, the cross sum of real P and Q is
+// (E(P + Q) - E(P - Q)) / 4, and T1_ij T2_ji expands into the four cross sums
+// (R_re, S_re) - (R_im, S_im) + i (R_re, S_im) + i (R_im, S_re).  pol holds the eight real
+// operands P +- Q in that order ((8, X, N*M) f64, rr+ rr- ii+ ii- ri+ ri- ir+ ir-).
+int ipie_b200_exchange_complex(const double* pol, const void* ghalf, int W, int X, int M, int N, void* part,
+                               void* exx, int accumulate, void* stream) {
+  if (pol == nullptr || part == nullptr || W <= 0) return (int)cudaErrorInvalidValue;
+  cudaStream_t st = ST(stream);
+  const double2 coef[8] = {make_double2(0.125, 0.0),  make_double2(-0.125, 0.0), make_double2(-0.125, 0.0),
+                           make_double2(0.125, 0.0),  make_double2(0.0, 0.125),  make_double2(0.0, -0.125),
+                           make_double2(0.0, 0.125),  make_double2(0.0, -0.125)};
+  const size_t stride = (size_t)X * N * M;
+  for (int k = 0; k < 8; ++k) {
+    int rows = 0;
+    cudaError_t e = launch_exchange(pol + k * stride, CC2(ghalf), W, X, M, N, C2(part), &rows, st);
+    if (e != cudaSuccess) return (int)e;
+    e = launch_scaled_row_sum(CC2(part), rows, W, coef[k], C2(exx), (k > 0 || accumulate) ? 1 : 0, st);
+    if (e != cudaSuccess) return (int)e;
+  }
+  return 0;
 }
 
 int ipie_b200_local_energy_single_det_batch(int rhf, const double* rchola, const double* rcholb, const void* rH1a,

@@ -67,6 +67,127 @@ cudaError_t launch_vhs(const double* chol_packed, const int* idx_i, const int* i
 }
 
 // ---------------------------------------------------------------------------
+// Complex-Cholesky pieces (ipie's GenericComplexChol), each built from real-operand
+// GEMMs of the same core: a complex operand R = R_re + i R_im enters as two launches,
+// the second scaled by i in the epilogue.
+//
+// Force bias / Coulomb vector: out[w][xoff + x] (+)= (sr + i si) sum_k R_part[x][k] Ghalf[w][k],
+// out rows of `ld` complex.
+// ---------------------------------------------------------------------------
+struct EpiVbiasC {
+  double2* v;
+  int ld, xoff;
+  int accumulate;
+  double sr, si;
+  __device__ __forceinline__ void operator()(int, int x, int col, double v0, double v1) const {
+    const size_t idx = (size_t)(col >> 1) * ld + xoff + x;
+    double2 r = make_double2(sr * v0 - si * v1, sr * v1 + si * v0);
+    if (accumulate) r = cadd(r, v[idx]);
+    v[idx] = r;
+  }
+};
+
+cudaError_t launch_force_bias_c(const double* rpart, const double2* ghalf, int W, int X, int K, double2* out, int ld,
+                                int xoff, int accumulate, double sr, double si, cudaStream_t st) {
+  using C = CfgBig;
+  LoadRowK<C, C::BM> la{rpart, 0, K};
+  LoadWalkerCplx<C, C::BN> lb{reinterpret_cast<const double*>(ghalf), 2LL * K};
+  return launch_dmma_gemm<C>(X, 2 * W, K, 1, la, lb, EpiVbiasC{out, ld, xoff, accumulate, sr, si}, st);
+}
+
+// VHS of a complex Cholesky: V_w = i sqrt(dt) C . xs_w with C = [A | B] (M*M, F) complex and
+// xs (F, W) complex, as two launches on C_re (mode 0: write) and C_im (mode 1: accumulate i x):
+//   C xs = (P0 - Q1) + i (P1 + Q0),  (P0, P1) = C_re (xs_re, xs_im),  (Q0, Q1) = C_im (xs_re, xs_im),
+//   V = i sqrt(dt) C xs:  Re V = -sdt (P1 + Q0),  Im V = sdt (P0 - Q1).
+// Rows p = i M + j of C map to V_w[i][j] directly (no symmetry).
+struct EpiVHSFull {
+  double2* vhs;
+  int M;
+  double sdt;
+  int mode;
+  __device__ __forceinline__ void operator()(int, int p, int col, double v0, double v1) const {
+    const int w = col >> 1;
+    double2* dst = vhs + (size_t)w * M * M + p;
+    if (mode == 0) {
+      *dst = make_double2(-sdt * v1, sdt * v0);
+    } else {
+      const double2 o = *dst;
+      *dst = make_double2(o.x - sdt * v0, o.y - sdt * v1);
+    }
+  }
+};
+
+cudaError_t launch_vhs_full(const double* cpart, int M, int F, const double2* xshifted, int W, double sqrt_dt,
+                            double2* vhs, int mode, cudaStream_t st) {
+  using C = CfgBig;
+  LoadRowK<C, C::BM> la{cpart, 0, F};
+  LoadRowR<C, C::BN> lb{reinterpret_cast<const double*>(xshifted), 0, 2LL * W};
+  return launch_dmma_gemm<C>(M * M, 2 * W, F, 1, la, lb, EpiVHSFull{vhs, M, sqrt_dt, mode}, st);
+}
+
+// Local energy of the complex-Cholesky form, one CTA per walker:
+//   e1b = sum_s Ghalf_s . rH1_s + ecore,  ecoul = 1/2 sum_x X1[x] X2[x],  e2b = ecoul - exx.
+__global__ void __launch_bounds__(256) energy_complex_kernel(const double2* __restrict__ ga,
+                                                              const double2* __restrict__ gb, int NMa, int NMb,
+                                                              const double2* __restrict__ rh1a,
+                                                              const double2* __restrict__ rh1b, double ecore,
+                                                              const double2* __restrict__ x1,
+                                                              const double2* __restrict__ x2, int X,
+                                                              const double2* __restrict__ exx,
+                                                              double2* __restrict__ energy) {
+  __shared__ double2 red[2][8];
+  const int w = blockIdx.x, tid = threadIdx.x;
+  double2 e1 = make_double2(0.0, 0.0), ec = make_double2(0.0, 0.0);
+  for (int k = tid; k < NMa; k += 256) e1 = cadd(e1, cmul(ga[(size_t)w * NMa + k], rh1a[k]));
+  for (int k = tid; k < NMb; k += 256) e1 = cadd(e1, cmul(gb[(size_t)w * NMb + k], rh1b[k]));
+  for (int x = tid; x < X; x += 256) ec = cadd(ec, cmul(x1[(size_t)w * X + x], x2[(size_t)w * X + x]));
+  e1 = warp_sum2(e1);
+  ec = warp_sum2(ec);
+  if ((tid & 31) == 0) {
+    red[0][tid >> 5] = e1;
+    red[1][tid >> 5] = ec;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double2 a = make_double2(ecore, 0.0), c = make_double2(0.0, 0.0);
+    for (int k = 0; k < 8; ++k) {
+      a = cadd(a, red[0][k]);
+      c = cadd(c, red[1][k]);
+    }
+    const double2 e2 = csub(cscale(c, 0.5), exx[w]);
+    energy[(size_t)w * 3 + 0] = cadd(a, e2);
+    energy[(size_t)w * 3 + 1] = a;
+    energy[(size_t)w * 3 + 2] = e2;
+  }
+}
+
+// out[w] (accumulate: +=) coef * sum_t part[t][w]
+__global__ void scaled_row_sum_kernel(const double2* __restrict__ part, int rows, int W, double2 coef,
+                                      double2* __restrict__ out, int accumulate) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int t = 0; t < rows; ++t) acc = cadd(acc, part[(size_t)t * W + w]);
+  const double2 r = cmul(coef, acc);
+  out[w] = accumulate ? cadd(out[w], r) : r;
+}
+
+cudaError_t launch_scaled_row_sum(const double2* part, int rows, int W, double2 coef, double2* out, int accumulate,
+                                  cudaStream_t st) {
+  scaled_row_sum_kernel<<<(W + 127) / 128, 128, 0, st>>>(part, rows, W, coef, out, accumulate);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_energy_complex(const double2* ga, const double2* gb, int W, int NMa, int NMb, const double2* rh1a,
+                                  const double2* rh1b, double ecore, const double2* x1, const double2* x2, int X,
+                                  const double2* exx, double2* energy, cudaStream_t st) {
+  energy_complex_kernel<<<W, 256, 0, st>>>(ga, gb, NMa, NMb, rh1a, rh1b, ecore, x1, x2, X, exx, energy);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // One-body: phi_out[w] = expH1 . phi_in[w]; expH1 real (M x M) or complex.
 // ---------------------------------------------------------------------------
 struct EpiStoreC {

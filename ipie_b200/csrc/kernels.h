@@ -52,6 +52,15 @@ cudaError_t launch_one_body(const double* expH1, int cplx, const double2* phi_in
                             cudaStream_t st);
 cudaError_t launch_taylor(const double2* vhs, const double2* phi_in, double2* phi_out, double2* t0, double2* t1, int W,
                           int M, int N, int nmax, cudaStream_t st);
+cudaError_t launch_force_bias_c(const double* rpart, const double2* ghalf, int W, int X, int K, double2* out, int ld,
+                                int xoff, int accumulate, double sr, double si, cudaStream_t st);
+cudaError_t launch_vhs_full(const double* cpart, int M, int F, const double2* xshifted, int W, double sqrt_dt,
+                            double2* vhs, int mode, cudaStream_t st);
+cudaError_t launch_scaled_row_sum(const double2* part, int rows, int W, double2 coef, double2* out, int accumulate,
+                                  cudaStream_t st);
+cudaError_t launch_energy_complex(const double2* ga, const double2* gb, int W, int NMa, int NMb, const double2* rh1a,
+                                  const double2* rh1b, double ecore, const double2* x1, const double2* x2, int X,
+                                  const double2* exx, double2* energy, cudaStream_t st);
 cudaError_t launch_exchange(const double* rchol, const double2* ghalf, int W, int X, int M, int N, double2* part,
                             int* ntiles, cudaStream_t st);
 

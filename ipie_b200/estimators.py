@@ -29,9 +29,44 @@ def _energy_work(walkers, hamiltonian, rhf):
     return buf
 
 
+def _local_energy_complex(hamiltonian, walkers, trial):
+    """Complex-Cholesky UHF local energy (ipie ``local_energy_sd.py:406-460``): X1 = sum_s rchol_s . G_s and
+    X2 = sum_s rcholbar_s . G_s give ecoul = X1 . X2 / 2, the exchange 1/2 sum_x tr(T1 T2) per spin runs as
+    eight real exchange passes (polarisation), and the combine adds the one-body term."""
+    W, X, M = walkers.nwalkers, hamiltonian.nchol, walkers.nbasis
+    rows = max(lib().ipie_b200_exchange_rows(W, X, M, n) for n in (walkers.nup, walkers.ndown) if n > 0)
+    need = 2 * W * X + rows * W + W
+    buf = getattr(walkers, "_energy_work_cplx", None)
+    if buf is None or buf.numel() < need:
+        buf = torch.empty(need, dtype=C128, device=walkers.device)
+        walkers._energy_work_cplx = buf
+    x1, x2 = buf[: W * X], buf[W * X: 2 * W * X]
+    part, exx = buf[2 * W * X: 2 * W * X + rows * W], buf[2 * W * X + rows * W: need]
+    exx.zero_()
+    for xv, name in ((x1, "chol"), (x2, "cholbar")):
+        xv.zero_()
+        for s_, g, n in (("a", walkers.Ghalfa, walkers.nup), ("b", walkers.Ghalfb, walkers.ndown)):
+            if n == 0:
+                continue
+            re, im = trial._cplx[name + s_]
+            call("ipie_b200_force_bias_complex", ptr(re), ptr(im), ptr(g), W, X, n * M, ptr(xv), X, 0, 1, stream())
+    for s_, g, n in (("a", walkers.Ghalfa, walkers.nup), ("b", walkers.Ghalfb, walkers.ndown)):
+        if n == 0:
+            continue
+        call("ipie_b200_exchange_complex", ptr(trial._cplx["pol" + s_]), ptr(g), W, X, M, n, ptr(part), ptr(exx), 1,
+             stream())
+    energy = torch.empty(W, 3, dtype=C128, device=walkers.device)
+    call("ipie_b200_energy_complex", ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), W, walkers.nup * M,
+         walkers.ndown * M, ptr(trial._rH1a), ptr(trial._rH1b), hamiltonian.ecore, ptr(x1), ptr(x2), X, ptr(exx),
+         ptr(energy), stream())
+    return energy
+
+
 def _local_energy(hamiltonian, walkers, trial, rhf):
     if not trial.half_rotated:
         raise RuntimeError("trial.half_rotate(hamiltonian) must run before computing local energies")
+    if getattr(hamiltonian, "complex_chol", False):
+        return _local_energy_complex(hamiltonian, walkers, trial)
     W = walkers.nwalkers
     work = _energy_work(walkers, hamiltonian, rhf)
     energy = torch.empty(W, 3, dtype=C128, device=walkers.device)
@@ -191,7 +226,7 @@ class EnergyEstimator:
         # ipie recomputes the Green's function here; it is skipped while the cached one is current
         if not walkers.gf_current(trial):
             trial.calc_greens_function(walkers)
-        if self.precision == "mixed":
+        if self.precision == "mixed" and not getattr(hamiltonian, "complex_chol", False):
             energy = local_energy_mixed(system, hamiltonian, walkers, trial, rhf=walkers.rhf)
         else:
             energy = local_energy_batch(system, hamiltonian, walkers, trial)

@@ -35,6 +35,8 @@ def tiled_triu_indices(M, rows=32, cols=4):
 
 
 class GenericRealChol:
+    complex_chol = False
+
     def __init__(self, h1e, chol, ecore=0.0, device="cuda", verbose=False):
         h1e = np.asarray(h1e)
         chol = np.asarray(chol)
@@ -70,9 +72,49 @@ class GenericRealChol:
         return self.nbasis * (self.nbasis + 1) // 2
 
 
+class GenericComplexChol:
+    """ipie's ``GenericComplexChol`` (``hamiltonians/generic.py:100-150``): complex Cholesky
+    vectors L (M*M, X) and their Hermitian parts ``A_x = (L_x + L_x^H)/2``,
+    ``B_x = i (L_x - L_x^H)/2``; 2X auxiliary fields (A first, then B).  The device keeps
+    ``C = [A | B]`` (M*M, 2X) as real and imaginary parts, the left operand of the VHS."""
+
+    complex_chol = True
+
+    def __init__(self, h1e, chol, ecore=0.0, device="cuda", verbose=False):
+        h1e = np.asarray(h1e)
+        chol = np.asarray(chol, dtype=np.complex128)
+        assert h1e.shape[0] == 2, "h1e must carry both spin components"
+        self.H1 = h1e
+        self.ecore = float(ecore)
+        self.nbasis = h1e.shape[-1]
+        self.nchol = chol.shape[-1]
+        self.nfields = 2 * self.nchol
+        assert self.nbasis ** 2 == chol.shape[0]
+        self.chunked = False
+        M, X = self.nbasis, self.nchol
+        self.chol = np.ascontiguousarray(chol)  # host copy (set-up only)
+        # h1e_mod = h1e - 1/2 L L^H, allocated with H1's dtype as ipie does (generic.py:116-118):
+        # for a real H1 the (antisymmetric) imaginary part is dropped
+        view = self.chol.reshape(M, M * X)
+        v0 = 0.5 * view @ view.T.conj()
+        h1e_mod = np.array([h1e[0] - v0, h1e[1] - v0])
+        self.h1e_mod = h1e_mod if np.iscomplexobj(h1e) else h1e_mod.real.copy()
+        L = self.chol.reshape(M, M, X)
+        LH = L.transpose(1, 0, 2).conj()
+        self.A = np.ascontiguousarray((0.5 * (L + LH)).reshape(M * M, X))
+        self.B = np.ascontiguousarray((0.5j * (L - LH)).reshape(M * M, X))
+        self.device = torch.device(device)
+        C = np.concatenate([self.A, self.B], axis=1)
+        self.c_re = torch.from_numpy(np.ascontiguousarray(C.real)).to(self.device)
+        self.c_im = torch.from_numpy(np.ascontiguousarray(C.imag)).to(self.device)
+        if verbose:
+            print(f"# nbasis {M}  nchol {X}  complex Cholesky, {2 * C.real.nbytes / 1e9:.3f} GB of [A | B] on {self.device}")
+
+
 def Generic(h1e, chol, ecore=0.0, shmem=False, chol_packed=None, verbose=False):
-    """Factory with ipie's signature (``hamiltonians/generic.py:153-157``); real Cholesky only."""
+    """Factory with ipie's signature (``hamiltonians/generic.py:153-157``): complex Cholesky
+    vectors give :class:`GenericComplexChol`, real ones :class:`GenericRealChol`."""
     chol = np.asarray(chol)
     if chol.dtype == np.complex128:
-        raise NotImplementedError("complex Cholesky Hamiltonians are not supported by the B200 walker step")
+        return GenericComplexChol(h1e, chol, ecore, verbose=verbose)
     return GenericRealChol(h1e, chol, ecore, verbose=verbose)

@@ -29,15 +29,24 @@ F64 = torch.float64
 
 
 def construct_mean_field_shift(hamiltonian, trial):
-    """``mf = 1j L^T Re(G_a+G_b) - L^T Im(G_a+G_b)`` (ipie ``phaseless_base.py:153-172``)."""
+    """``mf = 1j L^T Re(G_a+G_b) - L^T Im(G_a+G_b)`` (ipie ``phaseless_base.py:153-172``); for a
+    complex Cholesky ``mf = [1j A^T g ; 1j B^T g]`` (``:199-218``)."""
     g = (trial.G[0] + trial.G[1]).ravel()
+    if getattr(hamiltonian, "complex_chol", False):
+        return np.concatenate([1.0j * (hamiltonian.A.T @ g), 1.0j * (hamiltonian.B.T @ g)])
     return 1.0j * (hamiltonian.chol.T @ g.real) - hamiltonian.chol.T @ g.imag
 
 
 def construct_one_body_propagator(hamiltonian, mf_shift, dt):
-    """``expH1_s = expm(-dt/2 (h1e_mod_s - 1j L.mf))`` (ipie ``phaseless_base.py:27-74``)."""
+    """``expH1_s = expm(-dt/2 (h1e_mod_s - 1j L.mf))`` (ipie ``phaseless_base.py:27-74``); for a
+    complex Cholesky the shift is ``1j (A mf[:X] + B mf[X:])`` (``:78-106``)."""
     M = hamiltonian.nbasis
-    shift = 1.0j * np.einsum("mx,x->m", hamiltonian.chol, mf_shift).reshape(M, M)
+    if getattr(hamiltonian, "complex_chol", False):
+        X = hamiltonian.nchol
+        shift = 1.0j * np.einsum("mx,x->m", hamiltonian.A, mf_shift[:X]).reshape(M, M)
+        shift = shift + 1.0j * np.einsum("mx,x->m", hamiltonian.B, mf_shift[X:]).reshape(M, M)
+    else:
+        shift = 1.0j * np.einsum("mx,x->m", hamiltonian.chol, mf_shift).reshape(M, M)
     H1 = hamiltonian.h1e_mod - np.array([shift, shift])
     return np.array([scipy.linalg.expm(-0.5 * dt * H1[0]), scipy.linalg.expm(-0.5 * dt * H1[1])])
 
@@ -163,7 +172,7 @@ class PhaselessGeneric:
             self._workspace(walkers, hamiltonian)
 
     def _workspace(self, walkers, hamiltonian):
-        W, M, X = walkers.nwalkers, walkers.nbasis, hamiltonian.nchol
+        W, M, X = walkers.nwalkers, walkers.nbasis, hamiltonian.nfields
         ws = self.ws
         if ws is None or (ws.W, ws.M, ws.na, ws.nb, ws.X) != (W, M, walkers.nup, walkers.ndown, X):
             self.ws = Workspace(W, M, walkers.nup, walkers.ndown, X, walkers.device)
@@ -176,6 +185,8 @@ class PhaselessGeneric:
         Cholesky FP16 hi/lo (padded), expH1 - I as FP16 hi/lo (the FP16 orbital chain, which
         takes blocks of M <= 256 and N <= 32) and as TF32 hi/lo (the per-term products)."""
         M, X = hamiltonian.nbasis, hamiltonian.nchol
+        if getattr(hamiltonian, "complex_chol", False):
+            raise NotImplementedError("the mixed form takes real Cholesky Hamiltonians (precision='fp64' for complex ones)")
         if M % 4 or X % 4 or self.expH1_complex:
             raise NotImplementedError("the mixed form needs nbasis and nchol multiples of 4 and a real expH1")
         dev = self.device
@@ -240,9 +251,9 @@ class PhaselessGeneric:
         walkers.sync_alias()
 
     def draw_fields(self, walkers, hamiltonian):
-        """N(0,1) auxiliary fields (W, X) into the workspace (ipie ``phaseless_base.py:296-298``)."""
+        """N(0,1) auxiliary fields (W, nfields) into the workspace (ipie ``phaseless_base.py:296-298``)."""
         ws = self.ws
-        W, X = walkers.nwalkers, hamiltonian.nchol
+        W, X = walkers.nwalkers, hamiltonian.nfields
         if self.rng == "numpy":
             xi = np.random.normal(0.0, 1.0, X * W).reshape(W, X)
             ws.xi_copied.synchronize()  # the previous step's upload has left the pinned buffer
@@ -264,7 +275,7 @@ class PhaselessGeneric:
     def propagate_walkers_two_body(self, walkers, hamiltonian, trial):
         """Force bias, shifted fields, VHS and exp(VHS) (ipie ``phaseless_base.py:282-310``)."""
         ws = self.ws
-        W, X = walkers.nwalkers, hamiltonian.nchol
+        W, X = walkers.nwalkers, hamiltonian.nfields
         self.timer.start("force_bias")
         force_bias_into(hamiltonian, walkers, trial, ws.vbias)
         self.timer.stop("force_bias")
@@ -285,6 +296,11 @@ class PhaselessGeneric:
         M = hamiltonian.nbasis
         if out is None:
             out = torch.empty(W, M, M, dtype=C128, device=xshifted.device)
+        if getattr(hamiltonian, "complex_chol", False):
+            # V = i sqrt(dt) (A xs[:X] + B xs[X:]) (ipie phaseless_generic.py:99-111)
+            call("ipie_b200_construct_vhs_complex", ptr(hamiltonian.c_re), ptr(hamiltonian.c_im), M,
+                 hamiltonian.nfields, ptr(xshifted.contiguous()), W, self.sqrt_dt, ptr(out), stream())
+            return out
         call("ipie_b200_construct_vhs", ptr(hamiltonian.chol_packed), ptr(hamiltonian.sym_idx_i),
              ptr(hamiltonian.sym_idx_j), M, hamiltonian.nchol, ptr(xshifted.contiguous()), W, self.sqrt_dt, ptr(out),
              stream())
@@ -333,7 +349,7 @@ class PhaselessGeneric:
             cmf, cfb = self.propagate_walkers_two_body(walkers, hamiltonian, trial)
             self.propagate_walkers_one_body(walkers)
         else:
-            W, X = walkers.nwalkers, hamiltonian.nchol
+            W, X = walkers.nwalkers, hamiltonian.nfields
             self.timer.start("force_bias")
             force_bias_into(hamiltonian, walkers, trial, ws.vbias)
             self.timer.stop("force_bias")

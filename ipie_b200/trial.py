@@ -56,8 +56,10 @@ class SingleDet:
         """``rH1_s = psi_s^H h1``, ``rchol_s[x, i*M+n] = sum_m psi*_mi L[m,n,x]``
         (ipie ``trial_wavefunction/half_rotate.py:11-116``)."""
         M, X = hamiltonian.nbasis, hamiltonian.nchol
+        if getattr(hamiltonian, "complex_chol", False):
+            return self._half_rotate_complex(hamiltonian)
         if np.iscomplexobj(self.psi):
-            raise NotImplementedError("complex trial orbitals are not supported by the B200 walker step")
+            raise NotImplementedError("complex trial orbitals need a complex Cholesky Hamiltonian here")
         L = hamiltonian.chol.reshape(M, M, X)
         rH1a = np.einsum("pi,pq->iq", self.psi0a.conj(), hamiltonian.H1[0], optimize=True)
         rH1b = np.einsum("pi,pq->iq", self.psi0b.conj(), hamiltonian.H1[1], optimize=True)
@@ -75,6 +77,40 @@ class SingleDet:
         else:
             self._rH1b = torch.from_numpy(np.ascontiguousarray(rH1b.astype(np.complex128))).to(dev)
             self._rcholb = torch.from_numpy(np.ascontiguousarray(rcholb)).to(dev)
+        self.half_rotated = True
+
+    def _half_rotate_complex(self, hamiltonian):
+        """Complex-Cholesky branch of ``half_rotate_generic`` (``half_rotate.py:42-46,84-113``, stored as
+        ``single_det.py:164-173``): L, ``Lbar = L^T*`` per vector, A and B, each half-rotated per spin.
+        The device keeps what the kernels take: real and imaginary parts of rA, rB (force bias) and of
+        rchol, rcholbar (Coulomb vectors), and for the exchange the eight real operands
+        ``rchol_a +- rcholbar_b`` per spin (``ipie_b200_exchange_complex``)."""
+        M, X = hamiltonian.nbasis, hamiltonian.nchol
+        L = hamiltonian.chol.reshape(M, M, X)
+        K = {"chol": L, "cholbar": L.transpose(1, 0, 2).conj(), "A": hamiltonian.A.reshape(M, M, X),
+             "B": hamiltonian.B.reshape(M, M, X)}
+        dev = self.device
+        d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        rH1a = np.einsum("pi,pq->iq", self.psi0a.conj(), hamiltonian.H1[0], optimize=True)
+        rH1b = np.einsum("pi,pq->iq", self.psi0b.conj(), hamiltonian.H1[1], optimize=True)
+        self._rH1a = d(rH1a.astype(np.complex128))
+        self._rH1b = d(rH1b.astype(np.complex128))
+        self._cplx = {}
+        for s_, psi in (("a", self.psi0a), ("b", self.psi0b)):
+            r = {k: np.einsum("mi,mnx->xin", psi.conj(), v, optimize=True).reshape(X, -1) for k, v in K.items()}
+            setattr(self, "_rchol" + s_, r["chol"])  # host copies, ipie's attribute names
+            setattr(self, "_rcholbar" + s_, r["cholbar"])
+            setattr(self, "_rA" + s_, r["A"])
+            setattr(self, "_rB" + s_, r["B"])
+            for k in ("chol", "cholbar", "A", "B"):
+                self._cplx[k + s_] = (d(r[k].real), d(r[k].imag))
+            R, S = r["chol"], r["cholbar"]
+            pol = []
+            for a, b in (("real", "real"), ("imag", "imag"), ("real", "imag"), ("imag", "real")):
+                P, Q = getattr(R, a), getattr(S, b)
+                pol += [P + Q, P - Q]
+            self._cplx["pol" + s_] = d(np.stack(pol))
+        self.spin_symmetric = False
         self.half_rotated = True
 
     def calculate_energy(self, system, hamiltonian):
@@ -100,8 +136,9 @@ class SingleDet:
         return ovlp
 
     def calc_force_bias(self, hamiltonian, walkers, mpi_handler=None):
-        """``vbias`` (W, X) complex (ipie ``propagation/force_bias.py:79-121``)."""
-        vbias = torch.empty(walkers.nwalkers, hamiltonian.nchol, dtype=torch.complex128, device=self.device)
+        """``vbias`` (W, nfields) complex (ipie ``propagation/force_bias.py:79-121``; complex Cholesky
+        ``:124-150``)."""
+        vbias = torch.empty(walkers.nwalkers, hamiltonian.nfields, dtype=torch.complex128, device=self.device)
         force_bias_into(hamiltonian, walkers, self, vbias)
         return vbias
 
@@ -124,6 +161,19 @@ def overlap_into(walkers, trial, ovlp_out):
 
 
 def force_bias_into(hamiltonian, walkers, trial, vbias_out):
+    if getattr(hamiltonian, "complex_chol", False):
+        # [rA . G ; rB . G]: per block the alpha term written, the beta term added
+        W, X, M = walkers.nwalkers, hamiltonian.nchol, walkers.nbasis
+        for xoff, name in ((0, "A"), (X, "B")):
+            first = True
+            for s_, g, n in (("a", walkers.Ghalfa, walkers.nup), ("b", walkers.Ghalfb, walkers.ndown)):
+                if n == 0:
+                    continue
+                re, im = trial._cplx[name + s_]
+                call("ipie_b200_force_bias_complex", ptr(re), ptr(im), ptr(g), W, X, n * M, ptr(vbias_out),
+                     2 * X, xoff, 0 if first else 1, stream())
+                first = False
+        return
     call(
         "ipie_b200_construct_force_bias_batch_single_det",
         ptr(trial._rchola), ptr(trial._rcholb), ptr(walkers.Ghalfa), ptr(walkers.Ghalfb),

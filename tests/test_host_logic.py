@@ -96,3 +96,37 @@ def test_tiled_packing_covers_the_upper_triangle_once(M):
     pairs = set(zip(i.tolist(), j.tolist()))
     assert len(pairs) == len(i)
     assert all(a <= b < M for a, b in pairs)
+
+
+def test_complex_cholesky_host_setup_matches_ipie():
+    """``Generic`` picks the complex-Cholesky class for complex vectors; its h1e_mod, the trial's
+    half rotations, the mean-field shift and the one-body propagator (all host set-up) equal ipie's."""
+    from ipie_b200 import SingleDet
+    from ipie_b200.hamiltonian import GenericComplexChol
+    from ipie_b200.propagation import construct_mean_field_shift, construct_one_body_propagator
+    from tests._systems import load
+
+    f = load("complex_uhf_m20.npz")
+    s = synthetic.generate_complex(20, (4, 3), 60, decay=30.0, seed=3, uhf=True)
+    ham = GenericComplexChol(s.h1e, s.chol, s.ecore, device="cpu")
+    assert ham.complex_chol and ham.nfields == 2 * s.nchol
+    np.testing.assert_allclose(ham.h1e_mod, f["h1e_mod"], rtol=0, atol=1e-13 * np.abs(f["h1e_mod"]).max())
+    trial = SingleDet(s.psi, (s.nup, s.ndown), s.nbasis, device="cpu")
+    trial.half_rotate(ham)
+    for k in ("rchola", "rcholb", "rcholbara", "rcholbarb", "rAa", "rAb", "rBa", "rBb"):
+        ref = f[k]
+        assert np.max(np.abs(getattr(trial, "_" + k) - ref)) <= 1e-13 * np.abs(ref).max(), k
+    for k in ("rH1a", "rH1b"):
+        ref = f[k]
+        assert np.max(np.abs(getattr(trial, "_" + k).numpy() - ref)) <= 1e-13 * np.abs(ref).max(), k
+    # the device operands: C = [A | B] parts and the polarised exchange stacks
+    C = ham.c_re.numpy() + 1j * ham.c_im.numpy()
+    assert np.array_equal(C[:, : s.nchol], ham.A) and np.array_equal(C[:, s.nchol:], ham.B)
+    pol = trial._cplx["pola"].numpy()
+    R, S = f["rchola"], f["rcholbara"]
+    np.testing.assert_allclose(pol[4], R.real + S.imag, atol=1e-13)
+    np.testing.assert_allclose(pol[7], R.imag - S.real, atol=1e-13)
+    mf = construct_mean_field_shift(ham, trial)
+    assert np.max(np.abs(mf - f["mf_shift"])) <= 1e-12 * np.abs(f["mf_shift"]).max()
+    expH1 = construct_one_body_propagator(ham, mf, 0.005)
+    assert np.max(np.abs(expH1 - f["expH1"])) <= 1e-12
