@@ -4,7 +4,8 @@ Mirror of ipie's ``AFQMC`` (``qmc/afqmc.py:297-392`` build, ``:508-633`` run):
 same arguments, same step order (reortho every ``stabilize_freq`` steps,
 propagate, weight clip, pair branch every ``pop_control_freq`` steps,
 accumulate, energy every block, eshift update).  The block estimates are
-kept in ``self.block_data`` (ipie writes them to HDF5) as rows of
+kept in ``self.block_data`` (and written to an estimator file in ipie's HDF5
+layout when ``run`` is given ``estimator_filename``) as rows of
 ``[Weight, WeightFactor, HybridEnergy, ENumer, EDenom, ETotal, E1Body, E2Body]``.
 """
 from __future__ import annotations
@@ -113,6 +114,10 @@ class AFQMC:
         row = [acc_vals[0].real, acc_vals[1].real, acc_vals[2].real, d[0].real, d[1].real, d[2].real, d[3].real,
                d[4].real]
         self.block_data.append(row)
+        if getattr(self, "estimator_filename", None):
+            from .io import write_estimates
+
+            write_estimates(self.estimator_filename, self.block_data, metadata=self.metadata())
         if self.verbose:
             print(f"{block:>17d} " + " ".join(f"{v: .16e}" for v in row))
 
@@ -160,6 +165,11 @@ class AFQMC:
             self.eshift += self.accumulators.eshift - self.eshift
 
     def run(self, walkers=None, estimator_filename=None, verbose=True, additional_estimators=None):
+        """The step loop (``afqmc.py:508-633``); with ``estimator_filename`` the block estimates are
+        also written there after every block in ipie's estimator-file layout
+        (:func:`ipie_b200.io.write_estimates`; ipie writes ``estimates.0.h5`` when no name is given,
+        this driver writes nothing then)."""
+        self.estimator_filename = estimator_filename
         self.setup_run(walkers)
         total_steps = self.params.num_steps_per_block * self.params.num_blocks
         t0 = time.time()
@@ -168,3 +178,36 @@ class AFQMC:
         torch.cuda.synchronize()
         self.timers["run"] = time.time() - t0
         return np.array(self.block_data)
+
+    def metadata(self):
+        """JSON of the run parameters (the ``metadata`` entry of the estimator file)."""
+        import json
+
+        p = self.params
+        return json.dumps({
+            "system": {"nup": int(self.walkers.nup), "ndown": int(self.walkers.ndown)},
+            "hamiltonian": {"nbasis": int(self.hamiltonian.nbasis), "nchol": int(self.hamiltonian.nchol),
+                            "complex_chol": bool(getattr(self.hamiltonian, "complex_chol", False))},
+            "qmc": {"nwalkers": p.num_walkers, "num_blocks": p.num_blocks, "num_steps": p.num_steps_per_block,
+                    "timestep": p.timestep, "num_stblz": p.num_stblz, "pop_control_freq": p.pop_control_freq,
+                    "rng_seed": p.rng_seed},
+            "propagator": {"precision": self.propagator.precision, "rng": self.propagator.rng},
+        }, indent=4)
+
+    @staticmethod
+    def build_from_hdf5(num_elec, ham_file, wfn_file, num_walkers=100, seed=None, num_steps_per_block=25,
+                        num_blocks=100, timestep=0.005, stabilize_freq=5, pop_control_freq=5, num_dets_chunk=1,
+                        num_dets_for_trial_props=100, pack_cholesky=True, verbose=True, **kwargs):
+        """ipie's ``AFQMC.build_from_hdf5`` (``qmc/afqmc.py:394-475``): Hamiltonian and trial from
+        files in ipie's or QMCPACK's HDF5 layouts (:mod:`ipie_b200.io`), then :meth:`build` with the
+        electron counts read from the wavefunction file; ``kwargs`` go to :meth:`build`."""
+        from .io import get_hamiltonian, get_trial_wavefunction
+
+        ham = get_hamiltonian(ham_file, verbose=verbose, pack_chol=pack_cholesky)
+        trial = get_trial_wavefunction(num_elec, ham.nbasis, wfn_file, ndet_chunks=num_dets_chunk,
+                                       ndets_props=num_dets_for_trial_props, verbose=verbose)
+        trial.half_rotate(ham)
+        return AFQMC.build(trial.nelec, ham, trial, num_walkers=num_walkers, seed=seed,
+                           num_steps_per_block=num_steps_per_block, num_blocks=num_blocks, timestep=timestep,
+                           stabilize_freq=stabilize_freq, pop_control_freq=pop_control_freq, verbose=verbose,
+                           **kwargs)
