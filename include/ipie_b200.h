@@ -292,6 +292,28 @@ int ipie_b200_construct_vhs_mixed(const void* cp_hi, const void* cp_lo, const in
                                   int f16_planes, double v_scale, void* v_re_hi, void* v_re_lo, void* v_im_hi,
                                   void* v_im_lo, unsigned int* status, void* stream);
 
+/* Number of 16 x 16 orbital-pair blocks (I <= J) of the block-tiled VHS operand:
+ * nb (nb + 1) / 2 with nb = ceil(M / 16); the operand has 256 rows per block. */
+int ipie_b200_vhs_blocks(int M);
+
+/* Block-tiled Cholesky operand of ipie_b200_construct_vhs_blocks: row r (of
+ * 256 * ipie_b200_vhs_blocks(M)) = packed Cholesky row rowmap[r] (-1: zeros) x scale,
+ * split into binary16 head/remainder (R, Xp), Xp = X rounded up to 8.  Block k = (I, J),
+ * row-major over I <= J; its row 16 a + b is the pair (16 I + a, 16 J + b) (a zero row
+ * when either index is >= M). */
+int ipie_b200_vhs_block_pack(const double* chol_packed, const int* rowmap, int M, int X, double scale, void* cb_hi,
+                             void* cb_lo, void* stream);
+
+/* The f16_planes output of ipie_b200_construct_vhs_mixed (same values and layout, and the
+ * pad columns [M, Mp) written with zeros) from the block-tiled Cholesky operand: the
+ * product runs with the fields as its left operand, so that a thread holds a 16 x 8 half
+ * block of one walker's plane and writes it as 16-byte runs in both orientations.
+ * flags bit 0: persistent CTAs.  replaces (mixed form): propagation/phaseless_generic.py:66-97. */
+int ipie_b200_construct_vhs_blocks(const void* cb_hi, const void* cb_lo, int M, int X, const void* xs_hi,
+                                   const void* xs_lo, int W, double sqrt_dt, double cb_scale, double v_scale,
+                                   void* v_re_hi, void* v_re_lo, void* v_im_hi, void* v_im_lo, int flags,
+                                   unsigned int* status, void* stream);
+
 /* 1 when ipie_b200_propagate_orbitals_mixed16 takes this spin block (M <= 256, 1 <= N <= 32). */
 int ipie_b200_orbital_chain16_fits(int M, int N);
 

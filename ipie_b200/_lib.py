@@ -43,6 +43,9 @@ SIGNATURES = {
     "ipie_b200_field_shift_mixed": [P, P, P, I, I, D, D, P, P, P, P, P, P],
     "ipie_b200_construct_vhs_mixed": [P, P, P, P, I, I, P, P, I, D, D, I, D, P, P, P, P, P, P],
     "ipie_b200_orbital_chain16_fits": [I, I],
+    "ipie_b200_vhs_blocks": [I],
+    "ipie_b200_vhs_block_pack": [P, P, I, I, D, P, P, P],
+    "ipie_b200_construct_vhs_blocks": [P, P, I, I, P, P, I, D, D, D, P, P, P, P, I, P, P],
     "ipie_b200_propagate_orbitals_mixed16": [P, P, D, P, P, P, P, D, P, P, I, I, I, I, P, P],
     "ipie_b200_propagate_orbitals_mixed": [P, P, I, P, P, P, P, P, P, P, I, I, I, I, P, P],
     "ipie_b200_rchol_pad_split": [P, I, I, I, D, P, P, P],

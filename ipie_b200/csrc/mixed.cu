@@ -399,6 +399,101 @@ struct EpiVHSF16 {
   }
 };
 
+// VHS for the FP16 orbital chain, block-tiled: the product runs transposed -- rows (w, c) of
+// the fields (c = re/im), columns the Cholesky rows of one 16 x 16 block of orbital pairs
+// (i, j) = (16 I + a, 16 J + b), I <= J, row-major in the block (a diagonal block carries all
+// 256 pairs, both triangles) -- so that a thread holds one walker's re or im part of a whole
+// block half (rows a = 8g .. 8g + 7 for column group g).  It writes them as 16-byte runs of
+// 8 halves: its 8 rows i, columns 16 J .. 16 J + 15 (two runs), and for an off-diagonal block
+// the transposed rows j = 16 J + b, columns 16 I + 8g .. + 7; every run starts on a multiple of
+// 8 halves of a row of ld (a multiple of 8) halves, so each store is 16-byte aligned and whole
+// 32-byte sectors are written by one or two neighbouring runs.  V = i sqrt(dt) S: the re part of
+// S (c = 0) gives the imaginary planes, the im part (c = 1) the real planes.  Rows i >= M are
+// skipped; columns in [M, ld) receive the zero products of the zero Cholesky rows.
+__device__ __forceinline__ void pack8_f16(const float* x, float s, uint4& hi, uint4& lo) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float y0 = x[2 * k] * s, y1 = x[2 * k + 1] * s;
+    const __half a0 = __float2half_rn(y0), a1 = __float2half_rn(y1);
+    const __half b0 = __float2half_rn(y0 - __half2float(a0)), b1 = __float2half_rn(y1 - __half2float(a1));
+    h[k] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
+    l[k] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
+  }
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+struct EpiVHSBlock {
+  __half *re_hi, *re_lo, *im_hi, *im_lo;
+  int M, ld, W, nb;  // nb: 16-orbital blocks per side
+  float f;           // sqrt(dt) v_scale / (operand scales)
+  __device__ __forceinline__ void operator()(int, int row, int col0, const float* v, uint8_t*) const {
+    const int w = row >> 1, c = row & 1;
+    if (w >= W) return;
+    int blk = col0 >> 8, I = 0;  // tile = block index, row-major over I <= J
+    while (blk >= nb - I) {
+      blk -= nb - I;
+      ++I;
+    }
+    const int J = I + blk;
+    const int g = (col0 >> 7) & 1;
+    __half* hi = c ? re_hi : im_hi;
+    __half* lo = c ? re_lo : im_lo;
+    const float s = c ? -f : f;
+    const size_t base = (size_t)w * M * ld;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int i = 16 * I + 8 * g + a;
+      if (i < M) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j0 = 16 * J + 8 * h;
+          if (j0 < ld) {
+            uint4 ph, pl;
+            pack8_f16(v + a * 16 + 8 * h, s, ph, pl);
+            const size_t o = base + (size_t)i * ld + j0;
+            *reinterpret_cast<uint4*>(hi + o) = ph;
+            *reinterpret_cast<uint4*>(lo + o) = pl;
+          }
+        }
+      }
+    }
+    if (I == J) return;
+#pragma unroll
+    for (int b = 0; b < 16; ++b) {
+      const int j = 16 * J + b;
+      if (j < M) {
+        float t[8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) t[a] = v[a * 16 + b];
+        uint4 ph, pl;
+        pack8_f16(t, s, ph, pl);
+        const size_t o = base + (size_t)j * ld + 16 * I + 8 * g;
+        *reinterpret_cast<uint4*>(hi + o) = ph;
+        *reinterpret_cast<uint4*>(lo + o) = pl;
+      }
+    }
+  }
+};
+
+// Rows of the block-tiled Cholesky operand gathered from the packed one: row r takes packed
+// row rowmap[r] (or zeros for -1), scaled and split into binary16 head and remainder; (R, ldx).
+__global__ void vhs_block_pack_kernel(const double* __restrict__ cp, const int* __restrict__ rowmap, long long R,
+                                      int X, int ldx, double scale, __half* __restrict__ hi, __half* __restrict__ lo) {
+  const long long n = R * ldx;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / ldx;
+    const int x = (int)(e - r * ldx);
+    const int p = rowmap[r];
+    const double val = (p >= 0 && x < X) ? cp[(long long)p * X + x] : 0.0;
+    __half h, l;
+    split_f16(val, scale, h, l);
+    hi[e] = h;
+    lo[e] = l;
+  }
+}
+
 // One Taylor term / one-body factor on the orbitals of walker z (one spin):
 // accumulators (columns c*N + n, c = re/im of the right operand):
 //   one-body (NA = 1):  U = E . T
@@ -782,6 +877,34 @@ cudaError_t mixed_vhs(const void* cp_hi, const void* cp_lo, const int* ii, const
   return launch_umma<BN, 1, 3, 2, EpiVHSSplit<128>, KIND_F16>(maps, X, 0, 0, grid, epi, status, st, false, false);
 }
 
+int vhs_blocks(int M) {
+  const int nb = (M + 15) / 16;
+  return nb * (nb + 1) / 2;
+}
+
+// The block-tiled VHS (EpiVHSBlock): fields (2W, X) as the left operand, the block-tiled
+// Cholesky (vhs_blocks(M) * 256, X) as the right one, 128 x 256 tiles with the walker tiles
+// fastest so that each Cholesky block is read from DRAM once while the fields stay in L2.
+cudaError_t mixed_vhs_blocks(const void* cb_hi, const void* cb_lo, int X, int M, const void* xs_hi, const void* xs_lo,
+                             int W, double sqrt_dt, double cb_scale, double v_scale, void* re_hi, void* re_lo,
+                             void* im_hi, void* im_lo, int persistent, unsigned* status, cudaStream_t st) {
+  constexpr int BN = 256;
+  const int ldx = f16_ld(X);
+  const int nblk = vhs_blocks(M);
+  GemmMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  cudaError_t e;
+  if ((e = make_map_f16(&maps.a_hi[0], xs_hi, 2LL * W, X, ldx, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_lo[0], xs_lo, 2LL * W, X, ldx, kBM)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_hi, cb_hi, 256LL * nblk, X, ldx, BN)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_lo, cb_lo, 256LL * nblk, X, ldx, BN)) != cudaSuccess) return e;
+  dim3 grid(nblk, (2 * W + kBM - 1) / kBM, 1);
+  using H = __half*;
+  const EpiVHSBlock epi{H(re_hi), H(re_lo), H(im_hi), H(im_lo), M, f16_ld(M), W, (M + 15) / 16,
+                        (float)(sqrt_dt / (cb_scale * kFieldScaleF16) * v_scale)};
+  return launch_umma<BN, 1, 3, 2, EpiVHSBlock, KIND_F16>(maps, X, 0, 0, grid, epi, status, st, true, persistent != 0);
+}
+
 // Orbital update of one spin block: phi_out = E exp(V) E phi_in (Taylor order nmax),
 // every product on the tensor cores as 3-pass TF32; phi accumulates in FP64.
 // E enters as its difference from the identity: (E - I) hi/lo (M, Mp) fp32 with Mp % 4 == 0; V: planar (W, M, M) hi/lo;
@@ -873,6 +996,31 @@ extern "C" int ipie_b200_construct_vhs_mixed(const void* cp_hi, const void* cp_l
   return (int)umma::mixed_vhs(cp_hi, cp_lo, idx_i, idx_j, M * (M + 1) / 2, X, M, xs_hi, xs_lo, W, sqrt_dt, cp_scale,
                               f16_planes, v_scale, v_re_hi, v_re_lo, v_im_hi, v_im_lo, status,
                               reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ipie_b200_vhs_blocks(int M) { return M > 0 ? umma::vhs_blocks(M) : 0; }
+
+extern "C" int ipie_b200_vhs_block_pack(const double* chol_packed, const int* rowmap, int M, int X, double scale,
+                                        void* cb_hi, void* cb_lo, void* stream) {
+  if (M <= 0 || X <= 0 || !(scale > 0.0)) return (int)cudaErrorInvalidValue;
+  const long long R = 256LL * umma::vhs_blocks(M);
+  const long long n = R * f16_ld(X);
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  umma::vhs_block_pack_kernel<<<(unsigned)blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      chol_packed, rowmap, R, X, f16_ld(X), scale, reinterpret_cast<__half*>(cb_hi), reinterpret_cast<__half*>(cb_lo));
+  note_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int ipie_b200_construct_vhs_blocks(const void* cb_hi, const void* cb_lo, int M, int X, const void* xs_hi,
+                                              const void* xs_lo, int W, double sqrt_dt, double cb_scale,
+                                              double v_scale, void* v_re_hi, void* v_re_lo, void* v_im_hi,
+                                              void* v_im_lo, int flags, unsigned int* status, void* stream) {
+  if (M <= 0 || X <= 0 || W <= 0 || !(cb_scale > 0.0) || !(v_scale > 0.0)) return (int)cudaErrorInvalidValue;
+  return (int)umma::mixed_vhs_blocks(cb_hi, cb_lo, X, M, xs_hi, xs_lo, W, sqrt_dt, cb_scale, v_scale, v_re_hi,
+                                     v_re_lo, v_im_hi, v_im_lo, flags & 1, status,
+                                     reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int ipie_b200_orbital_chain16_fits(int M, int N) { return umma::orbital_chain16_fits(M, N) ? 1 : 0; }

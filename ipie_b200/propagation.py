@@ -141,6 +141,7 @@ class PhaselessGeneric:
         self.ws = None
         self.timer = _NoTimer()
         self.fused = True  # one launch per spin for one-body + exp(VHS) + one-body
+        self.vhs_flags = 1  # block-tiled mixed VHS: bit 0 = persistent CTAs (1.41 vs 1.50 ms at c2)
         # "fp64": the plain form (ipie's arithmetic); "mixed": force bias, VHS and the orbital
         # update as 3-pass TF32 tensor-core products, FP64 everywhere else
         if precision not in ("fp64", "mixed"):
@@ -230,9 +231,35 @@ class PhaselessGeneric:
             l1 = float(hamiltonian.chol_packed.abs().sum(1).max().item())
             vbound = self.sqrt_dt * l1 * (9.0 + float(self.fbbound))
             self.v_scale = 2.0 ** (14 - math.frexp(vbound)[1]) if vbound > 0 else 1.0
+            # the chain's VHS planes come from the block-tiled product (16 x 16 pair blocks)
+            self.cb_hi, self.cb_lo = self._vhs_block_operand(hamiltonian, Xp)
         self.e_hi = torch.empty(2, M, M, dtype=f32, device=dev)
         self.e_lo = torch.empty(2, M, M, dtype=f32, device=dev)
         call("ipie_b200_split_tf32", ptr(e), ptr(self.e_hi), ptr(self.e_lo), e.numel(), stream())
+
+    def _vhs_block_operand(self, hamiltonian, Xp):
+        """Cholesky rows of the block-tiled VHS product: for every 16 x 16 block (I <= J) of
+        orbital pairs, row-major, the packed row of (16 I + a, 16 J + b) (zeros past M), x cp_scale
+        in binary16 head/remainder (``ipie_b200_vhs_block_pack``)."""
+        from .hamiltonian import tiled_triu_indices
+
+        M = hamiltonian.nbasis
+        ti, tj = tiled_triu_indices(M)
+        pidx = np.full((M + 16, M + 16), -1, dtype=np.int32)
+        pidx[ti, tj] = np.arange(len(ti), dtype=np.int32)
+        pidx[tj, ti] = np.arange(len(ti), dtype=np.int32)
+        nb = (M + 15) // 16
+        assert lib().ipie_b200_vhs_blocks(M) == nb * (nb + 1) // 2
+        a = np.arange(16)
+        rows = [pidx[16 * I + a[:, None], 16 * J + a[None, :]].ravel() for I in range(nb) for J in range(I, nb)]
+        rowmap = torch.from_numpy(np.ascontiguousarray(np.concatenate(rows))).to(self.device)
+        R = rowmap.numel()
+        hi = torch.empty(R, Xp, dtype=torch.float16, device=self.device)
+        lo = torch.empty(R, Xp, dtype=torch.float16, device=self.device)
+        call("ipie_b200_vhs_block_pack", ptr(hamiltonian.chol_packed), ptr(rowmap), M, hamiltonian.nchol,
+             self.cp_scale, ptr(hi), ptr(lo), stream())
+        torch.cuda.current_stream().synchronize()
+        return hi, lo
 
     # ------------------------------------------------------------- the step
     def propagate_walkers_one_body(self, walkers):
@@ -405,10 +432,14 @@ class PhaselessGeneric:
         self.timer.stop("field_shift")
         self.timer.start("vhs")
         v = ws.v_planar
-        call("ipie_b200_construct_vhs_mixed", ptr(self.cp_hi), ptr(self.cp_lo), ptr(hamiltonian.sym_idx_i),
-             ptr(hamiltonian.sym_idx_j), M, X, ptr(ws.xs_hi), ptr(ws.xs_lo), W, self.sqrt_dt, self.cp_scale,
-             int(self.chain16), self.v_scale if self.chain16 else 0.0, ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]),
-             ptr(walkers.status), stream())
+        if self.chain16:
+            call("ipie_b200_construct_vhs_blocks", ptr(self.cb_hi), ptr(self.cb_lo), M, X, ptr(ws.xs_hi),
+                 ptr(ws.xs_lo), W, self.sqrt_dt, self.cp_scale, self.v_scale, ptr(v[0]), ptr(v[1]), ptr(v[2]),
+                 ptr(v[3]), self.vhs_flags, ptr(walkers.status), stream())
+        else:
+            call("ipie_b200_construct_vhs_mixed", ptr(self.cp_hi), ptr(self.cp_lo), ptr(hamiltonian.sym_idx_i),
+                 ptr(hamiltonian.sym_idx_j), M, X, ptr(ws.xs_hi), ptr(ws.xs_lo), W, self.sqrt_dt, self.cp_scale, 0,
+                 0.0, ptr(v[0]), ptr(v[1]), ptr(v[2]), ptr(v[3]), ptr(walkers.status), stream())
         self.timer.stop("vhs")
         self.timer.start("orbitals")
         for s_, (phi_name, tmp_name, n) in enumerate((("phia", "phia_tmp", walkers.nup),

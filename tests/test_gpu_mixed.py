@@ -82,6 +82,45 @@ def test_mixed_vhs_3pass():
     walkers.check_status()
 
 
+@pytest.mark.parametrize("M,X,W,persistent", [(64, 128, 24, 0), (108, 216, 70, 1), (76, 152, 130, 0),
+                                              (200, 400, 9, 1), (200, 400, 200, 0)])
+def test_mixed_vhs_blocks(M, X, W, persistent):
+    """The block-tiled VHS (16 x 16 pair blocks, fields as the left operand) writes the same
+    binary16 planes as the packed-pair product, with the pad columns zero; M = 108 and 76 end on
+    partial blocks, W = 70 and 130 on partial walker tiles."""
+    from ipie_b200 import synthetic
+    from ipie_b200._lib import call, ptr, stream
+
+    s = synthetic.generate(M, (8, 8), X, decay=30.0, seed=23, uhf=True, chol_scale="stable")
+    ham, trial, walkers, prop, pm = _mixed_objects(s, W)
+    assert pm.chain16
+    ws = pm._workspace(walkers, ham)
+    rng = np.random.default_rng(7)
+    vb = dev(0.3 * (rng.normal(size=(W, X)) + 1j * rng.normal(size=(W, X))))
+    xi = dev(rng.normal(size=(W, X)))
+    xs = torch.empty(X, W, dtype=torch.complex128, device="cuda")
+    call("ipie_b200_field_shift_mixed", ptr(vb), ptr(xi), ptr(pm.mf_shift_dev), W, X, pm.sqrt_dt, 1.0, ptr(xs),
+         ptr(ws.xs_hi), ptr(ws.xs_lo), ptr(ws.cmf), ptr(ws.cfb), stream())
+    ref = prop.construct_VHS(ham, xs)
+    Mp = (M + 7) // 8 * 8
+    planes = [torch.full((W, M, Mp), float("nan"), dtype=torch.float16, device="cuda") for _ in range(4)]
+    call("ipie_b200_construct_vhs_blocks", ptr(pm.cb_hi), ptr(pm.cb_lo), M, X, ptr(ws.xs_hi), ptr(ws.xs_lo), W,
+         pm.sqrt_dt, pm.cp_scale, pm.v_scale, *(ptr(v) for v in planes), persistent, ptr(walkers.status), stream())
+    old = [torch.zeros(W, M, Mp, dtype=torch.float16, device="cuda") for _ in range(4)]
+    call("ipie_b200_construct_vhs_mixed", ptr(pm.cp_hi), ptr(pm.cp_lo), ptr(ham.sym_idx_i), ptr(ham.sym_idx_j), M, X,
+         ptr(ws.xs_hi), ptr(ws.xs_lo), W, pm.sqrt_dt, pm.cp_scale, 1, pm.v_scale, *(ptr(v) for v in old),
+         ptr(walkers.status), stream())
+    for k in range(4):
+        assert not torch.isnan(planes[k]).any(), k  # every element written, pad columns included
+        assert torch.count_nonzero(planes[k][:, :, M:]) == 0
+    got = ((planes[0].double() + planes[1].double()) + 1j * (planes[2].double() + planes[3].double()))[:, :, :M]
+    assert rel(got / pm.v_scale, ref) < 1e-5
+    prev = ((old[0].double() + old[1].double()) + 1j * (old[2].double() + old[3].double()))[:, :, :M]
+    # the same FP32 sums up to the order of the tensor cores' additions
+    assert rel(got, prev) < 1e-6
+    walkers.check_status()
+
+
 @pytest.mark.parametrize("M,N,W", [(64, 8, 6), (200, 32, 6), (108, 15, 6), (128, 16, 5), (64, 4, 300),
                                    (200, 13, 5), (256, 24, 4), (260, 4, 3)])
 def test_mixed_orbital_update_3pass(M, N, W):
