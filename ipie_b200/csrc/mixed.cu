@@ -60,19 +60,24 @@ cudaError_t make_map(CUtensorMap* m, const float* base, long long rows, long lon
 }
 
 // 2-D K-major FP16 operand: `rows` rows of `k` halves, row stride `ld` halves (ld % 8 == 0),
-// tiles of box_rows x 64 loaded 128B-swizzled; out-of-range elements read as 0.
-cudaError_t make_map_f16(CUtensorMap* m, const void* base, long long rows, long long k, long long ld, int box_rows) {
+// tiles of box_rows x 64 loaded 128B-swizzled (k32: box_rows x 32, 64B-swizzled, the tiles of
+// KIND_F16_K32); out-of-range elements read as 0.
+cudaError_t make_map_f16(CUtensorMap* m, const void* base, long long rows, long long k, long long ld, int box_rows,
+                         bool k32) {
   auto fn = encode_fn();
   if (fn == nullptr) return cudaErrorNotSupported;
   if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 8) || rows <= 0 || k <= 0) return cudaErrorInvalidValue;
   cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-  cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+  cuuint32_t box[2] = {k32 ? 32u : 64u, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, k32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+cudaError_t make_map_f16(CUtensorMap* m, const void* base, long long rows, long long k, long long ld, int box_rows) {
+  return make_map_f16(m, base, rows, k, ld, box_rows, false);
 }
 
 // 3-D batched K-major FP16 operand: `batch` matrices of `rows` x `k` halves (row stride ld
@@ -158,7 +163,7 @@ template <int BN, int NA, int NSPLIT, int STAGES, class Epi, int KIND = KIND_TF3
 cudaError_t launch_umma(const GemmMaps& maps, int K, int a_rows_per_batch, int b_rows_per_batch, dim3 tiles, Epi epi,
                         unsigned* status, cudaStream_t st, bool m_fast = false, bool persistent = true,
                         int m_group = 0) {
-  using S = GemmShape<BN, NA, NSPLIT, STAGES, EpiSmem<Epi>::value>;
+  using S = GemmShape<BN, NA, NSPLIT, STAGES, EpiSmem<Epi>::value, KIND>;
   auto kern = umma_gemm_kernel<BN, NA, NSPLIT, STAGES, Epi, KIND>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_BYTES);
   if (e != cudaSuccess) return e;
@@ -894,15 +899,17 @@ cudaError_t mixed_vhs_blocks(const void* cb_hi, const void* cb_lo, int X, int M,
   GemmMaps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = make_map_f16(&maps.a_hi[0], xs_hi, 2LL * W, X, ldx, kBM)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.a_lo[0], xs_lo, 2LL * W, X, ldx, kBM)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.b_hi, cb_hi, 256LL * nblk, X, ldx, BN)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.b_lo, cb_lo, 256LL * nblk, X, ldx, BN)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_hi[0], xs_hi, 2LL * W, X, ldx, kBM, true)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.a_lo[0], xs_lo, 2LL * W, X, ldx, kBM, true)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_hi, cb_hi, 256LL * nblk, X, ldx, BN, true)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.b_lo, cb_lo, 256LL * nblk, X, ldx, BN, true)) != cudaSuccess) return e;
   dim3 grid(nblk, (2 * W + kBM - 1) / kBM, 1);
   using H = __half*;
   const EpiVHSBlock epi{H(re_hi), H(re_lo), H(im_hi), H(im_lo), M, f16_ld(M), W, (M + 15) / 16,
                         (float)(sqrt_dt / (cb_scale * kFieldScaleF16) * v_scale)};
-  return launch_umma<BN, 1, 3, 2, EpiVHSBlock, KIND_F16>(maps, X, 0, 0, grid, epi, status, st, true, persistent != 0);
+  // 64-byte K rows: four 48 KB stages instead of two of 96 KB, so that three are in flight
+  return launch_umma<BN, 1, 3, 4, EpiVHSBlock, KIND_F16_K32>(maps, X, 0, 0, grid, epi, status, st, true,
+                                                            persistent != 0);
 }
 
 // Orbital update of one spin block: phi_out = E exp(V) E phi_in (Taylor order nmax),

@@ -154,6 +154,22 @@ __device__ __forceinline__ uint64_t desc_kmajor_sw128(const void* tile) {
   d |= (uint64_t)2 << 61;
   return d;
 }
+// The same for 64-byte rows stored 64B-swizzled (layout 4): 8-row groups 512 B apart.
+__device__ __forceinline__ uint64_t desc_kmajor_sw64(const void* tile) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_u32(tile) >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(512 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)4 << 61;
+  return d;
+}
+// descriptor of a tile of operand kind KIND (KIND_F16_K32 = 2: 64-byte rows; the others 128-byte)
+template <int KIND>
+__device__ __forceinline__ uint64_t desc_kmajor(const void* tile) {
+  if constexpr (KIND == 2) return desc_kmajor_sw64(tile);
+  else return desc_kmajor_sw128(tile);
+}
 // Instruction descriptor: kind::tf32, D fp32, A/B tf32, both K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool neg_a = false, bool neg_b = false) {
   return (1u << 4)                       // D format f32

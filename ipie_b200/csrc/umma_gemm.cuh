@@ -52,11 +52,13 @@ constexpr int kBK = 32;  // fp32 per 128-byte row
 // Operand kinds: a stage holds 128-byte K rows of either
 constexpr int KIND_TF32 = 0;  // fp32 words read as TF32 (32 per row, kind::tf32)
 constexpr int KIND_F16 = 1;   // FP16 (64 per row, kind::f16)
+constexpr int KIND_F16_K32 = 2;  // FP16, 32 per 64-byte row (64B swizzle): half-size stages, twice as many
 __host__ __device__ constexpr int kblock_elems(int kind) { return kind == KIND_F16 ? 64 : 32; }
+__host__ __device__ constexpr int row_bytes(int kind) { return kind == KIND_F16_K32 ? 64 : 128; }
+// k-blocks accumulated in TMEM before a drain: 128 FP16 / 64 TF32 elements of K either way
+__host__ __device__ constexpr int chunk_kb(int kind) { return kind == KIND_F16_K32 ? 4 : 2; }
 
 __host__ __device__ constexpr int tmem_cols_for(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : n <= 256 ? 256 : 512; }
-
-constexpr int kChunkKB = 2;  // k-blocks (of 32) accumulated in TMEM before a drain
 
 // Epilogue warps: one group of 4 (the four TMEM lane quarters) per 128 accumulator
 // columns; then a producer and an MMA warp.
@@ -127,10 +129,10 @@ struct EpiSmem<Epi, decltype((void)Epi::kSmemBytes)> {
   static constexpr int value = Epi::kSmemBytes;
 };
 
-template <int BN, int NA, int NSPLIT, int STAGES, int EPI_SMEM = 0>
+template <int BN, int NA, int NSPLIT, int STAGES, int EPI_SMEM = 0, int KIND = KIND_TF32>
 struct GemmShape {
-  static constexpr int A_TILE = kBM * kBK * 4;
-  static constexpr int B_TILE = BN * kBK * 4;
+  static constexpr int A_TILE = kBM * row_bytes(KIND);
+  static constexpr int B_TILE = BN * row_bytes(KIND);
   static constexpr int NAT = NA * (NSPLIT == 3 ? 2 : 1);
   static constexpr int NBT = NSPLIT == 3 ? 2 : 1;
   static constexpr int STAGE_BYTES = NAT * A_TILE + NBT * B_TILE;
@@ -152,7 +154,7 @@ template <int BN, int NA, int NSPLIT, int STAGES, class Epi, int KIND = KIND_TF3
 __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
     umma_gemm_kernel(const __grid_constant__ GemmMaps maps, int K, int a_rows_per_batch, int b_rows_per_batch,
                      TileOrder order, Epi epi, unsigned* status) {
-  using S = GemmShape<BN, NA, NSPLIT, STAGES, EpiSmem<Epi>::value>;
+  using S = GemmShape<BN, NA, NSPLIT, STAGES, EpiSmem<Epi>::value, KIND>;
   using R = GemmRoles<NA, BN>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -183,9 +185,11 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  constexpr int KB = kblock_elems(KIND);  // K elements per k-block (one 128-byte row)
+  constexpr int KB = kblock_elems(KIND);  // K elements per k-block (one row of the tile)
+  constexpr int KK = row_bytes(KIND) / 32;  // MMAs per k-block: 32 bytes of K each
+  constexpr int CKB = chunk_kb(KIND);
   const int nk = (K + KB - 1) / KB;
-  const int nchunks = (nk + kChunkKB - 1) / kChunkKB;
+  const int nchunks = (nk + CKB - 1) / CKB;
   const int ntiles = order.count();
 
   if (warp == R::kProducerWarp) {
@@ -225,13 +229,13 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
     __syncwarp();
   } else if (warp == R::kMmaWarp) {
     if (lane == 0) {
-      constexpr uint32_t idesc = KIND == KIND_F16 ? idesc_f16(kBM, BN) : idesc_tf32(kBM, BN);
+      constexpr uint32_t idesc = KIND != KIND_TF32 ? idesc_f16(kBM, BN) : idesc_tf32(kBM, BN);
       uint32_t g = 0, c = 0;  // stage uses and chunks so far (all tiles)
       bool ok = true;
       for (int l = blockIdx.x; l < ntiles && ok; l += gridDim.x) {
         for (int kb = 0; kb < nk; ++kb, ++g) {
-          const bool first = (kb % kChunkKB) == 0;
-          const bool last = (kb % kChunkKB) == kChunkKB - 1 || kb == nk - 1;
+          const bool first = (kb % CKB) == 0;
+          const bool last = (kb % CKB) == CKB - 1 || kb == nk - 1;
           const uint32_t buf = c & 1;
           if (first && c >= 2 && !mbar_wait(&cempty[buf], ((c >> 1) - 1) & 1, abort_flag, status)) {
             ok = false;
@@ -244,19 +248,19 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
           }
           tc_fence_after();
           uint8_t* st = smem + s * S::STAGE_BYTES;
-          const uint64_t db_hi = desc_kmajor_sw128(st + S::NAT * S::A_TILE);
-          const uint64_t db_lo = desc_kmajor_sw128(st + S::NAT * S::A_TILE + S::B_TILE);
+          const uint64_t db_hi = desc_kmajor<KIND>(st + S::NAT * S::A_TILE);
+          const uint64_t db_lo = desc_kmajor<KIND>(st + S::NAT * S::A_TILE + S::B_TILE);
 #pragma unroll
           for (int a = 0; a < NA; ++a) {
-            const uint64_t da_hi = desc_kmajor_sw128(st + (a * (S::NAT / NA)) * S::A_TILE);
-            const uint64_t da_lo = desc_kmajor_sw128(st + (a * 2 + 1) * S::A_TILE);
+            const uint64_t da_hi = desc_kmajor<KIND>(st + (a * (S::NAT / NA)) * S::A_TILE);
+            const uint64_t da_lo = desc_kmajor<KIND>(st + (a * 2 + 1) * S::A_TILE);
             const uint32_t d = tmem + (uint32_t)(buf * S::BUF_COLS + a * BN);
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
+            for (int kk = 0; kk < KK; ++kk) {
               // K steps wholly past K multiply TMA's zero fill: skip them
-              if (kk > 0 && kb * KB + kk * (KB / 4) >= K) break;
+              if (kk > 0 && kb * KB + kk * (KB / KK) >= K) break;
               // 32 bytes of K per MMA (8 tf32 or 16 fp16): advance the start address by 2 (16-byte units)
-              if constexpr (KIND == KIND_F16) {
+              if constexpr (KIND != KIND_TF32) {
                 mma_f16(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
                 if (NSPLIT == 3) {
                   mma_f16(d, da_hi + 2 * kk, db_lo + 2 * kk, idesc, 1u);
