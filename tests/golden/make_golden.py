@@ -2,7 +2,7 @@
 
 Run from the repository root with ipie's source tree available:
 
-    python tests/golden/make_golden.py /path/to/ipie-checkout [ad|pop|complex]
+    python tests/golden/make_golden.py /path/to/ipie-checkout [ad|pop|complex|ghf]
 
 ipie needs ``plum`` and ``h5py``, which are absent here; the small stand-ins in
 ``_ref_shims/`` are put first on ``sys.path``.  mpi4py is absent, so ipie
@@ -326,7 +326,75 @@ def complex_fixture(name, sysw, nwalkers, seed, nsteps=3):
     print("wrote", name)
 
 
+def ghf_fixture(name, sysw, nwalkers, seed, nsteps=3):
+    """ipie's GHF path (``SingleDetGHF``, ``GHFWalkers``): case "b" (block) builds the trial and
+    walkers from UHF ones, case "m" (mixed) a complex spin-mixed determinant; each with per-kernel
+    outputs on perturbed walkers (all four spin blocks perturbed), a 3-step walk with ipie's own
+    draws and a reorthogonalisation."""
+    from ipie.estimators.energy import local_energy
+    from ipie.trial_wavefunction.single_det_ghf import SingleDetGHF
+    from ipie.walkers.ghf_walkers import GHFWalkers
+
+    ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
+    M, na, nb = sysw.nbasis, sysw.nup, sysw.ndown
+    N = na + nb
+    W = nwalkers
+    rng = np.random.default_rng(seed)
+    out = {}
+    for case in ("b", "m"):
+        uhf = SingleDet(sysw.psi.copy(), (na, nb), M)
+        uhf.half_rotate(ham)
+        if case == "b":
+            trial = SingleDetGHF(uhf)
+            uw = UHFWalkersTrial(uhf, sysw.init.copy(), na, nb, M, W, MPIHandler())
+            uw.build(uhf)
+            walkers = GHFWalkers(uw)
+        else:
+            import scipy.linalg
+
+            base = np.zeros((2 * M, N))
+            base[:M, :na] = sysw.psi[:, :na]
+            base[M:, na:] = sysw.psi[:, na:]
+            A = rng.normal(size=(2 * M, 2 * M)) + 1j * rng.normal(size=(2 * M, 2 * M))
+            U = scipy.linalg.expm(0.08 * (A - A.conj().T))
+            psi = U @ base
+            out["m_psi"] = psi
+            trial = SingleDetGHF(psi.copy(), (na, nb), M)
+            walkers = GHFWalkers(psi.copy(), na, nb, M, W, MPIHandler())
+        walkers.build(trial)
+        prop = PhaselessGeneric(0.005)
+        prop.build(ham, trial, walkers, MPIHandler())
+        phi = walkers.phi + 0.15 * (rng.normal(size=walkers.phi.shape) + 1j * rng.normal(size=walkers.phi.shape))
+        walkers.phi = phi.copy()
+        out[case + "_phi_in"] = phi
+        out[case + "_ovlp"] = trial.calc_greens_function(walkers)
+        out[case + "_G"] = walkers.G.copy()
+        out[case + "_vbias"] = trial.calc_force_bias(ham, walkers, MPIHandler())
+        out[case + "_energy"] = local_energy(Generic((na, nb)), ham, walkers, trial)
+        out[case + "_mf_shift"] = prop.mf_shift
+        out[case + "_expH1"] = prop.expH1
+        walkers.ovlp = out[case + "_ovlp"].copy()
+        np.random.seed(seed + (1 if case == "b" else 2))
+        for step in range(nsteps):
+            prop.propagate_walkers(walkers, ham, trial, -3.0 if step else 0.0)
+        out[case + "_walk_weight"] = np.array(walkers.weight)
+        out[case + "_walk_ovlp"] = np.array(walkers.ovlp)
+        out[case + "_walk_phi"] = np.array(walkers.phi)
+        out[case + "_walk_hybrid_energy"] = np.array(walkers.hybrid_energy)
+        out[case + "_reortho_detR"] = np.array(walkers.reortho())
+        out[case + "_reortho_phi"] = np.array(walkers.phi)
+        out[case + "_reortho_ovlp"] = np.array(walkers.ovlp)
+    out["chol_checksum"] = checksum(sysw.chol)
+    out["psi_checksum"] = checksum(sysw.psi)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "ghf":
+        ghf = synthetic.generate(14, (4, 3), 40, decay=30.0, seed=8, uhf=True, chol_scale="stable")
+        ghf_fixture("ghf_m14.npz", ghf, nwalkers=5, seed=31)
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[2] == "complex":
         cplx = synthetic.generate_complex(20, (4, 3), 60, decay=30.0, seed=3, uhf=True)
         complex_fixture("complex_uhf_m20.npz", cplx, nwalkers=5, seed=21)
@@ -350,3 +418,5 @@ if __name__ == "__main__":
     ad_fixture("ad_onebody_m30.npz")
     cplx = synthetic.generate_complex(20, (4, 3), 60, decay=30.0, seed=3, uhf=True)
     complex_fixture("complex_uhf_m20.npz", cplx, nwalkers=5, seed=21)
+    ghf = synthetic.generate(14, (4, 3), 40, decay=30.0, seed=8, uhf=True, chol_scale="stable")
+    ghf_fixture("ghf_m14.npz", ghf, nwalkers=5, seed=31)
