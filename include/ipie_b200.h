@@ -152,6 +152,14 @@ int ipie_b200_walker_gather(const int* src, int W, int M, int na, int nb, const 
                             void* ghalfa_out, void* ghalfb_out, void* hybrid_energy_out, void* ovlp_out,
                             void* phase_out, double* unscaled_weight_out, void* stream);
 
+/* GHF determinants phi (W, 2M, N), N = na + nb (rows 0..M-1 alpha, M..2M-1 beta spin
+ * orbitals): scatter = 0 copies the spin-diagonal blocks phi[:, :M, :na] to pa (W, M, na)
+ * and phi[:, M:, na:] to pb (W, M, nb); scatter = 1 writes them back (the off-diagonal
+ * blocks are not touched).  These are the blocks ipie's GHF walkers propagate (their phia /
+ * phib views).  replaces: walkers/ghf_walkers.py:63-77 (phia/phib views as used by
+ * propagation/phaseless_generic.py:35-58 and phaseless_base.py:274-280). */
+int ipie_b200_ghf_blocks(void* phi, int W, int M, int na, int nb, void* pa, void* pb, int scatter, void* stream);
+
 /* ---- complex Cholesky Hamiltonians (ipie's GenericComplexChol: nfields = 2X, the first X
  * fields coupling to A = (L + L^H)/2, the rest to B = i (L - L^H)/2) ---- */
 

@@ -2,7 +2,8 @@
 
 The compute path is the in-tree CUDA library ``libipie_b200.so`` (sm_100a),
 reached through a thin ctypes layer (``ipie_b200._lib``).  Host classes mirror
-ipie's: ``Generic``/``GenericRealChol``/``GenericComplexChol``, ``SingleDet``, ``UHFWalkers``,
+ipie's: ``Generic``/``GenericRealChol``/``GenericComplexChol``, ``SingleDet``/``SingleDetGHF``,
+``UHFWalkers``/``GHFWalkers``,
 ``PhaselessGeneric``, ``PopController``, the single-determinant local energies,
 ``EnergyEstimator`` and ``AFQMC``.
 """
@@ -13,7 +14,9 @@ _LAZY = {
     "GenericRealChol": "hamiltonian",
     "GenericComplexChol": "hamiltonian",
     "SingleDet": "trial",
+    "SingleDetGHF": "ghf",
     "UHFWalkers": "walkers",
+    "GHFWalkers": "ghf",
     "PhaselessGeneric": "propagation",
     "PopController": "pop_control",
     "EnergyEstimator": "estimators",

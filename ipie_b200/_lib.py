@@ -44,6 +44,7 @@ SIGNATURES = {
     "ipie_b200_construct_vhs_mixed": [P, P, P, P, I, I, P, P, I, D, D, I, D, P, P, P, P, P, P],
     "ipie_b200_orbital_chain16_fits": [I, I],
     "ipie_b200_vhs_blocks": [I],
+    "ipie_b200_ghf_blocks": [P, I, I, I, I, P, P, I, P],
     "ipie_b200_vhs_block_pack": [P, P, I, I, D, P, P, P],
     "ipie_b200_construct_vhs_blocks": [P, P, I, I, P, P, I, D, D, D, P, P, P, P, I, P, P],
     "ipie_b200_propagate_orbitals_mixed16": [P, P, D, P, P, P, P, D, P, P, I, I, I, I, P, P],

@@ -92,9 +92,17 @@ class AFQMC:
             trial_wavefunction.half_rotate(hamiltonian)
         if walkers is None:
             init = np.asarray(trial_wavefunction.psi).copy()  # walkers_dispatch.py:42-58
-            walkers = UHFWalkers(init, num_elec[0], num_elec[1], hamiltonian.nbasis, num_walkers,
-                                 device=trial_wavefunction.device)
+            if getattr(trial_wavefunction, "ghf", False):
+                from .ghf import GHFWalkers  # walkers_dispatch.py:61-72
+
+                walkers = GHFWalkers(init, num_elec[0], num_elec[1], hamiltonian.nbasis, num_walkers,
+                                     device=trial_wavefunction.device)
+            else:
+                walkers = UHFWalkers(init, num_elec[0], num_elec[1], hamiltonian.nbasis, num_walkers,
+                                     device=trial_wavefunction.device)
             walkers.build(trial_wavefunction)
+        if graph and getattr(walkers, "ghf", False):
+            raise NotImplementedError("graph capture covers UHF walkers; GHF walkers step kernel by kernel")
         prop = PhaselessGeneric(timestep, rng=rng, seed=seed if seed is not None else 7, precision=precision)
         prop.build(hamiltonian, trial_wavefunction, walkers)
         # identical spin blocks (RHF trial, walkers started from it, equal one-body operators):

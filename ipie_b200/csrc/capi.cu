@@ -122,6 +122,10 @@ int ipie_b200_reortho(void* phia, void* phib, int W, int M, int na, int nb, cons
                              ST(stream));
 }
 
+int ipie_b200_ghf_blocks(void* phi, int W, int M, int na, int nb, void* pa, void* pb, int scatter, void* stream) {
+  return (int)launch_ghf_blocks(C2(phi), W, M, na, nb, C2(pa), C2(pb), scatter, ST(stream));
+}
+
 int ipie_b200_walker_copy(const int* src, int W, int M, int na, int nb, void* phia, void* phib, double* weight,
                           double* unscaled_weight, void* hybrid_energy, void* ovlp, void* phase, void* ghalfa,
                           void* ghalfb, void* stream) {

@@ -29,6 +29,8 @@ cudaError_t launch_update_weight(int W, const double2* ovlp_new, const double2* 
 cudaError_t launch_clip_weight(int W, const double* wbound, double* weight, cudaStream_t st);
 cudaError_t launch_reortho(double2* phia, double2* phib, int W, int M, int na, int nb, const double* detR_shift,
                            double* detR, double* log_detR, double2* ovlp, unsigned* status, cudaStream_t st);
+cudaError_t launch_ghf_blocks(double2* phi, int W, int M, int na, int nb, double2* pa, double2* pb, int scatter,
+                              cudaStream_t st);
 cudaError_t launch_walker_copy(const int* src, int W, int M, int na, int nb, double2* phia, double2* phib,
                                double* weight, double* unscaled_weight, double2* ehyb, double2* ovlp, double2* phase,
                                double2* ghalfa, double2* ghalfb, cudaStream_t st);

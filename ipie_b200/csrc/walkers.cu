@@ -605,4 +605,49 @@ cudaError_t launch_energy_combine(int W, int X, int Ka, int Kb, const double2* g
   return cudaGetLastError();
 }
 
+// GHF determinants (W, 2M, N), N = na + nb: the spin-diagonal blocks that the one-body
+// factors and exp(VHS) act on -- rows 0..M-1 x columns 0..na-1 and rows M..2M-1 x columns
+// na..N-1 -- copied to (W, M, na) and (W, M, nb) arrays (scatter = 0) or back (scatter = 1;
+// the off-diagonal blocks of phi are not touched).  One thread per element.
+__global__ void ghf_blocks_kernel(double2* __restrict__ phi, int W, int M, int na, int nb, double2* __restrict__ pa,
+                                  double2* __restrict__ pb, int scatter) {
+  const int N = na + nb;
+  const long long na_el = (long long)M * na, nb_el = (long long)M * nb;
+  const long long per = na_el + nb_el;
+  const long long n = (long long)W * per;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long w = e / per;
+    long long r = e - w * per;
+    size_t pi, qi;
+    double2* q;
+    if (r < na_el) {
+      const long long m = r / na, i = r - m * na;
+      pi = ((size_t)w * 2 * M + m) * N + i;
+      qi = ((size_t)w * M + m) * na + i;
+      q = pa;
+    } else {
+      r -= na_el;
+      const long long m = r / nb, j = r - m * nb;
+      pi = ((size_t)w * 2 * M + M + m) * N + na + j;
+      qi = ((size_t)w * M + m) * nb + j;
+      q = pb;
+    }
+    if (scatter)
+      phi[pi] = q[qi];
+    else
+      q[qi] = phi[pi];
+  }
+}
+
+cudaError_t launch_ghf_blocks(double2* phi, int W, int M, int na, int nb, double2* pa, double2* pb, int scatter,
+                              cudaStream_t st) {
+  if (W <= 0 || M <= 0 || na < 0 || nb < 0 || na + nb == 0 || (na > 0 && pa == nullptr) || (nb > 0 && pb == nullptr))
+    return cudaErrorInvalidValue;
+  long long blocks = ((long long)W * M * (na + nb) + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  ghf_blocks_kernel<<<(unsigned)blocks, 256, 0, st>>>(phi, W, M, na, nb, pa, pb, scatter);
+  note_launch();
+  return cudaGetLastError();
+}
+
 }  // namespace ipie_b200

@@ -65,14 +65,14 @@ def _local_energy_complex(hamiltonian, walkers, trial):
 def _local_energy(hamiltonian, walkers, trial, rhf):
     if not trial.half_rotated:
         raise RuntimeError("trial.half_rotate(hamiltonian) must run before computing local energies")
-    if getattr(hamiltonian, "complex_chol", False):
+    if getattr(hamiltonian, "complex_chol", False) or getattr(trial, "complex_rotated", False):
         return _local_energy_complex(hamiltonian, walkers, trial)
     W = walkers.nwalkers
     work = _energy_work(walkers, hamiltonian, rhf)
     energy = torch.empty(W, 3, dtype=C128, device=walkers.device)
     call("ipie_b200_local_energy_single_det_batch", int(rhf), ptr(trial._rchola), ptr(trial._rcholb),
          ptr(trial._rH1a), ptr(trial._rH1b), hamiltonian.ecore, ptr(walkers.Ghalfa), ptr(walkers.Ghalfb), W,
-         hamiltonian.nchol, hamiltonian.nbasis, walkers.nup, walkers.ndown, ptr(work), ptr(energy),
+         hamiltonian.nchol, walkers.nbasis, walkers.nup, walkers.ndown, ptr(work), ptr(energy),
          ptr(walkers.status), stream())
     return energy
 
@@ -226,7 +226,7 @@ class EnergyEstimator:
         # ipie recomputes the Green's function here; it is skipped while the cached one is current
         if not walkers.gf_current(trial):
             trial.calc_greens_function(walkers)
-        if self.precision == "mixed" and not getattr(hamiltonian, "complex_chol", False):
+        if self.precision == "mixed" and not getattr(hamiltonian, "complex_chol", False) and not getattr(walkers, "ghf", False):
             energy = local_energy_mixed(system, hamiltonian, walkers, trial, rhf=walkers.rhf)
         else:
             energy = local_energy_batch(system, hamiltonian, walkers, trial)

@@ -31,7 +31,12 @@ F64 = torch.float64
 def construct_mean_field_shift(hamiltonian, trial):
     """``mf = 1j L^T Re(G_a+G_b) - L^T Im(G_a+G_b)`` (ipie ``phaseless_base.py:153-172``); for a
     complex Cholesky ``mf = [1j A^T g ; 1j B^T g]`` (``:199-218``)."""
-    g = (trial.G[0] + trial.G[1]).ravel()
+    if getattr(trial, "ghf", False):
+        # Gaa + Gbb of the GHF trial's (2M, 2M) density (ipie phaseless_base.py:175-196)
+        M = hamiltonian.nbasis
+        g = (trial.Gfull[:M, :M] + trial.Gfull[M:, M:]).ravel()
+    else:
+        g = (trial.G[0] + trial.G[1]).ravel()
     if getattr(hamiltonian, "complex_chol", False):
         return np.concatenate([1.0j * (hamiltonian.A.T @ g), 1.0j * (hamiltonian.B.T @ g)])
     return 1.0j * (hamiltonian.chol.T @ g.real) - hamiltonian.chol.T @ g.imag
@@ -174,9 +179,17 @@ class PhaselessGeneric:
 
     def _workspace(self, walkers, hamiltonian):
         W, M, X = walkers.nwalkers, walkers.nbasis, hamiltonian.nfields
+        na, nb = walkers.nup, walkers.ndown
+        ghf = getattr(walkers, "ghf", False)
+        if ghf:
+            # the propagated spin-diagonal blocks of the (2M, N) determinants
+            M, na, nb = walkers.nbasis_spatial, walkers.nalpha, walkers.nbeta
         ws = self.ws
-        if ws is None or (ws.W, ws.M, ws.na, ws.nb, ws.X) != (W, M, walkers.nup, walkers.ndown, X):
-            self.ws = Workspace(W, M, walkers.nup, walkers.ndown, X, walkers.device)
+        if ws is None or (ws.W, ws.M, ws.na, ws.nb, ws.X) != (W, M, na, nb, X):
+            self.ws = Workspace(W, M, na, nb, X, walkers.device)
+            if ghf:
+                self.ws.ghf_pa = torch.empty(W, M, na, dtype=C128, device=walkers.device)
+                self.ws.ghf_pb = torch.empty(W, M, nb, dtype=C128, device=walkers.device)
             if self.precision == "mixed":
                 self.ws.add_mixed(self.chain16)
         return self.ws
@@ -360,6 +373,8 @@ class PhaselessGeneric:
         function of the step's starting orbitals, as in ipie, so moving the first
         one-body factor after it changes nothing.
         """
+        if getattr(walkers, "ghf", False):
+            return self._propagate_ghf(walkers, hamiltonian, trial, eshift)
         ws = self._workspace(walkers, hamiltonian)
         # The step's starting Green's function and overlap: the previous step ended with those of
         # the current orbitals (reortho and pair branch keep them consistent), so they are only
@@ -411,6 +426,51 @@ class PhaselessGeneric:
         self.timer.stop("greens_function")
         walkers.mark_gf_current(trial)
         self.update_weight(walkers, walkers.ovlp, ws.ovlp_new, cfb, cmf, eshift)
+
+    def _propagate_ghf(self, walkers, hamiltonian, trial, eshift):
+        """One step of GHF walkers (ipie ``phaseless_base.py:312-338`` with its GHF dispatches):
+        Green's function and force bias of the whole (2M, N) determinants, one-body factors and
+        exp(VHS) on their spin-diagonal blocks only (ipie's ``phia``/``phib`` views), copied out
+        and back by ``ipie_b200_ghf_blocks``."""
+        if self.precision == "mixed":
+            raise NotImplementedError("GHF walkers run in the FP64 form")
+        ws = self._workspace(walkers, hamiltonian)
+        if not walkers.gf_current(trial):
+            greens_function_into(walkers, trial, walkers.ovlp)
+        walkers.invalidate_gf()
+        W, X, M = walkers.nwalkers, hamiltonian.nfields, hamiltonian.nbasis
+        na, nb = walkers.nalpha, walkers.nbeta
+        self.timer.start("force_bias")
+        force_bias_into(hamiltonian, walkers, trial, ws.vbias)
+        self.timer.stop("force_bias")
+        self.vbias = ws.vbias
+        xi = self.draw_fields(walkers, hamiltonian)
+        call("ipie_b200_field_shift", ptr(ws.vbias), ptr(xi), ptr(self.mf_shift_dev), W, X, self.sqrt_dt, self.fbbound,
+             ptr(ws.xshifted), ptr(ws.cmf), ptr(ws.cfb), stream())
+        self.timer.start("vhs")
+        self.construct_VHS(hamiltonian, ws.xshifted, out=ws.vhs)
+        self.timer.stop("vhs")
+        self.timer.start("orbitals")
+        call("ipie_b200_ghf_blocks", ptr(walkers.phia), W, M, na, nb, ptr(ws.ghf_pa), ptr(ws.ghf_pb), 0, stream())
+        for s_, (src, dst, n) in enumerate(((ws.ghf_pa, ws.phia_tmp, na), (ws.ghf_pb, ws.phib_tmp, nb))):
+            if n == 0:
+                continue
+            if self.fused and not self.expH1_complex and M <= 256 and n <= 32:
+                call("ipie_b200_propagate_orbitals", ptr(ws.vhs), ptr(self.expH1_pad[s_]), self.lda_e, ptr(src),
+                     ptr(dst), W, M, n, self.exp_nmax, 1, 1, stream())
+            else:
+                cplx = int(self.expH1_complex)
+                call("ipie_b200_propagate_one_body", ptr(self.expH1_dev[s_]), cplx, ptr(src), ptr(dst), W, M, n,
+                     stream())
+                call("ipie_b200_apply_exponential_batch", ptr(ws.vhs), ptr(dst), ptr(src), ptr(ws.taylor), W, M, n,
+                     self.exp_nmax, stream())
+                call("ipie_b200_propagate_one_body", ptr(self.expH1_dev[s_]), cplx, ptr(src), ptr(dst), W, M, n,
+                     stream())
+        call("ipie_b200_ghf_blocks", ptr(walkers.phia), W, M, na, nb, ptr(ws.phia_tmp), ptr(ws.phib_tmp), 1, stream())
+        self.timer.stop("orbitals")
+        greens_function_into(walkers, trial, ws.ovlp_new)
+        walkers.mark_gf_current(trial)
+        self.update_weight(walkers, walkers.ovlp, ws.ovlp_new, ws.cfb, ws.cmf, eshift)
 
     def _mixed_two_body(self, walkers, hamiltonian, trial):
         """Force bias (TF32), shifted fields, VHS and the orbital update (3-pass TF32) of the mixed form."""

@@ -161,6 +161,12 @@ def overlap_into(walkers, trial, ovlp_out):
 
 
 def force_bias_into(hamiltonian, walkers, trial, vbias_out):
+    if getattr(trial, "complex_rotated", False):
+        # complex half-rotated Cholesky of a complex GHF trial: vbias = R . Ghalf
+        re, im = trial._cplx["chola"]
+        call("ipie_b200_force_bias_complex", ptr(re), ptr(im), ptr(walkers.Ghalfa), walkers.nwalkers,
+             hamiltonian.nchol, walkers.nup * walkers.nbasis, ptr(vbias_out), hamiltonian.nchol, 0, 0, stream())
+        return
     if getattr(hamiltonian, "complex_chol", False):
         # [rA . G ; rB . G]: per block the alpha term written, the beta term added
         W, X, M = walkers.nwalkers, hamiltonian.nchol, walkers.nbasis
@@ -177,5 +183,5 @@ def force_bias_into(hamiltonian, walkers, trial, vbias_out):
     call(
         "ipie_b200_construct_force_bias_batch_single_det",
         ptr(trial._rchola), ptr(trial._rcholb), ptr(walkers.Ghalfa), ptr(walkers.Ghalfb),
-        walkers.nwalkers, hamiltonian.nchol, hamiltonian.nbasis, walkers.nup, walkers.ndown, ptr(vbias_out), stream(),
+        walkers.nwalkers, hamiltonian.nchol, walkers.nbasis, walkers.nup, walkers.ndown, ptr(vbias_out), stream(),
     )
