@@ -33,7 +33,8 @@ def _local_energy_complex(hamiltonian, walkers, trial):
     """Complex-Cholesky UHF local energy (ipie ``local_energy_sd.py:406-460``): X1 = sum_s rchol_s . G_s and
     X2 = sum_s rcholbar_s . G_s give ecoul = X1 . X2 / 2, the exchange 1/2 sum_x tr(T1 T2) per spin runs as
     eight real exchange passes (polarisation), and the combine adds the one-body term."""
-    W, X, M = walkers.nwalkers, hamiltonian.nchol, walkers.nbasis
+    # rows of the rotated operands: X, or 2X for a GHF trial with complex Cholesky vectors ([RA ; RB])
+    W, X, M = walkers.nwalkers, getattr(trial, "_cplx_rows", hamiltonian.nchol), walkers.nbasis
     rows = max(lib().ipie_b200_exchange_rows(W, X, M, n) for n in (walkers.nup, walkers.ndown) if n > 0)
     need = 2 * W * X + rows * W + W
     buf = getattr(walkers, "_energy_work_cplx", None)

@@ -17,7 +17,9 @@ population control and estimator kernels of the UHF path run on it unchanged wit
   out and back (``phaseless_generic.py:35-58``, ``phaseless_base.py:274-280``).
 
 A complex trial makes R complex; its products then run on the complex-operand kernels of the
-complex-Cholesky path.  Real Cholesky Hamiltonians only.
+complex-Cholesky path.  With complex Cholesky vectors (ipie's ``GenericComplexChol``) the trial
+is rotated for the A and B fields, ``RA`` and ``RB``: the force bias is ``[RA . Ghalf ; RB . Ghalf]``
+and the energy runs over the 2X rows ``[RA ; RB]`` (``local_energy_sd.py:548-576,631-682``).
 """
 from __future__ import annotations
 
@@ -80,21 +82,31 @@ class SingleDetGHF(SingleDet):
     def half_rotate(self, hamiltonian, comm=None):
         """``R`` and ``rH1`` over both spin blocks (see the module docstring); ipie keeps the full
         Green's function for GHF instead (``single_det_ghf.py:114-121``), with the same products."""
-        if getattr(hamiltonian, "complex_chol", False):
-            raise NotImplementedError("GHF trials take real Cholesky Hamiltonians")
         M, X = hamiltonian.nbasis, hamiltonian.nchol
         if M != self.nbasis:
             raise AssertionError("Hamiltonian and trial basis sizes differ")
-        L = hamiltonian.chol.reshape(M, M, X)
         pa, pb = self.psi[:M].conj(), self.psi[M:].conj()
-        R = np.concatenate([np.einsum("pn,pqx->xnq", pa, L, optimize=True),
-                            np.einsum("pn,pqx->xnq", pb, L, optimize=True)], axis=2).reshape(X, -1)
+
+        def rotate(K):  # [psi_a^H K_x | psi_b^H K_x] as (X, N * 2M)
+            K = K.reshape(M, M, X)
+            return np.concatenate([np.einsum("pn,pqx->xnq", pa, K, optimize=True),
+                                   np.einsum("pn,pqx->xnq", pb, K, optimize=True)], axis=2).reshape(X, -1)
+
         H1 = hamiltonian.H1
         rH1 = np.concatenate([pa.T @ H1[0], pb.T @ H1[1]], axis=1)
         d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
         self._rH1a = d(rH1.astype(np.complex128))
         self._rH1b = d(np.zeros((0, 2 * M), dtype=np.complex128))
+        if getattr(hamiltonian, "complex_chol", False):
+            # A and B fields: force bias [RA . G ; RB . G], energy over the 2X rows [RA ; RB]
+            RA, RB = rotate(hamiltonian.A), rotate(hamiltonian.B)
+            R = np.concatenate([RA, RB], axis=0)
+            self._cplx = {"Aa": (d(RA.real), d(RA.imag)), "Ba": (d(RB.real), d(RB.imag))}
+        else:
+            R = rotate(hamiltonian.chol)
+            self._cplx = {}
         self._R = R
+        self._cplx_rows = R.shape[0]
         self.complex_rotated = bool(np.iscomplexobj(R) and np.abs(R.imag).max() > 0)
         if self.complex_rotated:
             re, im = d(R.real), d(R.imag)
@@ -102,7 +114,7 @@ class SingleDetGHF(SingleDet):
             for a, b in (("real", "real"), ("imag", "imag"), ("real", "imag"), ("imag", "real")):
                 P, Q = getattr(R, a), getattr(R, b)
                 pol += [P + Q, P - Q]
-            self._cplx = {"chola": (re, im), "cholbara": (re, im), "pola": d(np.stack(pol))}
+            self._cplx.update({"chola": (re, im), "cholbara": (re, im), "pola": d(np.stack(pol))})
             self._rchola = self._rcholb = None
         else:
             self._rchola = d(np.asarray(R.real, dtype=np.float64))

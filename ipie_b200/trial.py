@@ -161,7 +161,7 @@ def overlap_into(walkers, trial, ovlp_out):
 
 
 def force_bias_into(hamiltonian, walkers, trial, vbias_out):
-    if getattr(trial, "complex_rotated", False):
+    if getattr(trial, "complex_rotated", False) and not getattr(hamiltonian, "complex_chol", False):
         # complex half-rotated Cholesky of a complex GHF trial: vbias = R . Ghalf
         re, im = trial._cplx["chola"]
         call("ipie_b200_force_bias_complex", ptr(re), ptr(im), ptr(walkers.Ghalfa), walkers.nwalkers,

@@ -1,4 +1,4 @@
-"""numpy restatement of ipie's GHF walker step for a real Cholesky Hamiltonian (CPU oracle).
+"""numpy restatement of ipie's GHF walker step (CPU oracle).
 
 TEST INFRASTRUCTURE ONLY: the checker of the GHF path, imported by ``tests/`` and nothing
 in ``ipie_b200``.
@@ -17,7 +17,11 @@ way.  Restated here, each with its ipie citation:
   nalpha..N-1 (``ghf_walkers.py:63-77``, ``phaseless_generic.py:35-58``,
   ``phaseless_base.py:274-280``); the off-diagonal spin blocks are left as they are;
 * reorthogonalisation by a thin QR of the whole (2M, N) determinant (``ghf_walkers.py:124-151``);
-* the local energy from the four spin blocks of G (``estimators/local_energy_sd.py:513-730``).
+* the local energy from the four spin blocks of G (``estimators/local_energy_sd.py:513-780``);
+* with complex Cholesky vectors (ipie's ``GenericComplexChol``), the A/B fields of
+  ``oracle/complex_chol_oracle.py`` in the force bias, mean-field shift, VHS and energy
+  (``force_bias.py:186-213``, ``phaseless_base.py:219-239``, ``local_energy_sd.py:548-576,631-682,
+  733-780``).
 
 Walkers are ``afqmc_oracle.Walkers`` with ``phia`` holding the whole (W, 2M, N) determinant
 and ``phib`` empty, so that population control (whose buffers hold ``phi``) and the weight
@@ -48,6 +52,8 @@ class GHFSystem:
     chol_packed: np.ndarray = field(default=None)
     sym_idx: tuple = field(default=None)
     h1e_mod: np.ndarray = field(default=None)
+    A: np.ndarray = field(default=None)
+    B: np.ndarray = field(default=None)
     G: np.ndarray = field(default=None)
     mf_shift: np.ndarray = field(default=None)
     expH1: np.ndarray = field(default=None)
@@ -57,8 +63,12 @@ class GHFSystem:
         return self.chol.shape[-1]
 
     @property
+    def complex_chol(self):
+        return np.iscomplexobj(self.chol)
+
+    @property
     def nfields(self):
-        return self.nchol
+        return 2 * self.nchol if self.complex_chol else self.nchol
 
     @property
     def nocc(self):
@@ -71,12 +81,29 @@ class GHFSystem:
             psi = np.array(psi.real, dtype=np.float64)  # single_det_ghf.py:61-65
         self.psi = psi[:, : self.nocc]
         self.h1e_mod = O.construct_h1e_mod(self.chol, self.h1e)
+        if self.complex_chol and not np.iscomplexobj(self.h1e):
+            self.h1e_mod = self.h1e_mod.real.copy()  # generic.py:116-118
         self.sym_idx = np.triu_indices(M)
-        self.chol_packed = O.pack_cholesky(self.chol, M)
         self.G, _ = O.gab_mod(self.psi, self.psi)  # single_det_ghf.py:75
-        self.mf_shift = mean_field_shift_ghf(self.chol, self.G, M)
-        self.expH1 = O.one_body_propagator(self.h1e_mod, self.chol, self.mf_shift, self.dt, M)
+        if self.complex_chol:
+            from oracle import complex_chol_oracle as C
+
+            self.A, self.B = C.hermitian_parts(self.chol, M)
+            g = (self.G[:M, :M] + self.G[M:, M:]).ravel()
+            self.mf_shift = np.concatenate([1.0j * (self.A.T @ g), 1.0j * (self.B.T @ g)])
+            self.expH1 = C.one_body_propagator_complex(self.h1e_mod, self.A, self.B, self.mf_shift, self.dt, M)
+        else:
+            self.chol_packed = O.pack_cholesky(self.chol, M)
+            self.mf_shift = mean_field_shift_ghf(self.chol, self.G, M)
+            self.expH1 = O.one_body_propagator(self.h1e_mod, self.chol, self.mf_shift, self.dt, M)
         return self
+
+    def vhs(self, xshifted):
+        if self.complex_chol:
+            from oracle import complex_chol_oracle as C
+
+            return C.construct_vhs_complex(self, xshifted)
+        return O.construct_vhs(self, xshifted)
 
     def walkers(self, init, nwalkers):
         """``GHFWalkers(initial_walker, ...)`` (``ghf_walkers.py:79-113``) as oracle walkers."""
@@ -114,6 +141,8 @@ def force_bias_ghf(sys_: GHFSystem, w) -> np.ndarray:
     """``vbias = L^T vec(Gaa + Gbb)`` (real L applied to Re and Im); ipie ``force_bias.py:155-183``."""
     M, W = sys_.nbasis, w.nwalkers
     gc = (w.G[:, :M, :M] + w.G[:, M:, M:]).reshape(W, -1)
+    if sys_.complex_chol:
+        return np.concatenate([gc @ sys_.A, gc @ sys_.B], axis=1)  # force_bias.py:186-213
     return gc.real @ sys_.chol + 1.0j * (gc.imag @ sys_.chol)
 
 
@@ -124,15 +153,19 @@ def local_energy_ghf(sys_: GHFSystem, w) -> np.ndarray:
     Gaa, Gbb = w.G[:, :M, :M], w.G[:, M:, M:]
     Gab, Gba = w.G[:, :M, M:], w.G[:, M:, :M]
     e1b = Gaa.reshape(W, -1) @ sys_.h1e[0].ravel() + Gbb.reshape(W, -1) @ sys_.h1e[1].ravel() + sys_.ecore
-    Xv = (Gaa + Gbb).reshape(W, -1) @ sys_.chol
-    ecoul = 0.5 * np.einsum("wx,wx->w", Xv, Xv)
-    L = sys_.chol.T.reshape(-1, M, M)
+    gc = (Gaa + Gbb).reshape(W, -1)
+    ops = (sys_.A, sys_.B) if sys_.complex_chol else (sys_.chol,)
+    ecoul = np.zeros(W, dtype=np.complex128)
     exx = np.zeros(W, dtype=np.complex128)
-    for iw in range(W):
-        for Gs, Gt, f in ((Gaa[iw], Gaa[iw], 1.0), (Gbb[iw], Gbb[iw], 1.0), (Gab[iw], Gba[iw], 2.0)):
-            T1 = np.einsum("ji,xjk->xik", Gs, L, optimize=True)  # G^T L_x
-            T2 = np.einsum("ji,xjk->xik", Gt, L, optimize=True)
-            exx[iw] += f * np.einsum("xij,xji->", T1, T2, optimize=True)
+    for K in ops:
+        Xv = gc @ K
+        ecoul += 0.5 * np.einsum("wx,wx->w", Xv, Xv)
+        L = K.T.reshape(-1, M, M)
+        for iw in range(W):
+            for Gs, Gt, f in ((Gaa[iw], Gaa[iw], 1.0), (Gbb[iw], Gbb[iw], 1.0), (Gab[iw], Gba[iw], 2.0)):
+                T1 = np.einsum("ji,xjk->xik", Gs, L, optimize=True)  # G^T K_x
+                T2 = np.einsum("ji,xjk->xik", Gt, L, optimize=True)
+                exx[iw] += f * np.einsum("xij,xji->", T1, T2, optimize=True)
     exx *= 0.5
     e2b = ecoul - exx
     out = np.zeros((W, 3), dtype=np.complex128)
@@ -172,7 +205,7 @@ def propagate_walkers_ghf(sys_: GHFSystem, w, eshift: float, xi: np.ndarray | No
     xshifted = xi - xbar
     cmf = -sqrt_dt * np.einsum("wx,x->w", xshifted, sys_.mf_shift)
     cfb = np.einsum("wx,wx->w", xi, xbar) - 0.5 * np.einsum("wx,wx->w", xbar, xbar)
-    vhs = O.construct_vhs(sys_, xshifted.T.copy())
+    vhs = sys_.vhs(xshifted.T.copy())
     pa = O.apply_exponential(pa, vhs, sys_.exp_nmax)
     if sys_.nbeta > 0:
         pb = O.apply_exponential(pb, vhs, sys_.exp_nmax)

@@ -335,15 +335,22 @@ def ghf_fixture(name, sysw, nwalkers, seed, nsteps=3):
     from ipie.trial_wavefunction.single_det_ghf import SingleDetGHF
     from ipie.walkers.ghf_walkers import GHFWalkers
 
-    ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
     M, na, nb = sysw.nbasis, sysw.nup, sysw.ndown
     N = na + nb
     W = nwalkers
     rng = np.random.default_rng(seed)
     out = {}
-    for case in ("b", "m"):
+    # case "c": the spin-mixed trial with a complex Cholesky Hamiltonian (imaginary parts added
+    # to the same vectors as synthetic.generate_complex does)
+    crng = np.random.default_rng(seed + 500)
+    K = crng.normal(size=sysw.chol.shape) * 0.3 * np.abs(sysw.chol).max()
+    cchol = sysw.chol + 1.0j * K
+    out["c_chol_imag"] = K
+    for case in ("b", "m", "c"):
+        ham = HamGeneric(h1e=sysw.h1e.copy(), chol=(cchol if case == "c" else sysw.chol).copy(), ecore=sysw.ecore)
         uhf = SingleDet(sysw.psi.copy(), (na, nb), M)
-        uhf.half_rotate(ham)
+        if case != "c":
+            uhf.half_rotate(ham)
         if case == "b":
             trial = SingleDetGHF(uhf)
             uw = UHFWalkersTrial(uhf, sysw.init.copy(), na, nb, M, W, MPIHandler())
@@ -358,7 +365,10 @@ def ghf_fixture(name, sysw, nwalkers, seed, nsteps=3):
             A = rng.normal(size=(2 * M, 2 * M)) + 1j * rng.normal(size=(2 * M, 2 * M))
             U = scipy.linalg.expm(0.08 * (A - A.conj().T))
             psi = U @ base
-            out["m_psi"] = psi
+            if case == "m":
+                out["m_psi"] = psi
+            else:
+                psi = out["m_psi"]
             trial = SingleDetGHF(psi.copy(), (na, nb), M)
             walkers = GHFWalkers(psi.copy(), na, nb, M, W, MPIHandler())
         walkers.build(trial)
@@ -374,7 +384,7 @@ def ghf_fixture(name, sysw, nwalkers, seed, nsteps=3):
         out[case + "_mf_shift"] = prop.mf_shift
         out[case + "_expH1"] = prop.expH1
         walkers.ovlp = out[case + "_ovlp"].copy()
-        np.random.seed(seed + (1 if case == "b" else 2))
+        np.random.seed(seed + {"b": 1, "m": 2, "c": 3}[case])
         for step in range(nsteps):
             prop.propagate_walkers(walkers, ham, trial, -3.0 if step else 0.0)
         out[case + "_walk_weight"] = np.array(walkers.weight)

@@ -1,7 +1,8 @@
 """Parity of the GHF walker step (``SingleDetGHF``, ``GHFWalkers``) with ipie's outputs.
 
 ``ghf_m14.npz`` holds ipie's own results for a block-diagonal trial built from a UHF one
-(case "b") and a complex spin-mixed trial (case "m"): Green's function, force bias and local
+(case "b"), a complex spin-mixed trial (case "m") and that trial with complex Cholesky vectors
+(case "c"): Green's function, force bias and local
 energy of perturbed walkers, a 3-step walk with ipie's draws and a reorthogonalisation
 (``tests/golden/make_golden.py``).  Tolerances as for the FP64 UHF form.  Every call goes
 through the C ABI.
@@ -35,7 +36,7 @@ def ghf_objects(case, f, W):
     from ipie_b200.propagation import PhaselessGeneric
 
     s = synthetic.generate(14, (4, 3), 40, decay=30.0, seed=8, uhf=True, chol_scale="stable")
-    ham = Generic(s.h1e, s.chol, s.ecore)
+    ham = Generic(s.h1e, s.chol + 1.0j * f["c_chol_imag"] if case == "c" else s.chol, s.ecore)
     if case == "b":
         trial = SingleDetGHF(SingleDet(s.psi, (s.nup, s.ndown), s.nbasis))
         init = G.ghf_from_uhf(s.init, s.nup, s.nbasis)
@@ -50,7 +51,7 @@ def ghf_objects(case, f, W):
     return s, ham, trial, walkers, prop
 
 
-@pytest.mark.parametrize("case,fused", [("b", True), ("b", False), ("m", True), ("m", False)])
+@pytest.mark.parametrize("case,fused", [("b", True), ("b", False), ("m", True), ("m", False), ("c", False)])
 def test_ghf_step_matches_ipie(case, fused):
     from ipie_b200.estimators import local_energy_batch
 
@@ -58,7 +59,7 @@ def test_ghf_step_matches_ipie(case, fused):
     W = f[case + "_phi_in"].shape[0]
     s, ham, trial, walkers, prop = ghf_objects(case, f, W)
     prop.fused = fused
-    assert trial.complex_rotated == (case == "m")
+    assert trial.complex_rotated == (case in ("m", "c"))
     assert rel(prop.mf_shift, f[case + "_mf_shift"]) < 1e-12
     assert rel(prop.expH1, f[case + "_expH1"]) < 1e-12
     walkers.phi = dev(f[case + "_phi_in"])
@@ -69,7 +70,7 @@ def test_ghf_step_matches_ipie(case, fused):
     assert rel(trial.calc_force_bias(ham, walkers), f[case + "_vbias"]) < 1e-12
     assert rel(local_energy_batch(None, ham, walkers, trial), f[case + "_energy"]) < 1e-11
     walkers.ovlp = ovlp.clone()
-    np.random.seed(31 + (1 if case == "b" else 2))
+    np.random.seed(31 + {"b": 1, "m": 2, "c": 3}[case])
     for step in range(3):
         prop.propagate_walkers(walkers, ham, trial, -3.0 if step else 0.0)
     assert rel(walkers.weight, f[case + "_walk_weight"]) < TOL

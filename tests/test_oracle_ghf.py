@@ -3,7 +3,8 @@
 ``tests/golden/ghf_m14.npz`` was written by ``tests/golden/make_golden.py ... ghf`` running
 ipie's numpy path on ``synthetic.generate(14, (4, 3), 40, decay=30, seed=8, uhf=True,
 chol_scale="stable")``: case "b" with the trial and walkers built from UHF ones (block
-diagonal), case "m" with a complex spin-mixed determinant; per-kernel outputs on perturbed
+diagonal), case "m" with a complex spin-mixed determinant, case "c" that determinant with
+complex Cholesky vectors; per-kernel outputs on perturbed
 walkers, a 3-step walk with ipie's draws and a reorthogonalisation.  CPU only.
 """
 import numpy as np
@@ -25,7 +26,8 @@ def ghf_system(case, f=None):
 
     s = synthetic.generate(14, (4, 3), 40, decay=30.0, seed=8, uhf=True, chol_scale="stable")
     psi = G.ghf_from_uhf(s.psi, s.nup, s.nbasis) if case == "b" else f["m_psi"]
-    S = G.GHFSystem(nbasis=s.nbasis, nalpha=s.nup, nbeta=s.ndown, h1e=s.h1e, chol=s.chol, ecore=s.ecore,
+    chol = s.chol + 1.0j * f["c_chol_imag"] if case == "c" else s.chol
+    S = G.GHFSystem(nbasis=s.nbasis, nalpha=s.nup, nbeta=s.ndown, h1e=s.h1e, chol=chol, ecore=s.ecore,
                     psi=psi).build()
     init = G.ghf_from_uhf(s.init, s.nup, s.nbasis) if case == "b" else f["m_psi"]
     return s, S, init
@@ -38,7 +40,7 @@ def test_ghf_fixture_inputs_regenerate():
     np.testing.assert_allclose(checksum(s.psi), f["psi_checksum"], rtol=1e-13)
 
 
-@pytest.mark.parametrize("case", ["b", "m"])
+@pytest.mark.parametrize("case", ["b", "m", "c"])
 def test_ghf_oracle_matches_ipie(case):
     f = load("ghf_m14.npz")
     _, S, init = ghf_system(case, f)
@@ -54,7 +56,7 @@ def test_ghf_oracle_matches_ipie(case):
     assert rel(G.force_bias_ghf(S, w), f[case + "_vbias"]) < 1e-12
     assert rel(G.local_energy_ghf(S, w), f[case + "_energy"]) < 1e-11
     w.ovlp = ovlp.copy()
-    np.random.seed(31 + (1 if case == "b" else 2))
+    np.random.seed(31 + {"b": 1, "m": 2, "c": 3}[case])
     for step in range(3):
         G.propagate_walkers_ghf(S, w, -3.0 if step else 0.0)
     assert rel(w.weight, f[case + "_walk_weight"]) < 1e-10
