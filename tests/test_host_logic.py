@@ -130,3 +130,44 @@ def test_complex_cholesky_host_setup_matches_ipie():
     assert np.max(np.abs(mf - f["mf_shift"])) <= 1e-12 * np.abs(f["mf_shift"]).max()
     expH1 = construct_one_body_propagator(ham, mf, 0.005)
     assert np.max(np.abs(expH1 - f["expH1"])) <= 1e-12
+
+
+@pytest.mark.parametrize("case", ["b", "m", "c"])
+def test_ghf_half_rotation_reproduces_the_four_block_energy(case):
+    """The GHF trial's half rotation over both spin blocks (R = [psi_a^H K | psi_b^H K], rH1) gives
+    the force bias, one-body energy, Coulomb and exchange of ipie's full-G GHF formulas (the oracle):
+    the identities the device path relies on, checked in numpy on perturbed walkers."""
+    from ipie_b200.ghf import SingleDetGHF
+    from ipie_b200.hamiltonian import Generic
+    from oracle import ghf_oracle as G
+    from tests._systems import load
+
+    f = load("ghf_m14.npz")
+    s = synthetic.generate(14, (4, 3), 40, decay=30.0, seed=8, uhf=True, chol_scale="stable")
+    chol = s.chol + 1.0j * f["c_chol_imag"] if case == "c" else s.chol
+    psi = G.ghf_from_uhf(s.psi, s.nup, s.nbasis) if case == "b" else f["m_psi"]
+    from ipie_b200.hamiltonian import GenericComplexChol, GenericRealChol
+
+    ham = (GenericComplexChol if case == "c" else GenericRealChol)(s.h1e, chol, s.ecore, device="cpu")
+    trial = SingleDetGHF(psi, (s.nup, s.ndown), s.nbasis, device="cpu")
+    trial.half_rotate(ham)
+    S = G.GHFSystem(nbasis=s.nbasis, nalpha=s.nup, nbeta=s.ndown, h1e=s.h1e, chol=chol, ecore=s.ecore, psi=psi).build()
+    w = S.walkers(psi, 5)
+    w.phia = f[case + "_phi_in"].copy()
+    G.greens_function_ghf(S, w)
+    gh = w.Ghalfa.reshape(5, -1)  # (W, N * 2M)
+    R = trial._R
+    X = s.nchol
+    vb = gh @ R.T
+    ref_vb = G.force_bias_ghf(S, w)
+    assert np.max(np.abs(vb - ref_vb)) <= 1e-12 * np.abs(ref_vb).max()
+    rH1 = trial._rH1a.numpy().ravel()
+    e1 = gh @ rH1 + s.ecore
+    ecoul = 0.5 * np.einsum("wx,wx->w", vb, vb)
+    N, M2 = s.nup + s.ndown, 2 * s.nbasis
+    T = np.einsum("xnk,wmk->wxnm", R.reshape(R.shape[0], N, M2), w.Ghalfa, optimize=True)
+    exx = 0.5 * np.einsum("wxnm,wxmn->w", T, T, optimize=True)
+    ref = G.local_energy_ghf(S, w)
+    assert np.max(np.abs(e1 - ref[:, 1])) <= 1e-12 * np.abs(ref[:, 1]).max()
+    assert np.max(np.abs(ecoul - exx - ref[:, 2])) <= 1e-11 * np.abs(ref[:, 2]).max()
+    assert R.shape[0] == (2 * X if case == "c" else X)
