@@ -510,7 +510,7 @@ def run_ours(args):
     for _ in range(e2e_steps):
         step += 1
         af2.step(step)
-        wback.copy_(af2.walkers.weight)  # the step's result back to the host
+        wback.copy_(af2.walkers.weight, non_blocking=True)  # the step's result back to (pinned) host memory
     e1.record()
     torch.cuda.synchronize()
     t2 = barrier_max(e0.elapsed_time(e1) / 1e3, world)

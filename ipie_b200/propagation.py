@@ -11,7 +11,8 @@ Auxiliary fields: ``rng="numpy"`` (default) draws them exactly as ipie does,
 so a run fed the same seed consumes the same draws; ``rng="device"`` draws
 them on the GPU (Philox4x32-10), which keeps a step free of host work;
 ``rng="host"`` takes caller-supplied (W, X) host arrays from the iterator
-``propagator.host_fields`` and uploads one per step.
+``propagator.host_fields`` and uploads one per step (the next step's array on a copy stream
+while the current step computes).
 """
 from __future__ import annotations
 
@@ -301,8 +302,7 @@ class PhaselessGeneric:
             ws.xi.copy_(ws.xi_host, non_blocking=True)
             ws.xi_copied.record()
         elif self.rng == "host":
-            src = next(self.host_fields)  # (W, X) float64, ideally pinned host memory
-            ws.xi.copy_(src, non_blocking=True)
+            return self._host_fields(ws)
         else:
             # the counter lives on the device so that a step captured in a CUDA graph draws a
             # new block on every replay (same sequence as counting on the host)
@@ -311,6 +311,37 @@ class PhaselessGeneric:
             call("ipie_b200_normal_fill_dev", ptr(ws.xi), W * X, self.rng_seed, ptr(self.rng_counter_dev), stream())
             self.rng_counter += 1
         return ws.xi
+
+    def _host_fields(self, ws):
+        """This step's caller-supplied fields, uploaded while the previous step computed: each call
+        returns the buffer filled for it and starts the next array's copy into the other buffer on
+        a copy stream (after the compute stream has consumed that buffer), so the host-to-device
+        transfer overlaps the step instead of preceding it."""
+        cur = torch.cuda.current_stream()
+        pending = getattr(ws, "xi_pending", None)
+        if pending is None:
+            ws.xi.copy_(next(self.host_fields), non_blocking=True)  # (W, X) float64, pinned host memory
+            buf = ws.xi
+        else:
+            buf, ready = pending
+            cur.wait_event(ready)
+        nxt = next(self.host_fields, None)
+        if nxt is None:
+            ws.xi_pending = None
+            return buf
+        if getattr(ws, "xi_alt", None) is None:
+            ws.xi_alt = torch.empty_like(ws.xi)
+            ws.copy_stream = torch.cuda.Stream(device=ws.xi.device)
+        other = ws.xi_alt if buf is ws.xi else ws.xi
+        free = torch.cuda.Event()
+        free.record(cur)  # the previous step's field shift, which read `other`, is behind this point
+        ws.copy_stream.wait_event(free)
+        with torch.cuda.stream(ws.copy_stream):
+            other.copy_(nxt, non_blocking=True)
+            ready = torch.cuda.Event()
+            ready.record(ws.copy_stream)
+        ws.xi_pending = (other, ready)
+        return buf
 
     def propagate_walkers_two_body(self, walkers, hamiltonian, trial):
         """Force bias, shifted fields, VHS and exp(VHS) (ipie ``phaseless_base.py:282-310``)."""

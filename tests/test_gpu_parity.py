@@ -412,3 +412,28 @@ def test_cached_green_function_stays_current():
         assert rel(ov, fresh) < 1e-12
     w.phia = w.phia.clone()
     assert not w.gf_current(trial)
+
+
+def test_host_fields_prefetch_matches_numpy_draws():
+    """``rng="host"`` (each step's array uploaded on a copy stream during the previous step) walks
+    exactly as ``rng="numpy"`` fed the same draws."""
+    from ipie_b200 import synthetic
+    from ipie_b200.propagation import PhaselessGeneric
+
+    s = synthetic.generate(26, (5, 3), 60, decay=30.0, seed=6, uhf=True, chol_scale="stable")
+    W, nsteps = 12, 6
+    ham, trial, w1, p1 = gpu_objects(s, W)
+    _, _, w2, _ = gpu_objects(s, W)
+    p2 = PhaselessGeneric(0.005, rng="host")
+    p2.build(ham, trial, w2)
+    np.random.seed(77)
+    draws = [np.random.normal(0.0, 1.0, ham.nfields * W).reshape(W, ham.nfields) for _ in range(nsteps)]
+    p2.host_fields = iter([torch.from_numpy(d.copy()).pin_memory() for d in draws])
+    np.random.seed(77)
+    for step in range(nsteps):
+        p1.propagate_walkers(w1, ham, trial, 0.0 if step == 0 else -1.0)
+        p2.propagate_walkers(w2, ham, trial, 0.0 if step == 0 else -1.0)
+    torch.cuda.synchronize()
+    assert torch.equal(w1.weight, w2.weight)
+    assert torch.equal(w1.phia, w2.phia)
+    assert torch.equal(w1.ovlp, w2.ovlp)
