@@ -368,8 +368,9 @@ int ipie_b200_exchange_mixed(const void* r_hi, const void* r_lo, double r_scale,
                              int N, float* gwork, void* part, void* exx, unsigned int* status, void* stream);
 
 /* Local energy of the mixed form: the exchange as 3-pass FP16 tensor-core
- * products (T never stored, bilinear sums in FP64); Coulomb vector and e1b in
- * FP64.  Same contract and spin-alias convention as
+ * products (T never stored, bilinear sums in FP64); e1b in FP64; the Coulomb
+ * vector in FP64 without the trial reference, and with it as the trial's FP64
+ * vector plus the 3-pass FP16 product of G - G_T.  Same contract and spin-alias convention as
  * ipie_b200_local_energy_single_det_batch; rchola/rcholb FP64, r*_hi/lo and
  * r*_scale from ipie_b200_rchol_pad_split; gwork: 2*W*2*32*M floats; work:
  * W*X + rows*W complex with rows = sum over spin blocks of ceil(X*NP/128)

@@ -1101,6 +1101,13 @@ extern "C" int ipie_b200_exchange_mixed(const void* r_hi, const void* r_lo, doub
   return (int)cudaGetLastError();
 }
 
+// rows 1..W-1 of xv (W, X) = row 0 (the trial's Coulomb vector, before the per-walker deviations)
+__global__ void broadcast_row0_kernel(double2* __restrict__ xv, int W, int X) {
+  const long long n = (long long)(W - 1) * X;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    xv[X + e] = xv[e % X];
+}
+
 extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const double* rcholb, const void* ra_hi,
                                             const void* ra_lo, double ra_scale, const void* rb_hi, const void* rb_lo,
                                             double rb_scale, const void* rH1a, const void* rH1b, double ecore, const void* ghalfa,
@@ -1120,20 +1127,40 @@ extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const
   const int NPa = umma::exchange_np(na), NPb = nb > 0 ? umma::exchange_np(nb) : 8;
   if (NPa < 0 || NPb < 0 || M < 4 || !(ra_scale > 0.0) || (use_b && !(rb_scale > 0.0))) return (int)cudaErrorInvalidValue;
   const umma::GPad gp = umma::carve_gpad(gwork, W, 32, M);
-  // Coulomb vector in FP64 (DMMA): the Coulomb energy is the large, cancellation-free term
-  cudaError_t e = launch_force_bias(rchola, reinterpret_cast<const double2*>(ghalfa), W, X, na * M, xv, 0, st,
-                                    alias ? 2.0 : 1.0);
-  if (e == cudaSuccess && use_b)
-    e = launch_force_bias(rcholb, reinterpret_cast<const double2*>(ghalfb), W, X, nb * M, xv, 1, st);
-  if (e != cudaSuccess) return (int)e;
+  cudaError_t e;
+  if (delta) {
+    // Coulomb vector around the trial: X_T = sum_s rchol_s . G_T,s in FP64 (one walker's product,
+    // into row 0, then copied to every row), plus the 3-pass FP16 product of G - G_T added per
+    // spin block below, so that only the deviation carries the tensor cores' rounding
+    e = launch_force_bias(rchola, (CC)ghalf_trial_a, 1, X, na * M, xv, 0, st, alias ? 2.0 : 1.0);
+    if (e == cudaSuccess && use_b) e = launch_force_bias(rcholb, (CC)ghalf_trial_b, 1, X, nb * M, xv, 1, st);
+    if (e != cudaSuccess) return (int)e;
+    if (W > 1) {
+      long long blocks = ((long long)(W - 1) * X + 255) / 256;
+      if (blocks > 148 * 16) blocks = 148 * 16;
+      broadcast_row0_kernel<<<(unsigned)blocks, 256, 0, st>>>(xv, W, X);
+      note_launch();
+      if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    }
+  } else {
+    // Coulomb vector in FP64 (DMMA): the Coulomb energy is the large, cancellation-free term
+    e = launch_force_bias(rchola, reinterpret_cast<const double2*>(ghalfa), W, X, na * M, xv, 0, st,
+                          alias ? 2.0 : 1.0);
+    if (e == cudaSuccess && use_b)
+      e = launch_force_bias(rcholb, reinterpret_cast<const double2*>(ghalfb), W, X, nb * M, xv, 1, st);
+    if (e != cudaSuccess) return (int)e;
+  }
   // exchange: 3-pass FP16 tensor-core products (of G - G_T when the trial reference is given),
   // bilinear sums in FP64; the reference row adds raw(G_T) + K.(G - G_T) in FP64
   e = umma::pad_ghalf((CC)ghalfa, W, M, na, NPa, gp, st, delta ? (CC)ghalf_trial_a : nullptr);
+  if (e == cudaSuccess && delta)
+    e = umma::coulomb3(ra_hi, ra_lo, ra_scale, gp, W, X, M, NPa, xv, 1, alias ? 2.0 : 1.0, status, st);
   if (e == cudaSuccess) e = umma::exchange3(ra_hi, ra_lo, ra_scale, gp, W, X, M, na, part, status, st);
   if (e != cudaSuccess) return (int)e;
   int rows = umma::exchange3_rows(X, na);
   if (use_b) {
     e = umma::pad_ghalf((CC)ghalfb, W, M, nb, NPb, gp, st, delta ? (CC)ghalf_trial_b : nullptr);
+    if (e == cudaSuccess && delta) e = umma::coulomb3(rb_hi, rb_lo, rb_scale, gp, W, X, M, NPb, xv, 1, 1.0, status, st);
     if (e == cudaSuccess)
       e = umma::exchange3(rb_hi, rb_lo, rb_scale, gp, W, X, M, nb, part + (size_t)rows * W, status, st);
     if (e != cudaSuccess) return (int)e;
