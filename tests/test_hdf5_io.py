@@ -189,3 +189,74 @@ def test_estimator_file_round_trip(tmp_path):
         assert f["metadata"][()] == b'{"qmc": {"dt": 0.005}}'
         assert f["block_size_1/offset/energy"][()] == 3
         assert sorted(f["block_size_1/data"].keys()) == ["000000000", "000000001"]
+
+
+def _chunked_file(path, arr, chunk, deflate):
+    """A file holding one 2-D float64 dataset in chunked layout (version-1 B-tree of type 1), the
+    chunks optionally deflate-compressed: built by hand from the format specification so the
+    reader's chunk path is exercised without h5py."""
+    import struct
+    import zlib
+
+    from ipie_b200.h5lite import _Writer, _dtype_msg, _message, _object_header, SIGNATURE
+
+    w = _Writer(leaf_k=4)
+    w.alloc(96)
+    rows, cols = arr.shape
+    cr, cc = chunk
+    keys = []
+    for r0 in range(0, rows, cr):
+        for c0 in range(0, cols, cc):
+            blk = np.zeros((cr, cc))
+            sub = arr[r0:r0 + cr, c0:c0 + cc]
+            blk[: sub.shape[0], : sub.shape[1]] = sub
+            raw = blk.astype("<f8").tobytes()
+            if deflate:
+                raw = zlib.compress(raw)
+            a = w.alloc(len(raw))
+            w.put(a, raw)
+            keys.append((len(raw), r0, c0, a))
+    ksize = 8 + 8 * 3
+    node = w.alloc(24 + len(keys) * (ksize + 8) + ksize)
+    body = b""
+    for size, r0, c0, a in keys:
+        body += struct.pack("<IIQQQ", size, 0, r0, c0, 0) + struct.pack("<Q", a)
+    body += struct.pack("<IIQQQ", 0, 0, rows, cols, 0)
+    w.put(node, b"TREE" + struct.pack("<BBH", 1, 0, len(keys)) + b"\xff" * 16 + body)
+    space = struct.pack("<BBBB", 2, 2, 0, 1) + struct.pack("<QQ", rows, cols)
+    layout = struct.pack("<BBBQ", 3, 2, 3, node) + struct.pack("<III", cr, cc, 8)
+    msgs = [_message(0x0001, space), _message(0x0003, _dtype_msg(np.dtype("<f8")), 1), _message(0x0008, layout)]
+    if deflate:
+        msgs.append(_message(0x000B, struct.pack("<BB6xHHHH", 1, 1, 1, 0, 1, 1) + struct.pack("<I4x", 6)))
+    hdr = _object_header(msgs)
+    oh = w.alloc(len(hdr))
+    w.put(oh, hdr)
+    names = b"\0" * 8 + b"data\0\0\0\0"
+    hd = w.alloc(len(names))
+    w.put(hd, names)
+    heap = w.alloc(32)
+    w.put(heap, b"HEAP" + struct.pack("<B3xQ", 0, len(names)) + b"\xff" * 8 + struct.pack("<Q", hd))
+    snod = w.alloc(8 + 8 * 40)
+    w.put(snod, b"SNOD" + struct.pack("<BBH", 1, 0, 1) + struct.pack("<QQII16x", 8, oh, 0, 0))
+    bt = w.alloc(24 + 33 * 8 + 32 * 8)
+    w.put(bt, b"TREE" + struct.pack("<BBH", 0, 0, 1) + b"\xff" * 16 + struct.pack("<QQQ", 0, snod, 8))
+    ghdr = _object_header([_message(0x0011, struct.pack("<QQ", bt, heap))])
+    root = w.alloc(len(ghdr))
+    w.put(root, ghdr)
+    sb = SIGNATURE + struct.pack("<BBBBBBBBHHI", 0, 0, 0, 0, 0, 8, 8, 0, 4, 16, 0)
+    sb += struct.pack("<Q", 0) + b"\xff" * 8 + struct.pack("<Q", len(w.buf)) + b"\xff" * 8
+    sb += struct.pack("<QQII", 0, root, 1, 0) + struct.pack("<QQ", bt, heap)
+    w.put(0, sb)
+    with open(path, "wb") as fh:
+        fh.write(bytes(w.buf))
+
+
+@pytest.mark.parametrize("deflate", [False, True])
+def test_h5lite_reads_chunked_datasets(tmp_path, deflate):
+    arr = np.random.default_rng(5).normal(size=(13, 10))
+    p = tmp_path / "chunked.h5"
+    _chunked_file(p, arr, (4, 3), deflate)
+    with h5lite.File(p) as f:
+        d = f["data"]
+        assert d.shape == (13, 10)
+        np.testing.assert_array_equal(d[()], arr)
