@@ -201,10 +201,11 @@ int ipie_b200_energy_complex(const void* ghalfa, const void* ghalfb, int W, int 
  * out: exx (W) complex = sum_x sum_ij T_ij T_ji.  Limit: ipie_b200_exchange_rows(W,X,M,N) * W
  * <= 1048576 (e.g. W=2048, X=1600, M=200, N=32 fits); larger calls return
  * cudaErrorInvalidValue (1) before any work.  The array is shared by all calls
- * and keeps the last call's partials; calls overlapping on the GPU race.  The
- * first call on a device looks up the array's address (cudaGetSymbolAddress,
- * that device current); make it before any stream capture on that device.
- * Allocates nothing. */
+ * and keeps the last call's partials; calls overlapping on the GPU race.  Every
+ * call looks up the array's address on the current device (cudaGetSymbolAddress),
+ * so a device reset does not leave a stale address; the first call on a device
+ * also loads the library's device code there: make it before any stream capture
+ * on that device.  Allocates nothing. */
 int ipie_b200_exchange_noalloc(const double* rchol, const void* ghalf, int W, int X, int M, int N, void* exx,
                                void* stream);
 
@@ -439,25 +440,10 @@ int ipie_b200_rotate_onebody(const void* psi_conj, const double* h1, int M, int 
  * mixed-precision form (lo may be NULL).  No counterpart in ipie. */
 int ipie_b200_split_tf32(const double* x, float* hi, float* lo, long long n, void* stream);
 
-/* Validation entry of the tcgen05 TF32 GEMM core: c[row][a][col] =
- * sum_k A_a[row][k] B[col][k] for a < na (na = 1 or 2), A_a (M,K) and B (N,K)
- * row-major fp32 with K % 4 == 0; nsplit = 1 (TF32) or 3 (hi/lo split, the
- * *_lo operands used).  No counterpart in ipie. */
-int ipie_b200_umma_gemm_test(const float* a0_hi, const float* a0_lo, const float* a1_hi, const float* a1_lo,
-                             const float* b_hi, const float* b_lo, float* c, int M, int N, int K, int na, int nsplit,
-                             unsigned int* status, void* stream);
-
 /* Split FP64 values, scaled by a power of two, into FP16 head and remainder:
  * x * scale ~= hi + lo (IEEE binary16 arrays; lo may be NULL).  ~2^-22 relative
  * while |x * scale| lies in [2^-3, 65504].  No counterpart in ipie. */
 int ipie_b200_split_f16(const double* x, void* hi, void* lo, long long n, double scale, void* stream);
-
-/* Validation entry of the tcgen05 GEMM core on FP16 operands (kind::f16, FP32
- * accumulation): c[row][col] = sum_k A[row][k] B[col][k], A (M,K) and B (N,K)
- * row-major binary16 with K % 8 == 0; nsplit = 1 or 3 (hi/lo, the *_lo operands
- * used).  No counterpart in ipie. */
-int ipie_b200_umma_gemm_f16_test(const void* a_hi, const void* a_lo, const void* b_hi, const void* b_lo, float* c,
-                                 int M, int N, int K, int nsplit, unsigned int* status, void* stream);
 
 #ifdef __cplusplus
 }

@@ -5,6 +5,7 @@
 #include <mutex>
 
 #include "../../include/ipie_b200.h"
+#include "../../include/ipie_b200_testing.h"
 #include "kernels.h"
 #include "umma_gemm.cuh"
 

@@ -18,14 +18,14 @@
 //     has to start at zero (each call writes every partial it later reads);
 //   * calls that overlap on the GPU (two streams at once) race on the array.
 //
-// Set-up: the first call on a device, with that device current, looks the
-// array's device address up with cudaGetSymbolAddress and caches it; make that
-// first call before any stream capture on the device.
+// Set-up: every call, with the caller's device current, looks the array's
+// device address up with cudaGetSymbolAddress (a host-side table lookup), so
+// the address stays right after a device reset or a new primary context.  The
+// first call on a device also loads the library's device code there (the set-up
+// of the array); make that first call before any stream capture on the device.
 #include "../../include/ipie_b200.h"
 #include "common.cuh"
 #include "kernels.h"
-
-#include <mutex>
 
 namespace ipie_b200 {
 
@@ -33,24 +33,13 @@ static constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 static constexpr size_t kNoAllocScratchElems = kNoAllocScratchBytes / sizeof(double2);
 static __device__ __align__(256) double2 g_exchange_scratch[kNoAllocScratchElems];
 
-static constexpr int kMaxDevices = 64;
-static std::mutex g_scratch_mu;
-static double2* g_scratch_addr[kMaxDevices] = {nullptr};
-
-// Device address of g_exchange_scratch on the current device (cached per device).
+// Device address of g_exchange_scratch on the current device and context.  The
+// host-side name of the array is only a stand-in: kernels get this address.
 static cudaError_t scratch_address(double2** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_exchange_scratch);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (g_scratch_addr[dev] == nullptr) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_exchange_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_addr[dev] = static_cast<double2*>(p);
-  }
-  *out = g_scratch_addr[dev];
+  *out = static_cast<double2*>(p);
   return cudaSuccess;
 }
 

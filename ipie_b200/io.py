@@ -24,13 +24,13 @@ from .h5lite import File, write_file
 def write_hamiltonian(hcore: np.ndarray, LXmn: np.ndarray, e0: float, filename: str = "hamiltonian.h5") -> None:
     """``hcore`` (M, M), ``LXmn`` (naux, M, M), ``e0``; ipie ``utils/io.py:31-43``."""
     if hcore.ndim != 2:
-        raise AssertionError("Incorrect shape for hcore, expected 2-dimensional array")
+        raise AssertionError(f"hcore must be a 2-d (M, M) array, got {hcore.ndim} dimensions")
     nmo = hcore.shape[0]
     naux = LXmn.size // (nmo * nmo)
     if LXmn.ndim != 3:
-        raise AssertionError("Incorrect shape for LXmn, expected 3-dimensional array")
+        raise AssertionError(f"LXmn must be a 3-d (naux, M, M) array, got {LXmn.ndim} dimensions")
     if LXmn.shape[0] != naux:
-        raise AssertionError(f"Incorrect first dimension for LXmn: found {LXmn.shape[0]} expected {naux}")
+        raise AssertionError(f"LXmn has {LXmn.shape[0]} Cholesky vectors along axis 0, its size implies {naux}")
     write_file(filename, {"hcore": np.asarray(hcore), "LXmn": np.asarray(LXmn), "e0": np.float64(e0)})
 
 
@@ -41,11 +41,11 @@ def read_hamiltonian(filename: str) -> Tuple[np.ndarray, np.ndarray, float]:
         LXmn = np.array(f["LXmn"][()])
         e0 = float(f["e0"][()])
     if hcore.ndim != 2:
-        raise AssertionError("Incorrect shape for hcore, expected 2-dimensional array")
+        raise AssertionError(f"hcore must be a 2-d (M, M) array, got {hcore.ndim} dimensions")
     nmo = hcore.shape[0]
     naux = LXmn.size // (nmo * nmo)
     if LXmn.ndim != 3 or LXmn.shape[0] != naux:
-        raise AssertionError("Incorrect shape for LXmn")
+        raise AssertionError(f"LXmn of shape {LXmn.shape} is not (naux, M, M) with M = {nmo}")
     return hcore, LXmn, e0
 
 
@@ -59,14 +59,14 @@ def write_wavefunction(wfn, filename: str = "wavefunction.h5", phi0=None) -> Non
     elif len(wfn) == 2:
         write_noci_wavefunction(wfn, filename, phi0=phi0)
     else:
-        raise RuntimeError("Unknown wavefunction time.")
+        raise RuntimeError("wavefunction is neither an array/list, a (ci, occa, occb) triple nor a (ci, [psia, psib]) pair")
 
 
 def write_single_det_wavefunction(wfn, filename: str, phi0=None) -> None:
     """ipie ``utils/io.py:108-128``: UHF as psi_T_alpha/beta (+ phi0_*), RHF as psi_T_alpha only."""
     if isinstance(wfn, list) or np.asarray(wfn).ndim == 3:
         if len(wfn) != 2:
-            raise AssertionError("Expected list for UHF wavefunction.")
+            raise AssertionError("a UHF wavefunction is a pair [psia, psib]")
         tree = {"psi_T_alpha": np.asarray(wfn[0]), "psi_T_beta": np.asarray(wfn[1])}
         init = wfn if phi0 is None else phi0
         tree["phi0_alpha"] = np.asarray(init[0])
@@ -74,7 +74,7 @@ def write_single_det_wavefunction(wfn, filename: str, phi0=None) -> None:
     else:
         wfn = np.asarray(wfn)
         if wfn.ndim != 2:
-            raise AssertionError("Expected 2D array for RHF wavefunction.")
+            raise AssertionError("an RHF wavefunction is one (M, N) array")
         tree = {"psi_T_alpha": wfn, "phi0_alpha": wfn if phi0 is None else np.asarray(phi0[0])}
     write_file(filename, tree)
 
@@ -82,7 +82,7 @@ def write_single_det_wavefunction(wfn, filename: str, phi0=None) -> None:
 def write_particle_hole_wavefunction(wfn: tuple, filename: str, phi0=None) -> None:
     """ipie ``utils/io.py:131-138``."""
     if len(wfn) != 3:
-        raise AssertionError("Expected (ci, occa, occb).")
+        raise AssertionError("a particle-hole wavefunction is the triple (ci, occa, occb)")
     write_file(filename, {"ci_coeffs": np.asarray(wfn[0]), "occ_alpha": np.asarray(wfn[1]),
                           "occ_beta": np.asarray(wfn[2])})
 
@@ -128,7 +128,7 @@ def read_wavefunction(filename: str):
     try:
         return read_single_det_wavefunction(filename)
     except Exception as exc:
-        raise RuntimeError("Unknown file format.") from exc
+        raise RuntimeError(f"{filename}: no wavefunction layout recognised") from exc
 
 
 def determine_wavefunction_type(filename: str) -> str:
@@ -143,7 +143,7 @@ def determine_wavefunction_type(filename: str) -> str:
         return "single_determinant"
     if "Wavefunction" in keys:
         return "qmcpack"
-    raise RuntimeError("Unknown wavefunction.")
+    raise RuntimeError(f"{filename}: no wavefunction datasets found")
 
 
 # ---------------------------------------------------------------- QMCPACK layouts (utils/io.py:273-717)
@@ -297,7 +297,7 @@ def write_qmcpack_wfn(filename, wfn, walker_type, nelec, norb, init=None, mode="
                 grp[f"PsiT_{2 * idet + 1:d}"] = _nomsd_single(scipy.sparse.csr_matrix(w[:, na:].conj().T))
         name = "NOMSD"
     else:
-        raise RuntimeError("Unknown wavefunction type passed.")
+        raise RuntimeError("wavefunction to write is neither particle-hole (ci, occa, occb) nor NOCI (ci, determinants)")
     coeffs = np.asarray(coeffs)
     grp["ci_coeffs"] = to_qmcpack_complex(coeffs)
     grp["dims"] = np.array([norb, na, nb, wt, len(coeffs)], dtype=np.int32)
@@ -323,7 +323,7 @@ def read_qmcpack_nomsd_hdf5(wgroup, nelec=None):
     dims = wgroup["dims"][()]
     nmo, na, nb = int(dims[0]), int(dims[1]), int(dims[2])
     if nelec is not None:
-        assert na == nelec[0] and nb == nelec[1], "Number of electrons does not match wavefunction"
+        assert na == nelec[0] and nb == nelec[1], f"file holds {na}+{nb} electrons, the caller asked for {nelec[0]}+{nelec[1]}"
     uhf = int(dims[3]) == 2
     nci = int(dims[4])
     coeffs = from_qmcpack_complex(wgroup["ci_coeffs"][()], (nci,))
@@ -364,7 +364,7 @@ def read_qmcpack_wfn_hdf(filename, nelec=None, get_nelec=False):
             g = f["Wavefunction/PHMSD"]
             wfn, psi0 = read_qmcpack_phmsd_hdf5(g, nelec=nelec)
         else:
-            raise KeyError("Wavefunction not found.")
+            raise KeyError("no Wavefunction/NOMSD or Wavefunction/PHMSD group in the file")
         dims = g["dims"][()]
     if get_nelec:
         return wfn, psi0, (int(dims[1]), int(dims[2]))
@@ -473,7 +473,7 @@ def extract_observable(filename, name="energy", block_idx=1):
     with File(filename) as f:
         data = np.concatenate([f[f"{grp}/data/{d}"][()].real for d in f[f"{grp}/data"].keys()])
         if name not in f[f"{grp}/shape"].keys():
-            raise RuntimeError(f"Unknown value for name={name}")
+            raise RuntimeError(f"estimator file has no quantity {name!r}")
         shape = f[f"{grp}/shape/{name}"][()]
         offset = int(f[f"{grp}/offset/{name}"][()])
         size = int(f[f"{grp}/size/{name}"][()])

@@ -318,14 +318,20 @@ class PhaselessGeneric:
         a copy stream (after the compute stream has consumed that buffer), so the host-to-device
         transfer overlaps the step instead of preceding it."""
         cur = torch.cuda.current_stream()
+        src = self.host_fields
         pending = getattr(ws, "xi_pending", None)
+        if pending is not None and pending[0] is not src:
+            # the caller replaced the iterator: the array prefetched from the old one is not this
+            # step's (the copy still lands in a buffer that nothing reads before it is rewritten)
+            cur.wait_event(pending[2])
+            pending = None
         if pending is None:
-            ws.xi.copy_(next(self.host_fields), non_blocking=True)  # (W, X) float64, pinned host memory
+            ws.xi.copy_(next(src), non_blocking=True)  # (W, X) float64, pinned host memory
             buf = ws.xi
         else:
-            buf, ready = pending
+            _, buf, ready = pending
             cur.wait_event(ready)
-        nxt = next(self.host_fields, None)
+        nxt = next(src, None)
         if nxt is None:
             ws.xi_pending = None
             return buf
@@ -340,7 +346,7 @@ class PhaselessGeneric:
             other.copy_(nxt, non_blocking=True)
             ready = torch.cuda.Event()
             ready.record(ws.copy_stream)
-        ws.xi_pending = (other, ready)
+        ws.xi_pending = (src, other, ready)
         return buf
 
     def propagate_walkers_two_body(self, walkers, hamiltonian, trial):

@@ -437,3 +437,33 @@ def test_host_fields_prefetch_matches_numpy_draws():
     assert torch.equal(w1.weight, w2.weight)
     assert torch.equal(w1.phia, w2.phia)
     assert torch.equal(w1.ovlp, w2.ovlp)
+
+
+def test_host_fields_new_iterator_drops_prefetch():
+    """Replacing ``propagator.host_fields`` part-way through an iterator: the array prefetched from
+    the old iterator is dropped and the next step takes the new iterator's first array."""
+    from ipie_b200 import synthetic
+    from ipie_b200.propagation import PhaselessGeneric
+
+    s = synthetic.generate(26, (5, 3), 60, decay=30.0, seed=6, uhf=True, chol_scale="stable")
+    W, k, nsteps = 12, 3, 7
+    ham, trial, w1, p1 = gpu_objects(s, W)
+    _, _, w2, _ = gpu_objects(s, W)
+    p2 = PhaselessGeneric(0.005, rng="host")
+    p2.build(ham, trial, w2)
+    np.random.seed(91)
+    draws = [np.random.normal(0.0, 1.0, ham.nfields * W).reshape(W, ham.nfields) for _ in range(nsteps)]
+    pinned = [torch.from_numpy(d.copy()).pin_memory() for d in draws]
+    # the first iterator holds k steps' arrays plus two that are never used
+    stale = [torch.from_numpy(np.full_like(draws[0], 3.0)).pin_memory() for _ in range(2)]
+    p2.host_fields = iter(pinned[:k] + stale)
+    np.random.seed(91)
+    for step in range(nsteps):
+        if step == k:
+            p2.host_fields = iter(pinned[k:])
+        p1.propagate_walkers(w1, ham, trial, 0.0 if step == 0 else -1.0)
+        p2.propagate_walkers(w2, ham, trial, 0.0 if step == 0 else -1.0)
+    torch.cuda.synchronize()
+    assert torch.equal(w1.weight, w2.weight)
+    assert torch.equal(w1.phia, w2.phia)
+    assert torch.equal(w1.ovlp, w2.ovlp)

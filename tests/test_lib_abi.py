@@ -3,17 +3,18 @@
 No compute calls: these run without a GPU.
 """
 import ctypes
+import glob
 import os
 import re
 
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "ipie_b200.h")
+HEADERS = sorted(glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
-def declared():
-    src = open(HEADER).read()
+def declared(headers=HEADERS):
+    src = "".join(open(h).read() for h in headers)
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(ipie_b200_\w+)\s*\(", src)))
 
@@ -30,6 +31,11 @@ def test_header_declares_entry_points():
     names = declared()
     assert "ipie_b200_greens_function_single_det_batch" in names
     assert len(names) >= 15
+
+
+def test_product_header_holds_no_testing_entries():
+    product = declared([os.path.join(ROOT, "include", "ipie_b200.h")])
+    assert not [n for n in product if n.endswith("_test")]
 
 
 def test_library_exports_every_declared_symbol(lib):

@@ -64,11 +64,35 @@ def test_noalloc_matches_workspace_entry_point_twice(W, X, M, N):
         assert err < TOL, err
 
 
-def test_noalloc_rejects_sizes_beyond_its_scratch():
+def test_noalloc_smaller_call_after_larger_one():
+    """A large call leaves its partials in the shared array; a following call with fewer walkers
+    (a different row stride) and other data must read only what it wrote itself."""
     lib = _lib()
-    rchol, ghalf = _inputs(4, 8, 4, 2, seed=1)
-    exx = torch.zeros(4, dtype=torch.complex128, device="cuda")
-    # 4096 walkers x 400 partial rows exceed the 1048576-entry array: rejected before any launch
-    rc = lib.ipie_b200_exchange_noalloc(_p(rchol), _p(ghalf), 4096, 1600, 200, 32, _p(exx), _stream())
+    big = (2048, 1600, 200, 32)
+    rchol, ghalf = _inputs(*big, seed=3)
+    exx = torch.empty(big[0], dtype=torch.complex128, device="cuda")
+    assert lib.ipie_b200_exchange_noalloc(_p(rchol), _p(ghalf), *big, _p(exx), _stream()) == 0
+    del rchol, ghalf, exx
+    small = (300, 500, 40, 8)
+    rchol, ghalf = _inputs(*small, seed=11)
+    ref = _with_workspace(rchol, ghalf, *small)
+    exx = torch.full((small[0],), complex(np.nan, np.nan), dtype=torch.complex128, device="cuda")
+    assert lib.ipie_b200_exchange_noalloc(_p(rchol), _p(ghalf), *small, _p(exx), _stream()) == 0
+    torch.cuda.synchronize()
+    err = (exx - ref).abs().max().item() / ref.abs().max().item()
+    assert err < TOL, err
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    """8192 walkers x 129 partial rows exceed the 1048576-entry array and are rejected before any
+    launch.  The buffers are sized for the call (small M and N keep them cheap), so a broken size
+    check would give a wrong answer here rather than touch memory outside them."""
+    lib = _lib()
+    W, X, M, N = 8192, 2064, 8, 8
+    assert lib.ipie_b200_exchange_rows(W, X, M, N) * W > 1048576
+    rchol, ghalf = _inputs(W, X, M, N, seed=1)
+    exx = torch.zeros(W, dtype=torch.complex128, device="cuda")
+    rc = lib.ipie_b200_exchange_noalloc(_p(rchol), _p(ghalf), W, X, M, N, _p(exx), _stream())
     assert rc == 1  # cudaErrorInvalidValue
     torch.cuda.synchronize()
+    assert bool((exx == 0).all())
