@@ -87,9 +87,47 @@ def load_peaks():
             d = json.load(fh)
         peaks.update({k: d[k] for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained") if k in d})
         peaks["source"] = "measured"
-    # FP64 and TF32 peaks: cuBLAS 8192^3 GEMMs measured on this pool's B200 (python bench.py --measure-peaks)
+    # FP64 and TF32 peaks: measured in the run (gemm_peaks) before the forms are timed; these
+    # are the values an earlier measurement on this pool's B200s gave, kept only as a fallback
     peaks["fp64_tflops"] = 35.47
     peaks["tf32_tflops"] = 755.8
+    peaks["fp64_tf32_source"] = "earlier cuBLAS 8192^3 measurement on B200"
+    return peaks
+
+
+def _best_time(fn, iters=5):
+    import torch
+
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    out = 1e9
+    for _ in range(iters):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        out = min(out, a.elapsed_time(b) / 1e3)
+    return out
+
+
+def gemm_peaks(peaks):
+    """cuBLAS FP64 and TF32 GEMM rates (8192^3, best of 5, CUDA events), measured in this run on
+    this GPU: the denominators of the FP64 form's phases and of the TF32 products."""
+    import torch
+
+    n = 8192
+    for key, dt, tf32 in (("fp64_tflops", torch.float64, False), ("tf32_tflops", torch.float32, True)):
+        prev = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(n, n, device="cuda", dtype=dt)
+        b = torch.randn(n, n, device="cuda", dtype=dt)
+        peaks[key] = round(2 * n ** 3 / _best_time(lambda: a @ b) / 1e12, 2)
+        torch.backends.cuda.matmul.allow_tf32 = prev
+        del a, b
+    torch.cuda.empty_cache()
+    peaks["fp64_tf32_source"] = "measured in this run: cuBLAS 8192^3 GEMM, best of 5"
     return peaks
 
 
@@ -202,32 +240,43 @@ def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5, gr
     return af, s
 
 
-def cpu_oracle_rate(wl, walkers_sample=64, steps=2, energy_walkers=2):
-    """Oracle (numpy port) walker-steps/s on the host cores for a bounded sample."""
-    from ipie_b200 import synthetic
-    from oracle import afqmc_oracle as O
+class CpuSample:
+    """ipie's numpy walker step restated (the oracle) on the host cores, on a bounded sample of a
+    workload: ``walkers`` walkers propagated one step plus the local energy of ``energy_walkers``
+    walkers, amortised at one evaluation per 25 steps as in the driver loop."""
 
-    p = WORKLOADS[wl]
-    s = synthetic.generate(p["nbasis"], p["nocc"], p["nchol"], p["decay"], seed=7, uhf=p["uhf"], chol_scale="stable")
-    S = O.System(s.nbasis, s.nup, s.ndown, s.h1e, s.chol, s.ecore, s.psi).build()
-    w = O.Walkers.from_initial(s.init, s.nup, walkers_sample)
-    np.random.seed(7)
-    O.greens_function(S, w)
-    t0 = time.perf_counter()
-    for step in range(1, steps + 1):
+    def __init__(self, wl, walkers=32, energy_walkers=1):
+        from ipie_b200 import synthetic
+        from oracle import afqmc_oracle as O
+
+        p = WORKLOADS[wl]
+        s = synthetic.generate(p["nbasis"], p["nocc"], p["nchol"], p["decay"], seed=7, uhf=p["uhf"],
+                               chol_scale="stable")
+        self.O = O
+        self.S = O.System(s.nbasis, s.nup, s.ndown, s.h1e, s.chol, s.ecore, s.psi).build()
+        self.w = O.Walkers.from_initial(s.init, s.nup, walkers)
+        np.random.seed(7)
+        O.greens_function(self.S, self.w)
+        self.walkers, self.energy_walkers = walkers, energy_walkers
+        self.sample = (f"{walkers} walkers x 1 propagation step + local energy of {energy_walkers} walker(s) "
+                       f"(amortised 1 per 25 steps), same system")
+
+    def step(self):
+        """One sample: returns (walker-steps/s, seconds the sample took)."""
+        O, S, w = self.O, self.S, self.w
+        t0 = time.perf_counter()
         O.propagate_walkers(S, w, 0.0)
-    t_prop = (time.perf_counter() - t0) / (steps * walkers_sample)
-    sub = w.copy()
-    sub.phia, sub.phib = w.phia[:energy_walkers].copy(), w.phib[:energy_walkers].copy()
-    sub.log_shift = w.log_shift[:energy_walkers]
-    t0 = time.perf_counter()
-    O.greens_function(S, sub)
-    O.local_energy_single_det_uhf_batch(S, sub)
-    t_en = (time.perf_counter() - t0) / energy_walkers
-    rate = 1.0 / (t_prop + t_en / 25.0)
-    sample = (f"{walkers_sample} walkers x {steps} propagation steps + local energy of {energy_walkers} walkers "
-              f"(amortised 1 per 25 steps), same system")
-    return rate, sample, t_prop, t_en
+        t1 = time.perf_counter()
+        sub = w.copy()
+        n = self.energy_walkers
+        sub.phia, sub.phib = w.phia[:n].copy(), w.phib[:n].copy()
+        sub.log_shift = w.log_shift[:n]
+        O.greens_function(S, sub)
+        O.local_energy_single_det_uhf_batch(S, sub)
+        t2 = time.perf_counter()
+        t_prop = (t1 - t0) / self.walkers
+        t_en = (t2 - t1) / n
+        return 1.0 / (t_prop + t_en / 25.0), t2 - t0
 
 
 def blas_threads():
@@ -246,13 +295,14 @@ def run_reference(args):
         return 0
     wl = args.workload
     p = WORKLOADS[wl]
-    rates = []
-    sample = ""
+    cpu = CpuSample(wl, walkers=args.ref_walkers, energy_walkers=1)
     for _ in range(max(args.warmup, 0)):
-        pass  # the oracle has no warm-up state; each timed step is an independent bounded sample
+        cpu.step()
+    rates, secs = [], []
     for _ in range(max(args.steps, 1)):
-        r, sample, _, _ = cpu_oracle_rate(wl, walkers_sample=args.ref_walkers, steps=1, energy_walkers=1)
+        r, dt = cpu.step()
         rates.append(r)
+        secs.append(dt)
     value = float(np.median(rates))
     cores = blas_threads()
     line = {
@@ -263,15 +313,19 @@ def run_reference(args):
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": (args.walkers or p["walkers"]) / value * 1e3,
+        # a step of this arm is one bounded sample (below), timed by the wall clock
+        "ms_per_step": float(np.median(secs)) * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
         "config": line_config(wl, args.walkers or p["walkers"], int(os.environ.get("WORLD_SIZE", "1"))),
-        "reference_path": "ipie's numpy walker step (oracle restatement, pinned to ipie) on the host cores",
-        "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": "port", "sample": sample},
+        "reference_path": ("ipie's numpy walker step (the oracle: numpy restatement pinned to ipie's outputs) on "
+                           "the host cores; ipie's own run of the same sample is timed against it on the build "
+                           "host (the ipie source does not travel to the GPU host)"),
+        "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": "port",
+                         "sample": cpu.sample},
         "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -299,20 +353,53 @@ def train_control_variate(wl, W, rank, steps=100, epochs=60):
     return cv, info
 
 
-def precision_shift(wl, W, rank, steps=100):
+def statistics_runs(wl, W, rank, steps, cv=None, dt=0.005):
     """Block energies of the FP64 and mixed forms over ``steps`` steps with identical draws and no
     population control (a flipped branching decision would swap whole walkers between the runs and
-    hide the precision effect); returns the largest difference in mEh and both series."""
-    out = {}
+    hide the precision effect), and of the mixed + control-variate estimator evaluated on the mixed
+    run's walkers at the same block ends (the control variate changes the estimator, not the walk).
+
+    Returns {form: block ETotal series (blocks 1..n)} and, per form, ipie's reblocking analysis
+    (:func:`ipie_b200.analysis.reblock_mixed`) of the blocks after ipie's equilibration time 2/dt
+    and of the paired differences to FP64 over the same blocks."""
+    from ipie_b200.analysis import reblock_mixed
+
+    series = {}
+    seconds = {}
     for form in ("fp64", "mixed"):
-        af, _ = build_afqmc(wl, W, "device", 4242 + rank, precision=form, pop_control_freq=10 ** 9)
+        af, _ = build_afqmc(wl, W, "device", 4242 + rank, precision=form, pop_control_freq=10 ** 9, graph=True)
         af.setup_run()
+        cv_est, e_cv = None, []
+        if form == "mixed" and cv is not None:
+            from ipie_b200.control_variate import ControlVariateEnergyEstimator
+
+            cv_est = ControlVariateEnergyEstimator(cv, fraction=8, seed=99 + rank, precision="mixed")
+        t0 = time.perf_counter()
         for step in range(1, steps + 1):
             af.step(step)
-        out[form] = np.array(af.block_data)[:, 5].real
+            if cv_est is not None and step % af.params.num_steps_per_block == 0:
+                d = cv_est.compute_estimator(af.system, af.walkers, af.hamiltonian, af.trial)
+                e_cv.append(float((d[0] / d[1]).real))
+        seconds[form] = time.perf_counter() - t0
+        series[form] = np.array(af.block_data)[1:, 5].real
+        if cv_est is not None:
+            series["mixed_cv"] = np.array(e_cv)
         del af
-    n = min(len(out["fp64"]), len(out["mixed"]))
-    return float(np.max(np.abs(out["mixed"][:n] - out["fp64"][:n]))) * 1e3, out
+    n = min(len(v) for v in series.values())
+    series = {k: v[:n] for k, v in series.items()}
+    eq = min(int(round(2.0 / dt / 25)), max(n - 8, 0))  # ipie's equilibration time, in 25-step blocks
+    out = {"blocks": n, "equilibration_blocks": eq, "steps": steps, "seconds": seconds, "forms": {}}
+    for form, v in series.items():
+        rb = reblock_mixed(v[eq:])
+        entry = {"energy_Eh": rb["mean"], "error_mEh": rb["error"] * 1e3, "error_ac_mEh": rb["error_ac"] * 1e3,
+                 "reblock_converged": rb["converged"], "block": rb["block"]}
+        if form != "fp64":
+            d = reblock_mixed(v[eq:] - series["fp64"][eq:])
+            entry["vs_fp64_mEh"] = d["mean"] * 1e3
+            entry["vs_fp64_err_mEh"] = max(d["error"], d["error_ac"]) * 1e3
+            entry["vs_fp64_max_block_mEh"] = float(np.max(np.abs(v - series["fp64"]))) * 1e3
+        out["forms"][form] = entry
+    return series, out
 
 
 def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clock=False, cv=None):
@@ -405,6 +492,58 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
     return res
 
 
+# tensor pipe of each mixed-form phase: every product is a 3-pass head/remainder product on FP16
+# operands (kind::f16, the bf16 tensor rate) -- force bias, VHS and the orbital chain
+MIXED_PIPE = {"force_bias": "f16", "vhs": "f16", "orbitals": "f16"}
+
+
+def phase_roofline(r, form, fl, fl_ipie, W, peaks, wl):
+    """Roofline of the phase with the largest CUDA-event time in ``r`` (one timed form), and every
+    tensor-core phase's fraction of its pipe's peak.
+
+    ``achieved`` counts ALGORITHMIC FLOPs: the per-walker figure of ``flops_per_walker`` (identical
+    RHF spin blocks counted once when they are computed once) x walkers x launches / event time.
+    The mixed form executes each product as 3 passes (head x head, head x remainder, remainder x
+    head): ``achieved_executed`` counts those; ``achieved_ipie_work`` counts both spin blocks."""
+    phases = r["phases"]
+    dom = max((k for k in phases if k in fl), key=lambda k: phases[k][1])
+    n_launch, tot_ms = phases[dom]
+    passes = 3 if form == "mixed" else 1
+
+    def pipe_of(k):
+        if form != "mixed":
+            return "fp64", peaks["fp64_tflops"], f"cuBLAS DGEMM 8192^3 ({peaks['fp64_tf32_source']})"
+        if MIXED_PIPE.get(k, "tf32") == "f16":
+            return ("f16", peaks["bf16_tflops"],
+                    f"{peaks['source']} cuBLAS bf16 8192^3 burst (MEASURED_PEAKS.json; fp16 runs at the bf16 rate)")
+        return "tf32", peaks["tf32_tflops"], f"cuBLAS TF32 8192^3 ({peaks['fp64_tf32_source']})"
+
+    def rate(k, per_walker):
+        n, ms = phases[k]
+        return per_walker * W * n / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+
+    pipe, peak, src = pipe_of(dom)
+    achieved = rate(dom, fl[dom])
+    tensor_phases = [k for k in sorted(phases) if k in fl and k != "greens_function" and phases[k][1] > 0]
+    return {
+        "kernel": dom, "bound": "tensor", "pipe": pipe + (" (3 passes)" if passes == 3 else " (DMMA)"),
+        "achieved": round(achieved, 3), "peak": peak, "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+        "frac_of": "measured" if "measured" in src else "fallback",
+        "achieved_executed": round(passes * achieved, 3),
+        "achieved_ipie_work": round(rate(dom, fl_ipie[dom]), 3),
+        "algorithmic_gflop_per_launch": round(fl[dom] * W * n_launch / max(n_launch, 1) / 1e9, 3),
+        "launch_ms": round(tot_ms / max(n_launch, 1), 4),
+        "traffic": DRAM_TRAFFIC.get((wl, form, dom)),
+        "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled by walkers)",
+        "peak_source": src,
+        "phase_ms_per_step": {k: round(v[1] / r["phase_steps"], 4) for k, v in sorted(phases.items())},
+        "phase_frac_of_peak": {k: round(rate(k, fl[k]) / pipe_of(k)[1], 4) for k in tensor_phases},
+        "phase_frac_executed": {k: round(passes * rate(k, fl[k]) / pipe_of(k)[1], 4) for k in tensor_phases},
+        "phase_pipe": {k: pipe_of(k)[0] for k in tensor_phases},
+        "phase_timing": f"{r['phase_steps']} steps launched kernel by kernel with CUDA events between phases",
+    }
+
+
 def run_ours(args):
     import torch
 
@@ -414,6 +553,8 @@ def run_ours(args):
     W = args.walkers or p["walkers"]
     M, na, nb, X = p["nbasis"], p["nocc"], p["nocc"], p["nchol"]
     peaks = load_peaks()
+    if torch.cuda.is_available():
+        gemm_peaks(peaks)
     forms = ["fp64", "mixed"] if args.form == "both" else [args.form]
 
     runs = {}
@@ -424,45 +565,17 @@ def run_ours(args):
         cv, cv_info = train_control_variate(wl, W, rank, steps=args.cv_steps)
         runs["mixed_cv"] = timed_run(wl, W, "mixed", args, rank, world, local, cv=cv)
         cv_info["estimator_error"] = runs["mixed_cv"].pop("cv_error", None)
-        del cv
+    else:
+        cv = None
     head = "mixed" if "mixed" in runs else "fp64"
     r = runs[head]
     t = r["t"]
     value = W * args.steps * world / t
 
-    # roofline of the dominant kernel phase of the headline form (work executed)
     alias = r["alias"]
     fl, fl_energy = flops_per_walker(M, na, nb, X, alias=alias)
     fl_ipie, fl_energy_ipie = flops_per_walker(M, na, nb, X, alias=False)
-    phases = r["phases"]
-    dom = max((k for k in phases if k in fl), key=lambda k: phases[k][1])
-    n_launch, tot_ms = phases[dom]
-    # tensor pipe of each mixed-form phase: every product is a 3-pass hi/lo product on FP16
-    # operands (kind::f16, same tensor rate as bf16) -- the force bias, VHS and the orbital chain
-    mixed_pipe = {"force_bias": "f16", "vhs": "f16", "orbitals": "f16"}
-    pipe_peak = {"f16": (peaks["bf16_tflops"], "f16 (3 passes)",
-                         f"{peaks['source']} cuBLAS bf16 8192^3 on B200 (MEASURED_PEAKS.json; fp16 runs at the bf16 rate)"),
-                 "tf32": (peaks["tf32_tflops"], "tf32 (3 passes)", "measured cuBLAS TF32 8192^3 on B200 (tcgen05)")}
-    if head == "mixed":
-        achieved = 3 * fl[dom] * W * n_launch / (tot_ms / 1e3) / 1e12
-        peak, pipe, src = pipe_peak[mixed_pipe.get(dom, "tf32")]
-    else:
-        achieved = fl[dom] * W * n_launch / (tot_ms / 1e3) / 1e12
-        peak, pipe, src = peaks["fp64_tflops"], "fp64 (DMMA)", "measured cuBLAS DGEMM 8192^3 on B200"
-    roofline = {
-        "kernel": dom, "bound": "tensor", "pipe": pipe, "achieved": round(achieved, 3), "peak": peak,
-        "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": DRAM_TRAFFIC.get((wl, head, dom)),
-        "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled by walkers)",
-        "peak_source": src,
-        "phase_ms_per_step": {k: round(v[1] / r["phase_steps"], 4) for k, v in sorted(phases.items())},
-        # every tensor-core phase against its pipe's peak (executed FLOPs: 3 passes in the mixed form)
-        "phase_frac_of_peak": {k: round((3 if head == "mixed" else 1) * fl[k] * W * v[0] / (v[1] / 1e3) / 1e12
-                                        / (pipe_peak[mixed_pipe.get(k, "tf32")][0] if head == "mixed" else peak), 4)
-                               for k, v in sorted(phases.items()) if k in fl and k != "greens_function" and v[1] > 0},
-        "phase_pipe": ({k: mixed_pipe.get(k, "tf32") for k in phases if k in fl and k != "greens_function"}
-                       if head == "mixed" else None),
-        "phase_timing": f"{r['phase_steps']} steps launched kernel by kernel with CUDA events between phases",
-    }
+    roofline = phase_roofline(r, head, fl, fl_ipie, W, peaks, wl)
     step_flops = (sum(v for k, v in fl.items() if k != "orbitals") * W + fl_energy * W / 25.0)
     step_flops_ipie = (sum(v for k, v in fl_ipie.items() if k != "orbitals") * W + fl_energy_ipie * W / 25.0)
 
@@ -471,23 +584,44 @@ def run_ours(args):
         forms_out[form] = {"walker_steps_per_s": W * args.steps * world / rr["t"], "ms_per_step": rr["t"] / args.steps * 1e3,
                            "gpu_launches": int(rr["launches"]), "cuda_graph_steps": rr["graph"],
                            "block_etotal": [round(float(x), 9) for x in rr["blocks"][:, 5]]}
-    shift = None
+    if "fp64" in runs and head != "fp64":
+        forms_out["fp64"]["roofline"] = phase_roofline(runs["fp64"], "fp64", fl, fl_ipie, W, peaks, wl)
+    shift = shift_err = None
+    stats = None
     if "mixed" in runs and "fp64" in runs:
         a, b = runs["mixed"]["blocks"][:, 5], runs["fp64"]["blocks"][:, 5]
         n = min(len(a), len(b))
         # with population control a single flipped branching decision moves whole walkers
         forms_out["trajectory_shift_with_branching_mEh"] = float(np.max(np.abs(a[:n] - b[:n]))) * 1e3
-        shift, series = precision_shift(wl, W, rank)
-        forms_out["precision_shift_runs"] = {k: [round(float(x), 9) for x in v] for k, v in series.items()}
         forms_out["mixed_over_fp64"] = forms_out["mixed"]["walker_steps_per_s"] / forms_out["fp64"]["walker_steps_per_s"]
         forms_out["mixed"]["estimator_shift_mEh"] = runs["mixed"].get("estimator_shift_mEh")
+        if args.stat_steps > 0:
+            series, stats = statistics_runs(wl, W, rank, args.stat_steps, cv=cv)
+            stats["block_etotal"] = {k: [round(float(x), 9) for x in v] for k, v in series.items()}
+            e0 = stats["forms"]["fp64"]["error_mEh"]
+            for form, st in stats["forms"].items():
+                if form not in forms_out:
+                    continue
+                # statistical efficiency 1/(sigma^2 t) against the FP64 form: >1 means the form reaches
+                # a given error bar in less time; sigma from the reblocked block energies, t = ms/step
+                t_ratio = forms_out["fp64"]["ms_per_step"] / forms_out[form]["ms_per_step"]
+                st["efficiency_vs_fp64"] = (e0 / st["error_mEh"]) ** 2 * t_ratio if st["error_mEh"] > 0 else None
+                forms_out[form]["statistics"] = st
+                if form != "fp64":
+                    st["within_0p1_mEh"] = bool(abs(st["vs_fp64_mEh"]) - 2 * st["vs_fp64_err_mEh"] <= 0.1)
+            shift = abs(stats["forms"]["mixed"]["vs_fp64_mEh"])
+            shift_err = stats["forms"]["mixed"]["vs_fp64_err_mEh"]
+            if "mixed_cv" in stats["forms"] and "mixed_cv" in forms_out:
+                st = stats["forms"]["mixed_cv"]
+                gain = st["efficiency_vs_fp64"] / stats["forms"]["mixed"]["efficiency_vs_fp64"]
+                st["cv_gain_over_mixed"] = gain
+                st["note"] = ("the control variate's cheaper energy evaluations outweigh its added noise" if gain > 1
+                              else "the control variate's added noise cancels its cheaper energy evaluations")
     if "mixed_cv" in runs and "fp64" in runs:
-        a, b = runs["mixed_cv"]["blocks"][1:, 5], runs["fp64"]["blocks"][1:, 5]
-        n = min(len(a), len(b))
-        forms_out["mixed_cv"]["energy_shift_vs_fp64_mEh"] = float(np.max(np.abs(a[:n] - b[:n]))) * 1e3
         forms_out["mixed_cv_over_fp64"] = (forms_out["mixed_cv"]["walker_steps_per_s"]
                                           / forms_out["fp64"]["walker_steps_per_s"])
         forms_out["mixed_cv"]["training"] = cv_info
+    del cv
 
     # ---------------- end to end through the public API (headline form) ----------------
     e2e_steps = min(args.steps, args.e2e_steps)
@@ -521,8 +655,11 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            rcpu, sample, _, _ = cpu_oracle_rate(wl, walkers_sample=args.ref_walkers, steps=2, energy_walkers=1)
-            cpu = {"value": rcpu, "unit": "walker-steps/s", "cores": blas_threads(), "kind": "port", "sample": sample}
+            sampler = CpuSample(wl, walkers=args.ref_walkers, energy_walkers=1)
+            sampler.step()  # warm-up
+            rcpu = float(np.median([sampler.step()[0] for _ in range(2)]))
+            cpu = {"value": rcpu, "unit": "walker-steps/s", "cores": blas_threads(), "kind": "port",
+                   "sample": sampler.sample + ", median of 2 after 1 warm-up"}
         line = {
             "metric": METRIC,
             "value": value,
@@ -539,9 +676,14 @@ def run_ours(args):
             "config": line_config(wl, W, world, head),
             "forms": forms_out,
             "energy_shift_mEh": shift,
-            "energy_shift_method": ("max |block E(mixed) - block E(fp64)| over 100 steps (4 blocks) of 2 runs with "
-                                    "identical draws and no population control; estimator-only shift on identical "
-                                    "walkers in forms.mixed.estimator_shift_mEh"),
+            "energy_shift_err_mEh": shift_err,
+            "energy_shift_method": (f"|mean of block E(mixed) - block E(fp64)| over the blocks after ipie's "
+                                    f"equilibration time (2/dt) of two {args.stat_steps}-step runs with identical "
+                                    "draws and no population control, reblocked error (ipie's reblock_mixed: "
+                                    "Flyvbjerg-Petersen and autocorrelation, the larger); per form in "
+                                    "forms.*.statistics; estimator-only shift on identical walkers in "
+                                    "forms.mixed.estimator_shift_mEh"),
+            "statistics": ({k: v for k, v in stats.items() if k != "forms"} if stats else None),
             "e2e": {"value": e2e_value, "unit": "walker-steps/s", "h2d_bytes_per_step": W * X * 8,
                     "d2h_bytes_per_step": W * 8, "steps": e2e_steps,
                     "fields": "host-supplied N(0,1) draws in pinned memory, one (W, X) array per step"},
@@ -609,6 +751,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cv", action="store_true", help="skip the learned control-variate form")
     ap.add_argument("--cv-steps", type=int, default=100, help="plain-method steps generating control-variate training data")
+    ap.add_argument("--stat-steps", type=int, default=1000,
+                    help="steps of the FP64/mixed/control-variate statistics runs (0: skip); 25 steps per block")
     ap.add_argument("--form", choices=["fp64", "mixed", "both"], default="both",
                     help="which forms to time; with both, the mixed form is the headline and the FP64 form its reference")
     ap.add_argument("--measure-peaks", action="store_true", help="print measured GEMM/copy peaks and exit")

@@ -111,8 +111,11 @@ def kernels_fixture(name, sysw, nwalkers, seed):
     print("wrote", name)
 
 
-def run_fixture(name, sysw, nwalkers, num_blocks, seed, snap_steps=()):
-    """ipie's own AFQMC.build(...).run() end to end; block estimates + final walker state."""
+def run_fixture(name, sysw, nwalkers, num_blocks, seed, snap_steps=(), steps_per_block=25, keep_walkers=None):
+    """ipie's own AFQMC.build(...).run() end to end; block estimates + final walker state.
+
+    ``keep_walkers``: store the orbitals of that many leading walkers only (plus checksums of all
+    of them) and ipie's local energies of the final walkers, for batches too large to commit."""
     ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
     trial = SingleDet(sysw.psi.copy(), (sysw.nup, sysw.ndown), sysw.nbasis)
     trial.half_rotate(ham)
@@ -122,7 +125,7 @@ def run_fixture(name, sysw, nwalkers, num_blocks, seed, snap_steps=()):
         trial,
         num_walkers=nwalkers,
         seed=seed,
-        num_steps_per_block=25,
+        num_steps_per_block=steps_per_block,
         num_blocks=num_blocks,
         timestep=0.005,
         stabilize_freq=5,
@@ -140,12 +143,18 @@ def run_fixture(name, sysw, nwalkers, num_blocks, seed, snap_steps=()):
         unscaled_weight=np.array(w.unscaled_weight),
         ovlp=np.array(w.ovlp),
         hybrid_energy=np.array(w.hybrid_energy),
-        phia=np.array(w.phia),
-        phib=np.array(w.phib),
+        phia=np.array(w.phia)[:keep_walkers],
+        phib=np.array(w.phib)[:keep_walkers],
         total_weight=np.array(afqmc.pcontrol.total_weight),
         chol_checksum=checksum(sysw.chol),
         psi_checksum=checksum(sysw.psi),
     )
+    if keep_walkers is not None:
+        out["phia_checksum"] = checksum(np.array(w.phia))
+        out["phib_checksum"] = checksum(np.array(w.phib))
+        # ipie's local energies of the final walkers (the estimator's own call path)
+        greens_function_single_det(w, trial)
+        out["energy"] = local_energy_single_det_uhf_batch(Generic((sysw.nup, sysw.ndown)), ham, w, trial)
     np.savez_compressed(os.path.join(HERE, name), **out)
     print("wrote", name, "ETotal per block", data[:, 3].real if data.shape[1] > 3 else data)
 
@@ -400,7 +409,54 @@ def ghf_fixture(name, sysw, nwalkers, seed, nsteps=3):
     print("wrote", name)
 
 
+def analysis_fixture(name):
+    """ipie's autocorrelation reblocking (``analysis/autocorr.py:54-105``) on seeded series:
+    white noise and AR(1) series with correlation 0.5 and 0.9, of several lengths."""
+    from ipie.analysis.autocorr import reblock_by_autocorr
+
+    rng = np.random.default_rng(2024)
+    out = {}
+    cases = []
+    for n in (40, 257, 1000):
+        for phi in (0.0, 0.5, 0.9):
+            e = rng.normal(size=n)
+            y = np.empty(n)
+            y[0] = e[0]
+            for i in range(1, n):
+                y[i] = phi * y[i - 1] + e[i]
+            y = -150.0 + 1e-3 * y
+            df = reblock_by_autocorr(y)
+            key = f"n{n}_phi{int(phi * 10)}"
+            cases.append(key)
+            out[key + "_y"] = y
+            out[key + "_ref"] = np.array([df["ETotal_ac"].values[0], df["ETotal_error_ac"].values[0],
+                                          df["ETotal_nsamp_ac"].values[0], df["ac"].values[0]], dtype=np.float64)
+    out["cases"] = np.array(cases)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name)
+
+
+def config_fixtures():
+    """Parity runs at the workload sizes themselves (the stable Cholesky amplitude).
+
+    * RHF M=26, 5+5 electrons, X=120, 64 walkers, 3 blocks of 25 steps with reortho
+      and pair branch every 5 steps (ipie's AFQMC.run, seed 7);
+    * UHF M=108, 15+15 electrons, X=600, 640 walkers, one block of 10 steps with its
+      energy evaluation (ipie's AFQMC.run, seed 7)."""
+    c0 = synthetic.workload("c0_rhf_m26", chol_scale="stable")
+    run_fixture("run_c0_rhf_m26_w64.npz", c0, nwalkers=64, num_blocks=3, seed=7)
+    c1 = synthetic.workload("c1_uhf_m108", chol_scale="stable")
+    run_fixture("run_c1_uhf_m108_w640.npz", c1, nwalkers=640, num_blocks=1, seed=7, steps_per_block=10,
+                keep_walkers=4)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "analysis":
+        analysis_fixture("reblock_autocorr.npz")
+        sys.exit(0)
+    if len(sys.argv) > 2 and sys.argv[2] == "configs":
+        config_fixtures()
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[2] == "ghf":
         ghf = synthetic.generate(14, (4, 3), 40, decay=30.0, seed=8, uhf=True, chol_scale="stable")
         ghf_fixture("ghf_m14.npz", ghf, nwalkers=5, seed=31)

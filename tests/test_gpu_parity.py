@@ -11,7 +11,7 @@ import pytest
 torch = pytest.importorskip("torch")
 
 from oracle import afqmc_oracle as O  # noqa: E402
-from tests._systems import RUN_PARAMS, fixture_system, load, oracle_system  # noqa: E402
+from tests._systems import RUN_PARAMS, compare_walkers, fixture_system, load, oracle_system  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -104,7 +104,7 @@ def test_afqmc_run_matches_ipie(name):
     trial = SingleDet(s.psi, (s.nup, s.ndown), s.nbasis)
     trial.half_rotate(ham)
     afqmc = AFQMC.build((s.nup, s.ndown), ham, trial, num_walkers=p["nwalkers"], seed=p["seed"],
-                        num_steps_per_block=25, num_blocks=p["num_blocks"], timestep=0.005, stabilize_freq=5,
+                        num_steps_per_block=p["steps"], num_blocks=p["num_blocks"], timestep=0.005, stabilize_freq=5,
                         pop_control_freq=5, verbose=False)
     blocks = afqmc.run()
     ref = f["blocks"].real
@@ -118,8 +118,14 @@ def test_afqmc_run_matches_ipie(name):
     assert rel(w.unscaled_weight, f["unscaled_weight"]) < TOL
     assert rel(w.ovlp, f["ovlp"]) < TOL
     assert rel(w.hybrid_energy, f["hybrid_energy"]) < TOL
-    assert rel(w.phia, f["phia"]) < TOL
-    assert rel(w.phib, f["phib"]) < TOL
+    compare_walkers(rel, w.phia.cpu().numpy(), w.phib.cpu().numpy(), f, TOL)
+    if "energy" in f:
+        # local energies of the final walkers (ipie's estimator call on them)
+        from ipie_b200.estimators import local_energy_single_det_uhf_batch
+
+        trial.calc_greens_function(w)
+        e = local_energy_single_det_uhf_batch(None, ham, w, trial)
+        assert rel(e, f["energy"]) < TOL
 
 
 def test_known_answer_pair_branch():

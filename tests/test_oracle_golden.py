@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import afqmc_oracle as O
-from tests._systems import RUN_PARAMS, checksum, fixture_system, load, oracle_system
+from tests._systems import RUN_PARAMS, checksum, compare_walkers, fixture_system, load, oracle_system
 
 KERNEL_FIXTURES = ["kernels_rhf_m26.npz", "kernels_uhf_m30.npz"]
 
@@ -79,7 +79,7 @@ def test_oracle_run_matches_ipie_afqmc_run(name):
     w = O.Walkers.from_initial(s.init, s.nup, p["nwalkers"])
     O.greens_function(S, w)
     w.ovlp = O.greens_function(S, w)
-    blocks = O.run_afqmc(S, w, num_blocks=p["num_blocks"], seed=p["seed"])
+    blocks = O.run_afqmc(S, w, num_blocks=p["num_blocks"], num_steps_per_block=p["steps"], seed=p["seed"])
     ref = f["blocks"]
     # ipie's block row: Weight, WeightFactor, HybridEnergy, ENumer, EDenom, ETotal, E1Body, E2Body
     for b, row in zip(blocks, ref):
@@ -92,8 +92,10 @@ def test_oracle_run_matches_ipie_afqmc_run(name):
     assert rel(w.unscaled_weight, f["unscaled_weight"]) < 1e-10
     assert rel(w.ovlp, f["ovlp"]) < 1e-10
     assert rel(w.hybrid_energy, f["hybrid_energy"]) < 1e-10
-    assert rel(w.phia, f["phia"]) < 1e-10
-    assert rel(w.phib, f["phib"]) < 1e-10
+    compare_walkers(rel, w.phia, w.phib, f, 1e-10)
+    if "energy" in f:
+        O.greens_function(S, w)
+        assert rel(O.local_energy_single_det_uhf_batch(S, w), f["energy"]) < 1e-10
 
 
 def test_known_answer_pair_branch():
