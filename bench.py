@@ -354,44 +354,52 @@ def train_control_variate(wl, W, rank, steps=100, epochs=60):
 
 
 def statistics_runs(wl, W, rank, steps, cv=None, dt=0.005):
-    """Block energies of the FP64 and mixed forms over ``steps`` steps with identical draws and no
-    population control (a flipped branching decision would swap whole walkers between the runs and
-    hide the precision effect), and of the mixed + control-variate estimator evaluated on the mixed
-    run's walkers at the same block ends (the control variate changes the estimator, not the walk).
+    """Block energies of the FP64 and mixed forms over ``steps`` driver steps, run in lockstep with
+    identical draws and the same population control: the FP64 run draws its pair branch, the mixed
+    run forms the same pairs from its own weights (``PopController.follow``), so the two stay the
+    same walk and differ only by precision.  The mixed + control-variate estimator is evaluated on
+    the mixed run's walkers at the same block ends (the control variate changes the estimator, not
+    the walk).
 
     Returns {form: block ETotal series (blocks 1..n)} and, per form, ipie's reblocking analysis
     (:func:`ipie_b200.analysis.reblock_mixed`) of the blocks after ipie's equilibration time 2/dt
     and of the paired differences to FP64 over the same blocks."""
     from ipie_b200.analysis import reblock_mixed
 
-    series = {}
-    seconds = {}
+    runs = {}
     for form in ("fp64", "mixed"):
-        af, _ = build_afqmc(wl, W, "device", 4242 + rank, precision=form, pop_control_freq=10 ** 9, graph=True)
+        af, _ = build_afqmc(wl, W, "device", 4242 + rank, precision=form, graph=True)
         af.setup_run()
-        cv_est, e_cv = None, []
-        if form == "mixed" and cv is not None:
-            from ipie_b200.control_variate import ControlVariateEnergyEstimator
+        runs[form] = af
+    runs["mixed"].pcontrol.follow(runs["fp64"].pcontrol)
+    cv_est, e_cv = None, []
+    if cv is not None:
+        from ipie_b200.control_variate import ControlVariateEnergyEstimator
 
-            cv_est = ControlVariateEnergyEstimator(cv, fraction=8, seed=99 + rank, precision="mixed")
-        t0 = time.perf_counter()
-        for step in range(1, steps + 1):
-            af.step(step)
-            if cv_est is not None and step % af.params.num_steps_per_block == 0:
-                d = cv_est.compute_estimator(af.system, af.walkers, af.hamiltonian, af.trial)
-                e_cv.append(float((d[0] / d[1]).real))
-        seconds[form] = time.perf_counter() - t0
-        series[form] = np.array(af.block_data)[1:, 5].real
-        if cv_est is not None:
-            series["mixed_cv"] = np.array(e_cv)
-        del af
+        cv_est = ControlVariateEnergyEstimator(cv, fraction=8, seed=99 + rank, precision="mixed")
+    nblk = runs["fp64"].params.num_steps_per_block
+    t0 = time.perf_counter()
+    for step in range(1, steps + 1):
+        for form in ("fp64", "mixed"):  # the leader branches first
+            runs[form].step(step)
+        if cv_est is not None and step % nblk == 0:
+            af = runs["mixed"]
+            d = cv_est.compute_estimator(af.system, af.walkers, af.hamiltonian, af.trial)
+            e_cv.append(float((d[0] / d[1]).real))
+    seconds = time.perf_counter() - t0
+    series = {form: np.array(af.block_data)[1:, 5].real for form, af in runs.items()}
+    if cv_est is not None:
+        series["mixed_cv"] = np.array(e_cv)
+    del runs
     n = min(len(v) for v in series.values())
     series = {k: v[:n] for k, v in series.items()}
-    eq = min(int(round(2.0 / dt / 25)), max(n - 8, 0))  # ipie's equilibration time, in 25-step blocks
-    out = {"blocks": n, "equilibration_blocks": eq, "steps": steps, "seconds": seconds, "forms": {}}
+    eq = min(int(round(2.0 / dt / nblk)), max(n - 8, 0))  # ipie's equilibration time, in blocks
+    out = {"blocks": n, "equilibration_blocks": eq, "steps": steps, "seconds": seconds,
+           "coupling": "identical device draws; the mixed run takes the FP64 run's pair-branch pairs", "forms": {}}
     for form, v in series.items():
         rb = reblock_mixed(v[eq:])
-        entry = {"energy_Eh": rb["mean"], "error_mEh": rb["error"] * 1e3, "error_ac_mEh": rb["error_ac"] * 1e3,
+        entry = {"energy_Eh": rb["mean"], "error_mEh": max(rb["error"], rb["error_ac"]) * 1e3,
+                 "error_fp_mEh": rb["error"] * 1e3, "error_ac_mEh": rb["error_ac"] * 1e3,
                  "reblock_converged": rb["converged"], "block": rb["block"]}
         if form != "fp64":
             d = reblock_mixed(v[eq:] - series["fp64"][eq:])

@@ -22,8 +22,12 @@ import torch
 from ._lib import call, ptr, stream
 
 
-def pair_branch_table(absw, max_weight, min_weight, rand=np.random.rand):
-    """ipie's pairing walk (``pop_controller.py:338-391``): returns (new |w|, status 0/1/2) in walker order."""
+def pair_branch_table(absw, max_weight, min_weight, rand=np.random.rand, pairs=None):
+    """ipie's pairing walk (``pop_controller.py:338-391``): returns (new |w|, status 0/1/2) in walker order.
+
+    ``pairs`` (a list), when given, receives each pair's decision as (low walker, high walker,
+    high walker kept) in walker indices, so that another walker set can be branched the same way
+    (:meth:`PopController.follow`)."""
     n = absw.size
     w = absw.astype(np.float64).copy()
     st = np.ones(n, dtype=np.int64)
@@ -35,6 +39,8 @@ def pair_branch_table(absw, max_weight, min_weight, rand=np.random.rand):
         if ws[s] < min_weight or ws[e] > max_weight:
             wab = ws[s] + ws[e]
             r = rand()
+            if pairs is not None:
+                pairs.append((int(order[s]), int(order[e]), bool(r < ws[e] / wab)))
             if r < ws[e] / wab:
                 ws[e] = 0.5 * wab
                 ss[e] = 2
@@ -54,6 +60,20 @@ def pair_branch_table(absw, max_weight, min_weight, rand=np.random.rand):
     out_w[order] = ws
     out_s[order] = ss
     return out_w, out_s
+
+
+def apply_pairs(absw, pairs):
+    """(new |w|, status) of a pair branch whose pairs and survivors are given (the ``pairs`` list of
+    :func:`pair_branch_table`), applied to the weights ``absw``: each pair's survivor carries half
+    the pair's summed weight."""
+    neww = absw.astype(np.float64).copy()
+    status = np.ones(neww.size, dtype=np.int64)
+    for i, j, keep_j in pairs:
+        half = 0.5 * (neww[i] + neww[j])
+        keep, drop = (j, i) if keep_j else (i, j)
+        neww[keep], status[keep] = half, 2
+        neww[drop], status[drop] = 0.0, 0
+    return neww, status
 
 
 def comb_parent_counts(weights, target_weight, r):
@@ -98,6 +118,18 @@ class PopController:
         self.target_weight = self.ntot_walkers
         self.total_weight = self.ntot_walkers
         self._src = None
+        self.leader = None  # see follow()
+        self.last_pairs = []
+
+    def follow(self, leader):
+        """Branch with ``leader``'s pairs instead of drawing: each pair (i, j) the leader formed at
+        its last pair branch is formed here too, from this walker set's own weights, and the same
+        walker of the pair survives.  Two runs of one system that differ only in arithmetic
+        (precision forms) then keep the same population and stay comparable step by step; the
+        leader must branch first at every step.  Pair branch only."""
+        if self.method != "pair_branch":
+            raise NotImplementedError("follow() couples pair-branch population control")
+        self.leader = leader
 
     def pop_control(self, walkers, comm=None, rand=None):
         """Rescale by total |w| / target, then the configured method (``pop_controller.py:78-125``).
@@ -139,7 +171,11 @@ class PopController:
              ptr(walkers.Ghalfb), stream())
 
     def _pair_branch(self, walkers, w, rand):
-        neww, status = pair_branch_table(np.abs(w), self.max_weight, self.min_weight, rand)
+        if self.leader is not None:
+            neww, status = apply_pairs(np.abs(w), self.leader.last_pairs)
+        else:
+            self.last_pairs = []
+            neww, status = pair_branch_table(np.abs(w), self.max_weight, self.min_weight, rand, pairs=self.last_pairs)
         cloned = np.nonzero(status == 2)[0]
         killed = np.nonzero(status == 0)[0]
         w[cloned] = neww[cloned]

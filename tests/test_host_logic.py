@@ -171,3 +171,24 @@ def test_ghf_half_rotation_reproduces_the_four_block_energy(case):
     assert np.max(np.abs(e1 - ref[:, 1])) <= 1e-12 * np.abs(ref[:, 1]).max()
     assert np.max(np.abs(ecoul - exx - ref[:, 2])) <= 1e-11 * np.abs(ref[:, 2]).max()
     assert R.shape[0] == (2 * X if case == "c" else X)
+
+
+def test_pair_branch_pairs_replay():
+    """The pairs recorded by the pairing walk, applied to the same weights, give the walk's own
+    result; applied to perturbed weights they branch the same walkers."""
+    from ipie_b200.pop_control import apply_pairs, pair_branch_table
+
+    rng = np.random.default_rng(3)
+    absw = np.exp(rng.normal(0.0, 1.5, size=300))
+    absw *= absw.size / absw.sum()
+    draws = rng.uniform(size=300)
+    it = iter(draws)
+    pairs = []
+    neww, status = pair_branch_table(absw, 4.0, 0.1, lambda: next(it), pairs=pairs)
+    assert len(pairs) > 10
+    w2, s2 = apply_pairs(absw, pairs)
+    assert np.array_equal(s2, status)
+    assert np.array_equal(w2, neww)
+    w3, s3 = apply_pairs(absw * (1 + 1e-9 * rng.normal(size=absw.size)), pairs)
+    assert np.array_equal(s3, status)
+    assert np.allclose(w3, neww, rtol=1e-8)
