@@ -225,7 +225,8 @@ DRAM_TRAFFIC = {
 }
 
 
-def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5, graph=False):
+def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5, graph=False, population="host",
+                paired_copies=False):
     from ipie_b200 import AFQMC, Generic, SingleDet, synthetic
 
     p = WORKLOADS[wl]
@@ -236,7 +237,7 @@ def build_afqmc(wl, walkers, rng, seed, precision="fp64", pop_control_freq=5, gr
     af = AFQMC.build((s.nup, s.ndown), ham, trial, num_walkers=walkers, seed=seed, num_steps_per_block=25,
                      num_blocks=10 ** 6, timestep=0.005, stabilize_freq=5, pop_control_freq=pop_control_freq,
                      verbose=False, rng=rng,
-                     precision=precision, graph=graph)
+                     precision=precision, graph=graph, population=population, paired_copies=paired_copies)
     return af, s
 
 
@@ -368,7 +369,7 @@ def statistics_runs(wl, W, rank, steps, cv=None, dt=0.005):
 
     runs = {}
     for form in ("fp64", "mixed"):
-        af, _ = build_afqmc(wl, W, "device", 4242 + rank, precision=form, graph=True)
+        af, _ = build_afqmc(wl, W, "device", 4242 + rank, precision=form, graph=True, paired_copies=True)
         af.setup_run()
         runs[form] = af
     runs["mixed"].pcontrol.follow(runs["fp64"].pcontrol)
@@ -395,7 +396,8 @@ def statistics_runs(wl, W, rank, steps, cv=None, dt=0.005):
     series = {k: v[:n] for k, v in series.items()}
     eq = min(int(round(2.0 / dt / nblk)), max(n - 8, 0))  # ipie's equilibration time, in blocks
     out = {"blocks": n, "equilibration_blocks": eq, "steps": steps, "seconds": seconds,
-           "coupling": "identical device draws; the mixed run takes the FP64 run's pair-branch pairs", "forms": {}}
+           "coupling": ("identical device draws; the mixed run takes the FP64 run's pair-branch pairs; killed "
+                        "walkers receive their own pair's survivor (ipie's multi-rank copy semantics)"), "forms": {}}
     for form, v in series.items():
         rb = reblock_mixed(v[eq:])
         entry = {"energy_Eh": rb["mean"], "error_mEh": max(rb["error"], rb["error_ac"]) * 1e3,
@@ -419,7 +421,10 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
 
     # each step's propagation and weight clip replay from a captured CUDA graph (device draws)
     graph = rng == "device"
-    af, _ = build_afqmc(wl, W, rng, 7 + rank, precision=precision, graph=graph)
+    # throughput mode: population control decided on the device (no host round trip, inside the
+    # step graph), killed walkers copying their own pair's survivor
+    af, _ = build_afqmc(wl, W, rng, 7 + rank, precision=precision, graph=graph, population="device",
+                        paired_copies=True)
     af.setup_run()
     if cv is not None:
         from ipie_b200.control_variate import ControlVariateEnergyEstimator
@@ -448,7 +453,7 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
     af.use_graph = graph
     nblocks0 = len(af.block_data)
     launches0 = _lib.launch_count()
-    replays0 = af.graphs.replays if af.graphs is not None else 0
+    replayed0 = af.graphs.replayed_launches if af.graphs is not None else 0
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -469,7 +474,7 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
     # kernels launched in the timed region: ordinary launches plus the captured ones replayed
     launches = _lib.launch_count() - launches0
     if af.graphs is not None:
-        launches += (af.graphs.replays - replays0) * af.graphs.launches_per_step
+        launches += af.graphs.replayed_launches - replayed0
     res = {
         "t": barrier_max(ev0.elapsed_time(ev1) / 1e3, world),
         "phases": timer.summary(),
@@ -633,7 +638,7 @@ def run_ours(args):
 
     # ---------------- end to end through the public API (headline form) ----------------
     e2e_steps = min(args.steps, args.e2e_steps)
-    af2, _ = build_afqmc(wl, W, "host", 7 + rank, precision=head)
+    af2, _ = build_afqmc(wl, W, "host", 7 + rank, precision=head, population="device", paired_copies=True)
     rng = np.random.default_rng(1234 + rank)
     fields = [torch.from_numpy(rng.standard_normal((W, X))).pin_memory() for _ in range(args.warmup + e2e_steps)]
     af2.propagator.host_fields = iter(fields)

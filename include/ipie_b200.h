@@ -19,7 +19,8 @@
  *     twice, with the same results as two identical blocks;
  *   - `status` (optional, device unsigned int) collects numerical trouble
  *     bits: 1 non-finite value, 2 singular overlap pivot, 4 bad shape,
- *     8 zero column in Gram-Schmidt.  Kernels never trap; the caller reads
+ *     8 zero column in Gram-Schmidt, 16 zero total weight in population
+ *     control.  Kernels never trap; the caller reads
  *     the word (ipie raises Python exceptions at the matching places).
  *
  * Each function names the ipie routine (file:line inside the ipie project)
@@ -139,6 +140,25 @@ int ipie_b200_reortho(void* phia, void* phib, int W, int M, int na, int nb, cons
 int ipie_b200_walker_copy(const int* src, int W, int M, int na, int nb, void* phia, void* phib, double* weight,
                           double* unscaled_weight, void* hybrid_energy, void* ovlp, void* phase, void* ghalfa,
                           void* ghalfb, void* stream);
+/* Pair-branch population control decided on the device (no host round trip;
+ * capturable in a CUDA graph).  Rescales weight by total |w| / target_weight
+ * (unscaled_weight <- the weights before), sorts |w| stably, pairs walkers
+ * inward from both ends while the lightest is below min_weight or the heaviest
+ * above max_weight, and draws one uniform per pair (Philox4x32-10 keyed by
+ * seed, counter block *counter, advanced by one per call) to choose the
+ * survivor, which takes half the pair's weight.  out: src (W) int for
+ * ipie_b200_walker_copy -- killed walkers receive the highest-index survivor
+ * (paired = 0: ipie's single-process semantics) or their own pair's survivor
+ * (paired = 1: ipie's semantics when pairs span ranks), others -1;
+ * total_weight[0] = total |w|; wbound[0] = 0.1 total |w| (the next steps' weight
+ * clip; may be NULL); uniforms (W/2 doubles, may be NULL) the draws of the
+ * pairs formed, in pair order.  2 <= W <= 8192.  A total below 1e-8 leaves the
+ * weights untouched and sets status bit 16 (ipie raises ValueError there).
+ * replaces: walkers/pop_controller.py:78-125 (pop_control rescale) and
+ *           :304-429 (pair_branch decisions) */
+int ipie_b200_pair_branch(int W, double* weight, double* unscaled_weight, double target_weight, double min_weight,
+                          double max_weight, unsigned long long seed, unsigned long long* counter, int paired, int* src,
+                          double* total_weight, double* wbound, double* uniforms, unsigned int* status, void* stream);
 /* Out-of-place resampling: walker d of the *_out arrays becomes walker src[d]
  * of the inputs (orbitals, half-rotated Green's functions, hybrid energy,
  * overlap, phase, unscaled weight; sources may repeat).  ghalf*, phase may be

@@ -73,6 +73,7 @@ SIGNATURES = {
     "ipie_b200_umma_gemm_f16_test": [P, P, P, P, P, I, I, I, I, P, P],
     "ipie_b200_normal_fill": [P, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_ulonglong, P],
     "ipie_b200_normal_fill_dev": [P, ctypes.c_longlong, ctypes.c_ulonglong, P, P],
+    "ipie_b200_pair_branch": [I, P, P, D, D, D, ctypes.c_ulonglong, P, I, P, P, P, P, P, P],
 }
 
 _lib = None

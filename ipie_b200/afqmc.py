@@ -78,14 +78,21 @@ class AFQMC:
         self.timers = {}
         self.use_graph = False
         self.graphs = None
+        self.population = "host"
+        self.paired_copies = False
 
     @staticmethod
     def build(num_elec, hamiltonian, trial_wavefunction, walkers=None, num_walkers=100, seed=None,
               num_steps_per_block=25, num_blocks=100, timestep=0.005, stabilize_freq=5, pop_control_freq=5,
-              verbose=True, mpi_handler=None, rng="numpy", spin_alias="auto", precision="fp64", graph=False):
+              verbose=True, mpi_handler=None, rng="numpy", spin_alias="auto", precision="fp64", graph=False,
+              population="host", paired_copies=False):
         """ipie's ``AFQMC.build`` (``qmc/afqmc.py:297-392``) plus the B200 options: ``rng`` ("numpy":
-        ipie's draws; "device": on-GPU draws), ``precision`` ("fp64" | "mixed"), ``spin_alias`` and
-        ``graph`` (replay each step's device work from a captured CUDA graph; needs rng="device")."""
+        ipie's draws; "device": on-GPU draws), ``precision`` ("fp64" | "mixed"), ``spin_alias``,
+        ``graph`` (replay each step's device work from a captured CUDA graph; needs rng="device") and
+        ``population`` ("host": ipie's pair branch decided on the host with numpy's draws; "device":
+        decided on the GPU with device draws, no host round trip, captured in the step graph) and
+        ``paired_copies`` (a killed walker receives its own pair's survivor, ipie's multi-rank
+        semantics, instead of the highest-index survivor, its single-process semantics)."""
         params = QMCParams(num_walkers, num_walkers, num_blocks, num_steps_per_block, timestep, stabilize_freq,
                            pop_control_freq, seed)
         if not trial_wavefunction.half_rotated:
@@ -114,6 +121,10 @@ class AFQMC:
         af.use_graph = bool(graph)
         if af.use_graph and rng != "device":
             raise ValueError("graph=True needs rng='device'")
+        if population not in ("host", "device"):
+            raise ValueError(f"population must be 'host' or 'device', not {population!r}")
+        af.population = population
+        af.paired_copies = bool(paired_copies)
         return af
 
     def _block(self, block, est, acc_vals):
@@ -136,7 +147,16 @@ class AFQMC:
         w, ham, trial, p = self.walkers, self.hamiltonian, self.trial, self.params
         self.eshift = 0.0
         w.orthogonalise()
-        self.pcontrol = PopController(p.num_walkers, p.num_steps_per_block)
+        if self.population == "device":
+            # the clip bound lives on the device from here on: 0.1 x the target weight until the
+            # first population control writes 0.1 x the total weight
+            ws = self.propagator._workspace(w, ham)
+            ws.wbound.fill_(0.10 * p.num_walkers)
+            seed = p.rng_seed if p.rng_seed is not None else 7
+            self.pcontrol = PopController(p.num_walkers, p.num_steps_per_block, device=True, seed=seed + 7919,
+                                          wbound=ws.wbound, paired=self.paired_copies)
+        else:
+            self.pcontrol = PopController(p.num_walkers, p.num_steps_per_block, paired=self.paired_copies)
         self.accumulators = WalkerAccumulator(p.num_steps_per_block, w.device)
         self.estimator = EnergyEstimator(precision=self.propagator.precision)
         self.estimator.compute_estimator(self.system, w, ham, trial)
@@ -147,21 +167,35 @@ class AFQMC:
     def step(self, step):
         """Body of ``run``'s loop for step number ``step`` (1-based; ``afqmc.py:561-633``)."""
         w, ham, trial, prop, p = self.walkers, self.hamiltonian, self.trial, self.propagator, self.params
-        if step % p.num_stblz == 0:
-            w.orthogonalise()
+        reortho = step % p.num_stblz == 0
+        popc = step % p.pop_control_freq == 0
+        dev_pop = self.pcontrol.device
+        # the clip bound: host scalar, or kept on the device by device population control
+        wbound = None if dev_pop else self.pcontrol.total_weight * 0.10
         if self.use_graph and step > 1:
             if self.graphs is None:
                 from .graphs import StepGraphs
 
                 self.graphs = StepGraphs(prop, w, ham, trial)
-            self.graphs.step(np.real(self.eshift), self.pcontrol.total_weight * 0.10)
+            # the accumulation follows population control, so it joins the graph unless a
+            # host-decided population control comes between them
+            acc_in_graph = dev_pop or not popc
+            self.graphs.step(np.real(self.eshift), wbound, reortho=reortho,
+                             pcontrol=self.pcontrol if (popc and dev_pop) else None,
+                             accumulators=self.accumulators if acc_in_graph else None)
+            if popc and not dev_pop:
+                self.pcontrol.pop_control(w)
+            if not acc_in_graph:
+                self.accumulators.update(w)
         else:
+            if reortho:
+                w.orthogonalise()
             prop.propagate_walkers(w, ham, trial, self.eshift)
             if step > 1:
-                prop.clip_weights(w, self.pcontrol.total_weight * 0.10)
-        if step % p.pop_control_freq == 0:
-            self.pcontrol.pop_control(w)
-        self.accumulators.update(w)
+                prop.clip_weights(w, wbound)
+            if popc:
+                self.pcontrol.pop_control(w)
+            self.accumulators.update(w)
         if step % p.num_steps_per_block == 0:
             block = step // p.num_steps_per_block
             self.estimator.compute_estimator(self.system, w, ham, trial)

@@ -19,6 +19,7 @@ enum StatusBits : unsigned int {
   STATUS_SINGULAR = 1u << 1,      // exactly singular pivot in an overlap LU
   STATUS_BAD_SHAPE = 1u << 2,     // a kernel was launched with sizes it does not support
   STATUS_ZERO_NORM = 1u << 3,     // a zero column met in Gram-Schmidt
+  STATUS_ZERO_WEIGHT = 1u << 4,   // total walker weight below 1e-8 in population control
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {

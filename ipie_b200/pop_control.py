@@ -102,10 +102,29 @@ METHODS = ("pair_branch", "comb", "stochastic_reconfiguration")
 
 
 class PopController:
+    """``device=True`` (pair branch only) decides on the GPU (``ipie_b200_pair_branch``) with device
+    uniforms (Philox keyed by ``seed``): no host round trip, so a step with population control can be
+    replayed from a CUDA graph; the total weight and the clip bound then stay on the device
+    (``total_weight_dev``, and ``wbound``, the weight-clip bound tensor the caller hands in).
+
+    ``paired`` selects what a killed walker of the pair branch receives: False (default) the buffer
+    of the highest-index survivor, as ipie does in one process (every send carries the same tag and
+    its single-process communicator keeps the last); True its own pair's survivor, as ipie does
+    when the pairs span ranks.  The first reproduces ipie's single-process runs; it also copies
+    one walker into every killed slot, which thins the population's diversity over long runs."""
+
     def __init__(self, num_walkers_local, num_steps, mpi_handler=None, pop_control_method="pair_branch",
-                 min_weight=0.1, max_weight=4, reconfiguration_freq=50, verbose=False):
+                 min_weight=0.1, max_weight=4, reconfiguration_freq=50, verbose=False, device=False, seed=7,
+                 paired=False, wbound=None):
         if pop_control_method not in METHODS:
             raise NotImplementedError(f"population control {pop_control_method!r}: one of {METHODS}")
+        if device and pop_control_method != "pair_branch":
+            raise NotImplementedError("population control on the device is pair branch only")
+        self.device = bool(device)
+        self.seed = int(seed)
+        self.paired = bool(paired)
+        self.wbound = wbound
+        self._dev = None
         self.method = pop_control_method
         self.reconfiguration_counter = 0
         self.reconfiguration_freq = reconfiguration_freq
@@ -138,6 +157,8 @@ class PopController:
         """
         if self.ntot_walkers == 1:
             return
+        if self.device:
+            return self._pair_branch_device(walkers)
         w = walkers.weight.cpu().numpy()
         absw = np.abs(w)
         if self.method == "comb":
@@ -161,6 +182,33 @@ class PopController:
             self.reconfiguration_counter = 0
             return self._reconfigure(walkers, np.abs(w), rand or np.random.rand)
 
+    def _device_state(self, walkers):
+        if self._dev is None or self._dev["src"].numel() != walkers.nwalkers:
+            dev = walkers.device
+            self._dev = {
+                "src": torch.empty(walkers.nwalkers, dtype=torch.int32, device=dev),
+                "counter": torch.zeros(1, dtype=torch.int64, device=dev),
+                "total": torch.full((1,), float(self.target_weight), dtype=torch.float64, device=dev),
+                "uniforms": None,
+            }
+        return self._dev
+
+    @property
+    def total_weight_dev(self):
+        return None if self._dev is None else self._dev["total"]
+
+    def _pair_branch_device(self, walkers, uniforms=None):
+        """Rescale and pair on the device, then the walker copies; nothing returns to the host."""
+        d = self._device_state(walkers)
+        call("ipie_b200_pair_branch", walkers.nwalkers, ptr(walkers.weight), ptr(walkers.unscaled_weight),
+             float(self.target_weight), float(self.min_weight), float(self.max_weight), self.seed, ptr(d["counter"]),
+             int(self.paired), ptr(d["src"]), ptr(d["total"]), ptr(self.wbound), ptr(uniforms), ptr(walkers.status),
+             stream())
+        call("ipie_b200_walker_copy", ptr(d["src"]), walkers.nwalkers, walkers.nbasis, walkers.nup, walkers.ndown,
+             ptr(walkers.phia), ptr(walkers.phib), ptr(walkers.weight), ptr(walkers.unscaled_weight),
+             ptr(walkers.hybrid_energy), ptr(walkers.ovlp), ptr(walkers.phase), ptr(walkers.Ghalfa),
+             ptr(walkers.Ghalfb), stream())
+
     def _copy(self, walkers, src):
         if self._src is None or self._src.numel() != walkers.nwalkers:
             self._src = torch.empty(walkers.nwalkers, dtype=torch.int32, device=walkers.device)
@@ -172,17 +220,22 @@ class PopController:
 
     def _pair_branch(self, walkers, w, rand):
         if self.leader is not None:
-            neww, status = apply_pairs(np.abs(w), self.leader.last_pairs)
+            pairs = self.leader.last_pairs
+            neww, status = apply_pairs(np.abs(w), pairs)
         else:
-            self.last_pairs = []
-            neww, status = pair_branch_table(np.abs(w), self.max_weight, self.min_weight, rand, pairs=self.last_pairs)
+            self.last_pairs = pairs = []
+            neww, status = pair_branch_table(np.abs(w), self.max_weight, self.min_weight, rand, pairs=pairs)
         cloned = np.nonzero(status == 2)[0]
         killed = np.nonzero(status == 0)[0]
         w[cloned] = neww[cloned]
         walkers.weight.copy_(torch.from_numpy(w))
         if killed.size:
             src = np.full(walkers.nwalkers, -1, dtype=np.int32)
-            if cloned.size:
+            if self.paired:
+                for i, j, keep_j in pairs:
+                    keep, drop = (j, i) if keep_j else (i, j)
+                    src[drop] = keep
+            elif cloned.size:
                 src[killed] = cloned.max()
             self._copy(walkers, src)
         return neww, status

@@ -163,6 +163,9 @@ class UHFWalkers:
         s = int(self.status.item())
         if s:
             self.status.zero_()
+            if s & 16:
+                # device population control met a vanishing total weight (ipie pop_controller.py:103-107)
+                raise ValueError("total walker weight fell below 1e-8 in population control")
             names = []
             for bit, name in ((1, "non-finite weight/overlap/energy"), (2, "singular overlap matrix"),
                               (4, "unsupported shape"), (8, "zero column in Gram-Schmidt")):
