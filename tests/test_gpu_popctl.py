@@ -63,7 +63,8 @@ def test_device_pair_branch_matches_pairing_walk(W, paired):
     cloned = np.nonzero(status == 2)[0]
     if killed.any():
         if paired:
-            want = {(j if keep_j else i): (i if keep_j else j) for i, j, keep_j in pairs}
+            # killed walker -> its pair's survivor
+            want = {(i if keep_j else j): (j if keep_j else i) for i, j, keep_j in pairs}
             for k in np.nonzero(killed)[0]:
                 assert d["src"][k] == want[k]
         else:
