@@ -9,29 +9,34 @@
 // kind::f16, FP32 accumulators in TMEM) of operands split into binary16 head and
 // remainder after a power-of-two scale: E - I by e_scale and V by v_scale (fixed
 // per call, chosen by the caller), and the right operand B (the walker's current
-// T_k or phi) by its own exact scale, 2^(14 - e) for max|B| = f 2^e, f in [0.5, 1),
-// found with a CTA-wide max before B is written.  The split carries ~2^-22
-// relative accuracy of every entry within ~2^16 of the largest, like the TF32
-// split.  phi accumulates in TMEM as head/tail float pairs (~2^-47 relative)
-// between the first one-body factor, read from FP64 global memory, and the
-// last, written to it in FP64.
+// T_k or phi) by a per-walker power of two: the walker's starting orbitals by their
+// exact scale, 2^(14 - e) for max|phi| = f 2^e, f in [0.5, 1) (a CTA-wide max, once
+// per walker), every later B by that scale / 16.  The split carries ~2^-22 relative
+// accuracy of every entry down to ~2^-13 of the orbitals' largest, and an absolute
+// error near 2^-35 of it below; a B entry beyond 2^5 times it (far beyond any
+// Taylor term of a convergent series) raises the non-finite status bit.  phi
+// accumulates in TMEM as head/tail float pairs (~2^-47 relative) between the
+// first one-body factor, read from FP64 global memory, and the last, written to
+// it in FP64.
 //
 // What stays on chip: B (planar rows -- Re of orbital n at row n, Im at row
-// BN/2 + n -- FP16 head and remainder) lives in shared memory for the whole
-// chain; each term's epilogue writes the next term's operand straight into the
-// 128B-swizzled K-major layout the MMA reads, so T_k never goes to global
-// memory.  Only the left operands stream through TMA: the walker's VHS planes
-// (re/im, hi/lo; 3-D tensor map, rows and columns past M zero-filled without
-// traffic; the same ~0.3 MB for every term, so after the first term they come
-// from L2) and the shared E - I.
+// BN/2 + n -- FP16 head and remainder) lives in shared memory, double-buffered:
+// each term's epilogue writes the next term's operand straight into the other
+// buffer, in the 128B-swizzled K-major layout the MMA reads, so T_k never goes to
+// global memory, and the next term's MMAs start on the k-blocks of the first
+// 128-row tile while the epilogue still works on the second.  Only the left
+// operands stream through TMA: the walker's VHS planes (re/im, hi/lo; 3-D tensor
+// map, rows and columns past M zero-filled without traffic; the same ~0.3 MB for
+// every term, so after the first term they come from L2) and the shared E - I.
 //
 // Roles (BN = 64: 576 threads): warps 0..4G-1 epilogue (warp w: TMEM lane quarter
 // w % 4, i.e. one output row per thread, and orbital group w / 4 of G = BN / 16
 // groups of 8), then one warp whose lane 0 is the TMA producer and one whose lane
 // 0 issues the MMAs.  Barriers: full/empty per stage (TMA <-> MMA), accb[mt]
-// (MMA -> epilogue, once per 128-row tile and term), bready (epilogue -> MMA, one
-// arrival per epilogue thread per term: B written and TMEM read), and the named
-// barrier 1 of the epilogue threads around the CTA-wide max of each new B.
+// (MMA -> epilogue, once per 128-row tile and term), bready[h] (epilogue -> MMA,
+// one arrival per epilogue thread per term and 128-row half of B: that half
+// written and that tile's accumulator read), and the named barrier 1 of the
+// epilogue threads around the CTA-wide max of each walker's starting orbitals.
 // Every mbarrier wait is bounded (umma.cuh); a timeout raises the status bit and
 // all roles leave their loops (the epilogue threads still meet at their named
 // barrier in the same order), then TMEM is released.
@@ -60,7 +65,6 @@ struct Chain16Maps {
 };
 
 constexpr int kATile = 128 * 128;        // bytes: 128 rows x 64 halves
-constexpr int kStages = 4;
 constexpr int kStageBytes = 2 * kATile;  // re and im planes of one part (hi or lo)
 constexpr int kMaxM = 256;
 constexpr int kKB = kMaxM / 64;          // k-blocks of 64 reserved for B (M <= 256)
@@ -72,6 +76,8 @@ struct Chain16Roles {
   static constexpr int kEpiThreads = 32 * kEpiWarps;
   static constexpr int kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
   static constexpr int kThreads = kEpiThreads + 64;
+  // stages of the left-operand ring next to the two B buffers (2 x 2 x kKB x BN x 128 bytes)
+  static constexpr int kStages = BN == 64 ? 3 : 5;
 };
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -150,18 +156,21 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int KB = (M + 63) / 64, MT = (M + 127) / 128;
   constexpr int kBTile = BN * 128;
-  constexpr int kH = BN / 2;  // Im rows start here
+  constexpr int kBRegion = kKB * kBTile;  // one of hi / lo of one buffer
+  constexpr int kH = BN / 2;              // Im rows start here
   using R = Chain16Roles<BN>;
   constexpr int kEpiThreads = R::kEpiThreads, kThreads = R::kThreads;
   constexpr int kProducerWarp = R::kProducerWarp, kMmaWarp = R::kMmaWarp;
-  uint8_t* b_hi = smem;
-  uint8_t* b_lo = smem + kKB * kBTile;
-  uint8_t* stg = smem + 2 * kKB * kBTile;
-  uint64_t* full = reinterpret_cast<uint64_t*>(stg + kStages * kStageBytes);
-  uint64_t* empty = full + kStages;
-  uint64_t* accb = empty + kStages;  // one per 128-row tile (M <= 256)
-  uint64_t* bready = accb + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bready + 1);
+  constexpr int kSt = R::kStages;
+  // two B buffers (hi, lo each): the epilogue of term g writes buffer (g + 1) & 1 while the MMAs
+  // of term g read buffer g & 1
+  uint8_t* bbuf = smem;
+  uint8_t* stg = smem + 4 * kBRegion;
+  uint64_t* full = reinterpret_cast<uint64_t*>(stg + kSt * kStageBytes);
+  uint64_t* empty = full + kSt;
+  uint64_t* accb = empty + kSt;  // one per 128-row tile (M <= 256)
+  uint64_t* bready = accb + 2;   // one per 128-row half of B (its rows come from that tile)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bready + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   unsigned* smax = reinterpret_cast<unsigned*>(tmem_slot + 2);  // [3]
   // TMEM columns: accumulators 2 m-tiles x 2 left operands x BN, then phi as head/tail float
@@ -170,19 +179,20 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < kSt; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
     mbar_init(&accb[0], 1);
     mbar_init(&accb[1], 1);
-    mbar_init(bready, kEpiThreads);
+    mbar_init(&bready[0], kEpiThreads);
+    mbar_init(&bready[1], kEpiThreads);
     *abort_flag = 0;
     smax[0] = smax[1] = smax[2] = 0u;
     mbar_fence_init();
   }
-  // rows n >= N (and kH + n >= kH + N) and k >= M of B stay zero for the whole kernel
-  for (int i = threadIdx.x; i < 2 * kKB * kBTile / 16; i += kThreads)
+  // rows n >= N (and kH + n >= kH + N) and k >= M of both B buffers stay zero for the whole kernel
+  for (int i = threadIdx.x; i < 4 * kBRegion / 16; i += kThreads)
     reinterpret_cast<int4*>(smem)[i] = make_int4(0, 0, 0, 0);
   fence_proxy_async_smem();
   if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
@@ -206,7 +216,7 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
           for (int mt = 0; mt < MT && ok; ++mt)
             for (int kb = 0; kb < KB && ok; ++kb)
               for (int part = 0; part < 2; ++part, ++g) {
-                const uint32_t s = g % kStages, r = g / kStages;
+                const uint32_t s = g % kSt, r = g / kSt;
                 if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) {
                   ok = false;
                   break;
@@ -234,15 +244,21 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
       for (int w = blockIdx.x; w < W && ok; w += gridDim.x)
         for (int t = 0; t < nterms && ok; ++t, ++term) {
           const bool onebody = (t == 0 || t == nterms - 1);
-          if (!mbar_wait(bready, term & 1, abort_flag, status)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
+          uint8_t* b_hi = bbuf + (term & 1) * 2 * kBRegion;
+          uint8_t* b_lo = b_hi + kBRegion;
           for (int mt = 0; mt < MT && ok; ++mt)
-            for (int kb = 0; kb < KB && ok; ++kb)
+            for (int kb = 0; kb < KB && ok; ++kb) {
+              // B's k-blocks 0-1 are rows 0..127 of the previous term's output (tile 0), k-blocks
+              // 2-3 rows 128..255 (tile 1): start on a half as soon as the epilogue has written it
+              if (mt == 0 && (kb & 1) == 0) {
+                if (!mbar_wait(&bready[kb >> 1], term & 1, abort_flag, status)) {
+                  ok = false;
+                  break;
+                }
+                tc_fence_after();
+              }
               for (int part = 0; part < 2; ++part, ++g) {
-                const uint32_t s = g % kStages, r = g / kStages;
+                const uint32_t s = g % kSt, r = g / kSt;
                 if (!mbar_wait(&full[s], r & 1, abort_flag, status)) {
                   ok = false;
                   break;
@@ -271,6 +287,7 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
                 mma_commit(&empty[s]);
                 if (kb == KB - 1 && part == 1) mma_commit(&accb[mt]);
               }
+            }
         }
     }
     __syncwarp();
@@ -282,8 +299,8 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
     const int c0 = half * kHalf;                     // this warp's first orbital
     const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
     uint32_t term = 0, u = 0;
-    bool ok = true, voted_out = false;
-    // the walker loop ends only through the votes, which every epilogue thread takes together
+    bool ok = true;
+    // the walker loop ends only through the vote, which every epilogue thread takes together
     for (int w = blockIdx.x; w < W; w += gridDim.x) {
       const double2* pin = phi_in + (size_t)w * M * N;
       double2* pout = phi_out + (size_t)w * M * N;
@@ -297,141 +314,129 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
       }
       float mx;
       if (!epi_max_vote(pmax, ok && !*abort_flag, smax, u, kEpiThreads, mx)) break;
-      float sb = b_scale_for(mx);  // scale of the current B
-      for (int i = threadIdx.x; i < M * N; i += kEpiThreads) {
-        const int m = i / N, n = i - m * N;
-        const double2 z = pin[i];
-        put_b16<BN>(b_hi, b_lo, n, m, (float)z.x, sb);
-        put_b16<BN>(b_hi, b_lo, kH + n, m, (float)z.y, sb);
+      const float s_in = b_scale_for(mx);
+      // every later B of this walker (phi after a one-body factor, the Taylor terms) takes one
+      // fixed scale, 2^4 below the starting orbitals' exact one: entries up to 2^6 times the
+      // largest orbital entry stay below binary16's range, and the smallest ones keep an absolute
+      // error near 2^-35 of it.  No CTA-wide maximum per term, so the next term's products start
+      // as soon as the first half of its operand is written.
+      const float s_fix = s_in * 0.0625f;
+      {
+        uint8_t* b_hi = bbuf + (term & 1) * 2 * kBRegion;
+        uint8_t* b_lo = b_hi + kBRegion;
+        for (int i = threadIdx.x; i < M * N; i += kEpiThreads) {
+          const int m = i / N, n = i - m * N;
+          const double2 z = pin[i];
+          put_b16<BN>(b_hi, b_lo, n, m, (float)z.x, s_in);
+          put_b16<BN>(b_hi, b_lo, kH + n, m, (float)z.y, s_in);
+        }
       }
       fence_proxy_async_smem();
-      mbar_arrive(bready);
+      mbar_arrive(&bready[0]);
+      mbar_arrive(&bready[1]);
+      bool overflow = false;
       for (int t = 0; t < nterms; ++t, ++term) {
         const bool onebody = (t == 0 || t == nterms - 1);
         const bool last = t == nterms - 1;
+        const float sb = t == 0 ? s_in : s_fix;  // scale of the B this term multiplied
         // the accumulator holds the product of the scaled operands
         const float unscale = onebody ? 1.0f / (e_scale * sb) : 1.0f / ((float)t * v_scale * sb);
-        // the next B's values (unscaled) wait in this warp's own, already read accumulator
-        // columns until the CTA-wide max gives their scale
-        float lmax = 0.0f;
+        uint8_t* n_hi = bbuf + ((term + 1) & 1) * 2 * kBRegion;  // the next term's B
+        uint8_t* n_lo = n_hi + kBRegion;
 #pragma unroll
         for (int mt = 0; mt < 2; ++mt) {
           if (mt >= MT) break;
           // each 128-row tile has its own accumulator barrier, so the first tile's epilogue
-          // overlaps the second tile's MMAs; a failed wait skips the work, not the vote below
+          // overlaps the second tile's MMAs; a failed wait skips the work, not the arrivals
           if (ok && !mbar_wait(&accb[mt], term & 1, abort_flag, status)) ok = false;
           ok = __all_sync(0xffffffffu, ok) != 0;
-          if (!ok) continue;
-          tc_fence_after();
+          if (ok) tc_fence_after();
           // a warp whose 32 rows all lie past M, or whose orbitals all lie past N, has nothing to do
-          if (mt * 128 + quarter * 32 >= M || c0 >= N) continue;
-          const int m = mt * 128 + quarter * 32 + lane;
-          const bool row_ok = m < M;
-          const uint32_t dc0 = lane_base + (uint32_t)((mt * 2 + 0) * BN);
-          const uint32_t dc1 = lane_base + (uint32_t)((mt * 2 + 1) * BN);
-          const uint32_t ac = lane_base + (uint32_t)(4 * BN + mt * 2 * BN);  // acc: head [0, BN), tail [BN, 2BN)
-          // real parts, then imaginary parts; TMEM reads/writes are warp-collective, so every
-          // lane takes part and rows past M only skip their global writes
+          if (ok && mt * 128 + quarter * 32 < M && c0 < N) {
+            const int m = mt * 128 + quarter * 32 + lane;
+            const bool row_ok = m < M;
+            const uint32_t dc0 = lane_base + (uint32_t)((mt * 2 + 0) * BN);
+            const uint32_t dc1 = lane_base + (uint32_t)((mt * 2 + 1) * BN);
+            const uint32_t ac = lane_base + (uint32_t)(4 * BN + mt * 2 * BN);  // phi: head [0, BN), tail [BN, 2BN)
+            // real parts, then imaginary parts; TMEM reads/writes are warp-collective, so every
+            // lane takes part and rows past M only skip their global and shared-memory writes
 #pragma unroll
-          for (int p = 0; p < 2; ++p) {
-            // p = 0: Re = D0[n] - D1[kH + n]; p = 1: Im = D0[kH + n] + D1[n]
-            // (one-body: D0[n] and D0[kH + n] with the real left operand E - I)
-            const int cx = (p ? kH : 0) + c0, cy = (p ? 0 : kH) + c0;
-            uint32_t x[8], y[8], ha[8], ta[8], nbits[8];
-            tmem_ld8(tmem + dc0 + cx, x);
-            if (!onebody) tmem_ld8(tmem + dc1 + cy, y);
-            if (t > 0) {
-              tmem_ld8(tmem + ac + cx, ha);
-              tmem_ld8(tmem + ac + BN + cx, ta);
-            }
-            tmem_wait_ld();
-            reg_after_wait(x);
-            if (!onebody) reg_after_wait(y);
-            if (t > 0) {
-              reg_after_wait(ha);
-              reg_after_wait(ta);
-            }
-            double base[8];
-            if (t == 0) {
+            for (int p = 0; p < 2; ++p) {
+              // p = 0: Re = D0[n] - D1[kH + n]; p = 1: Im = D0[kH + n] + D1[n]
+              // (one-body: D0[n] and D0[kH + n] with the real left operand E - I)
+              const int cx = (p ? kH : 0) + c0, cy = (p ? 0 : kH) + c0;
+              uint32_t x[8], y[8], ha[8], ta[8];
+              tmem_ld8(tmem + dc0 + cx, x);
+              if (!onebody) tmem_ld8(tmem + dc1 + cy, y);
+              if (t > 0) {
+                tmem_ld8(tmem + ac + cx, ha);
+                tmem_ld8(tmem + ac + BN + cx, ta);
+              }
+              tmem_wait_ld();
+              reg_after_wait(x);
+              if (!onebody) reg_after_wait(y);
+              if (t > 0) {
+                reg_after_wait(ha);
+                reg_after_wait(ta);
+              }
+              double base[8];
+              if (t == 0) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                  const double* src = reinterpret_cast<const double*>(pin + (size_t)m * N + c0 + q) + p;
+                  base[q] = (row_ok && c0 + q < N) ? *src : 0.0;
+                }
+              }
 #pragma unroll
               for (int q = 0; q < 8; ++q) {
-                const double* src = reinterpret_cast<const double*>(pin + (size_t)m * N + c0 + q) + p;
-                base[q] = (row_ok && c0 + q < N) ? *src : 0.0;
+                const int n = c0 + q;
+                float uq = __uint_as_float(x[q]);
+                if (!onebody) uq = p ? uq + __uint_as_float(y[q]) : uq - __uint_as_float(y[q]);
+                const float vq = uq * unscale;  // (E - I) phi, or T_t
+                const bool live = row_ok && n < N;
+                float nb = 0.0f;  // the next B value
+                if (t == 0) {
+                  // phi after the first one-body factor, kept as a head/tail float pair
+                  const double o = base[q] + (double)vq;
+                  const float hh = (float)o;
+                  ha[q] = __float_as_uint(hh);
+                  ta[q] = __float_as_uint((float)(o - (double)hh));
+                  nb = hh;
+                } else if (last) {
+                  const double o = (double)__uint_as_float(ha[q]) + (double)__uint_as_float(ta[q]) + (double)vq;
+                  if (live) reinterpret_cast<double*>(pout + (size_t)m * N + n)[p] = o;
+                } else {
+                  float a = __uint_as_float(ha[q]), b = __uint_as_float(ta[q]);
+                  ff_add(a, b, vq);
+                  ha[q] = __float_as_uint(a);
+                  ta[q] = __float_as_uint(b);
+                  nb = t < nmax ? vq : a + b;
+                }
+                if (!last && live) {
+                  overflow |= !(fabsf(nb * s_fix) < 32768.0f);
+                  put_b16<BN>(n_hi, n_lo, (p ? kH : 0) + n, m, nb, s_fix);
+                }
               }
-            }
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const int n = c0 + q;
-              float uq = __uint_as_float(x[q]);
-              if (!onebody) uq = p ? uq + __uint_as_float(y[q]) : uq - __uint_as_float(y[q]);
-              const float vq = uq * unscale;  // (E - I) phi, or T_t
-              const bool live = row_ok && n < N;
-              float nb = 0.0f;  // the next B value
-              if (t == 0) {
-                // phi after the first one-body factor, kept as a head/tail float pair
-                const double o = base[q] + (double)vq;
-                const float hh = (float)o;
-                ha[q] = __float_as_uint(hh);
-                ta[q] = __float_as_uint((float)(o - (double)hh));
-                nb = hh;
-              } else if (last) {
-                const double o = (double)__uint_as_float(ha[q]) + (double)__uint_as_float(ta[q]) + (double)vq;
-                if (live) reinterpret_cast<double*>(pout + (size_t)m * N + n)[p] = o;
-              } else {
-                float a = __uint_as_float(ha[q]), b = __uint_as_float(ta[q]);
-                ff_add(a, b, vq);
-                ha[q] = __float_as_uint(a);
-                ta[q] = __float_as_uint(b);
-                nb = t < nmax ? vq : a + b;
+              if (!last) {
+                tmem_st8(tmem + ac + cx, ha);
+                tmem_st8(tmem + ac + BN + cx, ta);
               }
-              if (!live) nb = 0.0f;
-              nbits[q] = __float_as_uint(nb);
-              lmax = fmaxf(lmax, fabsf(nb));
-            }
-            if (!last) {
-              tmem_st8(tmem + ac + cx, ha);
-              tmem_st8(tmem + ac + BN + cx, ta);
-              tmem_st8(tmem + dc0 + cx, nbits);
             }
           }
+          if (!last) {
+            // this half of the next B is written and this tile's accumulator read: the MMAs of
+            // the next term may start on it (and overwrite the accumulator)
+            tc_fence_before();
+            fence_proxy_async_smem();
+            mbar_arrive(&bready[mt]);
+          }
         }
+        if (MT == 1 && !last) mbar_arrive(&bready[1]);
         tmem_wait_st();
-        if (!last) {
-          // B of the next term, scaled by its own exact power of two
-          if (!epi_max_vote(lmax, ok && !*abort_flag, smax, u, kEpiThreads, mx)) {
-            voted_out = true;
-            break;
-          }
-          sb = b_scale_for(mx);
-          if (c0 < N) {
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-              if (mt >= MT || mt * 128 + quarter * 32 >= M) continue;  // warp-uniform: the loads are collective
-              const int m = mt * 128 + quarter * 32 + lane;
-              const uint32_t dc0 = lane_base + (uint32_t)((mt * 2 + 0) * BN);
-#pragma unroll
-              for (int p = 0; p < 2; ++p) {
-                uint32_t hb[8];
-                tmem_ld8(tmem + dc0 + (p ? kH : 0) + c0, hb);
-                tmem_wait_ld();
-                reg_after_wait(hb);
-                if (m < M)
-#pragma unroll
-                  for (int q = 0; q < 8; ++q)
-                    if (c0 + q < N) put_b16<BN>(b_hi, b_lo, (p ? kH : 0) + c0 + q, m, __uint_as_float(hb[q]), sb);
-              }
-            }
-          }
-        }
-        tc_fence_before();
-        if (!last) {
-          fence_proxy_async_smem();
-          mbar_arrive(bready);
-        }
       }
-      // a failed vote stops all epilogue threads together; a failed wait in the last term is
-      // carried into the next walker's first vote
-      if (voted_out) break;
+      // a Taylor term beyond binary16's range at the fixed scale: the walker's orbitals are wrong
+      if (overflow) flag(status, STATUS_NONFINITE);
+      tc_fence_before();
     }
   }
 
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
 template <int BN>
 cudaError_t launch_chain16(const Chain16Maps& maps, float e_scale, float v_scale, const double2* phi_in,
                            double2* phi_out, int W, int M, int N, int nmax, unsigned* status, cudaStream_t st) {
-  const size_t smem = 1024 + 2 * (size_t)kKB * BN * 128 + kStages * kStageBytes + 256;
+  const size_t smem = 1024 + 4 * (size_t)kKB * BN * 128 + Chain16Roles<BN>::kStages * kStageBytes + 256;
   auto kern = orbital_chain16_kernel<BN>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

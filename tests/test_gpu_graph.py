@@ -29,7 +29,9 @@ def _run(precision, graph, steps=12):
 def test_graph_replay_matches_launches(precision):
     af_g, got = _run(precision, True)
     _, ref = _run(precision, False)
-    assert af_g.graphs.captures == 2  # one graph per orbital-buffer parity
+    # one graph per orbital-buffer parity and step variant: plain steps (with the accumulation),
+    # and the reortho steps 5 and 10 (pair branch decided on the host after the replay)
+    assert af_g.graphs.captures == 4
     assert af_g.graphs.replays == 11
     for a, b in zip(got, ref):
         assert np.array_equal(a, b)
