@@ -172,7 +172,8 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
   uint64_t* bready = accb + 2;   // one per 128-row half of B (its rows come from that tile)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bready + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  unsigned* smax = reinterpret_cast<unsigned*>(tmem_slot + 2);  // [3]
+  unsigned* smax = reinterpret_cast<unsigned*>(tmem_slot + 2);  // [3]: the walkers' starting maxima
+  unsigned* tmax = smax + 3;  // [4]: max |B| of global term g in slot g % 4
   // TMEM columns: accumulators 2 m-tiles x 2 left operands x BN, then phi as head/tail float
   // pairs (2 m-tiles x [head BN | tail BN])
   constexpr uint32_t kTmemCols = 8 * BN;
@@ -189,6 +190,7 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
     mbar_init(&bready[1], kEpiThreads);
     *abort_flag = 0;
     smax[0] = smax[1] = smax[2] = 0u;
+    tmax[0] = tmax[1] = tmax[2] = tmax[3] = 0u;
     mbar_fence_init();
   }
   // rows n >= N (and kH + n >= kH + N) and k >= M of both B buffers stay zero for the whole kernel
@@ -315,12 +317,17 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
       float mx;
       if (!epi_max_vote(pmax, ok && !*abort_flag, smax, u, kEpiThreads, mx)) break;
       const float s_in = b_scale_for(mx);
-      // every later B of this walker (phi after a one-body factor, the Taylor terms) takes one
-      // fixed scale, 2^4 below the starting orbitals' exact one: entries up to 2^6 times the
-      // largest orbital entry stay below binary16's range, and the smallest ones keep an absolute
-      // error near 2^-35 of it.  No CTA-wide maximum per term, so the next term's products start
-      // as soon as the first half of its operand is written.
-      const float s_fix = s_in * 0.0625f;
+      // The scale of every later B is chosen before it is computed, so that the next term's
+      // products can start as soon as the first half of B is written (no CTA-wide maximum on the
+      // critical path).  It comes from the exact maxima of the earlier B's of the walker, which
+      // the epilogue threads reduce into tmax while they write them: phi after the first one-body
+      // factor takes s_in / 2; T_1 = V phi the scale of 2^5 x max|phi|; T_t (t >= 2) that of
+      // max|T_(t-1)| x 4 x the last growth ratio max|T_(t-1)| / max|T_(t-2)| (the ratios of a
+      // Taylor series fall like (t-1)/t); phi before the last one-body factor that of 2 x the sum
+      // of the maxima.  A scale that comes out too small for its B costs a few bits below the
+      // entries at 2^-13 of the largest (their absolute error stays near 2^-30 of it); one too
+      // large for its B is caught (|B x scale| >= 2^15 raises the non-finite status bit).
+      float s_cur = s_in, m_prev = 0.0f, m_sum = 0.0f;
       {
         uint8_t* b_hi = bbuf + (term & 1) * 2 * kBRegion;
         uint8_t* b_lo = b_hi + kBRegion;
@@ -338,11 +345,30 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
       for (int t = 0; t < nterms; ++t, ++term) {
         const bool onebody = (t == 0 || t == nterms - 1);
         const bool last = t == nterms - 1;
-        const float sb = t == 0 ? s_in : s_fix;  // scale of the B this term multiplied
+        // every epilogue thread has written this term's B and reduced its maximum into
+        // tmax[term % 4] (the wait returns at once; it orders those writes before the reads here)
+        if (ok && !mbar_wait(&bready[1], term & 1, abort_flag, status)) ok = false;
+        const float m_cur = __uint_as_float(*reinterpret_cast<volatile unsigned*>(&tmax[term & 3]));
+        if (threadIdx.x == 0) tmax[(term + 2) & 3] = 0u;  // for the B two terms ahead
+        const float sb = s_cur;  // scale of the B this term multiplies
         // the accumulator holds the product of the scaled operands
         const float unscale = onebody ? 1.0f / (e_scale * sb) : 1.0f / ((float)t * v_scale * sb);
+        // scale of the B this term's epilogue writes
+        float s_next;
+        if (t == 0) {
+          s_next = s_in * 0.5f;
+        } else if (t == 1) {
+          s_next = b_scale_for(m_cur * 32.0f);
+          m_sum = m_cur;
+        } else {
+          const float pred = m_cur * 4.0f * fmaxf(m_cur / fmaxf(m_prev, 1e-30f), 1e-6f);
+          s_next = t < nmax ? b_scale_for(pred) : b_scale_for(2.0f * (m_sum + m_cur + pred));
+          m_sum += m_cur;
+        }
+        m_prev = m_cur;
         uint8_t* n_hi = bbuf + ((term + 1) & 1) * 2 * kBRegion;  // the next term's B
         uint8_t* n_lo = n_hi + kBRegion;
+        float lmax = 0.0f;
 #pragma unroll
         for (int mt = 0; mt < 2; ++mt) {
           if (mt >= MT) break;
@@ -413,8 +439,9 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
                   nb = t < nmax ? vq : a + b;
                 }
                 if (!last && live) {
-                  overflow |= !(fabsf(nb * s_fix) < 32768.0f);
-                  put_b16<BN>(n_hi, n_lo, (p ? kH : 0) + n, m, nb, s_fix);
+                  overflow |= !(fabsf(nb * s_next) < 32768.0f);
+                  lmax = fmaxf(lmax, fabsf(nb));
+                  put_b16<BN>(n_hi, n_lo, (p ? kH : 0) + n, m, nb, s_next);
                 }
               }
               if (!last) {
@@ -424,6 +451,11 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
             }
           }
           if (!last) {
+            if (mt == MT - 1) {
+              // the next B's maximum, complete once every epilogue thread has arrived below
+              const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(lmax));
+              if (lane == 0 && bits) atomicMax(&tmax[(term + 1) & 3], bits);
+            }
             // this half of the next B is written and this tile's accumulator read: the MMAs of
             // the next term may start on it (and overwrite the accumulator)
             tc_fence_before();
@@ -433,6 +465,7 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
         }
         if (MT == 1 && !last) mbar_arrive(&bready[1]);
         tmem_wait_st();
+        s_cur = s_next;
       }
       // a Taylor term beyond binary16's range at the fixed scale: the walker's orbitals are wrong
       if (overflow) flag(status, STATUS_NONFINITE);
