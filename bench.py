@@ -751,6 +751,28 @@ def measure_peaks():
     return 0
 
 
+def profile_round(args):
+    """A few driver steps of one form launched kernel by kernel (no CUDA graph, device draws): the
+    target of the ncu captures summarised under profiles/, e.g.
+    ncu --set full --clock-control none -k regex:orbital_chain16 -s 1 -c 1 python bench.py
+    --profile-round --walkers 512"""
+    import torch
+
+    torch.cuda.set_device(0)
+    wl = args.workload
+    W = args.walkers or WORKLOADS[wl]["walkers"]
+    af, _ = build_afqmc(wl, W, "device", 7, precision=args.form if args.form != "both" else "mixed",
+                        population="device", paired_copies=True)
+    af.setup_run()
+    for step in range(1, 4):
+        af.step(step)
+    af.estimator.compute_estimator(af.system, af.walkers, af.hamiltonian, af.trial)
+    torch.cuda.synchronize()
+    af.walkers.check_status()
+    print(json.dumps({"profile_round": wl, "walkers": W, "steps": 3, "energy_evaluations": 2}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -769,9 +791,13 @@ def main():
     ap.add_argument("--form", choices=["fp64", "mixed", "both"], default="both",
                     help="which forms to time; with both, the mixed form is the headline and the FP64 form its reference")
     ap.add_argument("--measure-peaks", action="store_true", help="print measured GEMM/copy peaks and exit")
+    ap.add_argument("--profile-round", action="store_true",
+                    help="run 3 steps + 2 energy evaluations of one form kernel by kernel (an ncu target) and exit")
     args = ap.parse_args()
     if args.measure_peaks:
         return measure_peaks()
+    if args.profile_round:
+        return profile_round(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -455,6 +455,55 @@ int ipie_b200_onebody_adjoint(int W, int M, int na, int nb, const void* ghalfa, 
  * (trial_wavefunction/half_rotate.py:55-56). */
 int ipie_b200_rotate_onebody(const void* psi_conj, const double* h1, int M, int N, void* rh1, void* stream);
 
+/* ---- response through the walk: ipie's AD-AFQMC propagator in forward mode ----
+ * Every walker carries its orbitals phi and their derivative dphi along the
+ * coupling lambda of a one-body perturbation (h1 -> h1 + lambda V), stacked as
+ * one (2M, N) block [phi; dphi] per walker (walker_stride = 2 M N complex, dphi
+ * at phi + M N).  The orbital propagation runs ipie_b200_propagate_orbitals on
+ * the block operators [[E, 0], [dE, E]] (E = expH1, dE its derivative) and
+ * [[V, 0], [dV, V]] (ipie_b200_ad_block_vhs); the entries below do the rest.
+ * replaces: addons/adafqmc/propagation/propagator.py:190-249 (propagate_walkers)
+ *           with the derivative torch autograd takes of it in
+ *           addons/adafqmc/qmc/adafqmc.py:300-344 (ad_block_gradient) */
+
+/* O = phi^T psi_conj, Ghalf = O^-1 phi^T (W,N,M), log det O (W) and their
+ * derivatives dGhalf = O^-1 dphi^T - (O^-1 dO) Ghalf, d log det O = tr(O^-1 dO).
+ * N <= 32.  replaces: addons/adafqmc/trial_wavefunction/sdtrial.py:40-57
+ * (calc_overlap, get_ghalf) and the torch.det of propagator.py:232. */
+int ipie_b200_ad_greens_function(const void* phi, const void* dphi, long long walker_stride, int W, int M, int N,
+                                 const void* psi_conj, void* ghalf, void* dghalf, void* logdet, void* dlogdet,
+                                 unsigned int* status, void* stream);
+/* xbar = -sqrt(dt) (i vbias - mf) scaled to |xbar| <= bound, xshifted = x - xbar
+ * written (X, W), fb = sum_x x xbar - xbar^2 / 2, mfs = -sqrt(dt) sum_x xshifted mf,
+ * and the derivatives of all of them from dvbias.  vbias, dvbias (W,X) complex,
+ * x (W,X) double, mf (X) complex.  replaces: propagator.py:201-203 (force bias
+ * bound), :219-220 (shifted fields), :235-238 (expfb, expmf exponents). */
+int ipie_b200_ad_field_shift(const void* vbias, const void* dvbias, const double* x, const void* mf, int W, int X,
+                             double sqrt_dt, double bound, void* xshifted, void* dxshifted, void* fb, void* dfb,
+                             void* mfs, void* dmfs, void* stream);
+/* w <- w |ratio exp(fb) exp(mfs) exp(c)| max(cos theta, 0), theta = arg(ratio
+ * exp(mfs)), ratio = exp(2 (logdet_new - logdet_old)); then w <- min(w, 0.1
+ * sum w); dweight follows (dc = derivative of c).  One CTA.
+ * replaces: propagator.py:232-249 (weight update and cap). */
+int ipie_b200_ad_update_weight(int W, const void* logdet_old, const void* dlogdet_old, const void* logdet_new,
+                               const void* dlogdet_new, const void* fb, const void* dfb, const void* mfs,
+                               const void* dmfs, double c, double dc, double* weight, double* dweight,
+                               unsigned int* status, void* stream);
+/* Modified Gram-Schmidt of each walker's phi (M, N) in place, the same column
+ * operations applied to dphi.  replaces: addons/adafqmc/walkers/rhf_walkers.py:
+ * 22-27 (reorthogonalize; every observable is invariant under phi -> phi T). */
+int ipie_b200_ad_reortho(void* phi, void* dphi, long long walker_stride, int W, int M, int N, unsigned int* status,
+                         void* stream);
+/* out (W, 2M, 2M) complex = [[V, 0], [dV, V]] from V, dV (W, M, M) complex. */
+int ipie_b200_ad_block_vhs(const void* vhs, const void* dvhs, int W, int M, void* out, void* stream);
+/* out = a + s b over n complex entries (the Green's functions G +- s dG whose local energies
+ * give the energy's derivative by polarisation: the local energy is quadratic in G). */
+int ipie_b200_ad_axpy(const void* a, const void* b, double s, long long n, void* out, void* stream);
+/* out[d] = in[src[d]], blocks of len complex entries (in != out): the stochastic
+ * reconfiguration copy of the walkers' [phi; dphi].
+ * replaces: addons/adafqmc/walkers/rhf_walkers.py:30-49 (the walker_states gather). */
+int ipie_b200_ad_gather(const int* src, int W, long long len, const void* in, void* out, void* stream);
+
 /* Split FP64 values into a TF32 head (round to nearest) and an FP32 remainder:
  * x ~= hi + lo, the operands of the 3-pass TF32 tensor-core products of the
  * mixed-precision form (lo may be NULL).  No counterpart in ipie. */

@@ -74,6 +74,13 @@ SIGNATURES = {
     "ipie_b200_normal_fill": [P, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_ulonglong, P],
     "ipie_b200_normal_fill_dev": [P, ctypes.c_longlong, ctypes.c_ulonglong, P, P],
     "ipie_b200_pair_branch": [I, P, P, D, D, D, ctypes.c_ulonglong, P, I, P, P, P, P, P, P],
+    "ipie_b200_ad_greens_function": [P, P, ctypes.c_longlong, I, I, I, P, P, P, P, P, P, P],
+    "ipie_b200_ad_field_shift": [P, P, P, P, I, I, D, D, P, P, P, P, P, P, P],
+    "ipie_b200_ad_update_weight": [I, P, P, P, P, P, P, P, P, D, D, P, P, P, P],
+    "ipie_b200_ad_reortho": [P, P, ctypes.c_longlong, I, I, I, P, P],
+    "ipie_b200_ad_block_vhs": [P, P, I, I, P, P],
+    "ipie_b200_ad_axpy": [P, P, D, ctypes.c_longlong, P, P],
+    "ipie_b200_ad_gather": [P, I, ctypes.c_longlong, P, P, P],
 }
 
 _lib = None

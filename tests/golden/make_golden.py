@@ -409,6 +409,80 @@ def ghf_fixture(name, sysw, nwalkers, seed, nsteps=3):
     print("wrote", name)
 
 
+def ad_walk_fixture(name):
+    """ipie's AD-AFQMC block derivative through the walk (``addons/adafqmc/qmc/adafqmc.py:222-344``,
+    ``ad_block`` and ``ad_block_gradient``) on a small RHF system, with the trial's orbital tangent
+    set to zero (no orbital relaxation), FakeComm, and torch's draws recorded: the auxiliary
+    fields of every step (``propagation/propagator.py:219``) and the stochastic-reconfiguration
+    uniforms (``walkers/rhf_walkers.py:41``)."""
+    import torch
+
+    from ipie.addons.adafqmc.hamiltonians.hamiltonian import HamObs
+    from ipie.addons.adafqmc.qmc.adafqmc import ADAFQMC
+    from ipie.addons.adafqmc.walkers.rhf_walkers import Walkers
+    from ipie.qmc.comm import FakeComm
+
+    class TrialwithTangent(torch.autograd.Function):
+        # the trial passes through unchanged; its derivative is the given tangent
+        # (ipie addons/adafqmc/utils/miscellaneous.py:162-175; that module imports pyscf)
+        @staticmethod
+        def forward(ctx, coupling, trial, tangent):
+            ctx.save_for_backward(tangent)
+            return trial
+
+        @staticmethod
+        def backward(ctx, grad_output):
+            (tangent,) = ctx.saved_tensors
+            return tangent * grad_output, None, None
+
+    sysw = synthetic.generate(14, (3, 3), 36, decay=30.0, seed=21, uhf=False, chol_scale="stable")
+    M, N, X = sysw.nbasis, sysw.nup, sysw.nchol
+    rng = np.random.default_rng(22)
+    V = rng.normal(0.0, 0.1, size=(M, M))
+    V = np.triu(V) + np.triu(V, 1).T
+    # the trial's full orbital set: its N occupied orbitals completed to an orthonormal basis
+    q, _ = np.linalg.qr(np.hstack([sysw.psi[:, :N], rng.normal(size=(M, M - N))]))
+    C = np.hstack([sysw.psi[:, :N], q[:, N:]])
+    L = sysw.chol.T.reshape(X, M, M)
+    hamobs = HamObs(N, M, torch.from_numpy(sysw.h1e[0].copy()), torch.from_numpy(L.copy()),
+                    torch.tensor(sysw.ecore, dtype=torch.float64), observable=(torch.from_numpy(V.copy()), torch.tensor(0.0, dtype=torch.float64)),
+                    obs_type="dipole")
+    W = 8
+    phi0 = np.eye(M)[:, :N][None] + 0.1 * (rng.normal(size=(W, M, N)) + 1j * rng.normal(size=(W, M, N)))
+    w0 = rng.uniform(0.5, 1.5, size=W)
+    walkers = Walkers(W, torch.from_numpy(phi0.copy()), torch.from_numpy(w0.copy()))
+    af = ADAFQMC.build(FakeComm(), lambda c, t, g: TrialwithTangent.apply(c, t, g), num_walkers_per_process=W,
+                       num_steps_per_block=10, ad_block_size=30, num_ad_blocks=1, timestep=0.005,
+                       stabilize_freq=5, pop_control_freq=5, seed=3)
+    draws, zetas = [], []
+    randn0, rand0 = torch.randn, torch.rand
+
+    def randn(*a, **k):
+        x = randn0(*a, **k)
+        draws.append(x.numpy().copy())
+        return x
+
+    def rand(*a, **k):
+        z = rand0(*a, **k)
+        zetas.append(float(z.item()))
+        return z
+
+    torch.manual_seed(5)
+    torch.randn, torch.rand = randn, rand
+    try:
+        out_w, e, obs, blkwts, wtsgrad = af.ad_block_gradient(hamobs, walkers, torch.from_numpy(C.copy()),
+                                                             torch.zeros(M, M, dtype=torch.float64))
+    finally:
+        torch.randn, torch.rand = randn0, rand0
+    out = dict(V=V, C=C, phi0=phi0, w0=w0, draws=np.array(draws), zetas=np.array(zetas),
+               energy=np.array(float(e)), dE_dlambda=np.array(float(obs[0])), total_weight=np.array(float(blkwts)),
+               dW_dlambda=np.array(float(wtsgrad[0])), final_phi=out_w.walker_states.numpy(),
+               final_weight=out_w.walker_weights.numpy(), chol_checksum=checksum(sysw.chol),
+               psi_checksum=checksum(sysw.psi))
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name, "E", float(e), "dE/dlambda", float(obs[0]), "W", float(blkwts), "dW", float(wtsgrad[0]))
+
+
 def analysis_fixture(name):
     """ipie's autocorrelation reblocking (``analysis/autocorr.py:54-105``) on seeded series:
     white noise and AR(1) series with correlation 0.5 and 0.9, of several lengths."""
@@ -451,6 +525,9 @@ def config_fixtures():
 
 
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "adwalk":
+        ad_walk_fixture("ad_walk_m14.npz")
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[2] == "analysis":
         analysis_fixture("reblock_autocorr.npz")
         sys.exit(0)
