@@ -504,6 +504,25 @@ int ipie_b200_ad_axpy(const void* a, const void* b, double s, long long n, void*
  * replaces: addons/adafqmc/walkers/rhf_walkers.py:30-49 (the walker_states gather). */
 int ipie_b200_ad_gather(const int* src, int W, long long len, const void* in, void* out, void* stream);
 
+/* ---- particle-hole multi-determinant trial ----
+ * Determinant by determinant (j), after the single-determinant Green's function
+ * (ipie_b200_greens_function_single_det_batch with D_j's one-hot orbitals) and,
+ * for energies, ipie_b200_local_energy_single_det_batch with D_j's half-rotated
+ * integrals: acc_ovlp += c_j^* O_j, acc_energy += c_j^* O_j E_j (W,3) (may be
+ * NULL), acc_g_s[occ_s[i], q] += c_j^* O_j ghalf_s[i, q] (full (W,M,M) Green's
+ * functions, may be NULL).  occa (na) occb (nb) device ints: D_j's orbitals.
+ * replaces: estimators/greens_function_multi_det.py:17-72 (greens_function_multi_det)
+ *           and :1113 (greens_function_multi_det_wicks_opt), estimators/
+ *           local_energy_batch.py:78-131 and local_energy_wicks.py:864 (energies). */
+int ipie_b200_multidet_accumulate(int W, int M, int na, int nb, double coeff_re, double coeff_im, const int* occa,
+                                  const int* occb, const void* ovlp, const void* energy, const void* ghalfa,
+                                  const void* ghalfb, void* acc_ovlp, void* acc_energy, void* acc_ga, void* acc_gb,
+                                  void* stream);
+/* energy (W,3), ga, gb (W,M,M) (each may be NULL) divided by acc_ovlp (W): the
+ * trial's local energies and Green's functions.  A zero total overlap sets status bit 1. */
+int ipie_b200_multidet_finalize(int W, int M, const void* acc_ovlp, void* energy, void* ga, void* gb,
+                                unsigned int* status, void* stream);
+
 /* Split FP64 values into a TF32 head (round to nearest) and an FP32 remainder:
  * x ~= hi + lo, the operands of the 3-pass TF32 tensor-core products of the
  * mixed-precision form (lo may be NULL).  No counterpart in ipie. */

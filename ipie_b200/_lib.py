@@ -81,6 +81,8 @@ SIGNATURES = {
     "ipie_b200_ad_block_vhs": [P, P, I, I, P, P],
     "ipie_b200_ad_axpy": [P, P, D, ctypes.c_longlong, P, P],
     "ipie_b200_ad_gather": [P, I, ctypes.c_longlong, P, P, P],
+    "ipie_b200_multidet_accumulate": [I, I, I, I, D, D, P, P, P, P, P, P, P, P, P, P, P],
+    "ipie_b200_multidet_finalize": [I, I, P, P, P, P, P, P],
 }
 
 _lib = None

@@ -483,6 +483,74 @@ def ad_walk_fixture(name):
     print("wrote", name, "E", float(e), "dE/dlambda", float(obs[0]), "W", float(blkwts), "dW", float(wtsgrad[0]))
 
 
+def multidet_fixture(name):
+    """ipie's particle-hole multi-determinant trial: the Wick's-theorem Green's function and overlap
+    (``estimators/greens_function_multi_det.py:1113``, ``greens_function_multi_det_wicks_opt``) and
+    local energy (``estimators/local_energy_wicks.py:864``,
+    ``local_energy_multi_det_trial_wicks_batch_opt``) on perturbed walkers, with ipie's naive
+    per-determinant path (``ParticleHoleNaive``, ``greens_function_multi_det``,
+    ``local_energy_batch.py:78`` ``local_energy_multi_det_trial_batch``) as a cross-check."""
+    import itertools
+
+    from ipie.estimators.greens_function_multi_det import (
+        greens_function_multi_det,
+        greens_function_multi_det_wicks_opt,
+    )
+    from ipie.estimators.local_energy_batch import local_energy_multi_det_trial_batch
+    from ipie.estimators.local_energy_wicks import local_energy_multi_det_trial_wicks_batch_opt
+    from ipie.trial_wavefunction.particle_hole import ParticleHoleNaive, ParticleHoleNonChunked
+
+    sysw = synthetic.generate(14, (4, 3), 42, decay=30.0, seed=31, uhf=True, chol_scale="stable")
+    M, na, nb = sysw.nbasis, sysw.nup, sysw.ndown
+    rng = np.random.default_rng(32)
+    # the reference (lowest orbitals) and a random selection of excited determinants up to four
+    # holes per spin, ordered by excitation level as ipie's inputs usually are
+    oa = [tuple(range(na))] + [c for c in itertools.combinations(range(M), na) if c != tuple(range(na))]
+    ob = [tuple(range(nb))] + [c for c in itertools.combinations(range(M), nb) if c != tuple(range(nb))]
+    pick_a = [0] + list(rng.choice(np.arange(1, len(oa)), 59))
+    pick_b = [0] + list(rng.choice(np.arange(1, len(ob)), 59))
+    occa = [np.array(oa[i]) for i in pick_a]
+    occb = [np.array(ob[i]) for i in pick_b]
+    ci = rng.normal(size=60) + 1j * rng.normal(size=60)
+    ci[0] = 3.0
+    ci /= np.linalg.norm(ci)
+    order = np.argsort([-abs(c) for c in ci], kind="stable")
+    ci, occa, occb = ci[order], [occa[i] for i in order], [occb[i] for i in order]
+    wfn = (ci, occa, occb)
+    ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
+    system = Generic((na, nb))
+    W = 6
+    init = np.hstack([np.eye(M)[:, :na], np.eye(M)[:, :nb]]) + 0.3 * rng.normal(size=(M, na + nb))
+    out = dict(ci=ci, occa=np.array(occa), occb=np.array(occb), init=init)
+    results = {}
+    for key, cls in (("opt", ParticleHoleNonChunked), ("naive", ParticleHoleNaive)):
+        trial = cls(wfn, (na, nb), M)
+        trial.build()
+        trial.half_rotate(ham)
+        walkers = UHFWalkersTrial(trial, init.copy(), na, nb, M, W, MPIHandler())
+        walkers.build(trial)
+        prng = np.random.default_rng(33)
+        walkers.phia = walkers.phia + 0.2 * (prng.normal(size=walkers.phia.shape) + 1j * prng.normal(size=walkers.phia.shape))
+        walkers.phib = walkers.phib + 0.2 * (prng.normal(size=walkers.phib.shape) + 1j * prng.normal(size=walkers.phib.shape))
+        if key == "opt":
+            ovlp = greens_function_multi_det_wicks_opt(walkers, trial)
+            # the energy normalises by walkers.ovlp, which a propagation step would have set
+            walkers.ovlp = ovlp
+            energy = local_energy_multi_det_trial_wicks_batch_opt(system, ham, walkers, trial)
+            out["phia"], out["phib"] = np.array(walkers.phia), np.array(walkers.phib)
+        else:
+            ovlp = greens_function_multi_det(walkers, trial)
+            energy = local_energy_multi_det_trial_batch(system, ham, walkers, trial)
+        results[key] = (np.array(ovlp), np.array(walkers.Ga), np.array(walkers.Gb), np.array(energy))
+    for a, b in zip(results["opt"], results["naive"]):
+        assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b))
+    out["ovlp"], out["Ga"], out["Gb"], out["energy"] = results["opt"]
+    out["chol_checksum"] = checksum(sysw.chol)
+    out["psi_checksum"] = checksum(sysw.psi)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name, "energies", out["energy"][:, 0])
+
+
 def analysis_fixture(name):
     """ipie's autocorrelation reblocking (``analysis/autocorr.py:54-105``) on seeded series:
     white noise and AR(1) series with correlation 0.5 and 0.9, of several lengths."""
@@ -525,6 +593,9 @@ def config_fixtures():
 
 
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "multidet":
+        multidet_fixture("multidet_m14.npz")
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[2] == "adwalk":
         ad_walk_fixture("ad_walk_m14.npz")
         sys.exit(0)
