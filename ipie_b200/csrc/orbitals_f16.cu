@@ -104,6 +104,44 @@ __device__ __forceinline__ void put_b16(uint8_t* bhi, uint8_t* blo, int n, int k
   *reinterpret_cast<__half*>(blo + o) = __float2half_rn(y - __half2float(h));
 }
 
+// Writes the binary16 head and remainder of v x s for an 8 x 8 block of B: on entry lane l of
+// the warp holds v[q] for K index k_base + l and orbital row n0 + q; groups of 8 lanes transpose
+// their 8 x 8 block with shuffles (three butterfly stages, each swapping the off-diagonal
+// halves), after which lane 8g + r holds orbital row n0 + r at K indices k_base + 8g .. + 7, one
+// 16-byte chunk of the K-major swizzled layout per plane.
+template <int BN>
+__device__ __forceinline__ void put_b16_block(uint8_t* bhi, uint8_t* blo, int n0, int k_base, float (&v)[8],
+                                              float s) {
+  const int lane = threadIdx.x & 31, r = lane & 7;
+#pragma unroll
+  for (int st = 4; st >= 1; st >>= 1) {
+    const bool upper = (r & st) != 0;
+#pragma unroll
+    for (int q0 = 0; q0 < 8; ++q0) {
+      if (q0 & st) continue;
+      const int q1 = q0 | st;
+      const float x = upper ? v[q0] : v[q1];
+      const float y = __shfl_xor_sync(0xffffffffu, x, st);
+      if (upper)
+        v[q0] = y;
+      else
+        v[q1] = y;
+    }
+  }
+  uint32_t hw[4], lw[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float y0 = v[2 * i] * s, y1 = v[2 * i + 1] * s;
+    const __half h0 = __float2half_rn(y0), h1 = __float2half_rn(y1);
+    const __half l0 = __float2half_rn(y0 - __half2float(h0)), l1 = __float2half_rn(y1 - __half2float(h1));
+    hw[i] = (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
+    lw[i] = (uint32_t)__half_as_ushort(l0) | ((uint32_t)__half_as_ushort(l1) << 16);
+  }
+  const uint32_t o = b16_offset<BN>(n0 + r, k_base + (lane & ~7));
+  *reinterpret_cast<uint4*>(bhi + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+  *reinterpret_cast<uint4*>(blo + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
 // (a, b) += x for a head/tail float pair a + b (|b| <= ulp(a)/2): Knuth's two-sum of a and x,
 // then the tail folded back; ~2^-47 relative, enough to accumulate the FP32 Taylor terms
 // of phi without a round trip through FP64 global memory.
@@ -413,6 +451,7 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
                   base[q] = (row_ok && c0 + q < N) ? *src : 0.0;
                 }
               }
+              float nbv[8];  // this lane's next-B values (row m, orbitals c0..c0+7)
 #pragma unroll
               for (int q = 0; q < 8; ++q) {
                 const int n = c0 + q;
@@ -438,13 +477,14 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
                   ta[q] = __float_as_uint(b);
                   nb = t < nmax ? vq : a + b;
                 }
-                if (!last && live) {
-                  overflow |= !(fabsf(nb * s_next) < 32768.0f);
-                  lmax = fmaxf(lmax, fabsf(nb));
-                  put_b16<BN>(n_hi, n_lo, (p ? kH : 0) + n, m, nb, s_next);
-                }
+                if (!live) nb = 0.0f;
+                overflow |= !(fabsf(nb * s_next) < 32768.0f);
+                lmax = fmaxf(lmax, fabsf(nb));
+                nbv[q] = nb;
               }
               if (!last) {
+                // rows past M and orbitals past N hold zeros, which is what B keeps there
+                put_b16_block<BN>(n_hi, n_lo, (p ? kH : 0) + c0, mt * 128 + quarter * 32, nbv, s_next);
                 tmem_st8(tmem + ac + cx, ha);
                 tmem_st8(tmem + ac + BN + cx, ta);
               }
