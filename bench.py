@@ -377,7 +377,7 @@ def statistics_runs(wl, W, rank, steps, cv=None, dt=0.005):
     if cv is not None:
         from ipie_b200.control_variate import ControlVariateEnergyEstimator
 
-        cv_est = ControlVariateEnergyEstimator(cv, fraction=8, seed=99 + rank, precision="mixed")
+        cv_est = ControlVariateEnergyEstimator(cv.clone(), fraction=8, seed=99 + rank, precision="mixed")
     nblk = runs["fp64"].params.num_steps_per_block
     t0 = time.perf_counter()
     for step in range(1, steps + 1):
@@ -429,7 +429,7 @@ def timed_run(wl, W, precision, args, rank, world, local, rng="device", with_clo
     if cv is not None:
         from ipie_b200.control_variate import ControlVariateEnergyEstimator
 
-        af.estimator = ControlVariateEnergyEstimator(cv, fraction=8, seed=7 + rank, precision="mixed")
+        af.estimator = ControlVariateEnergyEstimator(cv.clone(), fraction=8, seed=7 + rank, precision="mixed")
     step = 0
     for _ in range(args.warmup):
         step += 1

@@ -70,6 +70,16 @@ class ExchangeControlVariate:
         self.y_scale = 1.0
         self.trained = False
 
+    def clone(self):
+        """An independent copy (weights, optimiser state and normalisation)."""
+        import copy
+
+        new = copy.copy(self)
+        for name in ("master", "wbf", "grad", "m", "v", "mu", "sigma"):
+            setattr(new, name, getattr(self, name).clone())
+        new._rbuf_key = None
+        return new
+
     # ------------------------------------------------------------ training
     def fit(self, feats, y, base=None, epochs=60, batch=4096, lr=2e-3, holdout=0.1, seed=0):
         """Train on (features, exchange term) pairs; returns the train/holdout MSE history (normalised units).
@@ -123,6 +133,27 @@ class ExchangeControlVariate:
         self.t += 1
         call("ipie_b200_mlp_adam", ptr(self.master), ptr(self.wbf), ptr(self.grad), ptr(self.m), ptr(self.v), self.n,
              float(lr), self.t, stream())
+
+    def refine(self, feats, y, base, steps=4, batch=1024, lr=5e-4, seed=0):
+        """A few Adam steps on new (features, exchange term, linear term) pairs, keeping the feature
+        and target normalisation of :meth:`fit` (the online refit of the estimator)."""
+        n = feats.shape[0]
+        B = min(batch, n)
+        x = feats.float().contiguous().clone()
+        call("ipie_b200_normalize_features", ptr(x), n, self.F, ptr(self.mu), ptr(self.sigma), stream())
+        yt = (((y.double() - base.double()) - self.y_mean) / self.y_scale).float().contiguous()
+        key = ("refine", B)
+        if getattr(self, "_rbuf_key", None) != key:
+            self._rbuf = (torch.empty(4 * B * self.H, dtype=F32, device=self.device),
+                          torch.empty(B + 2 * B * self.H, dtype=F32, device=self.device),
+                          torch.empty(B, dtype=F32, device=self.device),
+                          torch.zeros(1, dtype=F32, device=self.device))
+            self._rbuf_key = key
+        acts, work, out, loss = self._rbuf
+        gen = torch.Generator(device="cpu").manual_seed(seed)
+        for _ in range(steps):
+            idx = torch.randperm(n, generator=gen)[:B].to(self.device, non_blocking=True)
+            self._step(x[idx].contiguous(), yt[idx].contiguous(), B, acts, work, out, loss, lr)
 
     def mse(self, x_norm, y_norm):
         pred = self.forward_normalised(x_norm)
@@ -260,7 +291,12 @@ class ControlVariateEnergyEstimator:
 
     names = ["ENumer", "EDenom", "ETotal", "E1Body", "E2Body"]
 
-    def __init__(self, cv, fraction=8, seed=11, precision="fp64"):
+    def __init__(self, cv, fraction=8, seed=11, precision="fp64", refit=True, buffer_blocks=8, refit_steps=2,
+                 refit_lr=5e-4):
+        """``refit``: after every block, the network takes ``refit_steps`` Adam steps on the exact
+        subsamples of the last ``buffer_blocks`` blocks (this block's included), so that it follows
+        walkers that drift away from its training data.  The prediction used for a block comes from
+        a network that has seen earlier blocks only, so the estimate stays unbiased."""
         self.cv = cv
         self.fraction = fraction
         self.precision = precision
@@ -268,21 +304,37 @@ class ControlVariateEnergyEstimator:
         self.parts = None
         self._out = None
         self.last = {}
+        self.refit, self.buffer_blocks, self.refit_steps, self.refit_lr = refit, buffer_blocks, refit_steps, refit_lr
+        self._buffer = []
+        self._calls = 0
 
     def compute_estimator(self, system=None, walkers=None, hamiltonian=None, trial=None):
+        W = walkers.nwalkers
+        S = max(1, W // self.fraction)
         if self.parts is None:
             self.parts = EnergyParts(hamiltonian, trial, walkers, precision=self.precision)
             self._out = torch.zeros(5, dtype=F64, device=walkers.device)
+            self._idx_host = torch.empty(S, dtype=torch.int32).pin_memory()
+            self._idx = torch.empty(S, dtype=torch.int32, device=walkers.device)
         p = self.parts
         p.compute(walkers)
         pred = self.cv.predict(p.feat, p.base)
-        W = walkers.nwalkers
-        S = max(1, W // self.fraction)
-        idx = torch.from_numpy(np.sort(self.rng.choice(W, S, replace=False)).astype(np.int32)).to(walkers.device)
+        self._idx_host.numpy()[...] = np.sort(self.rng.choice(W, S, replace=False))
+        self._idx.copy_(self._idx_host, non_blocking=True)
+        idx = self._idx
         y_s = p.exchange_term(walkers, idx)
         call("ipie_b200_cv_sums", W, ptr(walkers.weight), ptr(p.energy_noexx), ptr(pred), S, ptr(idx), ptr(y_s),
              ptr(self._out), stream())
         o = self._out.cpu().numpy()
+        if self.refit:
+            il = idx.long()
+            self._buffer.append((p.feat[il].clone(), y_s.clone(), p.base[il].clone()))
+            self._buffer = self._buffer[-self.buffer_blocks:]
+            f = torch.cat([b[0] for b in self._buffer])
+            y = torch.cat([b[1] for b in self._buffer])
+            b = torch.cat([b[2] for b in self._buffer])
+            self._calls += 1
+            self.cv.refine(f, y, b, steps=self.refit_steps, lr=self.refit_lr, seed=self._calls)
         numer = o[0] - o[1]
         self.last = {"cv": numer, "plain_subsample": o[3] - o[4], "denom": o[2]}
         self._data = np.array([numer, o[2], 0.0, 0.0, 0.0], dtype=np.complex128)
@@ -316,26 +368,32 @@ def generate_training_data(afqmc, steps=100, first_step=1):
 
 
 def subsample_variances(cv, parts, walkers, fraction=8, trials=64, seed=3):
-    """Spread of the subsampled exchange estimate over random subsamples, with and without the network.
+    """Spread of the subsampled exchange estimate over random subsamples: with no control variate,
+    with the full one (leading-vector term + network) and with the leading-vector term alone (the
+    method without the network).
 
-    Returns (std_without, std_with, exact) for the weighted exchange sum of the current walkers.
+    Returns (std_without, std_with, exact, std_linear) for the weighted exchange sum of the current
+    walkers.
     """
     parts.compute(walkers)
     y = parts.exchange_term(walkers)
     wt = walkers.weight.double()
     exact = float((wt * y).sum().item())
     pred = cv.predict(parts.feat, parts.base).double()
+    lin = parts.base.double()
     full_c = float((wt * pred).sum().item())
+    full_l = float((wt * lin).sum().item())
     rng = np.random.default_rng(seed)
     W = walkers.nwalkers
     S = max(1, W // fraction)
-    plain, with_cv = [], []
+    plain, with_cv, with_lin = [], [], []
     for _ in range(trials):
         idx = torch.from_numpy(rng.choice(W, S, replace=False)).to(walkers.device)
         f = W / S
         plain.append(f * float((wt[idx] * y[idx]).sum().item()))
         with_cv.append(full_c + f * float((wt[idx] * (y[idx] - pred[idx])).sum().item()))
-    return float(np.std(plain)), float(np.std(with_cv)), exact
+        with_lin.append(full_l + f * float((wt[idx] * (y[idx] - lin[idx])).sum().item()))
+    return float(np.std(plain)), float(np.std(with_cv)), exact, float(np.std(with_lin))
 
 
 def cv_estimator_error(cv, parts, walkers, fraction=8, trials=64, seed=5):
@@ -345,7 +403,8 @@ def cv_estimator_error(cv, parts, walkers, fraction=8, trials=64, seed=5):
     control variate and without it (plain subsample), and the mean difference with its
     standard error (zero within it: the estimator is unbiased).
     """
-    sd_plain, sd_cv, exact = subsample_variances(cv, parts, walkers, fraction=fraction, trials=trials, seed=seed)
+    sd_plain, sd_cv, exact, sd_lin = subsample_variances(cv, parts, walkers, fraction=fraction, trials=trials,
+                                                         seed=seed)
     y = parts.exchange_term(walkers)
     wt = walkers.weight.double()
     pred = cv.predict(parts.feat, parts.base).double()
@@ -361,5 +420,6 @@ def cv_estimator_error(cv, parts, walkers, fraction=8, trials=64, seed=5):
     wsum = float(wt.sum().item())
     d = np.asarray(diffs) / wsum * 1e3
     return {"noise_mEh": float(d.std()), "plain_subsample_noise_mEh": sd_plain / wsum * 1e3,
+            "linear_term_only_noise_mEh": sd_lin / wsum * 1e3,
             "mean_diff_mEh": float(d.mean()), "mean_diff_stderr_mEh": float(d.std() / np.sqrt(trials)),
             "fraction": fraction, "trials": trials}
