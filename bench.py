@@ -219,9 +219,9 @@ def barrier_max(value, world):
 # workload's walker count (the capture's traffic grows with the walkers it processes); the
 # capture and its command are summarised under profiles/.
 DRAM_TRAFFIC = {
-    # FP16 orbital chain at 512 walkers: 218.5 MB read + 35.4 MB written per launch
-    # (profiles/fp16_kernels_c2_w512.md), x4 for 2048 walkers (its traffic is per walker)
-    ("c2_rhf_m200", "mixed", "orbitals"): 4 * (218.5e6 + 35.4e6),
+    # FP16 orbital chain at 512 walkers: 219.6 MB read + 36.1 MB written per launch
+    # (profiles/orbital_chain16_pipelined_c2_w512.md), x4 for 2048 walkers (its traffic is per walker)
+    ("c2_rhf_m200", "mixed", "orbitals"): 4 * (219.57e6 + 36.08e6),
 }
 
 
