@@ -518,6 +518,405 @@ __global__ void __launch_bounds__(Chain16Roles<BN>::kThreads, 1)
   if (warp == 0) tmem_dealloc(tmem, kTmemCols);
 }
 
+// ---------------------------------------------------------------------------------------------
+// The same orbital update with the operand roles transposed (M <= 208): every product is
+//
+//     D[r][m] = sum_k' A[r][k'] B[m][k']   (tcgen05 kind::f16, M = 128 rows, N = Mp = M rounded up to 16)
+//
+// with the walker's current orbitals as A and the walker's VHS planes (or E - I) as B, so that
+// one MMA covers every row of V (N = 208 at M = 200) instead of 64 orbital columns: an MMA issues
+// in ~70 cycles whatever its size, which bound the 128 x 64 x 16 products of the kernel above, and
+// a 128 x 208 x 16 product runs ~100 cycles on the tensor core.
+//
+// A (shared memory, 128 rows x K' = 2 Mp, binary16, 32B-swizzled K-major 16-column k-blocks):
+// row 32 q + n holds orbital n, q = 2 h + c for the head (h = 0) or remainder (h = 1) of the split
+// and the output component c (0 = real, 1 = imaginary); its K' = [0, Mp) half is the real-part
+// operand and [Mp, 2 Mp) the imaginary-part one:
+//     real-output rows: [Re T | -Im T],   imaginary-output rows: [Im T | Re T]
+// against B = [Re V | Im V] along K' (the planes of one k-block loaded as separate stages), so that
+// D's lane 32 q + n, column m holds the head or remainder part of Re or Im (V T)[m][n] (for E - I
+// only the real half of K' runs: Re T x (E - I) and Im T x (E - I)).  Each product is four MMAs
+// per K step (A x B_head and A x B_remainder for both planes), the remainder x remainder term
+// riding along.  The epilogue adds lanes 32 q + n and 32 (q + 2) + n through a shared-memory
+// staging tile (different warps own those TMEM lanes).
+//
+// Pipeline: the epilogue of term g handles the output in 64-row chunks (the K chunks of the next
+// product): it loads the chunk's accumulator columns into the staging tile, writes the next
+// operand's rows of that chunk into A and arrives on aready[chunk]; the MMAs of term g + 1 start
+// on a chunk as soon as it is written.  D is double-buffered in TMEM (columns 0 and 256), so the
+// MMAs of term g + 1 run while the epilogue of term g still reads its buffer.  phi accumulates in
+// FP64 in phi_out (global memory, read back by the same thread every term); the binary16 scales of
+// the operands follow the kernel above (a predicted scale per Taylor term).
+constexpr int kTMaxM = 208;
+constexpr int kTEpiWarps = 16, kTEpiThreads = 32 * kTEpiWarps;
+constexpr int kTProducerWarp = kTEpiWarps, kTMmaWarp = kTEpiWarps + 1;
+constexpr int kTThreads = kTEpiThreads + 64;
+constexpr int kTStages = 3;
+constexpr int kTPitch = 68;  // floats per staging row: 64 columns + 4 (bank spread)
+constexpr int kTStagingBytes = 128 * kTPitch * 4;
+__host__ __device__ constexpr int t_a_bytes(int mp) { return 128 * 2 * mp * 2; }
+__host__ __device__ constexpr int t_stage_bytes(int mp) { return mp * 128; }
+__host__ __device__ constexpr size_t t_smem_bytes(int mp) {
+  return 1024 + (size_t)t_a_bytes(mp) + (size_t)kTStages * t_stage_bytes(mp) + kTStagingBytes + 256;
+}
+
+// byte offset of A element (row r, K' index k): 16-column k-blocks of 128 rows x 32 bytes, the two
+// 16-byte halves of a row swapped on every other group of 4 rows (TMA's and the MMA's 32B pattern)
+__device__ __forceinline__ uint32_t t_a_offset(int r, int k) {
+  return (uint32_t)((k >> 4) * 4096 + r * 32 + ((((k >> 3) & 1) ^ ((r >> 2) & 1)) << 4) + ((k & 7) << 1));
+}
+// binary16 head and remainder of v x s, four values packed per 8 bytes
+__device__ __forceinline__ void t_split4(const float (&v)[4], float s, uint2& hi, uint2& lo) {
+  uint32_t h[2], l[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const float y0 = v[2 * i] * s, y1 = v[2 * i + 1] * s;
+    const __half h0 = __float2half_rn(y0), h1 = __float2half_rn(y1);
+    const __half l0 = __float2half_rn(y0 - __half2float(h0)), l1 = __float2half_rn(y1 - __half2float(h1));
+    h[i] = (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
+    l[i] = (uint32_t)__half_as_ushort(l0) | ((uint32_t)__half_as_ushort(l1) << 16);
+  }
+  hi = make_uint2(h[0], h[1]);
+  lo = make_uint2(l[0], l[1]);
+}
+__device__ __forceinline__ uint2 t_neg(uint2 x) { return make_uint2(x.x ^ 0x80008000u, x.y ^ 0x80008000u); }
+__device__ __forceinline__ void t_put(uint8_t* a, int r, int k, uint2 v) {
+  *reinterpret_cast<uint2*>(a + t_a_offset(r, k)) = v;
+}
+// the next operand's entries for orbital n at rows m0 .. m0 + 3 (values x s, split): all eight
+// places they take in A
+__device__ __forceinline__ void t_put_a4(uint8_t* a, int mp, int n, int m0, const float (&tr)[4],
+                                         const float (&ti)[4], float s) {
+  uint2 rh, rl, ih, il;
+  t_split4(tr, s, rh, rl);
+  t_split4(ti, s, ih, il);
+  t_put(a, n, m0, rh);
+  t_put(a, n, mp + m0, t_neg(ih));
+  t_put(a, 32 + n, m0, ih);
+  t_put(a, 32 + n, mp + m0, rh);
+  t_put(a, 64 + n, m0, rl);
+  t_put(a, 64 + n, mp + m0, t_neg(il));
+  t_put(a, 96 + n, m0, il);
+  t_put(a, 96 + n, mp + m0, rl);
+}
+// AND of ok over the epilogue threads (named barrier 1), which also orders their shared-memory writes
+__device__ __forceinline__ bool t_epi_all(bool ok) {
+  uint32_t r;
+  asm volatile(
+      "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.and.pred q, 1, %2, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)ok), "r"(kTEpiThreads)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void t_epi_sync() { asm volatile("bar.sync 2, %0;\n" ::"r"(kTEpiThreads) : "memory"); }
+
+__global__ void __launch_bounds__(kTThreads, 1)
+    orbital_chain_t16_kernel(const __grid_constant__ Chain16Maps maps, float e_scale, float v_scale,
+                             const double2* __restrict__ phi_in, double2* __restrict__ phi_out, int W, int M, int N,
+                             int nmax, unsigned* status) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int Mp = (M + 15) & ~15;  // N of every product; K of each half of K'
+  const int KB16 = Mp / 16;       // 16-column k-blocks of A per half of K'
+  const int C = (Mp + 63) / 64;   // 64-row chunks of the output (64-column k-blocks of B)
+  const int stage_bytes = t_stage_bytes(Mp);
+  uint8_t* abuf = smem;
+  uint8_t* stg = smem + t_a_bytes(Mp);
+  float* staging = reinterpret_cast<float*>(stg + kTStages * stage_bytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(staging) + kTStagingBytes);
+  uint64_t* empty = full + kTStages;
+  uint64_t* accfull = empty + kTStages;  // [2] D buffer complete (MMA commit)
+  uint64_t* accempty = accfull + 2;      // [2] D buffer read (every epilogue thread)
+  uint64_t* aready = accempty + 2;       // [4] chunk of A written (every epilogue thread)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(aready + 4);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  unsigned* smax = reinterpret_cast<unsigned*>(tmem_slot + 2);  // [3]: the walkers' starting maxima
+  unsigned* tmax = smax + 3;  // [4]: max |operand| of global term g in slot g % 4
+  constexpr uint32_t kTmemCols = 512;  // D buffers at columns 0 and 256
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kTStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accfull[b], 1);
+      mbar_init(&accempty[b], kTEpiThreads);
+    }
+    for (int c = 0; c < 4; ++c) mbar_init(&aready[c], kTEpiThreads);
+    *abort_flag = 0;
+    smax[0] = smax[1] = smax[2] = 0u;
+    tmax[0] = tmax[1] = tmax[2] = tmax[3] = 0u;
+    mbar_fence_init();
+  }
+  // A's rows of orbitals past N and columns past M stay zero for the whole kernel
+  for (int i = threadIdx.x; i < t_a_bytes(Mp) / 16; i += kTThreads)
+    reinterpret_cast<int4*>(abuf)[i] = make_int4(0, 0, 0, 0);
+  fence_proxy_async_smem();
+  if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int nterms = nmax + 2;
+
+  if (warp == kTProducerWarp) {
+    // ------------------------------------------------------------ TMA producer
+    // lane p issues the loads of stages p, p + kProducers, ... (producer_lanes)
+    constexpr int kProducers = producer_lanes(kTStages);
+    if (lane < kProducers) {
+      if (lane == 0) {
+        tma_prefetch_desc(&maps.e_hi);
+        tma_prefetch_desc(&maps.e_lo);
+        for (int i = 0; i < 4; ++i) tma_prefetch_desc(&maps.v[i]);
+      }
+      uint32_t g = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < W && ok; w += gridDim.x)
+        for (int t = 0; t < nterms && ok; ++t) {
+          const bool onebody = (t == 0 || t == nterms - 1);
+          const int nparts = onebody ? 1 : 2;
+          for (int c = 0; c < C && ok; ++c)
+            for (int p = 0; p < nparts && ok; ++p)
+              for (int h = 0; h < 2; ++h, ++g) {
+                if ((int)(g % kProducers) != lane) continue;
+                const uint32_t s = g % kTStages, r = g / kTStages;
+                if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) {
+                  ok = false;
+                  break;
+                }
+                uint8_t* dst = stg + s * stage_bytes;
+                mbar_expect_tx(&full[s], stage_bytes);
+                // rows and columns past M are zero-filled by TMA (no traffic)
+                if (onebody)
+                  tma_load_2d(dst, h ? &maps.e_lo : &maps.e_hi, c * 64, 0, &full[s]);
+                else  // maps.v: re_hi, im_hi, re_lo, im_lo
+                  tma_load_3d(dst, &maps.v[2 * h + p], c * 64, 0, w, &full[s]);
+              }
+        }
+    }
+    __syncwarp();
+  } else if (warp == kTMmaWarp) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = idesc_f16(128, Mp);
+      uint32_t g = 0, term = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < W && ok; w += gridDim.x)
+        for (int t = 0; t < nterms && ok; ++t, ++term) {
+          const bool onebody = (t == 0 || t == nterms - 1);
+          const int nparts = onebody ? 1 : 2;
+          const uint32_t buf = term & 1;
+          if (term >= 2 && !mbar_wait(&accempty[buf], ((term >> 1) - 1) & 1, abort_flag, status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem + buf * 256;
+          bool first = true;
+          for (int c = 0; c < C && ok; ++c) {
+            if (!mbar_wait(&aready[c], term & 1, abort_flag, status)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const int kkc = min(4, (Mp - 64 * c) / 16);
+            for (int p = 0; p < nparts && ok; ++p)
+              for (int h = 0; h < 2; ++h, ++g) {
+                const uint32_t s = g % kTStages, r = g / kTStages;
+                if (!mbar_wait(&full[s], r & 1, abort_flag, status)) {
+                  ok = false;
+                  break;
+                }
+                tc_fence_after();
+                const uint64_t bdesc = desc_kmajor_sw128(stg + s * stage_bytes);
+                for (int kk = 0; kk < kkc; ++kk) {
+                  const uint64_t adesc = desc_kmajor_sw32(abuf + (p * KB16 + 4 * c + kk) * 4096);
+                  mma_f16(d, adesc, bdesc + 2 * kk, idesc, first ? 0u : 1u);
+                  first = false;
+                }
+                mma_commit(&empty[s]);
+              }
+          }
+          if (ok) mma_commit(&accfull[buf]);
+        }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue warps
+    // TMEM loads: warp w reads lane quarter w % 4, columns 16 (w / 4) .. + 15 of each chunk;
+    // outputs: thread (w, n = lane) takes rows 4 w .. 4 w + 3 of each chunk for orbital n
+    const int q = warp & 3, j = warp >> 2;
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    uint32_t term = 0, u = 0;
+    bool ok = true;
+    for (int w = blockIdx.x; w < W; w += gridDim.x) {
+      const double2* pin = phi_in + (size_t)w * M * N;
+      double2* pout = phi_out + (size_t)w * M * N;
+      float pmax = 0.0f;
+      for (int i = threadIdx.x; i < M * N; i += kTEpiThreads) {
+        const double2 z = pin[i];
+        pmax = fmaxf(pmax, fmaxf(fabsf((float)z.x), fabsf((float)z.y)));
+      }
+      float mx;
+      if (!epi_max_vote(pmax, ok && !*abort_flag, smax, u, kTEpiThreads, mx)) break;
+      const float s_in = b_scale_for(mx);
+      // the first operand: the walker's starting orbitals x their exact scale
+      for (int c = 0; c < C; ++c) {
+        const int m0 = 64 * c + 4 * warp;
+        if (m0 < Mp) {
+          float tr[4], ti[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int m = m0 + i;
+            const double2 z = (m < M && lane < N) ? pin[(size_t)m * N + lane] : make_double2(0.0, 0.0);
+            tr[i] = (float)z.x;
+            ti[i] = (float)z.y;
+          }
+          t_put_a4(abuf, Mp, lane, m0, tr, ti, s_in);
+        }
+      }
+      fence_proxy_async_smem();
+      for (int c = 0; c < C; ++c) mbar_arrive(&aready[c]);
+      float s_cur = s_in, m_prev = 0.0f, m_sum = 0.0f;
+      bool overflow = false;
+      for (int t = 0; t < nterms; ++t, ++term) {
+        const bool onebody = (t == 0 || t == nterms - 1);
+        const bool last = t == nterms - 1;
+        const uint32_t buf = term & 1;
+        // every epilogue thread has written this term's operand and reduced its maximum into
+        // tmax[term % 4] before its last arrival (the wait orders those writes before the read)
+        if (ok && !mbar_wait(&aready[C - 1], term & 1, abort_flag, status)) ok = false;
+        const float m_cur = __uint_as_float(*reinterpret_cast<volatile unsigned*>(&tmax[term & 3]));
+        if (threadIdx.x == 0) tmax[(term + 2) & 3] = 0u;  // for the operand two terms ahead
+        const float sb = s_cur;
+        const float unscale = onebody ? 1.0f / (e_scale * sb) : 1.0f / ((float)t * v_scale * sb);
+        // the scale of the operand this term writes (predicted as in the kernel above)
+        float s_next;
+        if (t == 0) {
+          s_next = s_in * 0.5f;
+        } else if (t == 1) {
+          s_next = b_scale_for(m_cur * 32.0f);
+          m_sum = m_cur;
+        } else {
+          const float pred = m_cur * 4.0f * fmaxf(m_cur / fmaxf(m_prev, 1e-30f), 1e-6f);
+          s_next = t < nmax ? b_scale_for(pred) : b_scale_for(2.0f * (m_sum + m_cur + pred));
+          m_sum += m_cur;
+        }
+        m_prev = m_cur;
+        if (ok && !mbar_wait(&accfull[buf], (term >> 1) & 1, abort_flag, status)) ok = false;
+        float lmax = 0.0f;
+        for (int c = 0; c < C; ++c) {
+          // this thread's FP64 orbitals of the chunk (phi, or the running sum), loaded before the
+          // staging round so that their latency passes behind it
+          const int m0 = 64 * c + 4 * warp;
+          double2 pv[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int m = m0 + i;
+            const size_t o = (size_t)m * N + lane;
+            pv[i] = (m0 < Mp && m < M && lane < N) ? (t == 0 ? pin[o] : pout[o]) : make_double2(0.0, 0.0);
+          }
+          // accumulator columns of this chunk -> staging (tcgen05.ld is warp-collective)
+          ok = __all_sync(0xffffffffu, ok) != 0;
+          const int col = 64 * c + 16 * j;
+          if (ok && col < Mp) {
+            tc_fence_after();
+            uint32_t x[16];
+            tmem_ld16(tmem + lane_base + buf * 256 + (uint32_t)col, x);
+            tmem_wait_ld();
+            reg_after_wait(x);
+            float4* dst = reinterpret_cast<float4*>(staging + (q * 32 + lane) * kTPitch + 16 * j);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              dst[i] = make_float4(__uint_as_float(x[4 * i]), __uint_as_float(x[4 * i + 1]),
+                                   __uint_as_float(x[4 * i + 2]), __uint_as_float(x[4 * i + 3]));
+          }
+          if (c == C - 1) {
+            // the buffer is read: the MMAs two terms ahead may overwrite it
+            tc_fence_before();
+            mbar_arrive(&accempty[buf]);
+          }
+          if (!t_epi_all(ok && !*abort_flag)) {
+            ok = false;
+            break;
+          }
+          if (m0 < Mp) {
+            const float4 rh = *reinterpret_cast<const float4*>(staging + lane * kTPitch + 4 * warp);
+            const float4 ih = *reinterpret_cast<const float4*>(staging + (32 + lane) * kTPitch + 4 * warp);
+            const float4 rl = *reinterpret_cast<const float4*>(staging + (64 + lane) * kTPitch + 4 * warp);
+            const float4 il = *reinterpret_cast<const float4*>(staging + (96 + lane) * kTPitch + 4 * warp);
+            const float vr[4] = {(rh.x + rl.x) * unscale, (rh.y + rl.y) * unscale, (rh.z + rl.z) * unscale,
+                                 (rh.w + rl.w) * unscale};
+            const float vi[4] = {(ih.x + il.x) * unscale, (ih.y + il.y) * unscale, (ih.z + il.z) * unscale,
+                                 (ih.w + il.w) * unscale};
+            float nr[4], ni[4];  // the next operand (orbital lane, rows m0 ..)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              const int m = m0 + i;
+              const bool live = m < M && lane < N;
+              nr[i] = 0.0f;
+              ni[i] = 0.0f;
+              if (!live) continue;
+              // t = 0: phi after the first one-body factor, where the FP64 sum starts
+              const double2 a = make_double2(pv[i].x + (double)vr[i], pv[i].y + (double)vi[i]);
+              pout[(size_t)m * N + lane] = a;
+              if (t == 0) {
+                nr[i] = (float)a.x;
+                ni[i] = (float)a.y;
+              } else if (!last) {
+                nr[i] = t < nmax ? vr[i] : (float)a.x;
+                ni[i] = t < nmax ? vi[i] : (float)a.y;
+              }
+              overflow |= !(fabsf(nr[i] * s_next) < 32768.0f) || !(fabsf(ni[i] * s_next) < 32768.0f);
+              lmax = fmaxf(lmax, fmaxf(fabsf(nr[i]), fabsf(ni[i])));
+            }
+            if (!last) t_put_a4(abuf, Mp, lane, m0, nr, ni, s_next);
+          }
+          if (!last) {
+            if (c == C - 1) {
+              // the next operand's maximum, complete once every epilogue thread has arrived
+              const unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(lmax));
+              if (lane == 0 && bits) atomicMax(&tmax[(term + 1) & 3], bits);
+            }
+            fence_proxy_async_smem();
+            mbar_arrive(&aready[c]);
+          }
+          t_epi_sync();  // the staging tile is free for the next chunk
+        }
+        if (!ok) break;
+        s_cur = s_next;
+      }
+      // a Taylor term beyond binary16's range at its predicted scale: the walker's orbitals are wrong
+      if (overflow) flag(status, STATUS_NONFINITE);
+      tc_fence_before();
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+}
+
+cudaError_t launch_chain_t16(const Chain16Maps& maps, float e_scale, float v_scale, const double2* phi_in,
+                             double2* phi_out, int W, int M, int N, int nmax, unsigned* status, cudaStream_t st) {
+  const int Mp = (M + 15) & ~15;
+  const size_t smem = t_smem_bytes(Mp);
+  cudaError_t e =
+      cudaFuncSetAttribute(orbital_chain_t16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  const int grid = W < sms ? W : sms;
+  orbital_chain_t16_kernel<<<grid, kTThreads, smem, st>>>(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax,
+                                                          status);
+  note_launch();
+  return cudaGetLastError();
+}
+
 template <int BN>
 cudaError_t launch_chain16(const Chain16Maps& maps, float e_scale, float v_scale, const double2* phi_in,
                            double2* phi_out, int W, int M, int N, int nmax, unsigned* status, cudaStream_t st) {
@@ -548,14 +947,18 @@ cudaError_t mixed_orbital_chain16(const void* e_hi, const void* e_lo, float e_sc
       !(v_scale > 0.0f))
     return cudaErrorInvalidValue;
   const int ld = f16_ld(M);
+  // M <= 208: the transposed kernel (every row of V in one MMA); else the 128-row tile kernel
+  const bool transposed = M <= kTMaxM;
+  const int box_rows = transposed ? (M + 15) & ~15 : 128;
   Chain16Maps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = make_map_f16(&maps.e_hi, e_hi, M, M, ld, 128)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.e_lo, e_lo, M, M, ld, 128)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.e_hi, e_hi, M, M, ld, box_rows)) != cudaSuccess) return e;
+  if ((e = make_map_f16(&maps.e_lo, e_lo, M, M, ld, box_rows)) != cudaSuccess) return e;
   const void* planes[4] = {v_re_hi, v_im_hi, v_re_lo, v_im_lo};
   for (int i = 0; i < 4; ++i)
-    if ((e = make_map_f16_batched(&maps.v[i], planes[i], W, M, M, ld, 128)) != cudaSuccess) return e;
+    if ((e = make_map_f16_batched(&maps.v[i], planes[i], W, M, M, ld, box_rows)) != cudaSuccess) return e;
+  if (transposed) return launch_chain_t16(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
   if (2 * N <= 32) return launch_chain16<32>(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
   return launch_chain16<64>(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
 }
