@@ -451,6 +451,19 @@ int ipie_b200_cv_sums(int W, const double* weight, const void* energy_noexx, con
 int ipie_b200_onebody_adjoint(int W, int M, int na, int nb, const void* ghalfa, const void* ghalfb,
                               const void* psia_conj, const void* psib_conj, const double* coeff, void* work, void* rdm,
                               void* stream);
+/* Vector-Jacobian product of the local energy with respect to the half-rotated Green's
+ * functions (no counterpart in ipie; its AD-AFQMC addon takes the same derivative with torch
+ * autograd through addons/adafqmc/estimators/estimator.py:4-23):
+ *   gbar_s[w] = ebar[w] * dE_w / dGhalf_s[w]   (holomorphic derivative, no conjugation)
+ * for E of ipie_b200_local_energy_single_det_batch with the same operands (rhf = 1: the
+ * doubled alpha-only energy, gbara only):
+ *   dE/dG_s = f1 rH1_s + 2 fc sum_x X_x L_s,x - 2 fx sum_x (L_s,x G_s^T) L_s,x,
+ *   X_x = sum_s L_s,x . G_s, L_s,x row x of rchol_s as (n_s, M).
+ * ebar (W) complex; work: W*X complex; out: gbara (W,na,M), gbarb (W,nb,M) complex.
+ * n_s * M <= 8192; FP64 on the CUDA cores (one CTA per walker and spin). */
+int ipie_b200_local_energy_vjp(int rhf, const double* rchola, const double* rcholb, const void* rH1a,
+                               const void* rH1b, const void* ghalfa, const void* ghalfb, int W, int X, int M, int na,
+                               int nb, const void* ebar, void* work, void* gbara, void* gbarb, void* stream);
 /* rH1 (N, M) complex = psi^H h1: the half-rotated one-body matrix for a given h1 (M, M) real
  * (trial_wavefunction/half_rotate.py:55-56). */
 int ipie_b200_rotate_onebody(const void* psi_conj, const double* h1, int M, int N, void* rh1, void* stream);

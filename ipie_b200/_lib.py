@@ -61,6 +61,7 @@ SIGNATURES = {
     "ipie_b200_cv_features": [I, I, I, I, I, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "ipie_b200_gather_walkers": [P, P, I, ctypes.c_longlong, P, P],
     "ipie_b200_cv_sums": [I, P, P, P, I, P, P, P, P],
+    "ipie_b200_local_energy_vjp": [I, P, P, P, P, P, P, I, I, I, I, I, P, P, P, P, P],
     "ipie_b200_onebody_adjoint": [I, I, I, I, P, P, P, P, P, P, P, P],
     "ipie_b200_rotate_onebody": [P, P, I, I, P, P],
     "ipie_b200_split_tf32": [P, P, P, ctypes.c_longlong, P],
@@ -122,6 +123,9 @@ def ptr(t):
         raise CudaLibError("ipie_b200 kernels take CUDA tensors only")
     if not t.is_contiguous():
         raise CudaLibError("ipie_b200 kernels take contiguous tensors only")
+    if t.is_conj() or t.is_neg():
+        # a lazy view: its memory still holds the unconjugated (or unnegated) values
+        raise CudaLibError("ipie_b200 kernels take materialised tensors (call resolve_conj() / resolve_neg())")
     return ctypes.c_void_p(t.data_ptr())
 
 

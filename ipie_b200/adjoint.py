@@ -18,7 +18,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from ._lib import call, ptr, stream
+from ._lib import call, lib, ptr, stream
 
 C128, F64 = torch.complex128, torch.float64
 
@@ -100,3 +100,53 @@ def energy_response(hamiltonian, trial, walkers, V):
     E = (e * wt).sum() / wt.sum()
     E.backward()
     return float(lam.grad.item()), float(E.item())
+
+
+class LocalEnergyGreens(torch.autograd.Function):
+    """Per-walker local energies (W,) complex as a function of the half-rotated Green's functions
+    ``ghalfa`` (W, na, M) and ``ghalfb`` (W, nb, M) at fixed Hamiltonian and trial; the backward is
+    the library's vector-Jacobian product (``ipie_b200_local_energy_vjp``).  ``rhf`` selects the
+    doubled alpha-only energy (``ghalfb`` then gets no gradient).
+
+    The energy is holomorphic in G, so for an upstream gradient g_w PyTorch's convention asks for
+    g_w conj(dE_w/dG): the kernel's ebar * dE/dG is taken with ebar = conj(g) and conjugated back.
+    ipie's AD-AFQMC addon differentiates the same energy with autograd through its torch
+    implementation (``addons/adafqmc/estimators/estimator.py:4-23``)."""
+
+    @staticmethod
+    def forward(ctx, ghalfa, ghalfb, hamiltonian, trial, rhf=False):
+        ga, gb = ghalfa.detach().contiguous(), ghalfb.detach().contiguous()
+        W, na, M = ga.shape
+        nb = gb.shape[1]
+        X = hamiltonian.nchol
+        dev = ga.device
+        rows = lib().ipie_b200_exchange_rows(W, X, M, na)
+        if not rhf and nb > 0:
+            rows += lib().ipie_b200_exchange_rows(W, X, M, nb)
+        work = torch.empty(W * X + rows * W, dtype=C128, device=dev)
+        energy = torch.empty(W, 3, dtype=C128, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        call("ipie_b200_local_energy_single_det_batch", int(rhf), ptr(trial._rchola), ptr(trial._rcholb),
+             ptr(trial._rH1a), ptr(trial._rH1b), hamiltonian.ecore, ptr(ga), ptr(gb), W, X, M, na, nb, ptr(work),
+             ptr(energy), ptr(status), stream())
+        ctx.save_for_backward(ga, gb)
+        ctx.ham, ctx.trial, ctx.rhf = hamiltonian, trial, rhf
+        return energy[:, 0].clone()
+
+    @staticmethod
+    def backward(ctx, grad_e):
+        ga, gb = ctx.saved_tensors
+        ham, trial, rhf = ctx.ham, ctx.trial, ctx.rhf
+        W, na, M = ga.shape
+        nb = gb.shape[1]
+        X = ham.nchol
+        ebar = grad_e.detach().to(C128).conj().resolve_conj().contiguous()
+        work = torch.empty(W * X, dtype=C128, device=ga.device)
+        gbara = torch.empty_like(ga)
+        gbarb = torch.empty_like(gb) if not rhf and nb > 0 else gbara
+        call("ipie_b200_local_energy_vjp", int(rhf), ptr(trial._rchola), ptr(trial._rcholb), ptr(trial._rH1a),
+             ptr(trial._rH1b), ptr(ga), ptr(gb), W, X, M, na, nb, ptr(ebar), ptr(work), ptr(gbara), ptr(gbarb),
+             stream())
+        ga_grad = gbara.conj()
+        gb_grad = None if (rhf or nb == 0) else gbarb.conj()
+        return ga_grad, gb_grad, None, None, None
