@@ -81,6 +81,58 @@ cudaError_t make_map_f16(CUtensorMap* m, const void* base, long long rows, long 
   return make_map_f16(m, base, rows, k, ld, box_rows, false);
 }
 
+// Output map of W matrices of rows x ld halves (row stride ld, matrix stride rows x ld) for
+// tensor stores of {bx, by, bz} boxes (no swizzle: the staging box is plain row-major).
+cudaError_t make_map_f16_store(CUtensorMap* m, void* base, long long W, long long rows, long long ld, int bx, int by,
+                               int bz) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 8) || rows <= 0 || W <= 0 || (bx * 2) % 16) return cudaErrorInvalidValue;
+  cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)rows, (cuuint64_t)W};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)rows * ld * 2};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// 2-D K-major FP16 operand and its remainder as the two planes of one 3-D map: the remainder
+// starts `plane` halves after the head (plane % 8 == 0); tiles of box_rows x 64 (k32: x 32) of
+// both planes land back to back in shared memory (the head tile, then the remainder tile).
+cudaError_t make_map_f16_planes(CUtensorMap* m, const void* base, long long rows, long long k, long long ld,
+                                long long plane, int box_rows, bool k32) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 8) || (plane % 8) || rows <= 0 || k <= 0 || plane <= 0)
+    return cudaErrorInvalidValue;
+  cuuint64_t dims[3] = {(cuuint64_t)k, (cuuint64_t)rows, 2};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)plane * 2};
+  cuuint32_t box[3] = {k32 ? 32u : 64u, (cuuint32_t)box_rows, 2};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, k32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// The head/remainder pair (hi, lo) of an operand of rows x ld halves as one two-plane map when lo
+// sits at a fixed offset >= rows x ld after hi (both halves of one allocation); else two maps.
+// Returns the planes flag of GemmMaps.
+static cudaError_t map_f16_pair(CUtensorMap* mhi, CUtensorMap* mlo, const void* hi, const void* lo, long long rows,
+                                long long k, long long ld, int box_rows, bool k32, int* planes) {
+  const uintptr_t h = reinterpret_cast<uintptr_t>(hi), l = reinterpret_cast<uintptr_t>(lo);
+  const long long d = l > h ? (long long)((l - h) / 2) : 0;
+  if (l > h && (l - h) % 16 == 0 && d >= rows * ld) {
+    *planes = 1;
+    return make_map_f16_planes(mhi, hi, rows, k, ld, d, box_rows, k32);
+  }
+  *planes = 0;
+  cudaError_t e = make_map_f16(mhi, hi, rows, k, ld, box_rows, k32);
+  if (e == cudaSuccess) e = make_map_f16(mlo, lo, rows, k, ld, box_rows, k32);
+  return e;
+}
+
 // 3-D batched K-major FP16 operand: `batch` matrices of `rows` x `k` halves (row stride ld
 // halves, ld % 8 == 0; matrix stride rows * ld), tiles of box_rows x 64 of one matrix; rows past
 // `rows` and columns past `k` read as 0 (no traffic).
@@ -430,13 +482,26 @@ __device__ __forceinline__ void pack8_f16(const float* x, float s, uint4& hi, ui
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// The epilogue goes through shared memory and TMA tensor stores: one 32 KB staging box of 64
+// walkers x 16 rows x 16 halves (the {16, 16, 64} box of the plane maps maps->out: re_hi, re_lo,
+// im_hi, im_lo), filled and stored eight times per tile -- real then imaginary plane, head then
+// remainder, the block (I, J) then its transpose (J, I) -- by the threads of the rows (c) that
+// feed that plane.  A thread's scattered 16-byte global stores (one 32-byte sector split between
+// two of them, 16 walkers per warp instruction) took ~30k cycles per tile and stalled the next
+// tile's products; the staged tensor stores leave the copy to the TMA engine.  Rows i >= M and
+// columns j >= ld of a box are clipped by the store.
 struct EpiVHSBlock {
-  __half *re_hi, *re_lo, *im_hi, *im_lo;
-  int M, ld, W, nb;  // nb: 16-orbital blocks per side
-  float f;           // sqrt(dt) v_scale / (operand scales)
-  __device__ __forceinline__ void operator()(int, int row, int col0, const float* v, uint8_t*) const {
+  int M, W, nb;  // nb: 16-orbital blocks per side
+  float f;       // sqrt(dt) v_scale / (operand scales)
+  static constexpr int kSmemBytes = 64 * 16 * 32;
+  static constexpr bool kUsesMaps = true;
+  static constexpr int kThreads = 256;  // the epilogue threads of the 128 x 256 tile (barrier 3)
+  __device__ __forceinline__ static void sync() { asm volatile("bar.sync 3, %0;\n" ::"r"(kThreads) : "memory"); }
+  __device__ __forceinline__ void operator()(int, int row, int col0, const float* v, uint8_t* smem,
+                                             const GemmMaps* maps) const {
     const int w = row >> 1, c = row & 1;
-    if (w >= W) return;
+    const int w0 = (row & ~127) >> 1, wl = w - w0;
+    const bool live = w < W;
     int blk = col0 >> 8, I = 0;  // tile = block index, row-major over I <= J
     while (blk >= nb - I) {
       blk -= nb - I;
@@ -444,40 +509,45 @@ struct EpiVHSBlock {
     }
     const int J = I + blk;
     const int g = (col0 >> 7) & 1;
-    __half* hi = c ? re_hi : im_hi;
-    __half* lo = c ? re_lo : im_lo;
     const float s = c ? -f : f;
-    const size_t base = (size_t)w * M * ld;
+    uint8_t* mine = smem + wl * 512;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      const int i = 16 * I + 8 * g + a;
-      if (i < M) {
+    for (int rd = 0; rd < 8; ++rd) {
+      const int pc = rd < 4 ? 1 : 0;  // the rows feeding this plane: c = 1 real, c = 0 imaginary
+      const int lo = rd & 1, tr = (rd >> 1) & 1;
+      if (tr && I == J) continue;  // the same for every thread of the tile
+      if (threadIdx.x == 0) bulk_wait_read_all();  // the previous box has left shared memory
+      sync();
+      if (live && c == pc) {
+        if (!tr) {
+          // rows 8g + a of the box, columns 16 J .. + 15
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int j0 = 16 * J + 8 * h;
-          if (j0 < ld) {
+          for (int a = 0; a < 8; ++a) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              uint4 ph, pl;
+              pack8_f16(v + a * 16 + 8 * h, s, ph, pl);
+              *reinterpret_cast<uint4*>(mine + (8 * g + a) * 32 + 16 * h) = lo ? pl : ph;
+            }
+          }
+        } else {
+          // rows b (orbital 16 J + b), columns 8g .. 8g + 7 (orbitals 16 I + 8g ..)
+#pragma unroll
+          for (int b = 0; b < 16; ++b) {
+            float t[8];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) t[a] = v[a * 16 + b];
             uint4 ph, pl;
-            pack8_f16(v + a * 16 + 8 * h, s, ph, pl);
-            const size_t o = base + (size_t)i * ld + j0;
-            *reinterpret_cast<uint4*>(hi + o) = ph;
-            *reinterpret_cast<uint4*>(lo + o) = pl;
+            pack8_f16(t, s, ph, pl);
+            *reinterpret_cast<uint4*>(mine + b * 32 + 16 * g) = lo ? pl : ph;
           }
         }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       }
-    }
-    if (I == J) return;
-#pragma unroll
-    for (int b = 0; b < 16; ++b) {
-      const int j = 16 * J + b;
-      if (j < M) {
-        float t[8];
-#pragma unroll
-        for (int a = 0; a < 8; ++a) t[a] = v[a * 16 + b];
-        uint4 ph, pl;
-        pack8_f16(t, s, ph, pl);
-        const size_t o = base + (size_t)j * ld + 16 * I + 8 * g;
-        *reinterpret_cast<uint4*>(hi + o) = ph;
-        *reinterpret_cast<uint4*>(lo + o) = pl;
+      sync();
+      if (threadIdx.x == 0) {
+        tma_store_3d(&maps->out[(pc ? 0 : 2) + lo], tr ? 16 * I : 16 * J, tr ? 16 * J : 16 * I, w0, smem);
+        bulk_commit();
       }
     }
   }
@@ -810,10 +880,12 @@ static cudaError_t coulomb3(const void* r_hi, const void* r_lo, double rscale, c
   GemmMaps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = make_map_f16(&maps.a_hi[0], r_hi, X, K, K, kBM)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.a_lo[0], r_lo, X, K, K, kBM)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.b_hi, gp.hi, 2LL * W, K, K, BN)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.b_lo, gp.lo, 2LL * W, K, K, BN)) != cudaSuccess) return e;
+  if ((e = map_f16_pair(&maps.a_hi[0], &maps.a_lo[0], r_hi, r_lo, X, K, K, kBM, false, &maps.a_planes)) !=
+      cudaSuccess)
+    return e;
+  if ((e = map_f16_pair(&maps.b_hi, &maps.b_lo, gp.hi, gp.lo, 2LL * W, K, K, BN, false, &maps.b_planes)) !=
+      cudaSuccess)
+    return e;
   dim3 grid((2 * W + BN - 1) / BN, (X + kBM - 1) / kBM, 1);
   // row tiles fastest: the Cholesky operand (X rows) stays in L2 while the Green's function streams
   const EpiVbiasF<BN> epi{xv, X, W, scale / rscale, gp.scale, accumulate};
@@ -830,10 +902,12 @@ static cudaError_t exchange3_np(const void* r_hi, const void* r_lo, double rscal
   GemmMaps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = make_map_f16(&maps.a_hi[0], r_hi, (long long)X * NP, M, Mp, kBM)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.a_lo[0], r_lo, (long long)X * NP, M, Mp, kBM)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.b_hi, gp.hi, (long long)W * 2 * NP, M, Mp, BN)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.b_lo, gp.lo, (long long)W * 2 * NP, M, Mp, BN)) != cudaSuccess) return e;
+  if ((e = map_f16_pair(&maps.a_hi[0], &maps.a_lo[0], r_hi, r_lo, (long long)X * NP, M, Mp, kBM, false,
+                        &maps.a_planes)) != cudaSuccess)
+    return e;
+  if ((e = map_f16_pair(&maps.b_hi, &maps.b_lo, gp.hi, gp.lo, (long long)W * 2 * NP, M, Mp, BN, false,
+                        &maps.b_planes)) != cudaSuccess)
+    return e;
   dim3 grid((W * 2 * NP + BN - 1) / BN, (X * NP + kBM - 1) / kBM, 1);
   // row tiles fastest, in groups of 148 (~15 MB of the padded Cholesky operand at M = 200):
   // one wave of CTAs multiplies a group against one Green's-function tile, the group stays in
@@ -900,14 +974,18 @@ cudaError_t mixed_vhs_blocks(const void* cb_hi, const void* cb_lo, int X, int M,
   GemmMaps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = make_map_f16(&maps.a_hi[0], xs_hi, 2LL * W, X, ldx, kBM, true)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.a_lo[0], xs_lo, 2LL * W, X, ldx, kBM, true)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.b_hi, cb_hi, 256LL * nblk, X, ldx, BN, true)) != cudaSuccess) return e;
-  if ((e = make_map_f16(&maps.b_lo, cb_lo, 256LL * nblk, X, ldx, BN, true)) != cudaSuccess) return e;
+  if ((e = map_f16_pair(&maps.a_hi[0], &maps.a_lo[0], xs_hi, xs_lo, 2LL * W, X, ldx, kBM, true, &maps.a_planes)) !=
+      cudaSuccess)
+    return e;
+  if ((e = map_f16_pair(&maps.b_hi, &maps.b_lo, cb_hi, cb_lo, 256LL * nblk, X, ldx, BN, true, &maps.b_planes)) !=
+      cudaSuccess)
+    return e;
   dim3 grid(nblk, (2 * W + kBM - 1) / kBM, 1);
   using H = __half*;
-  const EpiVHSBlock epi{H(re_hi), H(re_lo), H(im_hi), H(im_lo), M, f16_ld(M), W, (M + 15) / 16,
-                        (float)(sqrt_dt / (cb_scale * kFieldScaleF16) * v_scale)};
+  void* planes[4] = {re_hi, re_lo, im_hi, im_lo};
+  for (int p = 0; p < 4; ++p)
+    if ((e = make_map_f16_store(&maps.out[p], planes[p], W, M, f16_ld(M), 16, 16, 64)) != cudaSuccess) return e;
+  const EpiVHSBlock epi{M, W, (M + 15) / 16, (float)(sqrt_dt / (cb_scale * kFieldScaleF16) * v_scale)};
   // 64-byte K rows: four 48 KB stages instead of two of 96 KB, so that three are in flight
   return launch_umma<BN, 1, 3, 4, EpiVHSBlock, KIND_F16_K32>(maps, X, 0, 0, grid, epi, status, st, true,
                                                             persistent != 0);

@@ -44,6 +44,11 @@ struct GemmMaps {
   CUtensorMap a_lo[2];
   CUtensorMap b_hi;
   CUtensorMap b_lo;
+  CUtensorMap out[4];  // output maps of epilogues that store through TMA (EpiUsesMaps)
+  // 1: a_hi / b_hi are 3-D maps whose second plane is the remainder (lo at a fixed offset from
+  // hi in one allocation), so one copy of depth 2 brings both tiles (a_lo / b_lo unused): every
+  // copy a thread issues costs it about as much time whatever its size
+  int a_planes, b_planes;
 };
 
 constexpr int kBM = 128;
@@ -127,6 +132,17 @@ struct EpiSmem {
 template <class Epi>
 struct EpiSmem<Epi, decltype((void)Epi::kSmemBytes)> {
   static constexpr int value = Epi::kSmemBytes;
+};
+
+// Epilogues with kUsesMaps = true take the kernel's GemmMaps as a sixth argument (their TMA
+// stores name maps.out) and have thread 0 wait for its bulk stores before the CTA exits.
+template <class Epi, class = void>
+struct EpiUsesMaps {
+  static constexpr bool value = false;
+};
+template <class Epi>
+struct EpiUsesMaps<Epi, decltype((void)Epi::kUsesMaps)> {
+  static constexpr bool value = Epi::kUsesMaps;
 };
 
 template <int BN, int NA, int NSPLIT, int STAGES, int EPI_SMEM = 0, int KIND = KIND_TF32>
@@ -218,11 +234,19 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
           const int k = kb * KB;
 #pragma unroll
           for (int a = 0; a < NA; ++a) {
-            tma_load_2d(st + (a * (S::NAT / NA)) * S::A_TILE, &maps.a_hi[a], k, arow, &full[s]);
-            if (NSPLIT == 3) tma_load_2d(st + (a * 2 + 1) * S::A_TILE, &maps.a_lo[a], k, arow, &full[s]);
+            if (NSPLIT == 3 && maps.a_planes) {
+              tma_load_3d(st + (a * 2) * S::A_TILE, &maps.a_hi[a], k, arow, 0, &full[s]);
+            } else {
+              tma_load_2d(st + (a * (S::NAT / NA)) * S::A_TILE, &maps.a_hi[a], k, arow, &full[s]);
+              if (NSPLIT == 3) tma_load_2d(st + (a * 2 + 1) * S::A_TILE, &maps.a_lo[a], k, arow, &full[s]);
+            }
           }
-          tma_load_2d(st + S::NAT * S::A_TILE, &maps.b_hi, k, brow, &full[s]);
-          if (NSPLIT == 3) tma_load_2d(st + S::NAT * S::A_TILE + S::B_TILE, &maps.b_lo, k, brow, &full[s]);
+          if (NSPLIT == 3 && maps.b_planes) {
+            tma_load_3d(st + S::NAT * S::A_TILE, &maps.b_hi, k, brow, 0, &full[s]);
+          } else {
+            tma_load_2d(st + S::NAT * S::A_TILE, &maps.b_hi, k, brow, &full[s]);
+            if (NSPLIT == 3) tma_load_2d(st + S::NAT * S::A_TILE + S::B_TILE, &maps.b_lo, k, brow, &full[s]);
+          }
         }
       }
     }
@@ -318,8 +342,14 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
       // every epilogue thread takes this vote once per tile, so all of them leave together;
       // a column group hands its columns to the epilogue as a tile starting at its own offset
       if (!epi_all(ok && !*abort_flag, R::kEpiThreads)) break;
-      epi(z, mt * kBM + quarter * 32 + lane, nt * BN + group * (R::kGroupCols / NA), v, epi_smem);
+      if constexpr (EpiUsesMaps<Epi>::value)
+        epi(z, mt * kBM + quarter * 32 + lane, nt * BN + group * (R::kGroupCols / NA), v, epi_smem, &maps);
+      else
+        epi(z, mt * kBM + quarter * 32 + lane, nt * BN + group * (R::kGroupCols / NA), v, epi_smem);
     }
+  }
+  if constexpr (EpiUsesMaps<Epi>::value) {
+    if (threadIdx.x == 0) bulk_wait_all();
   }
   tc_fence_before();
   __syncthreads();

@@ -91,8 +91,9 @@ def _mixed_energy_operands(trial, hamiltonian):
             out.append(out[0])
             continue
         NP = 8 if n <= 8 else 16 if n <= 16 else 32
-        hi = torch.empty(X * NP * Mp, dtype=torch.float16, device=trial.device)
-        lo = torch.empty_like(hi)
+        # head and remainder in one allocation: the products load both tiles with one copy
+        hilo = torch.empty(2, X * NP * Mp, dtype=torch.float16, device=trial.device)
+        hi, lo = hilo[0], hilo[1]
         scale = 1.0
         if n > 0:
             rmax = float(r.abs().max().item()) or 1.0

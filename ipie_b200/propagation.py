@@ -119,8 +119,9 @@ class Workspace:
         f32, f16, dev = torch.float32, torch.float16, self.dev
         self.gwork = torch.empty(2 * W * 2 * 32 * M, dtype=f32, device=dev)
         Xp = (X + 7) // 8 * 8  # binary16 rows padded to 16 bytes
-        self.xs_hi = torch.empty(W, 2, Xp, dtype=f16, device=dev)
-        self.xs_lo = torch.empty(W, 2, Xp, dtype=f16, device=dev)
+        # head and remainder in one allocation: the VHS product loads both tiles with one copy
+        self.xs_hilo = torch.empty(2, W, 2, Xp, dtype=f16, device=dev)
+        self.xs_hi, self.xs_lo = self.xs_hilo[0], self.xs_hilo[1]
         if chain16:
             Mp = (M + 7) // 8 * 8
             self.v_planar = [torch.empty(W, M, Mp, dtype=f16, device=dev) for _ in range(4)]  # re_hi, re_lo, im_hi, im_lo
@@ -268,8 +269,8 @@ class PhaselessGeneric:
         rows = [pidx[16 * I + a[:, None], 16 * J + a[None, :]].ravel() for I in range(nb) for J in range(I, nb)]
         rowmap = torch.from_numpy(np.ascontiguousarray(np.concatenate(rows))).to(self.device)
         R = rowmap.numel()
-        hi = torch.empty(R, Xp, dtype=torch.float16, device=self.device)
-        lo = torch.empty(R, Xp, dtype=torch.float16, device=self.device)
+        hilo = torch.empty(2, R, Xp, dtype=torch.float16, device=self.device)  # one allocation (see add_mixed)
+        hi, lo = hilo[0], hilo[1]
         call("ipie_b200_vhs_block_pack", ptr(hamiltonian.chol_packed), ptr(rowmap), M, hamiltonian.nchol,
              self.cp_scale, ptr(hi), ptr(lo), stream())
         torch.cuda.current_stream().synchronize()
