@@ -1,5 +1,6 @@
 // Green's function and overlap for spin blocks of N <= 32 electrons, one
-// 128-thread CTA per walker (~47 KB of shared memory, three walkers per SM):
+// 128-thread CTA per walker (34 KB of shared memory, four walkers per SM: two Ghalf columns per
+// lane and pass keep a thread within 128 registers; measured 12% faster than three):
 //
 //   O = phi^T psi*  (N x N): phi and psi* stream through shared memory in
 //       16-row chunks; each thread accumulates a 2 x 4 block of O in registers;
@@ -10,7 +11,7 @@
 //       (one pivot per lane of warp 0, reduced with shuffles);
 //   Ghalf[i, m] = sum_r X[i, r] phi[m, perm(r)] (= (O^-1 phi^T)[i, m]): a
 //       register-tiled product -- warp w takes rows 8w..8w+7, lane l the
-//       columns l + 32q (q < 3, so 96 columns per pass), phi staged in shared
+//       columns l + 32q (q < 2, so 64 columns per pass), phi staged in shared
 //       memory 4 permuted columns at a time, transposed -- instead of one
 //       latency-bound pair of triangular solves per column.
 // ovlp_w = prod_s phase_s * exp(sum_s log|det O_s| - log_shift_w).
@@ -26,7 +27,7 @@ constexpr int kThreads = 128;
 constexpr int kChunk = 16;  // rows of phi / psi* per shared-memory chunk of the O product
 constexpr int kNP = 33;     // row stride of O in shared memory
 constexpr int kRC = 4;      // permuted columns of phi per staged chunk of the Ghalf product
-constexpr int kMQ = 3;      // columns of Ghalf per lane and pass (96 per pass)
+constexpr int kMQ = 2;      // columns of Ghalf per lane and pass (64 per pass)
 constexpr int kMS = 32 * kMQ + 1;  // row stride of the staged phi^T chunk (odd in 16-byte units)
 static_assert(kRC * kMS <= 2 * kChunk * 32, "the staged phi^T chunk reuses the O product's staging buffers");
 
@@ -230,7 +231,7 @@ __device__ void ghalf_block(const double2* __restrict__ phi, int M, int N, doubl
 }
 
 template <bool WITH_GHALF>
-__global__ void __launch_bounds__(kThreads, 3) gf_lu32_kernel(const double2* __restrict__ phia,
+__global__ void __launch_bounds__(kThreads, 4) gf_lu32_kernel(const double2* __restrict__ phia,
                                                               const double2* __restrict__ phib, int M, int na,
                                                               int nb, const double2* __restrict__ psia_c,
                                                               const double2* __restrict__ psib_c,
