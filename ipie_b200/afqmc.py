@@ -97,6 +97,12 @@ class AFQMC:
                            pop_control_freq, seed)
         if not trial_wavefunction.half_rotated:
             trial_wavefunction.half_rotate(hamiltonian)
+        if walkers is None and getattr(trial_wavefunction, "multidet", False):
+            # ipie starts them at the reference determinant, whose overlap with every excited
+            # determinant is zero: the determinant sums here need walkers that overlap all of them
+            raise NotImplementedError("with a particle-hole trial pass walkers that overlap every determinant "
+                                      "(e.g. the perturbed reference); walkers at the reference determinant "
+                                      "itself need Wick's theorem relative to it, which is not built")
         if walkers is None:
             init = np.asarray(trial_wavefunction.psi).copy()  # walkers_dispatch.py:42-58
             if getattr(trial_wavefunction, "ghf", False):
@@ -110,6 +116,9 @@ class AFQMC:
             walkers.build(trial_wavefunction)
         if graph and getattr(walkers, "ghf", False):
             raise NotImplementedError("graph capture covers UHF walkers; GHF walkers step kernel by kernel")
+        if graph and getattr(trial_wavefunction, "multidet", False):
+            raise NotImplementedError("graph capture covers single-determinant trials; a particle-hole trial "
+                                      "steps kernel by kernel")
         prop = PhaselessGeneric(timestep, rng=rng, seed=seed if seed is not None else 7, precision=precision)
         prop.build(hamiltonian, trial_wavefunction, walkers)
         # identical spin blocks (RHF trial, walkers started from it, equal one-body operators):

@@ -183,6 +183,10 @@ def local_energy_single_det_rhf_batch(system, hamiltonian, walkers, trial):
 
 def local_energy_batch(system, hamiltonian, walkers, trial):
     """Dispatch as ipie's ``local_energy_batch`` (``local_energy_batch.py:36-75``)."""
+    if getattr(trial, "multidet", False):
+        from .multidet import local_energy_multi_det_trial_wicks_batch_opt
+
+        return local_energy_multi_det_trial_wicks_batch_opt(system, hamiltonian, walkers, trial)
     if walkers.rhf:
         return local_energy_single_det_rhf_batch(system, hamiltonian, walkers, trial)
     return local_energy_single_det_uhf_batch(system, hamiltonian, walkers, trial)
@@ -226,6 +230,8 @@ class EnergyEstimator:
 
     def compute_estimator(self, system=None, walkers=None, hamiltonian=None, trial=None):
         # ipie recomputes the Green's function here; it is skipped while the cached one is current
+        if getattr(trial, "multidet", False) and self.precision == "mixed":
+            raise NotImplementedError("the particle-hole trial's energy runs in FP64 (precision='fp64')")
         if not walkers.gf_current(trial):
             trial.calc_greens_function(walkers)
         if self.precision == "mixed" and not getattr(hamiltonian, "complex_chol", False) and not getattr(walkers, "ghf", False):

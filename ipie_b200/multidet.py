@@ -61,6 +61,11 @@ class ParticleHole:
         self.half_rotated = False
         self.spin_symmetric = False
         self.ghf = False
+        self.multidet = True  # the propagator and estimators dispatch on it
+        # spin-orbital occupations: alpha orbitals i, beta orbitals nbasis + i (particle_hole.py:96-97)
+        self.spin_occs = [np.sort(np.concatenate([a, b + nbasis])) for a, b in zip(self.occa, self.occb)]
+        self.G = compute_1rdm(self.coeffs, self.spin_occs, nbasis, self.num_dets_for_props)
+        self._chol_t = None
 
     def build(self):
         """ipie builds its Wick's-theorem excitation tables here; the determinant sums need none."""
@@ -89,6 +94,63 @@ class ParticleHole:
 
     def calc_overlap(self, walkers):
         return _sweep(walkers, self, want_g=False, energy_of=None)[0]
+
+    def calc_force_bias(self, hamiltonian, walkers, mpi_handler=None, out=None):
+        """vbias[w, x] = sum_pq L_x[p, q] (Ga + Gb)[w, p, q] from the walkers' full Green's functions
+        (ipie ``propagation/force_bias.py:62-76``, ``construct_force_bias_batch_multi_det_trial``);
+        the Cholesky vectors as rows (X, M^2) held once per trial."""
+        if getattr(hamiltonian, "complex_chol", False):
+            raise NotImplementedError("the particle-hole trial takes real Cholesky Hamiltonians")
+        M, X, W = self.nbasis, hamiltonian.nchol, walkers.nwalkers
+        if self._chol_t is None:
+            L = np.asarray(hamiltonian.chol).reshape(M * M, X)
+            self._chol_t = torch.from_numpy(np.ascontiguousarray(L.T)).to(self.device)
+        if out is None:
+            out = torch.empty(W, X, dtype=C128, device=walkers.device)
+        ga, gb = walkers.Ga.contiguous(), walkers.Gb.contiguous()
+        call("ipie_b200_construct_force_bias_batch_single_det", ptr(self._chol_t), ptr(self._chol_t), ptr(ga),
+             ptr(gb), W, X, M, M, M, ptr(out), stream())
+        return out
+
+
+def _excitation_parity(from_orb, to_orb, di, dj):
+    """True when aligning determinant dj to di (one orbital from_orb of dj replaced by to_orb of di,
+    both sorted spin-orbital lists) is an odd permutation: the positions of the moved orbitals in
+    their lists, each counted past the orbitals moved before it (ipie ``utils/from_dice.py:23-36``,
+    ``get_perm``)."""
+    n = 0
+    for k, o in enumerate(from_orb):
+        n += int(np.nonzero(dj == o)[0][0]) - k
+    for k, o in enumerate(to_orb):
+        n += int(np.nonzero(di == o)[0][0]) - k
+    return n % 2 == 1
+
+
+def compute_1rdm(coeffs, spin_occs, nbasis, ndets):
+    """One-body density matrices (2, M, M) of the trial from its first ``ndets`` determinants
+    (orthonormal basis-orbital determinants): the diagonal occupations weighted by |c_i|^2 and,
+    for every pair differing by one orbital of one spin, the transition terms c_j^* c_i and their
+    conjugates with the permutation sign, over sum |c_i|^2 (ipie ``particle_hole.py:458-506``,
+    ``compute_1rdm``; the mean-field shift and the one-body propagator use it)."""
+    c = np.asarray(coeffs[:ndets], dtype=np.complex128)
+    P = np.zeros((2, nbasis, nbasis), dtype=np.complex128)
+    for i in range(ndets):
+        di = spin_occs[i]
+        for o in di:
+            P[int(o) // nbasis, int(o) % nbasis, int(o) % nbasis] += np.conj(c[i]) * c[i]
+        si = set(int(o) for o in di)
+        for j in range(i + 1, ndets):
+            dj = spin_occs[j]
+            sj = set(int(o) for o in dj)
+            frm, to = sorted(sj - si), sorted(si - sj)
+            if len(frm) != 1:
+                continue
+            phase = -1.0 if _excitation_parity(frm, to, di, dj) else 1.0
+            (ii, s_i), (aa, s_a) = (frm[0] % nbasis, frm[0] // nbasis), (to[0] % nbasis, to[0] // nbasis)
+            if s_i == s_a:
+                P[s_i, aa, ii] += np.conj(c[j]) * c[i] * phase
+                P[s_i, ii, aa] += c[j] * np.conj(c[i]) * phase
+    return P / np.sum(np.conj(c) * c)
 
 
 def _workspace(walkers, trial, energy):

@@ -175,6 +175,8 @@ class PhaselessGeneric:
             self.expH1_pad = torch.from_numpy(ep).to(dev)
         self.spin_symmetric = bool(np.array_equal(self.expH1[0], self.expH1[1]))
         if self.precision == "mixed":
+            if getattr(trial, "multidet", False):
+                raise NotImplementedError("the particle-hole trial propagates in FP64 (precision='fp64')")
             self._mixed_setup(hamiltonian, trial)
         if walkers is not None:
             self._workspace(walkers, hamiltonian)
@@ -417,7 +419,9 @@ class PhaselessGeneric:
         # The step's starting Green's function and overlap: the previous step ended with those of
         # the current orbitals (reortho and pair branch keep them consistent), so they are only
         # recomputed when the orbitals were replaced.  walkers.ovlp is overwritten by update_weight.
-        if not walkers.gf_current(trial):
+        # (a particle-hole trial's full Green's functions do not travel with population control's
+        # copies, so they are recomputed every step)
+        if not walkers.gf_current(trial) or getattr(trial, "multidet", False):
             self.timer.start("greens_function")
             greens_function_into(walkers, trial, walkers.ovlp)
             self.timer.stop("greens_function")

@@ -144,6 +144,10 @@ class SingleDet:
 
 
 def greens_function_into(walkers, trial, ovlp_out):
+    if getattr(trial, "multidet", False):
+        # full Green's functions walkers.Ga/Gb of the determinant sum and its overlap
+        ovlp_out.copy_(trial.calc_greens_function(walkers))
+        return
     call(
         "ipie_b200_greens_function_single_det_batch",
         ptr(walkers.phia), ptr(walkers.phib), walkers.nwalkers, walkers.nbasis, walkers.nup, walkers.ndown,
@@ -153,6 +157,9 @@ def greens_function_into(walkers, trial, ovlp_out):
 
 
 def overlap_into(walkers, trial, ovlp_out):
+    if getattr(trial, "multidet", False):
+        ovlp_out.copy_(trial.calc_overlap(walkers))
+        return
     call(
         "ipie_b200_calc_overlap_single_det_uhf",
         ptr(walkers.phia), ptr(walkers.phib), walkers.nwalkers, walkers.nbasis, walkers.nup, walkers.ndown,
@@ -161,6 +168,9 @@ def overlap_into(walkers, trial, ovlp_out):
 
 
 def force_bias_into(hamiltonian, walkers, trial, vbias_out):
+    if getattr(trial, "multidet", False):
+        trial.calc_force_bias(hamiltonian, walkers, out=vbias_out)
+        return
     if getattr(trial, "complex_rotated", False) and not getattr(hamiltonian, "complex_chol", False):
         # complex half-rotated Cholesky of a complex GHF trial: vbias = R . Ghalf
         re, im = trial._cplx["chola"]

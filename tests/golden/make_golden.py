@@ -490,7 +490,6 @@ def multidet_fixture(name):
     ``local_energy_multi_det_trial_wicks_batch_opt``) on perturbed walkers, with ipie's naive
     per-determinant path (``ParticleHoleNaive``, ``greens_function_multi_det``,
     ``local_energy_batch.py:78`` ``local_energy_multi_det_trial_batch``) as a cross-check."""
-    import itertools
 
     from ipie.estimators.greens_function_multi_det import (
         greens_function_multi_det,
@@ -500,27 +499,12 @@ def multidet_fixture(name):
     from ipie.estimators.local_energy_wicks import local_energy_multi_det_trial_wicks_batch_opt
     from ipie.trial_wavefunction.particle_hole import ParticleHoleNaive, ParticleHoleNonChunked
 
-    sysw = synthetic.generate(14, (4, 3), 42, decay=30.0, seed=31, uhf=True, chol_scale="stable")
+    sysw, wfn, init, rng = _multidet_system()
     M, na, nb = sysw.nbasis, sysw.nup, sysw.ndown
-    rng = np.random.default_rng(32)
-    # the reference (lowest orbitals) and a random selection of excited determinants up to four
-    # holes per spin, ordered by excitation level as ipie's inputs usually are
-    oa = [tuple(range(na))] + [c for c in itertools.combinations(range(M), na) if c != tuple(range(na))]
-    ob = [tuple(range(nb))] + [c for c in itertools.combinations(range(M), nb) if c != tuple(range(nb))]
-    pick_a = [0] + list(rng.choice(np.arange(1, len(oa)), 59))
-    pick_b = [0] + list(rng.choice(np.arange(1, len(ob)), 59))
-    occa = [np.array(oa[i]) for i in pick_a]
-    occb = [np.array(ob[i]) for i in pick_b]
-    ci = rng.normal(size=60) + 1j * rng.normal(size=60)
-    ci[0] = 3.0
-    ci /= np.linalg.norm(ci)
-    order = np.argsort([-abs(c) for c in ci], kind="stable")
-    ci, occa, occb = ci[order], [occa[i] for i in order], [occb[i] for i in order]
-    wfn = (ci, occa, occb)
+    ci, occa, occb = wfn
     ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
     system = Generic((na, nb))
     W = 6
-    init = np.hstack([np.eye(M)[:, :na], np.eye(M)[:, :nb]]) + 0.3 * rng.normal(size=(M, na + nb))
     out = dict(ci=ci, occa=np.array(occa), occb=np.array(occb), init=init)
     results = {}
     for key, cls in (("opt", ParticleHoleNonChunked), ("naive", ParticleHoleNaive)):
@@ -549,6 +533,98 @@ def multidet_fixture(name):
     out["psi_checksum"] = checksum(sysw.psi)
     np.savez_compressed(os.path.join(HERE, name), **out)
     print("wrote", name, "energies", out["energy"][:, 0])
+
+
+def _multidet_system():
+    """The synthetic system, particle-hole trial (reference + 59 random excited determinants) and
+    starting walker of the multi-determinant fixtures."""
+    import itertools
+
+    sysw = synthetic.generate(14, (4, 3), 42, decay=30.0, seed=31, uhf=True, chol_scale="stable")
+    M, na, nb = sysw.nbasis, sysw.nup, sysw.ndown
+    rng = np.random.default_rng(32)
+    # the reference (lowest orbitals) and a random selection of excited determinants up to four
+    # holes per spin, ordered by excitation level as ipie's inputs usually are
+    oa = [tuple(range(na))] + [c for c in itertools.combinations(range(M), na) if c != tuple(range(na))]
+    ob = [tuple(range(nb))] + [c for c in itertools.combinations(range(M), nb) if c != tuple(range(nb))]
+    pick_a = [0] + list(rng.choice(np.arange(1, len(oa)), 59))
+    pick_b = [0] + list(rng.choice(np.arange(1, len(ob)), 59))
+    occa = [np.array(oa[i]) for i in pick_a]
+    occb = [np.array(ob[i]) for i in pick_b]
+    ci = rng.normal(size=60) + 1j * rng.normal(size=60)
+    ci[0] = 3.0
+    ci /= np.linalg.norm(ci)
+    order = np.argsort([-abs(c) for c in ci], kind="stable")
+    ci, occa, occb = ci[order], [occa[i] for i in order], [occb[i] for i in order]
+    init = np.hstack([np.eye(M)[:, :na], np.eye(M)[:, :nb]]) + 0.3 * rng.normal(size=(M, na + nb))
+    return sysw, (ci, occa, occb), init, rng
+
+
+def multidet_run_fixture(name, nwalkers=10, num_blocks=2, steps=10, seed=5):
+    """ipie's own ``AFQMC.build(...).run()`` with the particle-hole trial (Wick's-theorem Green's
+    function, overlap and force bias, reortho and pair-branch population control every 5 steps) from
+    given walkers (the perturbed reference): block estimates and final walkers."""
+    from ipie.trial_wavefunction.particle_hole import ParticleHoleNonChunked
+
+    sysw, wfn, init, _ = _multidet_system()
+    M, na, nb = sysw.nbasis, sysw.nup, sysw.ndown
+    ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
+    trial = ParticleHoleNonChunked(wfn, (na, nb), M)
+    trial.build()
+    trial.half_rotate(ham)
+    # walkers started from the perturbed reference (every determinant of the trial overlaps them)
+    walkers = UHFWalkersTrial(trial, init.copy(), na, nb, M, nwalkers, MPIHandler())
+    walkers.build(trial)
+    afqmc = AFQMC.build((na, nb), ham, trial, walkers=walkers, num_walkers=nwalkers, seed=seed,
+                        num_steps_per_block=steps, num_blocks=num_blocks, timestep=0.005, stabilize_freq=5,
+                        pop_control_freq=5, verbose=False)
+    h5py.FILES.clear()
+    afqmc.run(estimator_filename="golden_run.h5", verbose=False)
+    data = h5py.FILES["golden_run.h5"]["block_size_1/data/000000000"][: num_blocks + 1]
+    w = afqmc.walkers
+    out = dict(blocks=data, weight=np.array(w.weight), unscaled_weight=np.array(w.unscaled_weight),
+               ovlp=np.array(w.ovlp), hybrid_energy=np.array(w.hybrid_energy), phia=np.array(w.phia),
+               phib=np.array(w.phib), chol_checksum=checksum(sysw.chol))
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name, "ETotal per block", data[:, 5].real)
+
+
+def multidet_prop_fixture(name, nsteps=4):
+    """Phaseless propagation with ipie's particle-hole trial (``PhaselessGeneric.propagate_walkers``,
+    ``propagation/phaseless_base.py:312-338``, with the trial's Wick's-theorem Green's function,
+    overlap and full-G force bias, ``propagation/force_bias.py:62-76``), the trial's 1-RDM
+    (``particle_hole.py:458-506``) and mean-field shift, numpy's global draws seeded per step; then
+    the local energy of the final walkers."""
+    from ipie.estimators.greens_function_multi_det import greens_function_multi_det_wicks_opt
+    from ipie.estimators.local_energy_wicks import local_energy_multi_det_trial_wicks_batch_opt
+    from ipie.trial_wavefunction.particle_hole import ParticleHoleNonChunked
+
+    sysw, wfn, init, _ = _multidet_system()
+    M, na, nb = sysw.nbasis, sysw.nup, sysw.ndown
+    ham = HamGeneric(h1e=sysw.h1e.copy(), chol=sysw.chol.copy(), ecore=sysw.ecore)
+    system = Generic((na, nb))
+    W = 8
+    trial = ParticleHoleNonChunked(wfn, (na, nb), M)
+    trial.build()
+    trial.half_rotate(ham)
+    walkers = UHFWalkersTrial(trial, init.copy(), na, nb, M, W, MPIHandler())
+    walkers.build(trial)
+    prop = PhaselessGeneric(0.005)
+    prop.build(ham, trial, walkers, MPIHandler())
+    out = dict(G=np.array(trial.G), mf_shift=np.array(prop.mf_shift), ovlp_init=np.array(walkers.ovlp))
+    for step in range(nsteps):
+        np.random.seed(400 + step)
+        prop.propagate_walkers(walkers, ham, trial, -3.0 if step else 0.0)
+        out[f"weight{step}"] = np.array(walkers.weight)
+        out[f"ovlp{step}"] = np.array(walkers.ovlp)
+        out[f"phia{step}"] = np.array(walkers.phia)
+        out[f"phib{step}"] = np.array(walkers.phib)
+    ovlp = greens_function_multi_det_wicks_opt(walkers, trial)
+    walkers.ovlp = ovlp
+    out["energy"] = np.array(local_energy_multi_det_trial_wicks_batch_opt(system, ham, walkers, trial))
+    out["chol_checksum"] = checksum(sysw.chol)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name, "weights", out[f"weight{nsteps - 1}"], "energies", out["energy"][:, 0])
 
 
 def analysis_fixture(name):
@@ -593,6 +669,10 @@ def config_fixtures():
 
 
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "multidet_prop":
+        multidet_prop_fixture("multidet_prop_m14.npz")
+        multidet_run_fixture("multidet_run_m14.npz")
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[2] == "multidet":
         multidet_fixture("multidet_m14.npz")
         sys.exit(0)
