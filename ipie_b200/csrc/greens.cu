@@ -1,9 +1,11 @@
 // Green's function and overlap for spin blocks of N <= 32 electrons, one
-// 128-thread CTA per walker (34 KB of shared memory, four walkers per SM: two Ghalf columns per
+// 128-thread CTA per walker (42 KB of shared memory, four walkers per SM: two Ghalf columns per
 // lane and pass keep a thread within 128 registers; measured 12% faster than three):
 //
 //   O = phi^T psi*  (N x N): phi and psi* stream through shared memory in
-//       16-row chunks; each thread accumulates a 2 x 4 block of O in registers;
+//       8-row chunks, a three-deep ring of cp.async copies issued two chunks
+//       ahead (one barrier per chunk); each thread accumulates a 2 x 4 block of
+//       O in registers;
 //   X = (P O)^-1 by Gauss-Jordan elimination in place in shared memory with
 //       partial pivoting on |.| (warp 0 picks the pivot, all threads update) --
 //       the pivots are those of the LU factorisation, so
@@ -12,8 +14,9 @@
 //   Ghalf[i, m] = sum_r X[i, r] phi[m, perm(r)] (= (O^-1 phi^T)[i, m]): a
 //       register-tiled product -- warp w takes rows 8w..8w+7, lane l the
 //       columns l + 32q (q < 2, so 64 columns per pass), phi staged in shared
-//       memory 4 permuted columns at a time, transposed -- instead of one
-//       latency-bound pair of triangular solves per column.
+//       memory 4 permuted columns at a time, transposed, through a four-deep
+//       cp.async ring issued three steps ahead -- instead of one latency-bound
+//       pair of triangular solves per column.
 // ovlp_w = prod_s phase_s * exp(sum_s log|det O_s| - log_shift_w).
 // Same contract as gf_overlap_kernel (walkers.cu), which keeps N > 32.
 #include "common.cuh"
@@ -24,12 +27,17 @@ namespace ipie_b200 {
 namespace {
 
 constexpr int kThreads = 128;
-constexpr int kChunk = 16;  // rows of phi / psi* per shared-memory chunk of the O product
+constexpr int kChunk = 8;   // rows of phi / psi* per shared-memory chunk of the O product
+constexpr int kORing = 3;   // chunks in the O product's copy ring
 constexpr int kNP = 33;     // row stride of O in shared memory
-constexpr int kRC = 4;      // permuted columns of phi per staged chunk of the Ghalf product
+constexpr int kRC = 4;      // permuted columns of phi per staged step of the Ghalf product
 constexpr int kMQ = 2;      // columns of Ghalf per lane and pass (64 per pass)
-constexpr int kMS = 32 * kMQ + 1;  // row stride of the staged phi^T chunk (odd in 16-byte units)
-static_assert(kRC * kMS <= 2 * kChunk * 32, "the staged phi^T chunk reuses the O product's staging buffers");
+constexpr int kMS = 32 * kMQ + 1;  // row stride of the staged phi^T step (odd in 16-byte units)
+constexpr int kGRing = 4;   // steps in the Ghalf product's copy ring
+constexpr int kOStage = 2 * kChunk * 32;  // double2 per O chunk (phi and psi*)
+constexpr int kGStage = kRC * kMS;        // double2 per Ghalf step
+constexpr int kStage = kORing * kOStage > kGRing * kGStage ? kORing * kOStage : kGRing * kGStage;
+static_assert(kChunk * 32 % kThreads == 0 && kRC * 32 * kMQ % kThreads == 0, "whole copies per thread");
 
 struct SpinDet32 {
   double logabs;
@@ -39,8 +47,8 @@ struct SpinDet32 {
 // O = phi^T psi* for one spin block into sO; then its inverse (of the row-permuted O) in place,
 // the row order in sPerm and log|det|, phase from the pivots.
 __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2* __restrict__ psic, int M, int N,
-                                  double2 (*sO)[kNP], double2 (*sPhi)[32], double2 (*sPsi)[32], int* sPerm,
-                                  double2* sPiv, double2* red, unsigned* status) {
+                                  double2 (*sO)[kNP], double2* sStage, int* sPerm, double2* sPiv, double2* red,
+                                  unsigned* status) {
   const int tid = threadIdx.x;
   // ---- O = phi^T psi*: thread (ti, tj) owns rows {ti, ti+16} x columns {tj + 8q}
   const int ti = tid >> 3, tj = tid & 7;
@@ -49,17 +57,31 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[a][q] = make_double2(0.0, 0.0);
-  for (int m0 = 0; m0 < M; m0 += kChunk) {
-    const int mc = min(kChunk, M - m0);
-    __syncthreads();
-    for (int e = tid; e < kChunk * 32; e += kThreads) {
-      const int r = e >> 5, c = e & 31;
-      const bool in = r < mc && c < N;
-      sPhi[r][c] = in ? phi[(size_t)(m0 + r) * N + c] : make_double2(0.0, 0.0);
-      sPsi[r][c] = in ? psic[(size_t)(m0 + r) * N + c] : make_double2(0.0, 0.0);
+  const int nch = (M + kChunk - 1) / kChunk;
+  // chunk ch (rows 8 ch ..) into ring slot ch % kORing: phi rows then psi* rows, zeros past M / N
+  auto issue = [&](int ch) {
+    if (ch < nch) {
+      double2* st = sStage + (ch % kORing) * kOStage;
+#pragma unroll
+      for (int u = 0; u < kChunk * 32 / kThreads; ++u) {
+        const int e = tid + u * kThreads, r = e >> 5, c = e & 31, m = ch * kChunk + r;
+        const bool in = m < M && c < N;
+        const size_t off = in ? (size_t)m * N + c : 0;
+        cp_async16(st + e, phi + off, in ? 16 : 0);
+        cp_async16(st + kChunk * 32 + e, psic + off, in ? 16 : 0);
+      }
     }
-    __syncthreads();
-#pragma unroll 4
+    cp_async_commit();  // (an empty group past the end keeps the group count per chunk)
+  };
+  issue(0);
+  issue(1);
+  for (int ch = 0; ch < nch; ++ch) {
+    cp_async_wait<1>();  // this thread's copies of chunk ch have landed
+    __syncthreads();     // everyone's have, and everyone is done with chunk ch - 1
+    issue(ch + 2);       // into the slot of chunk ch - 1
+    const double2(*sPhi)[32] = reinterpret_cast<const double2(*)[32]>(sStage + (ch % kORing) * kOStage);
+    const double2(*sPsi)[32] = reinterpret_cast<const double2(*)[32]>(sStage + (ch % kORing) * kOStage + kChunk * 32);
+#pragma unroll
     for (int r = 0; r < kChunk; ++r) {
       const double2 a0 = sPhi[r][ti], a1 = sPhi[r][ti + 16];
 #pragma unroll
@@ -72,6 +94,7 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
       }
     }
   }
+  cp_async_wait<0>();
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -178,10 +201,38 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
 }
 
 // Ghalf (N, M) of one spin block from X = (P O)^-1 in sO: Ghalf[i, m] = sum_r X[i, r] phi[m, perm(r)].
+// The steps (pass of 64 columns m, group of kRC permuted columns) run in one sequence through
+// the copy ring, passes included.
 __device__ void ghalf_block(const double2* __restrict__ phi, int M, int N, double2 (*sO)[kNP], const int* sPerm,
-                            double2* sPT, double2* __restrict__ ghalf, double2* __restrict__ ghalf2) {
+                            double2* sStage, double2* __restrict__ ghalf, double2* __restrict__ ghalf2) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int i0 = warp * 8;  // this warp's rows
+  // the next step to copy: columns from im0, permuted columns from ir0 (im0 >= M: none left)
+  int im0 = 0, ir0 = 0, slot = 0;
+  // phi[im0 + ml][perm(ir0 + rr)] as sPT[rr][ml] (consecutive threads take consecutive rr)
+  auto issue = [&]() {
+    if (im0 < M) {
+      double2* sPT = sStage + slot * kGStage;
+#pragma unroll
+      for (int u = 0; u < kRC * 32 * kMQ / kThreads; ++u) {
+        const int e = tid + u * kThreads, rr = e % kRC, ml = e / kRC;
+        const int r = ir0 + rr, m = im0 + ml;
+        const bool in = r < N && m < M;
+        cp_async16(sPT + rr * kMS + ml, phi + (in ? (size_t)m * N + sPerm[r] : 0), in ? 16 : 0);
+      }
+      ir0 += kRC;
+      if (ir0 >= N) {
+        ir0 = 0;
+        im0 += 32 * kMQ;
+      }
+    }
+    cp_async_commit();
+    slot = slot == kGRing - 1 ? 0 : slot + 1;
+  };
+  issue();
+  issue();
+  issue();
+  int cur = 0;  // ring slot of the step being multiplied
   for (int m0 = 0; m0 < M; m0 += 32 * kMQ) {
     double2 acc[8][kMQ];
 #pragma unroll
@@ -189,14 +240,11 @@ __device__ void ghalf_block(const double2* __restrict__ phi, int M, int N, doubl
 #pragma unroll
       for (int q = 0; q < kMQ; ++q) acc[a][q] = make_double2(0.0, 0.0);
     for (int r0 = 0; r0 < N; r0 += kRC) {
+      cp_async_wait<2>();
       __syncthreads();
-      // stage phi[m0 + ml][perm(r0 + rr)] as sPT[rr][ml]: consecutive threads take consecutive rr
-      for (int e = tid; e < kRC * 32 * kMQ; e += kThreads) {
-        const int rr = e % kRC, ml = e / kRC;
-        const int r = r0 + rr, m = m0 + ml;
-        sPT[rr * kMS + ml] = (r < N && m < M) ? phi[(size_t)m * N + sPerm[r]] : make_double2(0.0, 0.0);
-      }
-      __syncthreads();
+      issue();  // into the slot of the previous step
+      const double2* sPT = sStage + cur * kGStage;
+      cur = cur == kGRing - 1 ? 0 : cur + 1;
 #pragma unroll
       for (int rr = 0; rr < kRC; ++rr) {
         double2 x[8];
@@ -228,6 +276,7 @@ __device__ void ghalf_block(const double2* __restrict__ phi, int M, int N, doubl
       }
     }
   }
+  cp_async_wait<0>();
 }
 
 template <bool WITH_GHALF>
@@ -241,7 +290,7 @@ __global__ void __launch_bounds__(kThreads, 4) gf_lu32_kernel(const double2* __r
                                                               double2* __restrict__ ovlp, double2* __restrict__ logdet,
                                                               unsigned* status) {
   __shared__ double2 sO[32][kNP];
-  __shared__ double2 sStage[2 * kChunk * 32];  // phi / psi* chunks of O, then the staged phi^T chunks
+  __shared__ __align__(16) double2 sStage[kStage];  // the O product's chunk ring, then the Ghalf step ring
   __shared__ double2 sPiv[32];
   __shared__ double2 red[8];
   __shared__ int sPerm[32];
@@ -260,9 +309,7 @@ __global__ void __launch_bounds__(kThreads, 4) gf_lu32_kernel(const double2* __r
       continue;
     }
     const double2* phi = (s == 0 ? phia : phib) + (size_t)w * M * N;
-    auto sPhi = reinterpret_cast<double2(*)[32]>(sStage);
-    auto sPsi = reinterpret_cast<double2(*)[32]>(sStage + kChunk * 32);
-    const SpinDet32 d = invert_block(phi, s == 0 ? psia_c : psib_c, M, N, sO, sPhi, sPsi, sPerm, sPiv, red, status);
+    const SpinDet32 d = invert_block(phi, s == 0 ? psia_c : psib_c, M, N, sO, sStage, sPerm, sPiv, red, status);
     logsum += d.logabs;
     phase = cmul(phase, d.phase);
     if (threadIdx.x == 0) {

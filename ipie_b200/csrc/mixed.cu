@@ -468,28 +468,31 @@ struct EpiVHSF16 {
 // 32-byte sectors are written by one or two neighbouring runs.  V = i sqrt(dt) S: the re part of
 // S (c = 0) gives the imaginary planes, the im part (c = 1) the real planes.  Rows i >= M are
 // skipped; columns in [M, ld) receive the zero products of the zero Cholesky rows.
-__device__ __forceinline__ void pack8_f16(const float* x, float s, uint4& hi, uint4& lo) {
-  uint32_t h[4], l[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const float y0 = x[2 * k] * s, y1 = x[2 * k + 1] * s;
-    const __half a0 = __float2half_rn(y0), a1 = __float2half_rn(y1);
-    const __half b0 = __float2half_rn(y0 - __half2float(a0)), b1 = __float2half_rn(y1 - __half2float(a1));
-    h[k] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
-    l[k] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
-  }
-  hi = make_uint4(h[0], h[1], h[2], h[3]);
-  lo = make_uint4(l[0], l[1], l[2], l[3]);
+// binary16 head and remainder of the pair (y0, y1), packed two per word (y0 in the low half)
+__device__ __forceinline__ uint32_t split2_f16(float y0, float y1, uint32_t& lo) {
+  const __half2 h = __floats2half2_rn(y0, y1);
+  const float2 hf = __half22float2(h);
+  const __half2 l = __floats2half2_rn(y0 - hf.x, y1 - hf.y);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+  return *reinterpret_cast<const uint32_t*>(&h);
 }
 
 // The epilogue goes through shared memory and TMA tensor stores: one 32 KB staging box of 64
 // walkers x 16 rows x 16 halves (the {16, 16, 64} box of the plane maps maps->out: re_hi, re_lo,
-// im_hi, im_lo), filled and stored eight times per tile -- real then imaginary plane, head then
-// remainder, the block (I, J) then its transpose (J, I) -- by the threads of the rows (c) that
-// feed that plane.  A thread's scattered 16-byte global stores (one 32-byte sector split between
-// two of them, 16 walkers per warp instruction) took ~30k cycles per tile and stalled the next
-// tile's products; the staged tensor stores leave the copy to the TMA engine.  Rows i >= M and
-// columns j >= ld of a box are clipped by the store.
+// im_hi, im_lo), filled and stored eight times per tile -- real then imaginary plane, the
+// transposed block (J, I) then the block (I, J), head then remainder -- by the threads of the
+// rows (c) that feed that plane.  A thread's scattered 16-byte global stores (one 32-byte sector
+// split between two of them, 16 walkers per warp instruction) took ~30k cycles per tile and
+// stalled the next tile's products; the staged tensor stores leave the copy to the TMA engine.
+// Rows i >= M and columns j >= ld of a box are clipped by the store.
+//
+// Bank spread: a walker's part of the box is 512 bytes, so the 16 walkers of a warp instruction
+// would all write the same four banks if each wrote the same 16-byte chunk of its part.  Lane k
+// (k = (lane / 2) mod 8) writes its chunks in an order rotated by k instead: its block chunks
+// (8 rows x two 16-byte halves) rotated by k within each half of eight, which spreads the 16
+// lanes over all 32 banks (two wavefronts per instruction), and the transposed rows b rotated by
+// k mod 4 within each group of four (four wavefronts: a transposed row has one 16-byte half per
+// column group).  The values are split into head and remainder once per tile.
 struct EpiVHSBlock {
   int M, W, nb;  // nb: 16-orbital blocks per side
   float f;       // sqrt(dt) v_scale / (operand scales)
@@ -497,6 +500,50 @@ struct EpiVHSBlock {
   static constexpr bool kUsesMaps = true;
   static constexpr int kThreads = 256;  // the epilogue threads of the 128 x 256 tile (barrier 3)
   __device__ __forceinline__ static void sync() { asm volatile("bar.sync 3, %0;\n" ::"r"(kThreads) : "memory"); }
+  // chunk q of 16 (row q / 2 of the block half, 16-byte half q % 2) moved to position q's
+  // rotation: after the call, chunk i holds the original chunk (i & 8) | ((i + k) & 7)
+  __device__ __forceinline__ static void rotate(uint32_t (&x)[64], int k) {
+#pragma unroll
+    for (int st = 1; st < 8; st <<= 1) {
+      const bool r = (k & st) != 0;
+      uint32_t t[64];
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) t[4 * q + u] = r ? x[4 * ((q & 8) | ((q + st) & 7)) + u] : x[4 * q + u];
+#pragma unroll
+      for (int e = 0; e < 64; ++e) x[e] = t[e];
+    }
+  }
+  // one round's 16 chunks of the thread's part of the box (x: head or remainder pairs)
+  __device__ __forceinline__ static void put(const uint32_t (&x)[64], bool tr, int k, int g, uint8_t* mine) {
+    if (tr) {
+      // rows b (orbital 16 J + b), columns 8g .. 8g + 7 (orbitals 16 I + 8g ..): halves of the
+      // thread's rows a = 0 .. 7 at column b, b = 4 j + ((i + k) & 3) at instruction i
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int bb = (i + k) & 3, b = (i & ~3) | bb;
+        const bool mh = bb >= 2;
+        const uint32_t sel = (bb & 1) ? 0x7632u : 0x5410u;
+        const int m0 = 2 * (i >> 2);
+        uint32_t wd[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const uint32_t x0 = mh ? x[8 * (2 * t) + m0 + 1] : x[8 * (2 * t) + m0];
+          const uint32_t x1 = mh ? x[8 * (2 * t + 1) + m0 + 1] : x[8 * (2 * t + 1) + m0];
+          wd[t] = __byte_perm(x0, x1, sel);
+        }
+        *reinterpret_cast<uint4*>(mine + b * 32 + 16 * g) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+      }
+    } else {
+      // rows 8g + a of the box, columns 16 J .. 16 J + 15: chunk i (rotated) is the original chunk q
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int q = (i & 8) | ((i + k) & 7);
+        *reinterpret_cast<uint4*>(mine + 256 * g + 16 * q) = make_uint4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]);
+      }
+    }
+  }
   __device__ __forceinline__ void operator()(int, int row, int col0, const float* v, uint8_t* smem,
                                              const GemmMaps* maps) const {
     const int w = row >> 1, c = row & 1;
@@ -510,44 +557,38 @@ struct EpiVHSBlock {
     const int J = I + blk;
     const int g = (col0 >> 7) & 1;
     const float s = c ? -f : f;
+    const int k = (threadIdx.x >> 1) & 7;
     uint8_t* mine = smem + wl * 512;
+    // head / remainder pairs: word 8 a + m holds columns 2m, 2m + 1 of the thread's row a
+    uint32_t ph[64], pl[64];
 #pragma unroll
-    for (int rd = 0; rd < 8; ++rd) {
-      const int pc = rd < 4 ? 1 : 0;  // the rows feeding this plane: c = 1 real, c = 0 imaginary
-      const int lo = rd & 1, tr = (rd >> 1) & 1;
-      if (tr && I == J) continue;  // the same for every thread of the tile
-      if (threadIdx.x == 0) bulk_wait_read_all();  // the previous box has left shared memory
-      sync();
-      if (live && c == pc) {
-        if (!tr) {
-          // rows 8g + a of the box, columns 16 J .. + 15
+    for (int e = 0; e < 64; ++e) ph[e] = split2_f16(v[2 * e] * s, v[2 * e + 1] * s, pl[e]);
 #pragma unroll
-          for (int a = 0; a < 8; ++a) {
+    for (int half = 0; half < 2; ++half) {
+      const int pc = 1 - half;  // the rows feeding this plane: c = 1 real, c = 0 imaginary
+      const bool act = live && c == pc;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              uint4 ph, pl;
-              pack8_f16(v + a * 16 + 8 * h, s, ph, pl);
-              *reinterpret_cast<uint4*>(mine + (8 * g + a) * 32 + 16 * h) = lo ? pl : ph;
-            }
-          }
-        } else {
-          // rows b (orbital 16 J + b), columns 8g .. 8g + 7 (orbitals 16 I + 8g ..)
-#pragma unroll
-          for (int b = 0; b < 16; ++b) {
-            float t[8];
-#pragma unroll
-            for (int a = 0; a < 8; ++a) t[a] = v[a * 16 + b];
-            uint4 ph, pl;
-            pack8_f16(t, s, ph, pl);
-            *reinterpret_cast<uint4*>(mine + b * 32 + 16 * g) = lo ? pl : ph;
-          }
+      for (int rd = 0; rd < 4; ++rd) {
+        const int tr = rd < 2, lo = rd & 1;
+        if (tr && I == J) continue;  // the same for every thread of the tile
+        if (rd == 2 && act) {
+          rotate(ph, k);
+          rotate(pl, k);
         }
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      }
-      sync();
-      if (threadIdx.x == 0) {
-        tma_store_3d(&maps->out[(pc ? 0 : 2) + lo], tr ? 16 * I : 16 * J, tr ? 16 * J : 16 * I, w0, smem);
-        bulk_commit();
+        if (threadIdx.x == 0) bulk_wait_read_all();  // the previous box has left shared memory
+        sync();
+        if (act) {
+          if (lo)
+            put(pl, tr, k, g, mine);
+          else
+            put(ph, tr, k, g, mine);
+          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        }
+        sync();
+        if (threadIdx.x == 0) {
+          tma_store_3d(&maps->out[(pc ? 0 : 2) + lo], tr ? 16 * I : 16 * J, tr ? 16 * J : 16 * I, w0, smem);
+          bulk_commit();
+        }
       }
     }
   }

@@ -27,14 +27,6 @@ namespace {
 constexpr int kBK = 16;       // k chunk (doubles) of the streamed left operand
 constexpr int kLDA = kBK + 4;  // smem row stride of an A chunk (conflict-free fragment reads)
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
-  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::); }
-
 // Rows of the running term kept in shared memory: every k chunk of either pass
 // kind (K = M real or K = 2M complex-interleaved) reads rows < KROWS, and rows
 // >= M are zero.  kTSlack extra entries absorb the column overrun of the last
@@ -165,7 +157,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       pf_c = nc_;
     }
     cp_async_commit();
-    cp_async_wait_1();
+    cp_async_wait<1>();
     __syncthreads();
     const double* a_s = sA0 + (q & 1) * MPAD * kLDA;
     const int k0 = cur_c * kBK;
@@ -236,7 +228,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       cur_c += 1;
     }
   }
-  cp_async_wait_0();
+  cp_async_wait<0>();
 }
 
 template <int FM, int FN>
