@@ -103,22 +103,21 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
   __syncthreads();
   // ---- Gauss-Jordan with partial pivoting, in place: after step k row k holds the k-th row of
   // the reduced inverse and column k the multipliers.  Two barriers per step: warp 0 finishes
-  // the previous step (row k-1 x 1/p, column k-1 x -1/p), picks and swaps the pivot row; then
-  // all threads update the rest (thread: column tid % 32, rows tid / 32 + 4r).
+  // the previous step (column k-1 x -1/p), picks and swaps the pivot row and scales it by 1/p
+  // (1/p = conj(p) / |p|^2, one division); then all threads update the rest with the scaled row
+  // (thread: column tid % 32, rows tid / 32 + 4r).
   int swaps = 0;
   const int uj = tid & 31, ui = tid >> 5;
   for (int k = 0; k <= N; ++k) {
     if (tid < 32) {
       if (k > 0) {
+        // column k - 1 x -1/p, after the update of step k - 1 (which read it)
         const int kp = k - 1;
         const double2 pinv = red[5];
         if (tid < N && tid != kp) {
-          sO[kp][tid] = cmul(sO[kp][tid], pinv);
           const double2 v = cmul(sO[tid][kp], pinv);
           sO[tid][kp] = make_double2(-v.x, -v.y);
         }
-        __syncwarp();
-        if (tid == 0) sO[kp][kp] = pinv;
         __syncwarp();
       }
       if (k < N) {
@@ -150,24 +149,28 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
         }
         if (bi != k) ++swaps;  // warp-uniform: every lane of warp 0 counts
         __syncwarp();
+        // row k x 1/p, a_kk = 1/p
+        const double2 pv = sO[k][k];
+        const double rn = __drcp_rn(pv.x * pv.x + pv.y * pv.y);
+        const double2 pinv = make_double2(pv.x * rn, -pv.y * rn);
+        if (tid < N && tid != k) sO[k][tid] = cmul(sO[k][tid], pinv);
         if (tid == 0) {
-          const double2 pv = sO[k][k];
           if (pv.x == 0.0 && pv.y == 0.0) flag(status, STATUS_SINGULAR);
           sPiv[k] = pv;
-          red[5] = cdiv(make_double2(1.0, 0.0), pv);
+          sO[k][k] = pinv;
+          red[5] = pinv;
         }
       }
     }
     __syncthreads();
     if (k == N) break;
-    // a_ij -= (a_ik / a_kk) a_kj for i, j != k (row k and column k are only read here)
-    const double2 inv = red[5];
+    // a_ij -= a_ik (a_kj / a_kk) for i, j != k (the scaled row k; column k is only read here)
     if (uj < N && uj != k) {
       const double2 akj = sO[k][uj];
-      for (int i = ui; i < N; i += 4) {
-        if (i == k) continue;
-        const double2 f = cmul(sO[i][k], inv);
-        sO[i][uj] = csub(sO[i][uj], cmul(f, akj));
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int i = ui + 4 * r;
+        if (i < N && i != k) sO[i][uj] = csub(sO[i][uj], cmul(sO[i][k], akj));
       }
     }
     __syncthreads();
