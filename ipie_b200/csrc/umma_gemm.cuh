@@ -27,7 +27,15 @@
 // tcgen05.mma.  One-group epilogues may synchronise with bar.sync 1, 128
 // (epi_sync), never with __syncthreads.
 //
-// Tiles: TileOrder numbers the 128 x BN output tiles of nz batches; a tile
+// CTA pairs (CG = 2, clusters of two): a tile is 256 x BN; the even CTA of the pair (the
+// leader) issues tcgen05.mma.cta_group::2 for both, each CTA stages its own 128 rows of A and
+// BN / 2 rows of B (so each SM loads and reads half of B per product), and each CTA's epilogue
+// drains its own 128 rows of D from its own TMEM.  Both producers' copies complete on the
+// leader's full barrier (which expects both stages' bytes), the MMA commits arrive on the empty
+// and chunk-full barriers of both CTAs, and both epilogues arrive on the leader's chunk-empty
+// barrier.
+//
+// Tiles: TileOrder numbers the (128 CG) x BN output tiles of nz batches; a tile
 // (z, mt, nt) reads A rows from z * a_rows_per_batch + mt * 128 and B rows from
 // z * b_rows_per_batch + nt * BN (rows past a batch's own extent read the next
 // batch or TMA's zero fill; the epilogue drops them).  The CTAs are persistent:
@@ -145,10 +153,10 @@ struct EpiUsesMaps<Epi, decltype((void)Epi::kUsesMaps)> {
   static constexpr bool value = Epi::kUsesMaps;
 };
 
-template <int BN, int NA, int NSPLIT, int STAGES, int EPI_SMEM = 0, int KIND = KIND_TF32>
+template <int BN, int NA, int NSPLIT, int STAGES, int EPI_SMEM = 0, int KIND = KIND_TF32, int CG = 1>
 struct GemmShape {
   static constexpr int A_TILE = kBM * row_bytes(KIND);
-  static constexpr int B_TILE = BN * row_bytes(KIND);
+  static constexpr int B_TILE = BN / CG * row_bytes(KIND);  // this CTA's rows of B
   static constexpr int NAT = NA * (NSPLIT == 3 ? 2 : 1);
   static constexpr int NBT = NSPLIT == 3 ? 2 : 1;
   static constexpr int STAGE_BYTES = NAT * A_TILE + NBT * B_TILE;
@@ -161,16 +169,18 @@ struct GemmShape {
   static_assert(2 * NA * BN <= 512, "two accumulator buffers exceed TMEM");
   static_assert(STAGE_BYTES % 1024 == 0, "stage must keep 1024-byte alignment");
   static_assert(SMEM_BYTES <= 232448, "shared memory per CTA exceeded");
+  static_assert(CG == 1 || (CG == 2 && NA == 1 && KIND != KIND_TF32 && BN % 32 == 0),
+                "CTA pairs: one left operand, FP16, BN / 2 a multiple of 16");
 };
 
 // Persistent CTAs: CTA b computes tiles b, b + gridDim.x, ...; the stage ring, the chunk counter
 // and the two TMEM buffers run on across tiles, so one tile's epilogue overlaps the next tile's
 // loads and first MMAs.
-template <int BN, int NA, int NSPLIT, int STAGES, class Epi, int KIND = KIND_TF32>
+template <int BN, int NA, int NSPLIT, int STAGES, class Epi, int KIND = KIND_TF32, int CG = 1>
 __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
     umma_gemm_kernel(const __grid_constant__ GemmMaps maps, int K, int a_rows_per_batch, int b_rows_per_batch,
                      TileOrder order, Epi epi, unsigned* status) {
-  using S = GemmShape<BN, NA, NSPLIT, STAGES, EpiSmem<Epi>::value, KIND>;
+  using S = GemmShape<BN, NA, NSPLIT, STAGES, EpiSmem<Epi>::value, KIND, CG>;
   using R = GemmRoles<NA, BN>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -183,6 +193,10 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // CTA pairs: rank in the pair, the pair's index and count
+  const uint32_t rank = CG == 2 ? cluster_ctarank() : 0u;
+  const int unit = CG == 2 ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+  const int nunits = CG == 2 ? (int)(gridDim.x >> 1) : (int)gridDim.x;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
@@ -190,14 +204,20 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&cfull[b], 1);
-      mbar_init(&cempty[b], R::kEpiThreads);
+      mbar_init(&cempty[b], CG * R::kEpiThreads);
     }
     *abort_flag = 0;
     mbar_fence_init();
   }
-  if (warp == 0) tmem_alloc(tmem_slot, S::TMEM_COLS);
+  if (warp == 0) {
+    if constexpr (CG == 2)
+      tmem_alloc_pair(tmem_slot, S::TMEM_COLS);
+    else
+      tmem_alloc(tmem_slot, S::TMEM_COLS);
+  }
   tc_fence_before();
   __syncthreads();
+  if constexpr (CG == 2) cluster_sync_all();  // the peer's barriers are initialised before any arrive
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
@@ -218,20 +238,38 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
       if (NSPLIT == 3) tma_prefetch_desc(&maps.b_lo);
       uint32_t g = 0;  // stage uses so far (all tiles)
       bool ok = true;
-      for (int l = blockIdx.x; l < ntiles && ok; l += gridDim.x) {
+      for (int l = unit; l < ntiles && ok; l += nunits) {
         int z, mt, nt;
         order.decode(l, z, mt, nt);
-        const int arow = z * a_rows_per_batch + mt * kBM;
-        const int brow = z * b_rows_per_batch + nt * BN;
+        const int arow = z * a_rows_per_batch + mt * (kBM * CG) + (int)rank * kBM;
+        const int brow = z * b_rows_per_batch + nt * BN + (int)rank * (BN / CG);
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const uint32_t s = g % STAGES, r = g / STAGES;
           if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) {
             ok = false;
             break;
           }
-          mbar_expect_tx(&full[s], S::STAGE_BYTES);
           uint8_t* st = smem + s * S::STAGE_BYTES;
           const int k = kb * KB;
+          if constexpr (CG == 2) {
+            // both CTAs' copies complete on the leader's full barrier, which expects both stages
+            if (rank == 0) mbar_expect_tx(&full[s], 2 * S::STAGE_BYTES);
+            const uint32_t fb = mapa_shared(&full[s], 0);
+            if (NSPLIT == 3 && maps.a_planes) {
+              tma_load_3d_pair(st, &maps.a_hi[0], k, arow, 0, fb);
+            } else {
+              tma_load_2d_pair(st, &maps.a_hi[0], k, arow, fb);
+              if (NSPLIT == 3) tma_load_2d_pair(st + S::A_TILE, &maps.a_lo[0], k, arow, fb);
+            }
+            if (NSPLIT == 3 && maps.b_planes) {
+              tma_load_3d_pair(st + S::NAT * S::A_TILE, &maps.b_hi, k, brow, 0, fb);
+            } else {
+              tma_load_2d_pair(st + S::NAT * S::A_TILE, &maps.b_hi, k, brow, fb);
+              if (NSPLIT == 3) tma_load_2d_pair(st + S::NAT * S::A_TILE + S::B_TILE, &maps.b_lo, k, brow, fb);
+            }
+            continue;
+          }
+          mbar_expect_tx(&full[s], S::STAGE_BYTES);
 #pragma unroll
           for (int a = 0; a < NA; ++a) {
             if (NSPLIT == 3 && maps.a_planes) {
@@ -252,11 +290,11 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
     }
     __syncwarp();
   } else if (warp == R::kMmaWarp) {
-    if (lane == 0) {
-      constexpr uint32_t idesc = KIND != KIND_TF32 ? idesc_f16(kBM, BN) : idesc_tf32(kBM, BN);
+    if (lane == 0 && rank == 0) {
+      constexpr uint32_t idesc = KIND != KIND_TF32 ? idesc_f16(kBM * CG, BN) : idesc_tf32(kBM, BN);
       uint32_t g = 0, c = 0;  // stage uses and chunks so far (all tiles)
       bool ok = true;
-      for (int l = blockIdx.x; l < ntiles && ok; l += gridDim.x) {
+      for (int l = unit; l < ntiles && ok; l += nunits) {
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const bool first = (kb % CKB) == 0;
           const bool last = (kb % CKB) == CKB - 1 || kb == nk - 1;
@@ -284,7 +322,13 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
               // K steps wholly past K multiply TMA's zero fill: skip them
               if (kk > 0 && kb * KB + kk * (KB / KK) >= K) break;
               // 32 bytes of K per MMA (8 tf32 or 16 fp16): advance the start address by 2 (16-byte units)
-              if constexpr (KIND != KIND_TF32) {
+              if constexpr (CG == 2) {
+                mma_f16_pair(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
+                if (NSPLIT == 3) {
+                  mma_f16_pair(d, da_hi + 2 * kk, db_lo + 2 * kk, idesc, 1u);
+                  mma_f16_pair(d, da_lo + 2 * kk, db_hi + 2 * kk, idesc, 1u);
+                }
+              } else if constexpr (KIND != KIND_TF32) {
                 mma_f16(d, da_hi + 2 * kk, db_hi + 2 * kk, idesc, (!first || kk > 0) ? 1u : 0u);
                 if (NSPLIT == 3) {
                   mma_f16(d, da_hi + 2 * kk, db_lo + 2 * kk, idesc, 1u);
@@ -299,10 +343,18 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
               }
             }
           }
-          mma_commit(&empty[s]);
-          if (last) {
-            mma_commit(&cfull[buf]);
-            ++c;
+          if constexpr (CG == 2) {
+            mma_commit_pair(&empty[s]);
+            if (last) {
+              mma_commit_pair(&cfull[buf]);
+              ++c;
+            }
+          } else {
+            mma_commit(&empty[s]);
+            if (last) {
+              mma_commit(&cfull[buf]);
+              ++c;
+            }
           }
         }
       }
@@ -314,7 +366,9 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
     const int quarter = warp & 3, group = warp >> 2;
     uint32_t c = 0;  // chunks so far (all tiles)
     bool ok = true;
-    for (int l = blockIdx.x; l < ntiles; l += gridDim.x) {
+    // chunk-empty arrivals of a pair go to the leader's barriers (the peer's own are unused)
+    const uint32_t ce_remote[2] = {CG == 2 ? mapa_shared(&cempty[0], 0) : 0u, CG == 2 ? mapa_shared(&cempty[1], 0) : 0u};
+    for (int l = unit; l < ntiles; l += nunits) {
       int z, mt, nt;
       order.decode(l, z, mt, nt);
       float v[R::kGroupCols];
@@ -337,15 +391,19 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
           for (int i = 0; i < 32; ++i) v[q * 32 + i] += t[i];
         }
         tc_fence_before();
-        mbar_arrive_cta(&cempty[buf]);
+        if constexpr (CG == 2)
+          mbar_arrive_cluster(ce_remote[buf]);
+        else
+          mbar_arrive_cta(&cempty[buf]);
       }
       // every epilogue thread takes this vote once per tile, so all of them leave together;
       // a column group hands its columns to the epilogue as a tile starting at its own offset
       if (!epi_all(ok && !*abort_flag, R::kEpiThreads)) break;
+      const int row = mt * (kBM * CG) + (int)rank * kBM + quarter * 32 + lane;
       if constexpr (EpiUsesMaps<Epi>::value)
-        epi(z, mt * kBM + quarter * 32 + lane, nt * BN + group * (R::kGroupCols / NA), v, epi_smem, &maps);
+        epi(z, row, nt * BN + group * (R::kGroupCols / NA), v, epi_smem, &maps);
       else
-        epi(z, mt * kBM + quarter * 32 + lane, nt * BN + group * (R::kGroupCols / NA), v, epi_smem);
+        epi(z, row, nt * BN + group * (R::kGroupCols / NA), v, epi_smem);
     }
   }
   if constexpr (EpiUsesMaps<Epi>::value) {
@@ -353,7 +411,15 @@ __global__ void __launch_bounds__(GemmRoles<NA, BN>::kThreads, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, S::TMEM_COLS);
+  if constexpr (CG == 2) {
+    // neither CTA frees its TMEM or leaves while the pair's MMAs, copies or arrivals may still
+    // reach it
+    cluster_sync_all();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc_pair(tmem, S::TMEM_COLS);
+  } else {
+    if (warp == 0) tmem_dealloc(tmem, S::TMEM_COLS);
+  }
 }
 
 }  // namespace umma
