@@ -152,6 +152,26 @@ cudaError_t make_map_f16_batched(CUtensorMap* m, const void* base, long long bat
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// The four VHS planes of every walker as one 4-D map (planes `plane` halves apart in one
+// allocation): columns (k), rows, walkers, planes; box 16 columns x box_rows x 1 x 4, 32-byte
+// swizzled -- the last 16 columns of all four planes of a walker in one copy.
+cudaError_t make_map_f16_tail4(CUtensorMap* m, const void* base, long long batch, long long rows, long long k,
+                               long long ld, long long plane, int box_rows) {
+  auto fn = encode_fn();
+  if (fn == nullptr) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 8) || (plane % 8) || rows <= 0 || k <= 0 || batch <= 0 ||
+      ld < k || plane < batch * rows * ld)
+    return cudaErrorInvalidValue;
+  cuuint64_t dims[4] = {(cuuint64_t)k, (cuuint64_t)rows, (cuuint64_t)batch, 4};
+  cuuint64_t strides[3] = {(cuuint64_t)ld * 2, (cuuint64_t)rows * ld * 2, (cuuint64_t)plane * 2};
+  cuuint32_t box[4] = {16, (cuuint32_t)box_rows, 1, 4};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 // hi = FP16(x * scale), lo = FP16(x * scale - hi): the split of the FP16 3-pass product.
 __global__ void split_f16_kernel(const double* __restrict__ x, __half* __restrict__ hi, __half* __restrict__ lo,
                                  long long n, double scale) {

@@ -56,12 +56,17 @@ namespace umma {
 cudaError_t make_map_f16(CUtensorMap* m, const void* base, long long rows, long long k, long long ld, int box_rows);
 cudaError_t make_map_f16_batched(CUtensorMap* m, const void* base, long long batch, long long rows, long long k,
                                  long long ld, int box_rows);
+cudaError_t make_map_f16_tail4(CUtensorMap* m, const void* base, long long batch, long long rows, long long k,
+                               long long ld, long long plane, int box_rows);
 
 namespace {
 
 struct Chain16Maps {
   CUtensorMap e_hi, e_lo;  // E - I (M x Mp halves), box 128 x 64
   CUtensorMap v[4];        // VHS planes re_hi, im_hi, re_lo, im_lo (W, M, Mp halves), box 1 x 128 x 64
+  CUtensorMap vt;          // the four planes as one 4-D map, box 16 x rows x 1 x 4 (tail4)
+  int tail_plane[4];       // position of plane v[i] in vt's plane order
+  int tail4;               // vt is valid: the planes are equally spaced in one allocation
 };
 
 constexpr int kATile = 128 * 128;        // bytes: 128 rows x 64 halves
@@ -621,6 +626,7 @@ __global__ void __launch_bounds__(kTThreads, 1)
   const int KB16 = Mp / 16;       // 16-column k-blocks of A per half of K'
   const int C = (Mp + 63) / 64;   // 64-row chunks of the output (64-column k-blocks of B)
   const int stage_bytes = t_stage_bytes(Mp);
+  const bool tail4 = maps.tail4 != 0 && Mp - 64 * (C - 1) == 16;
   uint8_t* abuf = smem;
   uint8_t* stg = smem + t_a_bytes(Mp);
   float* staging = reinterpret_cast<float*>(stg + kTStages * stage_bytes);
@@ -678,23 +684,30 @@ __global__ void __launch_bounds__(kTThreads, 1)
         for (int t = 0; t < nterms && ok; ++t) {
           const bool onebody = (t == 0 || t == nterms - 1);
           const int nparts = onebody ? 1 : 2;
-          for (int c = 0; c < C && ok; ++c)
-            for (int p = 0; p < nparts && ok; ++p)
-              for (int h = 0; h < 2; ++h, ++g) {
-                if ((int)(g % kProducers) != lane) continue;
-                const uint32_t s = g % kTStages, r = g / kTStages;
-                if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) {
-                  ok = false;
-                  break;
-                }
-                uint8_t* dst = stg + s * stage_bytes;
-                mbar_expect_tx(&full[s], stage_bytes);
-                // rows and columns past M are zero-filled by TMA (no traffic)
-                if (onebody)
-                  tma_load_2d(dst, h ? &maps.e_lo : &maps.e_hi, c * 64, 0, &full[s]);
-                else  // maps.v: re_hi, im_hi, re_lo, im_lo
-                  tma_load_3d(dst, &maps.v[2 * h + p], c * 64, 0, w, &full[s]);
+          for (int c = 0; c < C && ok; ++c) {
+            // a Taylor term's last chunk of 16 columns: all four planes in one stage (tail4)
+            const bool t4 = tail4 && !onebody && c == C - 1;
+            const int nst = t4 ? 1 : 2 * nparts;
+            for (int q = 0; q < nst; ++q, ++g) {
+              const int p = q >> 1, h = q & 1;
+              if ((int)(g % kProducers) != lane) continue;
+              const uint32_t s = g % kTStages, r = g / kTStages;
+              if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1, abort_flag, status)) {
+                ok = false;
+                break;
               }
+              uint8_t* dst = stg + s * stage_bytes;
+              // 64 columns x Mp rows x 2 bytes either way (t4: 16 columns x 4 planes)
+              mbar_expect_tx(&full[s], stage_bytes);
+              // rows and columns past M are zero-filled by TMA (no traffic)
+              if (t4)
+                tma_load_4d(dst, &maps.vt, c * 64, 0, w, 0, &full[s]);
+              else if (onebody)
+                tma_load_2d(dst, h ? &maps.e_lo : &maps.e_hi, c * 64, 0, &full[s]);
+              else  // maps.v: re_hi, im_hi, re_lo, im_lo
+                tma_load_3d(dst, &maps.v[2 * h + p], c * 64, 0, w, &full[s]);
+            }
+          }
         }
     }
     __syncwarp();
@@ -723,6 +736,26 @@ __global__ void __launch_bounds__(kTThreads, 1)
             }
             tc_fence_after();
             const int kkc = min(4, (Mp - 64 * c) / 16);
+            if (tail4 && !onebody && c == C - 1) {
+              // one stage: plane v[2h + p] at position tail_plane[2h + p], 32-byte rows
+              const uint32_t s = g % kTStages, r = g / kTStages;
+              if (!mbar_wait(&full[s], r & 1, abort_flag, status)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              for (int p = 0; p < 2; ++p)
+                for (int h = 0; h < 2; ++h) {
+                  const uint64_t bdesc =
+                      desc_kmajor_sw32(stg + s * stage_bytes + maps.tail_plane[2 * h + p] * Mp * 32);
+                  const uint64_t adesc = desc_kmajor_sw32(abuf + (p * KB16 + 4 * c) * 4096);
+                  mma_f16(d, adesc, bdesc, idesc, first ? 0u : 1u);
+                  first = false;
+                }
+              mma_commit(&empty[s]);
+              ++g;
+              continue;
+            }
             for (int p = 0; p < nparts && ok; ++p)
               for (int h = 0; h < 2; ++h, ++g) {
                 const uint32_t s = g % kTStages, r = g / kTStages;
@@ -958,7 +991,29 @@ cudaError_t mixed_orbital_chain16(const void* e_hi, const void* e_lo, float e_sc
   const void* planes[4] = {v_re_hi, v_im_hi, v_re_lo, v_im_lo};
   for (int i = 0; i < 4; ++i)
     if ((e = make_map_f16_batched(&maps.v[i], planes[i], W, M, M, ld, box_rows)) != cudaSuccess) return e;
-  if (transposed) return launch_chain_t16(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
+  if (transposed) {
+    // planes equally spaced in one allocation (in any order): the 4-D map of their last columns
+    uintptr_t a[4], lo = ~uintptr_t(0);
+    for (int i = 0; i < 4; ++i) {
+      a[i] = reinterpret_cast<uintptr_t>(planes[i]);
+      lo = a[i] < lo ? a[i] : lo;
+    }
+    uintptr_t stride = 0;
+    for (int i = 0; i < 4; ++i)
+      if (a[i] != lo && (stride == 0 || a[i] - lo < stride)) stride = a[i] - lo;
+    int seen = 0;
+    bool even = stride > 0 && stride % 16 == 0;
+    for (int i = 0; i < 4 && even; ++i) {
+      const uintptr_t d = a[i] - lo;
+      const int pos = (int)(d / stride);
+      even = d % stride == 0 && pos < 4 && !(seen & (1 << pos));
+      seen |= 1 << pos;
+      maps.tail_plane[i] = pos;
+    }
+    maps.tail4 = even && make_map_f16_tail4(&maps.vt, reinterpret_cast<const void*>(lo), W, M, M, ld,
+                                            (long long)(stride / 2), box_rows) == cudaSuccess;
+    return launch_chain_t16(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
+  }
   if (2 * N <= 32) return launch_chain16<32>(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
   return launch_chain16<64>(maps, e_scale, v_scale, phi_in, phi_out, W, M, N, nmax, status, st);
 }

@@ -124,7 +124,9 @@ class Workspace:
         self.xs_hi, self.xs_lo = self.xs_hilo[0], self.xs_hilo[1]
         if chain16:
             Mp = (M + 7) // 8 * 8
-            self.v_planar = [torch.empty(W, M, Mp, dtype=f16, device=dev) for _ in range(4)]  # re_hi, re_lo, im_hi, im_lo
+            # re_hi, re_lo, im_hi, im_lo in one allocation: the chain loads the last columns of all
+            # four planes of a walker with one copy
+            self.v_planar = list(torch.empty(4, W, M, Mp, dtype=f16, device=dev).unbind(0))
             self.orb_work = torch.empty(0, dtype=f32, device=dev)
         else:
             self.v_planar = [torch.empty(W, M, M, dtype=f32, device=dev) for _ in range(4)]
