@@ -44,13 +44,14 @@ struct SpinDet32 {
   double2 phase;
 };
 
-// O = phi^T psi* for one spin block into sO; then its inverse (of the row-permuted O) in place,
-// the row order in sPerm and log|det|, phase from the pivots.
-__device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2* __restrict__ psic, int M, int N,
-                                  double2 (*sO)[kNP], double2* sStage, int* sPerm, double2* sPiv, double2* red,
-                                  unsigned* status) {
+// sO = phi^T psi* (or, GRAM, the Gram matrix phi^H phi: psic unused) of one spin block.  phi and
+// psi* stream through shared memory in 8-row chunks, a three-deep ring of cp.async copies issued
+// two chunks ahead (one barrier per chunk); thread (ti, tj) accumulates rows {ti, ti+16} x
+// columns {tj + 8q} in registers.  The caller synchronises before reading sO.
+template <bool GRAM>
+__device__ void o_product(const double2* __restrict__ phi, const double2* __restrict__ psic, int M, int N,
+                          double2 (*sO)[kNP], double2* sStage) {
   const int tid = threadIdx.x;
-  // ---- O = phi^T psi*: thread (ti, tj) owns rows {ti, ti+16} x columns {tj + 8q}
   const int ti = tid >> 3, tj = tid & 7;
   double2 acc[2][4];
 #pragma unroll
@@ -68,7 +69,7 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
         const bool in = m < M && c < N;
         const size_t off = in ? (size_t)m * N + c : 0;
         cp_async16(st + e, phi + off, in ? 16 : 0);
-        cp_async16(st + kChunk * 32 + e, psic + off, in ? 16 : 0);
+        if (!GRAM) cp_async16(st + kChunk * 32 + e, psic + off, in ? 16 : 0);
       }
     }
     cp_async_commit();  // (an empty group past the end keeps the group count per chunk)
@@ -80,10 +81,15 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
     __syncthreads();     // everyone's have, and everyone is done with chunk ch - 1
     issue(ch + 2);       // into the slot of chunk ch - 1
     const double2(*sPhi)[32] = reinterpret_cast<const double2(*)[32]>(sStage + (ch % kORing) * kOStage);
-    const double2(*sPsi)[32] = reinterpret_cast<const double2(*)[32]>(sStage + (ch % kORing) * kOStage + kChunk * 32);
+    const double2(*sPsi)[32] =
+        GRAM ? sPhi : reinterpret_cast<const double2(*)[32]>(sStage + (ch % kORing) * kOStage + kChunk * 32);
 #pragma unroll
     for (int r = 0; r < kChunk; ++r) {
-      const double2 a0 = sPhi[r][ti], a1 = sPhi[r][ti + 16];
+      double2 a0 = sPhi[r][ti], a1 = sPhi[r][ti + 16];
+      if (GRAM) {
+        a0.y = -a0.y;
+        a1.y = -a1.y;
+      }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const double2 b = sPsi[r][tj + 8 * q];
@@ -99,6 +105,15 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int q = 0; q < 4; ++q) sO[ti + 16 * a][tj + 8 * q] = acc[a][q];
+}
+
+// O = phi^T psi* for one spin block into sO; then its inverse (of the row-permuted O) in place,
+// the row order in sPerm and log|det|, phase from the pivots.
+__device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2* __restrict__ psic, int M, int N,
+                                  double2 (*sO)[kNP], double2* sStage, int* sPerm, double2* sPiv, double2* red,
+                                  unsigned* status) {
+  const int tid = threadIdx.x;
+  o_product<false>(phi, psic, M, N, sO, sStage);
   if (tid < 32) sPerm[tid] = tid;
   __syncthreads();
   // ---- Gauss-Jordan with partial pivoting, in place: after step k row k holds the k-th row of
@@ -334,6 +349,154 @@ __global__ void __launch_bounds__(kThreads, 4) gf_lu32_kernel(const double2* __r
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Reorthogonalisation of spin blocks of N <= 32 orbitals by Cholesky QR, the same unique thin QR
+// (positive real diag R) as Gram-Schmidt or a sign-fixed Householder factorisation:
+//   S = phi^H phi (o_product<true>), S = R^H R (Cholesky, right-looking, in shared memory; warp 0
+//   scales the pivot row, all threads update the trailing upper triangle), X = R^-1 (warp 0,
+//   lane i solving row i of X R = I, kept in the lower triangle of sO transposed plus the
+//   diagonal), phi <- phi X in place (16-row chunks of phi through the copy ring; lane i forms
+//   column i of four rows per warp, so each output row is one coalesced 512-byte store).
+// log det R = sum log R_kk.  Its error is that of the Gram matrix, ~cond(phi)^2 eps: walkers are
+// reorthogonalised every few steps, so phi stays close to orthonormal and cond(phi) near 1.
+__device__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 (*sO)[kNP], double2* sStage,
+                               double2* sDinv, unsigned* status) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  o_product<true>(phi, nullptr, M, N, sO, sStage);
+  __syncthreads();
+  // ---- S = R^H R in the upper triangle of sO
+  const int uj = tid & 31, ui = tid >> 5;
+  for (int k = 0; k < N; ++k) {
+    if (tid < 32) {
+      const double skk = sO[k][k].x;
+      __syncwarp();  // every lane has read the pivot before lane 0 replaces it
+      if (!(skk > 0.0)) flag(status, STATUS_ZERO_NORM);
+      const double d = sqrt(skk), dinv = 1.0 / d;
+      if (lane > k && lane < N) sO[k][lane] = cscale(sO[k][lane], dinv);
+      if (lane == 0) {
+        sO[k][k] = make_double2(d, 0.0);
+        sDinv[k] = make_double2(dinv, 0.0);
+      }
+    }
+    __syncthreads();
+    // S_ij -= conj(R_ki) R_kj for k < i <= j
+    if (uj > k && uj < N) {
+      const double2 rkj = sO[k][uj];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int i = ui + 4 * r;
+        if (i > k && i <= uj) sO[i][uj] = csub(sO[i][uj], cmulc(sO[k][i], rkj));
+      }
+    }
+    __syncthreads();
+  }
+  double logsum = 0.0;
+  if (tid < 32) {
+    // ---- X = R^-1 (upper): lane i, row i: X_ii = 1 / R_ii, X_ij = -(sum_{i<=k<j} X_ik R_kj) / R_jj
+    double2 x[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < j; ++k) {
+        const double2 rkj = sO[k][j];  // the same for every lane: a broadcast
+        acc.x += x[k].x * rkj.x - x[k].y * rkj.y;
+        acc.y += x[k].x * rkj.y + x[k].y * rkj.x;
+      }
+      const double di = j < N ? sDinv[j].x : 0.0;
+      x[j] = lane == j ? make_double2(di, 0.0) : (lane < j ? make_double2(-acc.x * di, -acc.y * di)
+                                                           : make_double2(0.0, 0.0));
+    }
+    // X_ij (i < j) to sO[j][i], below the diagonal: R is no longer read after the barrier
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (lane < j && j < N) sO[j][lane] = x[j];
+    if (lane < N) logsum = log(sO[lane][lane].x);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) logsum += __shfl_xor_sync(0xffffffffu, logsum, o);
+  }
+  __syncthreads();
+  // ---- phi <- phi X: lane i = column i, rows m0 + 4 warp + a
+  const int nch = (M + 15) / 16;
+  auto issue = [&](int ch) {
+    if (ch < nch) {
+      double2* st = sStage + (ch % kORing) * kOStage;
+#pragma unroll
+      for (int u = 0; u < 16 * 32 / kThreads; ++u) {
+        const int e = tid + u * kThreads, r = e >> 5, c = e & 31, m = ch * 16 + r;
+        const bool in = m < M && c < N;
+        cp_async16(st + e, phi + (in ? (size_t)m * N + c : 0), in ? 16 : 0);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(0);
+  issue(1);
+  for (int ch = 0; ch < nch; ++ch) {
+    cp_async_wait<1>();
+    __syncthreads();
+    issue(ch + 2);  // rows ahead of the ones rewritten below
+    const double2(*sPhi)[32] = reinterpret_cast<const double2(*)[32]>(sStage + (ch % kORing) * kOStage);
+    double2 acc[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) acc[a] = make_double2(0.0, 0.0);
+#pragma unroll 8
+    for (int r = 0; r < 32; ++r) {
+      // X[r][lane]: below the diagonal of sO transposed, the diagonal in sDinv, zero for r > lane
+      const double2 xr = r < lane ? sO[lane][r] : (r == lane && r < N ? sDinv[r] : make_double2(0.0, 0.0));
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const double2 p = sPhi[4 * warp + a][r];
+        acc[a].x += p.x * xr.x - p.y * xr.y;
+        acc[a].y += p.x * xr.y + p.y * xr.x;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int m = ch * 16 + 4 * warp + a;
+      if (m < M && lane < N) phi[(size_t)m * N + lane] = acc[a];
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  return logsum;  // valid in warp 0
+}
+
+// One CTA per walker: both spin blocks (the alpha block once when phib aliases it), then
+// detR = exp(sum log R_kk - detR_shift), log_detR += log detR, ovlp /= detR (the contract of
+// reortho_kernel in walkers.cu, which keeps N > 32).
+__global__ void __launch_bounds__(kThreads, 4) reortho_chol32_kernel(double2* __restrict__ phia,
+                                                                     double2* __restrict__ phib, int M, int na,
+                                                                     int nb, const double* __restrict__ detR_shift,
+                                                                     double* __restrict__ detR,
+                                                                     double* __restrict__ log_detR,
+                                                                     double2* __restrict__ ovlp, unsigned* status) {
+  __shared__ double2 sO[32][kNP];
+  __shared__ __align__(16) double2 sStage[kStage];
+  __shared__ double2 sDinv[32];
+  const int w = blockIdx.x;
+  const bool alias = (phib == phia) && (nb == na);
+  double logsum = 0.0, log_a = 0.0;
+  for (int s = 0; s < 2; ++s) {
+    const int N = s == 0 ? na : nb;
+    if (N == 0) continue;
+    if (s == 1 && alias) {
+      logsum += log_a;
+      continue;
+    }
+    const double l = cholqr_block((s == 0 ? phia : phib) + (size_t)w * M * N, M, N, sO, sStage, sDinv, status);
+    logsum += l;
+    if (s == 0) log_a = l;
+  }
+  if (threadIdx.x == 0) {
+    const double d = exp(logsum - detR_shift[w]);
+    detR[w] = d;
+    log_detR[w] += log(d);
+    ovlp[w] = cscale(ovlp[w], 1.0 / d);
+  }
+}
+
 }  // namespace
 
 bool gf_lu32_fits(int na, int nb) { return na >= 1 && na <= 32 && nb >= 0 && nb <= 32; }
@@ -348,6 +511,15 @@ cudaError_t launch_gf_lu32(const double2* phia, const double2* phib, int W, int 
   else
     gf_lu32_kernel<false><<<W, kThreads, 0, st>>>(phia, phib, M, na, nb, psia_c, psib_c, log_shift, nullptr,
                                                   nullptr, ovlp, logdet, status);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reortho_chol32(double2* phia, double2* phib, int W, int M, int na, int nb,
+                                  const double* detR_shift, double* detR, double* log_detR, double2* ovlp,
+                                  unsigned* status, cudaStream_t st) {
+  if (na < 1 || na > 32 || nb < 0 || nb > 32 || M <= 0 || W <= 0) return cudaErrorInvalidValue;
+  reortho_chol32_kernel<<<W, kThreads, 0, st>>>(phia, phib, M, na, nb, detR_shift, detR, log_detR, ovlp, status);
   note_launch();
   return cudaGetLastError();
 }

@@ -27,6 +27,10 @@ cudaError_t launch_update_weight(int W, const double2* ovlp_new, const double2* 
                                  const double* eshift, double dt, double ebound, const double* wbound, double2* ovlp,
                                  double2* ehyb, double* weight, unsigned* status, cudaStream_t st);
 cudaError_t launch_clip_weight(int W, const double* wbound, double* weight, cudaStream_t st);
+// Cholesky-QR reorthogonalisation for spin blocks of at most 32 orbitals (greens.cu)
+cudaError_t launch_reortho_chol32(double2* phia, double2* phib, int W, int M, int na, int nb,
+                                  const double* detR_shift, double* detR, double* log_detR, double2* ovlp,
+                                  unsigned* status, cudaStream_t st);
 cudaError_t launch_reortho(double2* phia, double2* phib, int W, int M, int na, int nb, const double* detR_shift,
                            double* detR, double* log_detR, double2* ovlp, unsigned* status, cudaStream_t st);
 cudaError_t launch_ghf_blocks(double2* phi, int W, int M, int na, int nb, double2* pa, double2* pb, int scatter,

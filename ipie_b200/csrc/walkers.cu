@@ -480,6 +480,9 @@ __global__ void __launch_bounds__(256) reortho_kernel(double2* __restrict__ phia
 
 cudaError_t launch_reortho(double2* phia, double2* phib, int W, int M, int na, int nb, const double* detR_shift,
                            double* detR, double* log_detR, double2* ovlp, unsigned* status, cudaStream_t st) {
+  // blocks of at most 32 orbitals: Cholesky QR (greens.cu); larger ones by Gram-Schmidt below
+  if (na >= 1 && na <= 32 && nb >= 0 && nb <= 32)
+    return launch_reortho_chol32(phia, phib, W, M, na, nb, detR_shift, detR, log_detR, ovlp, status, st);
   const int Nmax = max(na, nb);
   size_t smem = sizeof(double2) * ((size_t)M * pad_n(Nmax) + 64);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
