@@ -7,10 +7,10 @@
 //       ahead (one barrier per chunk); each thread accumulates a 2 x 4 block of
 //       O in registers;
 //   X = (P O)^-1 by Gauss-Jordan elimination in place in shared memory with
-//       partial pivoting on |.| (one warp picks the pivot, all threads update) --
+//       partial pivoting on |.| (warp 0 picks the pivot, all threads update) --
 //       the pivots are those of the LU factorisation, so
 //       log|det O| = sum log|pivot_k|, phase = (-1)^swaps prod pivot_k / |pivot_k|
-//       (one pivot per lane of the serial warp, reduced with shuffles);
+//       (one pivot per lane of warp 0, reduced with shuffles);
 //   Ghalf[i, m] = sum_r X[i, r] phi[m, perm(r)] (= (O^-1 phi^T)[i, m]): a
 //       register-tiled product -- warp w takes rows 8w..8w+7, lane l the
 //       columns l + 32q (q < 2, so 64 columns per pass), phi staged in shared
@@ -38,15 +38,6 @@ constexpr int kOStage = 2 * kChunk * 32;  // double2 per O chunk (phi and psi*)
 constexpr int kGStage = kRC * kMS;        // double2 per Ghalf step
 constexpr int kStage = kORing * kOStage > kGRing * kGStage ? kORing * kOStage : kGRing * kGStage;
 static_assert(kChunk * 32 % kThreads == 0 && kRC * 32 * kMQ % kThreads == 0, "whole copies per thread");
-
-// The warp of this CTA that runs the serial parts (pivot steps, triangular rows): the CTA's
-// warp-slot group on the SM modulo 4, so that the (up to four) resident CTAs use different
-// sub-partitions.  Only a performance choice: any warp index is correct.
-__device__ __forceinline__ int serial_warp() {
-  unsigned wid;  // warp 0's slot; the CTA's warps hold consecutive slots, slot s on sub-partition s % 4
-  asm volatile("mov.u32 %0, %%warpid;\n" : "=r"(wid));
-  return (int)(((wid >> 2) - wid) & 3);
-}
 
 struct SpinDet32 {
   double logabs;
@@ -120,40 +111,36 @@ __device__ void o_product(const double2* __restrict__ phi, const double2* __rest
 // the row order in sPerm and log|det|, phase from the pivots.
 __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2* __restrict__ psic, int M, int N,
                                   double2 (*sO)[kNP], double2* sStage, int* sPerm, double2* sPiv, double2* red,
-                                  unsigned* status, int sw) {
-  const int tid = threadIdx.x, lane = tid & 31;
-  const bool serial = (tid >> 5) == sw;  // the warp that runs the pivot steps and the determinant
+                                  unsigned* status) {
+  const int tid = threadIdx.x;
   o_product<false>(phi, psic, M, N, sO, sStage);
   if (tid < 32) sPerm[tid] = tid;
   __syncthreads();
   // ---- Gauss-Jordan with partial pivoting, in place: after step k row k holds the k-th row of
-  // the reduced inverse and column k the multipliers.  Two barriers per step: the serial warp
-  // finishes the previous step (column k-1 x -1/p), picks and swaps the pivot row and scales it
-  // by 1/p (1/p = conj(p) / |p|^2, one division); then all threads update the rest with the
-  // scaled row (thread: column tid % 32, rows tid / 32 + 4r).  The serial warp is chosen per
-  // CTA (sw) so that the walkers sharing an SM run their pivot chains on different SM
-  // sub-partitions: a CTA's warp w sits on sub-partition w, so with warp 0 everywhere the four
-  // chains queued on one (measured: ~2.8k cycles per step).
+  // the reduced inverse and column k the multipliers.  Two barriers per step: warp 0 finishes
+  // the previous step (column k-1 x -1/p), picks and swaps the pivot row and scales it by 1/p
+  // (1/p = conj(p) / |p|^2, one division); then all threads update the rest with the scaled row
+  // (thread: column tid % 32, rows tid / 32 + 4r).
   int swaps = 0;
   const int uj = tid & 31, ui = tid >> 5;
   for (int k = 0; k <= N; ++k) {
-    if (serial) {
+    if (tid < 32) {
       if (k > 0) {
         // column k - 1 x -1/p, after the update of step k - 1 (which read it)
         const int kp = k - 1;
         const double2 pinv = red[5];
-        if (lane < N && lane != kp) {
-          const double2 v = cmul(sO[lane][kp], pinv);
-          sO[lane][kp] = make_double2(-v.x, -v.y);
+        if (tid < N && tid != kp) {
+          const double2 v = cmul(sO[tid][kp], pinv);
+          sO[tid][kp] = make_double2(-v.x, -v.y);
         }
         __syncwarp();
       }
       if (k < N) {
         double best = -1.0;
         int bi = k;
-        if (lane >= k && lane < N) {
-          best = cabs2(sO[lane][k]);
-          bi = lane;
+        if (tid >= k && tid < N) {
+          best = cabs2(sO[tid][k]);
+          bi = tid;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -165,24 +152,24 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
           }
         }
         // swap rows k and bi (all N columns) and the row order
-        if (bi != k && lane < N) {
-          const double2 t = sO[k][lane];
-          sO[k][lane] = sO[bi][lane];
-          sO[bi][lane] = t;
+        if (bi != k && tid < N) {
+          const double2 t = sO[k][tid];
+          sO[k][tid] = sO[bi][tid];
+          sO[bi][tid] = t;
         }
-        if (bi != k && lane == 0) {
+        if (bi != k && tid == 0) {
           const int t = sPerm[k];
           sPerm[k] = sPerm[bi];
           sPerm[bi] = t;
         }
-        if (bi != k) ++swaps;  // warp-uniform: every lane of the serial warp counts
+        if (bi != k) ++swaps;  // warp-uniform: every lane of warp 0 counts
         __syncwarp();
         // row k x 1/p, a_kk = 1/p
         const double2 pv = sO[k][k];
         const double rn = __drcp_rn(pv.x * pv.x + pv.y * pv.y);
         const double2 pinv = make_double2(pv.x * rn, -pv.y * rn);
-        if (lane < N && lane != k) sO[k][lane] = cmul(sO[k][lane], pinv);
-        if (lane == 0) {
+        if (tid < N && tid != k) sO[k][tid] = cmul(sO[k][tid], pinv);
+        if (tid == 0) {
           if (pv.x == 0.0 && pv.y == 0.0) flag(status, STATUS_SINGULAR);
           sPiv[k] = pv;
           sO[k][k] = pinv;
@@ -203,12 +190,12 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
     }
     __syncthreads();
   }
-  // ---- log|det| and phase from the pivots, one per lane of the serial warp
-  if (serial) {
+  // ---- log|det| and phase from the pivots, one per lane of warp 0
+  if (tid < 32) {
     double la = 0.0;
     double2 ph = make_double2(1.0, 0.0);
-    if (lane < N) {
-      const double2 u = sPiv[lane];
+    if (tid < N) {
+      const double2 u = sPiv[tid];
       const double a = cabs_(u);
       la = log(a);
       ph = make_double2(u.x / a, u.y / a);
@@ -219,7 +206,7 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
       const double2 q = make_double2(__shfl_xor_sync(0xffffffffu, ph.x, o), __shfl_xor_sync(0xffffffffu, ph.y, o));
       ph = cmul(ph, q);
     }
-    if (lane == 0) {
+    if (tid == 0) {
       red[0] = make_double2(la, 0.0);
       red[1] = (swaps & 1) ? make_double2(-ph.x, -ph.y) : ph;
     }
@@ -325,11 +312,7 @@ __global__ void __launch_bounds__(kThreads, 4) gf_lu32_kernel(const double2* __r
   __shared__ double2 sPiv[32];
   __shared__ double2 red[8];
   __shared__ int sPerm[32];
-  __shared__ int sSerial;
   const int w = blockIdx.x;
-  if (threadIdx.x == 0) sSerial = serial_warp();
-  __syncthreads();
-  const int sw = sSerial;
   // spin aliasing: phib == phia with nb == na is one block counted twice
   const bool alias = (phib == phia) && (nb == na);
   double logsum = 0.0;
@@ -344,7 +327,7 @@ __global__ void __launch_bounds__(kThreads, 4) gf_lu32_kernel(const double2* __r
       continue;
     }
     const double2* phi = (s == 0 ? phia : phib) + (size_t)w * M * N;
-    const SpinDet32 d = invert_block(phi, s == 0 ? psia_c : psib_c, M, N, sO, sStage, sPerm, sPiv, red, status, sw);
+    const SpinDet32 d = invert_block(phi, s == 0 ? psia_c : psib_c, M, N, sO, sStage, sPerm, sPiv, red, status);
     logsum += d.logabs;
     phase = cmul(phase, d.phase);
     if (threadIdx.x == 0) {
@@ -369,22 +352,22 @@ __global__ void __launch_bounds__(kThreads, 4) gf_lu32_kernel(const double2* __r
 // ---------------------------------------------------------------------------------------------
 // Reorthogonalisation of spin blocks of N <= 32 orbitals by Cholesky QR, the same unique thin QR
 // (positive real diag R) as Gram-Schmidt or a sign-fixed Householder factorisation:
-//   S = phi^H phi (o_product<true>), S = R^H R (Cholesky, right-looking, in shared memory; the
-//   serial warp scales the pivot row, all threads update the trailing upper triangle), X = R^-1 (it,
+//   S = phi^H phi (o_product<true>), S = R^H R (Cholesky, right-looking, in shared memory; warp 0
+//   scales the pivot row, all threads update the trailing upper triangle), X = R^-1 (warp 0,
 //   lane i solving row i of X R = I, kept in the lower triangle of sO transposed plus the
 //   diagonal), phi <- phi X in place (16-row chunks of phi through the copy ring; lane i forms
 //   column i of four rows per warp, so each output row is one coalesced 512-byte store).
 // log det R = sum log R_kk.  Its error is that of the Gram matrix, ~cond(phi)^2 eps: walkers are
 // reorthogonalised every few steps, so phi stays close to orthonormal and cond(phi) near 1.
 __device__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 (*sO)[kNP], double2* sStage,
-                               double2* sDinv, unsigned* status, int sw) {
+                               double2* sDinv, unsigned* status) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   o_product<true>(phi, nullptr, M, N, sO, sStage);
   __syncthreads();
   // ---- S = R^H R in the upper triangle of sO
   const int uj = tid & 31, ui = tid >> 5;
   for (int k = 0; k < N; ++k) {
-    if (warp == sw) {
+    if (tid < 32) {
       const double skk = sO[k][k].x;
       __syncwarp();  // every lane has read the pivot before lane 0 replaces it
       if (!(skk > 0.0)) flag(status, STATUS_ZERO_NORM);
@@ -408,7 +391,7 @@ __device__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 
     __syncthreads();
   }
   double logsum = 0.0;
-  if (warp == sw) {
+  if (tid < 32) {
     // ---- X = R^-1 (upper): lane i, row i: X_ii = 1 / R_ii, X_ij = -(sum_{i<=k<j} X_ik R_kj) / R_jj
     double2 x[32];
 #pragma unroll
@@ -477,7 +460,7 @@ __device__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 
   }
   cp_async_wait<0>();
   __syncthreads();
-  return logsum;  // valid in the serial warp
+  return logsum;  // valid in warp 0
 }
 
 // One CTA per walker: both spin blocks (the alpha block once when phib aliases it), then
@@ -492,11 +475,7 @@ __global__ void __launch_bounds__(kThreads, 4) reortho_chol32_kernel(double2* __
   __shared__ double2 sO[32][kNP];
   __shared__ __align__(16) double2 sStage[kStage];
   __shared__ double2 sDinv[32];
-  __shared__ int sSerial;
   const int w = blockIdx.x;
-  if (threadIdx.x == 0) sSerial = serial_warp();
-  __syncthreads();
-  const int sw = sSerial;
   const bool alias = (phib == phia) && (nb == na);
   double logsum = 0.0, log_a = 0.0;
   for (int s = 0; s < 2; ++s) {
@@ -506,11 +485,11 @@ __global__ void __launch_bounds__(kThreads, 4) reortho_chol32_kernel(double2* __
       logsum += log_a;
       continue;
     }
-    const double l = cholqr_block((s == 0 ? phia : phib) + (size_t)w * M * N, M, N, sO, sStage, sDinv, status, sw);
+    const double l = cholqr_block((s == 0 ? phia : phib) + (size_t)w * M * N, M, N, sO, sStage, sDinv, status);
     logsum += l;
     if (s == 0) log_a = l;
   }
-  if (threadIdx.x == 32 * sw) {
+  if (threadIdx.x == 0) {
     const double d = exp(logsum - detR_shift[w]);
     detR[w] = d;
     log_detR[w] += log(d);
