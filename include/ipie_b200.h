@@ -353,7 +353,8 @@ int ipie_b200_orbital_chain16_fits(int M, int N);
  * e_hi/e_lo: (E - I) x e_scale (M, Mp) binary16 head/remainder (E real); v_*:
  * the f16_planes output of ipie_b200_construct_vhs_mixed with its v_scale.  When
  * the four planes lie equally spaced in one allocation (e.g. one (4, W, M, Mp)
- * array) the last 16 columns of all four come in one copy (faster for M = 16 mod 64).
+ * array) the last 16 columns of all four come in one copy (faster when M rounded up
+ * to a multiple of 16 ends 16 columns past a multiple of 64, as M = 200 does).
  * replaces (mixed form): propagation/phaseless_base.py:321-327. */
 int ipie_b200_propagate_orbitals_mixed16(const void* e_hi, const void* e_lo, double e_scale, const void* v_re_hi,
                                          const void* v_re_lo, const void* v_im_hi, const void* v_im_lo,
