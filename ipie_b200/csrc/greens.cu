@@ -179,13 +179,22 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
     }
     __syncthreads();
     if (k == N) break;
-    // a_ij -= a_ik (a_kj / a_kk) for i, j != k (the scaled row k; column k is only read here)
+    // a_ij -= a_ik (a_kj / a_kk) for i, j != k (the scaled row k; column k is only read here).
+    // All of a thread's loads first: interleaved, each row's store could alias (for the compiler)
+    // the next row's loads, which made the eight rows a serial chain (~1.7k cycles per step).
     if (uj < N && uj != k) {
       const double2 akj = sO[k][uj];
+      double2 a[8], f[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int i = min(ui + 4 * r, 31);
+        a[r] = sO[i][uj];
+        f[r] = sO[i][k];
+      }
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         const int i = ui + 4 * r;
-        if (i < N && i != k) sO[i][uj] = csub(sO[i][uj], cmul(sO[i][k], akj));
+        if (i < N && i != k) sO[i][uj] = csub(a[r], cmul(f[r], akj));
       }
     }
     __syncthreads();
@@ -379,13 +388,20 @@ __device__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 
       }
     }
     __syncthreads();
-    // S_ij -= conj(R_ki) R_kj for k < i <= j
+    // S_ij -= conj(R_ki) R_kj for k < i <= j (loads first, as in the Gauss-Jordan update)
     if (uj > k && uj < N) {
       const double2 rkj = sO[k][uj];
+      double2 a[8], f[8];
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         const int i = ui + 4 * r;
-        if (i > k && i <= uj) sO[i][uj] = csub(sO[i][uj], cmulc(sO[k][i], rkj));
+        a[r] = sO[i][uj];
+        f[r] = sO[k][i];
+      }
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int i = ui + 4 * r;
+        if (i > k && i <= uj) sO[i][uj] = csub(a[r], cmulc(f[r], rkj));
       }
     }
     __syncthreads();
