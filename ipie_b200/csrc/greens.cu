@@ -117,79 +117,73 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
   if (tid < 32) sPerm[tid] = tid;
   __syncthreads();
   // ---- Gauss-Jordan with partial pivoting, in place: after step k row k holds the k-th row of
-  // the reduced inverse and column k the multipliers.  Two barriers per step: warp 0 finishes
-  // the previous step (column k-1 x -1/p), picks and swaps the pivot row and scales it by 1/p
-  // (1/p = conj(p) / |p|^2, one division); then all threads update the rest with the scaled row
-  // (thread: column tid % 32, rows tid / 32 + 4r).
+  // the reduced inverse and column k the multipliers.  Two barriers per step: warp 0 picks the
+  // pivot (one redux.sync on a 32-bit key: the float bits of |a|^2 above the row index, so a
+  // pivot within ~2e-6 of the largest, the lowest row on ties), swaps it into row k and scales
+  // that row by 1/p (1/p = conj(p) / |p|^2, one reciprocal); then all threads update the rest with
+  // the scaled row (thread: column tid % 32, rows tid / 32 + 4r), the owners of column k-1 first
+  // applying that column's -1/p_{k-1} to their rows (deferred from step k-1: it commutes with the
+  // row swap and the row scaling; warp 0 applies it to row k's entry with the row scaling), which
+  // keeps a load-multiply-store off warp 0's serial chain.
   int swaps = 0;
   const int uj = tid & 31, ui = tid >> 5;
-  for (int k = 0; k <= N; ++k) {
+  double2 pinv_prev = make_double2(0.0, 0.0);
+  for (int k = 0; k < N; ++k) {
     if (tid < 32) {
-      if (k > 0) {
-        // column k - 1 x -1/p, after the update of step k - 1 (which read it)
-        const int kp = k - 1;
-        const double2 pinv = red[5];
-        if (tid < N && tid != kp) {
-          const double2 v = cmul(sO[tid][kp], pinv);
-          sO[tid][kp] = make_double2(-v.x, -v.y);
-        }
-        __syncwarp();
+      unsigned key = 0u;
+      if (tid >= k && tid < N)
+        key = (__float_as_uint((float)cabs2(sO[tid][k])) & ~31u) | (unsigned)(31 - tid);
+      const int bi = 31 - (int)(__reduce_max_sync(0xffffffffu, key) & 31u);
+      // swap rows k and bi (all N columns) and the row order
+      if (bi != k && tid < N) {
+        const double2 t = sO[k][tid];
+        sO[k][tid] = sO[bi][tid];
+        sO[bi][tid] = t;
       }
-      if (k < N) {
-        double best = -1.0;
-        int bi = k;
-        if (tid >= k && tid < N) {
-          best = cabs2(sO[tid][k]);
-          bi = tid;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-          if (ob > best || (ob == best && oi < bi)) {
-            best = ob;
-            bi = oi;
-          }
-        }
-        // swap rows k and bi (all N columns) and the row order
-        if (bi != k && tid < N) {
-          const double2 t = sO[k][tid];
-          sO[k][tid] = sO[bi][tid];
-          sO[bi][tid] = t;
-        }
-        if (bi != k && tid == 0) {
-          const int t = sPerm[k];
-          sPerm[k] = sPerm[bi];
-          sPerm[bi] = t;
-        }
-        if (bi != k) ++swaps;  // warp-uniform: every lane of warp 0 counts
-        __syncwarp();
-        // row k x 1/p, a_kk = 1/p
-        const double2 pv = sO[k][k];
-        const double rn = __drcp_rn(pv.x * pv.x + pv.y * pv.y);
-        const double2 pinv = make_double2(pv.x * rn, -pv.y * rn);
-        if (tid < N && tid != k) sO[k][tid] = cmul(sO[k][tid], pinv);
-        if (tid == 0) {
-          if (pv.x == 0.0 && pv.y == 0.0) flag(status, STATUS_SINGULAR);
-          sPiv[k] = pv;
-          sO[k][k] = pinv;
-          red[5] = pinv;
-        }
+      if (bi != k && tid == 0) {
+        const int t = sPerm[k];
+        sPerm[k] = sPerm[bi];
+        sPerm[bi] = t;
+      }
+      if (bi != k) ++swaps;  // warp-uniform: every lane of warp 0 counts
+      __syncwarp();
+      // row k x 1/p, a_kk = 1/p
+      const double2 pv = sO[k][k];
+      const double rn = __drcp_rn(pv.x * pv.x + pv.y * pv.y);
+      const double2 pinv = make_double2(pv.x * rn, -pv.y * rn);
+      if (tid < N && tid != k) {
+        double2 v = cmul(sO[k][tid], pinv);
+        // row k's entry of column k-1 also takes that column's deferred -1/p_{k-1}
+        if (tid == k - 1) v = cmul(v, make_double2(-pinv_prev.x, -pinv_prev.y));
+        sO[k][tid] = v;
+      }
+      if (tid == 0) {
+        if (pv.x == 0.0 && pv.y == 0.0) flag(status, STATUS_SINGULAR);
+        sPiv[k] = pv;
+        sO[k][k] = pinv;
+        red[5] = pinv;
       }
     }
     __syncthreads();
-    if (k == N) break;
     // a_ij -= a_ik (a_kj / a_kk) for i, j != k (the scaled row k; column k is only read here).
     // All of a thread's loads first: interleaved, each row's store could alias (for the compiler)
-    // the next row's loads, which made the eight rows a serial chain (~1.7k cycles per step).
+    // the next row's loads, which made the eight rows a serial chain.
+    const double2 pk = red[5];
     if (uj < N && uj != k) {
       const double2 akj = sO[k][uj];
       double2 a[8], f[8];
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
-        const int i = min(ui + 4 * r, 31);
+        const int i = ui + 4 * r;
         a[r] = sO[i][uj];
         f[r] = sO[i][k];
+      }
+      if (uj == k - 1) {
+        // column k-1 x -1/p_{k-1} for rows other than k-1 (row k's entry: warp 0 above)
+        const double2 m = make_double2(-pinv_prev.x, -pinv_prev.y);
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          if (ui + 4 * r != k - 1) a[r] = cmul(a[r], m);
       }
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
@@ -197,8 +191,19 @@ __device__ SpinDet32 invert_block(const double2* __restrict__ phi, const double2
         if (i < N && i != k) sO[i][uj] = csub(a[r], cmul(f[r], akj));
       }
     }
+    pinv_prev = pk;
     __syncthreads();
   }
+  // column N-1 x -1/p_{N-1} (rows other than N-1)
+  if (N > 0 && uj == N - 1) {
+    const double2 m = make_double2(-pinv_prev.x, -pinv_prev.y);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = ui + 4 * r;
+      if (i < N && i != N - 1) sO[i][uj] = cmul(sO[i][uj], m);
+    }
+  }
+  __syncthreads();
   // ---- log|det| and phase from the pivots, one per lane of warp 0
   if (tid < 32) {
     double la = 0.0;
