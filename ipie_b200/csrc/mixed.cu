@@ -874,22 +874,25 @@ __global__ void __launch_bounds__(256) ghalf_pad_f16_kernel(const double2* __res
   const double sw = ldexp(1.0, 14 - ex);
   if (tid == 0) scale[w] = sw;
   const long long base = (long long)w * 2 * NP * Mp;
-  for (int e = tid; e < 2 * NP * Mp; e += 256) {
-    const int m = e % Mp, t = e / Mp, j = t % NP, c = t / NP;
-    double val = 0.0;
+  // each entry read once, both planes written (real part at row j, imaginary at row NP + j)
+  for (int e = tid; e < NP * Mp; e += 256) {
+    const int m = e % Mp, j = e / Mp;
+    double2 z = make_double2(0.0, 0.0);
     if (j < N && m < M) {
-      double2 z = gw[(size_t)j * M + m];
+      z = gw[(size_t)j * M + m];
       if (gref != nullptr) {
         const double2 r = gref[(size_t)j * M + m];
         z.x -= r.x;
         z.y -= r.y;
       }
-      val = c ? z.y : z.x;
     }
     __half h, l;
-    split_f16(val, sw, h, l);
+    split_f16(z.x, sw, h, l);
     hi[base + e] = h;
     lo[base + e] = l;
+    split_f16(z.y, sw, h, l);
+    hi[base + NP * Mp + e] = h;
+    lo[base + NP * Mp + e] = l;
   }
 }
 
