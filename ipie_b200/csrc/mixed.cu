@@ -874,25 +874,32 @@ __global__ void __launch_bounds__(256) ghalf_pad_f16_kernel(const double2* __res
   const double sw = ldexp(1.0, 14 - ex);
   if (tid == 0) scale[w] = sw;
   const long long base = (long long)w * 2 * NP * Mp;
-  // each entry read once, both planes written (real part at row j, imaginary at row NP + j)
-  for (int e = tid; e < NP * Mp; e += 256) {
+  // each entry read once, both planes written (real part at row j, imaginary at row NP + j), two
+  // neighbouring columns per thread (Mp is even, so a pair never straddles a row)
+  for (int e = 2 * tid; e < NP * Mp; e += 2 * 256) {
     const int m = e % Mp, j = e / Mp;
-    double2 z = make_double2(0.0, 0.0);
-    if (j < N && m < M) {
-      z = gw[(size_t)j * M + m];
-      if (gref != nullptr) {
-        const double2 r = gref[(size_t)j * M + m];
-        z.x -= r.x;
-        z.y -= r.y;
+    double2 z[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      z[q] = make_double2(0.0, 0.0);
+      if (j < N && m + q < M) {
+        z[q] = gw[(size_t)j * M + m + q];
+        if (gref != nullptr) {
+          const double2 r = gref[(size_t)j * M + m + q];
+          z[q].x -= r.x;
+          z[q].y -= r.y;
+        }
       }
     }
-    __half h, l;
-    split_f16(z.x, sw, h, l);
-    hi[base + e] = h;
-    lo[base + e] = l;
-    split_f16(z.y, sw, h, l);
-    hi[base + NP * Mp + e] = h;
-    lo[base + NP * Mp + e] = l;
+    __half h0, l0, h1, l1;
+    split_f16(z[0].x, sw, h0, l0);
+    split_f16(z[1].x, sw, h1, l1);
+    *reinterpret_cast<__half2*>(hi + base + e) = __halves2half2(h0, h1);
+    *reinterpret_cast<__half2*>(lo + base + e) = __halves2half2(l0, l1);
+    split_f16(z[0].y, sw, h0, l0);
+    split_f16(z[1].y, sw, h1, l1);
+    *reinterpret_cast<__half2*>(hi + base + NP * Mp + e) = __halves2half2(h0, h1);
+    *reinterpret_cast<__half2*>(lo + base + NP * Mp + e) = __halves2half2(l0, l1);
   }
 }
 
