@@ -285,6 +285,7 @@ __device__ void ghalf_block(const double2* __restrict__ phi, int M, int N, doubl
         if (r0 + rr >= N) continue;  // uniform
 #pragma unroll
         for (int q = 0; q < kMQ; ++q) {
+          if (q > 0 && m0 + 32 * q >= M) break;  // a column group wholly past M (uniform): the last pass
           const double2 b = sPT[rr * kMS + lane + 32 * q];
 #pragma unroll
           for (int a = 0; a < 8; ++a) {
