@@ -219,13 +219,13 @@ def barrier_max(value, world):
 # workload's walker count (the capture's traffic grows with the walkers it processes); the
 # capture and its command are summarised under profiles/.
 DRAM_TRAFFIC = {
-    # FP16 orbital chain (transposed products) at 512 walkers: 221.8 MB read + 38.1 MB written per
+    # FP16 orbital chain (transposed products) at 512 walkers: 220.1 MB read + 35.9 MB written per
     # launch (profiles/orbital_chain_t16_c2_w512.md), x4 for 2048 walkers (its traffic is per walker)
-    ("c2_rhf_m200", "mixed", "orbitals"): 4 * (221.79e6 + 38.08e6),
-    # block-tiled VHS product with TMA-store epilogue at 512 walkers: 223.0 MB read + 162.2 MB
+    ("c2_rhf_m200", "mixed", "orbitals"): 4 * (220.10e6 + 35.86e6),
+    # block-tiled VHS product with TMA-store epilogue at 512 walkers: 244.9 MB read + 178.5 MB
     # written (profiles/vhs_blocks_tma_c2_w512.md); the Cholesky operand (~150 MB) is read once per
     # launch whatever the walker count, the fields and planes scale with it
-    ("c2_rhf_m200", "mixed", "vhs"): 4 * (223.0e6 - 150.0e6 + 162.2e6) + 150.0e6,
+    ("c2_rhf_m200", "mixed", "vhs"): 4 * (244.9e6 - 150.0e6 + 178.5e6) + 150.0e6,
 }
 
 
