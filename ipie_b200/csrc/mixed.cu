@@ -959,6 +959,37 @@ __global__ void __launch_bounds__(256) exchange_ref_row_kernel(const double2* __
   if (threadIdx.x == 0) out[w] = cadd(acc, raw_ref[0]);
 }
 
+// The trial's Coulomb vector (one walker): xv[x] (+)= scale sum_k rchol[x][k] g[k], one warp per x
+// (the FP64 force-bias GEMM with a single walker column left most SMs idle: 0.76 ms at c2).
+__global__ void __launch_bounds__(256) coulomb_row_kernel(const double* __restrict__ rchol,
+                                                          const double2* __restrict__ g, int X, int K,
+                                                          double2* __restrict__ xv, int accumulate, double scale) {
+  const int x = (int)((blockIdx.x * 256u + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (x >= X) return;
+  const double* r = rchol + (size_t)x * K;
+  double sx = 0.0, sy = 0.0;
+  for (int k = lane; k < K; k += 32) {
+    const double a = r[k];
+    const double2 b = g[k];
+    sx += a * b.x;
+    sy += a * b.y;
+  }
+  sx = warp_sum(sx);
+  sy = warp_sum(sy);
+  if (lane == 0) {
+    double2 v = make_double2(scale * sx, scale * sy);
+    if (accumulate) v = cadd(v, xv[x]);
+    xv[x] = v;
+  }
+}
+
+static cudaError_t coulomb_row(const double* rchol, const double2* g, int X, int K, double2* xv, int accumulate,
+                               double scale, cudaStream_t st) {
+  coulomb_row_kernel<<<(unsigned)((X + 7) / 8), 256, 0, st>>>(rchol, g, X, K, xv, accumulate, scale);
+  note_launch();
+  return cudaGetLastError();
+}
+
 static cudaError_t exchange_ref_row(const double2* g, const double2* gref, const double2* kmat, int W, int NM,
                                     const double2* raw_ref, double2* out, cudaStream_t st) {
   exchange_ref_row_kernel<<<W, 256, 0, st>>>(g, gref, kmat, NM, raw_ref, out);
@@ -1310,8 +1341,8 @@ extern "C" int ipie_b200_local_energy_mixed(int rhf, const double* rchola, const
     // Coulomb vector around the trial: X_T = sum_s rchol_s . G_T,s in FP64 (one walker's product,
     // into row 0, then copied to every row), plus the 3-pass FP16 product of G - G_T added per
     // spin block below, so that only the deviation carries the tensor cores' rounding
-    e = launch_force_bias(rchola, (CC)ghalf_trial_a, 1, X, na * M, xv, 0, st, alias ? 2.0 : 1.0);
-    if (e == cudaSuccess && use_b) e = launch_force_bias(rcholb, (CC)ghalf_trial_b, 1, X, nb * M, xv, 1, st);
+    e = umma::coulomb_row(rchola, (CC)ghalf_trial_a, X, na * M, xv, 0, alias ? 2.0 : 1.0, st);
+    if (e == cudaSuccess && use_b) e = umma::coulomb_row(rcholb, (CC)ghalf_trial_b, X, nb * M, xv, 1, 1.0, st);
     if (e != cudaSuccess) return (int)e;
     if (W > 1) {
       long long blocks = ((long long)(W - 1) * X + 255) / 256;
