@@ -125,7 +125,9 @@ int ipie_b200_update_weight(int W, const void* ovlp_new, const void* cfb, const 
 int ipie_b200_clip_weight(int W, const double* wbound, double* weight, void* stream);
 
 /* Thin QR of every spin block with positive diag(R) (in place), detR and
- * overlap rescale.
+ * overlap rescale: Cholesky QR for blocks of at most 32 orbitals (error ~cond(phi)^2
+ * eps; walkers reorthogonalised every few steps stay near orthonormal), modified
+ * Gram-Schmidt above.
  * replaces: walkers/uhf_walkers.py:108-143 (reortho) / :145-161
  * in/out: phia, phib, ovlp, log_detR; out: detR (W) double. */
 int ipie_b200_reortho(void* phia, void* phib, int W, int M, int na, int nb, const double* detR_shift, double* detR,
