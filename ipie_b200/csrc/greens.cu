@@ -374,8 +374,8 @@ __global__ void __launch_bounds__(kThreads, 4) gf_lu32_kernel(const double2* __r
 //   column i of four rows per warp, so each output row is one coalesced 512-byte store).
 // log det R = sum log R_kk.  Its error is that of the Gram matrix, ~cond(phi)^2 eps: walkers are
 // reorthogonalised every few steps, so phi stays close to orthonormal and cond(phi) near 1.
-__device__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 (*sO)[kNP], double2* sStage,
-                               double2* sDinv, unsigned* status) {
+__device__ __noinline__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 (*sO)[kNP], double2* sStage,
+                               double2* sDinv, double* sSpread, unsigned* status) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   o_product<true>(phi, nullptr, M, N, sO, sStage);
   __syncthreads();
@@ -434,9 +434,19 @@ __device__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 
 #pragma unroll
     for (int j = 0; j < 32; ++j)
       if (lane < j && j < N) sO[j][lane] = x[j];
-    if (lane < N) logsum = log(sO[lane][lane].x);
+    double rmax = 0.0, rmin = 1.0e300;
+    if (lane < N) {
+      const double r = sO[lane][lane].x;
+      logsum = log(r);
+      rmax = rmin = r;
+    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) logsum += __shfl_xor_sync(0xffffffffu, logsum, o);
+    for (int o = 16; o > 0; o >>= 1) {
+      logsum += __shfl_xor_sync(0xffffffffu, logsum, o);
+      rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+      rmin = fmin(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+    }
+    if (lane == 0) *sSpread = rmax / rmin;  // a lower bound on cond(phi); NaN when a pivot failed
   }
   __syncthreads();
   // ---- phi <- phi X: lane i = column i, rows m0 + 4 warp + a
@@ -485,6 +495,8 @@ __device__ double cholqr_block(double2* __restrict__ phi, int M, int N, double2 
   return logsum;  // valid in warp 0
 }
 
+constexpr double kCholQR2 = 20.0;  // R-diagonal spread above which a block gets a second pass
+
 // One CTA per walker: both spin blocks (the alpha block once when phib aliases it), then
 // detR = exp(sum log R_kk - detR_shift), log_detR += log detR, ovlp /= detR (the contract of
 // reortho_kernel in walkers.cu, which keeps N > 32).
@@ -497,6 +509,7 @@ __global__ void __launch_bounds__(kThreads, 4) reortho_chol32_kernel(double2* __
   __shared__ double2 sO[32][kNP];
   __shared__ __align__(16) double2 sStage[kStage];
   __shared__ double2 sDinv[32];
+  __shared__ double sSpread;
   const int w = blockIdx.x;
   const bool alias = (phib == phia) && (nb == na);
   double logsum = 0.0, log_a = 0.0;
@@ -507,7 +520,12 @@ __global__ void __launch_bounds__(kThreads, 4) reortho_chol32_kernel(double2* __
       logsum += log_a;
       continue;
     }
-    const double l = cholqr_block((s == 0 ? phia : phib) + (size_t)w * M * N, M, N, sO, sStage, sDinv, status);
+    double2* phi = (s == 0 ? phia : phib) + (size_t)w * M * N;
+    double l = cholqr_block(phi, M, N, sO, sStage, sDinv, &sSpread, status);
+    // CholQR2: a second pass over the (now nearly orthonormal) result when R's diagonal spreads
+    // by more than kCholQR2 (the first pass's error grows like cond(phi)^2 eps); R = R2 R1, so
+    // the log-determinants add
+    if (!(sSpread <= kCholQR2)) l += cholqr_block(phi, M, N, sO, sStage, sDinv, &sSpread, status);
     logsum += l;
     if (s == 0) log_a = l;
   }
