@@ -363,26 +363,28 @@ __device__ __forceinline__ void store_split(float* hi, float* lo, size_t i, T x)
   lo[i] = l;
 }
 
-// Force bias: rows x of rchol (X, K) fp32, B rows (w, c) of the planar Green's
-// function (W, 2, K) fp32 -> vbias[w][x] (complex double), scaled, optionally accumulated.
+// Force bias with the operands swapped: rows (w, c) of the Green's function, columns x of the
+// Cholesky operand; a thread writes component c of vbias[w][x] for its row's columns.
 template <int BN>
-struct EpiVbiasF {
+struct EpiVbiasT {
   double2* vbias;
   int X, W;
   double scale;               // overall factor, divided by the operands' power-of-two scales below
   const double* walker_scale;  // per-walker scale of the Green's-function operand (NULL: 1)
   int accumulate;
-  __device__ __forceinline__ void operator()(int, int x, int n0, const float* v, uint8_t*) const {
-    if (x >= X) return;
+  static constexpr int kCols = GemmRoles<1, BN>::kGroupCols;
+  __device__ __forceinline__ void operator()(int, int row, int x0, const float* v, uint8_t*) const {
+    const int w = row >> 1, c = row & 1;
+    if (w >= W) return;
+    const double f = walker_scale != nullptr ? scale / walker_scale[w] : scale;
+    double* out = reinterpret_cast<double*>(vbias + (size_t)w * X) + c;
 #pragma unroll
-    for (int q = 0; q < BN / 2; ++q) {
-      const int w = (n0 >> 1) + q;
-      if (w < W) {
-        const size_t i = (size_t)w * X + x;
-        const double f = walker_scale != nullptr ? scale / walker_scale[w] : scale;
-        double2 r = make_double2(f * (double)v[2 * q], f * (double)v[2 * q + 1]);
-        if (accumulate) r = cadd(r, vbias[i]);
-        vbias[i] = r;
+    for (int q = 0; q < kCols; ++q) {
+      const int x = x0 + q;
+      if (x < X) {
+        double r = f * (double)v[q];
+        if (accumulate) r += out[2 * (size_t)x];
+        out[2 * (size_t)x] = r;
       }
     }
   }
@@ -1002,24 +1004,24 @@ static cudaError_t exchange_ref_row(const double2* g, const double2* gref, const
 // with per-walker scales (the pads are zero in both, so K runs over them).
 static cudaError_t coulomb3(const void* r_hi, const void* r_lo, double rscale, const GPad& gp, int W, int X, int M,
                             int NP, double2* xv, int accumulate, double scale, unsigned* status, cudaStream_t st) {
-  // CTA pairs on 256 x 256 tiles: each SM stages 128 Cholesky rows and 128 Green's-function
-  // rows per K step (measured 0.44 -> 0.38 ms for the force-bias phase at 2048 walkers against
-  // single CTAs on 128 x 128 tiles)
-  constexpr int BN = 256, CG = 2;
+  // CTA pairs on 256 x 192 tiles, the Green's function's rows (w, c) as the 256-row side: each SM
+  // stages 128 of them and 96 Cholesky rows per K step.  At c2 (4096 x 1600) that is 16 x 9 = 144
+  // tiles, two full waves of 74 pairs (256 x 256 tiles the other way round: 112, 1.5 waves)
+  constexpr int BN = 192, CG = 2;
   const long long K = (long long)NP * f16_ld(M);
   GemmMaps maps;
   memset(&maps, 0, sizeof(maps));
   cudaError_t e;
-  if ((e = map_f16_pair(&maps.a_hi[0], &maps.a_lo[0], r_hi, r_lo, X, K, K, kBM, false, &maps.a_planes)) !=
+  if ((e = map_f16_pair(&maps.a_hi[0], &maps.a_lo[0], gp.hi, gp.lo, 2LL * W, K, K, kBM, false, &maps.a_planes)) !=
       cudaSuccess)
     return e;
-  if ((e = map_f16_pair(&maps.b_hi, &maps.b_lo, gp.hi, gp.lo, 2LL * W, K, K, BN / CG, false, &maps.b_planes)) !=
+  if ((e = map_f16_pair(&maps.b_hi, &maps.b_lo, r_hi, r_lo, X, K, K, BN / CG, false, &maps.b_planes)) !=
       cudaSuccess)
     return e;
-  dim3 grid((2 * W + BN - 1) / BN, (X + CG * kBM - 1) / (CG * kBM), 1);
-  // row tiles fastest: the Cholesky operand (X rows) stays in L2 while the Green's function streams
-  const EpiVbiasF<BN> epi{xv, X, W, scale / rscale, gp.scale, accumulate};
-  return launch_umma<BN, 1, 3, 3, EpiVbiasF<BN>, KIND_F16, CG>(maps, (int)K, 0, 0, grid, epi, status, st, true);
+  dim3 grid((X + BN - 1) / BN, (2 * W + CG * kBM - 1) / (CG * kBM), 1);
+  // row tiles fastest: a Cholesky tile stays in L2 while the Green's function streams past it
+  const EpiVbiasT<BN> epi{xv, X, W, scale / rscale, gp.scale, accumulate};
+  return launch_umma<BN, 1, 3, 4, EpiVbiasT<BN>, KIND_F16, CG>(maps, (int)K, 0, 0, grid, epi, status, st, true);
 }
 
 // Exchange partials of one spin block as a 3-pass FP16 product: (X*NP, M) x (W*2*NP, M)^T, rows
