@@ -44,8 +44,8 @@ def oracle_system(s, dt=0.005):
 RUN_PARAMS = {
     "run_rhf_m26.npz": dict(nwalkers=16, num_blocks=3, seed=7, steps=25),
     "run_uhf_m30.npz": dict(nwalkers=12, num_blocks=3, seed=9, steps=25),
-    # the workloads' own sizes: configs[0] (RHF M=26, 64 walkers, 3 blocks with pop control) and
-    # configs[1] (UHF M=108, 15+15, X=600, 640 walkers, one 10-step block and its energy)
+    # the workloads' own sizes: the small RHF workload (M=26, 64 walkers, 3 blocks with pop control)
+    # and the UHF one (M=108, 15+15, X=600, 640 walkers, one 10-step block and its energy)
     "run_c0_rhf_m26_w64.npz": dict(nwalkers=64, num_blocks=3, seed=7, steps=25),
     "run_c1_uhf_m108_w640.npz": dict(nwalkers=640, num_blocks=1, seed=7, steps=10),
 }

@@ -657,10 +657,10 @@ def analysis_fixture(name):
 def config_fixtures():
     """Parity runs at the workload sizes themselves (the stable Cholesky amplitude).
 
-    * RHF M=26, 5+5 electrons, X=120, 64 walkers, 3 blocks of 25 steps with reortho
-      and pair branch every 5 steps (ipie's AFQMC.run, seed 7);
-    * UHF M=108, 15+15 electrons, X=600, 640 walkers, one block of 10 steps with its
-      energy evaluation (ipie's AFQMC.run, seed 7)."""
+    * RHF M=26, 5+5 electrons, X=120, 64 walkers, 3 blocks of 25 steps with reortho and pair
+      branch every 5 steps (ipie's AFQMC.run, seed 7);
+    * UHF M=108, 15+15 electrons, X=600, 640 walkers, one block of 10 steps with its energy
+      evaluation (ipie's AFQMC.run, seed 7)."""
     c0 = synthetic.workload("c0_rhf_m26", chol_scale="stable")
     run_fixture("run_c0_rhf_m26_w64.npz", c0, nwalkers=64, num_blocks=3, seed=7)
     c1 = synthetic.workload("c1_uhf_m108", chol_scale="stable")
