@@ -307,21 +307,24 @@ __global__ void __launch_bounds__(256) field_shift_kernel(const double2* __restr
   }
 }
 
-// The same shift without the (X, W) transposed copy: one warp per walker walks its row of
-// vbias / xi with coalesced loads, writes the binary16 split and reduces cmf, cfb with shuffles
-// (the mixed form, which needs no FP64 transposed fields; every SM gets walkers).
+// The same shift without the (X, W) transposed copy: four warps per walker (two walkers per
+// block) walk its row of vbias / xi with coalesced loads, write the binary16 split and reduce cmf,
+// cfb with shuffles and shared memory (the mixed form, which needs no FP64 transposed fields; one
+// warp per walker left ~14 warps per SM, too few to cover the loads' latency).
+constexpr int kShiftWarps = 4;  // warps per walker
 __global__ void __launch_bounds__(256) field_shift_rows_kernel(const double2* __restrict__ vbias,
                                                                const double* __restrict__ xi,
                                                                const double2* __restrict__ mf, int W, int X,
                                                                double sqrt_dt, double bound, double2* __restrict__ cmf,
                                                                double2* __restrict__ cfb, __half* __restrict__ xs_hi,
                                                                __half* __restrict__ xs_lo) {
-  const int lane = threadIdx.x & 31;
-  const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (w >= W) return;  // whole warps leave together
+  __shared__ double2 part[8][2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = warp % kShiftWarps;
+  const int w = blockIdx.x * (8 / kShiftWarps) + warp / kShiftWarps;
+  const bool live = w < W;
   const int ldx = f16_ld(X);
   double2 acc_mf = make_double2(0.0, 0.0), acc_fb = make_double2(0.0, 0.0);
-  for (int x = lane; x < X; x += 32) {
+  for (int x = sub * 32 + lane; live && x < X; x += 32 * kShiftWarps) {
     const double2 v = vbias[(size_t)w * X + x];
     const double2 m = mf[x];
     double2 xb = make_double2(-sqrt_dt * (-v.y - m.x), -sqrt_dt * (v.x - m.y));
@@ -340,6 +343,15 @@ __global__ void __launch_bounds__(256) field_shift_rows_kernel(const double2* __
   acc_mf = warp_sum2(acc_mf);
   acc_fb = warp_sum2(acc_fb);
   if (lane == 0) {
+    part[warp][0] = acc_mf;
+    part[warp][1] = acc_fb;
+  }
+  __syncthreads();
+  if (live && sub == 0 && lane == 0) {
+    for (int k = 1; k < kShiftWarps; ++k) {
+      acc_mf = cadd(acc_mf, part[warp + k][0]);
+      acc_fb = cadd(acc_fb, part[warp + k][1]);
+    }
     cmf[w] = cscale(acc_mf, -sqrt_dt);
     cfb[w] = acc_fb;
   }
@@ -349,7 +361,7 @@ cudaError_t launch_field_shift(const double2* vbias, const double* xi, const dou
                                double bound, double2* xshifted, double2* cmf, double2* cfb, cudaStream_t st,
                                void* xs_hi, void* xs_lo) {
   if (xshifted == nullptr)
-    field_shift_rows_kernel<<<(W + 7) / 8, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, cmf, cfb,
+    field_shift_rows_kernel<<<(W + 1) / 2, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, cmf, cfb,
                                                          static_cast<__half*>(xs_hi), static_cast<__half*>(xs_lo));
   else
     field_shift_kernel<<<(W + 31) / 32, 256, 0, st>>>(vbias, xi, mf, W, X, sqrt_dt, bound, xshifted, cmf, cfb,
